@@ -1,0 +1,197 @@
+"""Drop-in ``solve_batch`` backend for the dFBA rollout.
+
+``B200LPBackend`` has the public contract of the reference's batched GPU LP
+service ``TemporalGpuLPBackend`` (``src/temporal_gpu_lp.py:18-199``) and of
+the CPU comparator ``RepeatedCpuLP.solve_batch``
+(``src/cpu_repeated_lp.py:783-818``):
+
+* ``solve_batch(requests, *, environment_ids=None) -> list[row]`` where each
+  request is ``(c, linprog_kwargs)`` and each row is a ``SimpleNamespace``
+  with ``success``, ``x``, ``fun``, ``message``, ``diagnostics`` (plus ``y``,
+  the HiGHS-convention row duals, and ``status``).  ``x``/``fun``/``y`` are
+  ``None`` when ``success`` is False (``src/temporal_gpu_lp.py:174-180``);
+  a failed solve is never replaced by a CPU solve.
+* ``reset(environment_ids=None)`` clears per-environment warm-start state
+  (``src/temporal_gpu_lp.py:72-84``).
+* ``name``, ``method``, ``history`` attributes.
+* invalid input raises ``ValueError`` before any state changes; an exception
+  during solving does not advance per-environment state
+  (``src/temporal_gpu_lp.py:182-186``).
+
+Success means: the engine's FP64 tolerances are met (status OPTIMAL) AND the
+reference's original-LP certificate gate passes on the returned primal/dual
+pair (``primal <= 1e-5, dual <= 1e-7, relative KKT gap <= 1e-7``,
+``src/gpu_block_lp.py:84``).
+"""
+
+from __future__ import annotations
+
+import time
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .engine import EngineOptions, LPEngine, SolveConfig
+from .problem import matrix_key, normalize
+
+PRIMAL_GATE = 1e-5
+DUAL_GATE = 1e-7
+GAP_GATE = 1e-7
+
+
+class B200LPBackend:
+    name = 'b200_batched_halpern_pdhg'
+    method = 'species_shared_persistent_halpern_pdhg_fp32_fp64'
+
+    def __init__(self, *, mode='previous', precision='mixed', iterations=20000,
+                 fp32_iterations=20000, check_interval=64, stage=None,
+                 options: EngineOptions | None = None, warm_start_model=None, device=None):
+        if mode not in ('cold', 'previous', 'mlp'):
+            raise ValueError('Unknown warm-start mode')
+        if mode == 'mlp' and warm_start_model is None:
+            raise ValueError('mode="mlp" needs a warm_start_model')
+        for name, value in (('iterations', iterations), ('fp32_iterations', fp32_iterations),
+                            ('check_interval', check_interval)):
+            if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)):
+                raise ValueError(f'{name} must be an integer')
+        if iterations < 0 or fp32_iterations < 0 or check_interval < 1:
+            raise ValueError('Invalid correction budget')
+        if not torch.cuda.is_available():
+            raise RuntimeError('CUDA is required (no CPU fallback)')
+        self.mode = mode
+        self.stage = stage
+        self.config = SolveConfig(precision=precision, max_iterations=int(iterations),
+                                  fp32_max_iterations=int(fp32_iterations),
+                                  check_every=int(check_interval))
+        self.config.native()  # validates
+        self.options = options or EngineOptions()
+        self.device = torch.device(device) if device is not None else torch.device('cuda')
+        self.model = warm_start_model
+        self._keys: list[str] = []
+        self._matrices = []
+        self._engine: LPEngine | None = None
+        self.last_certified: dict = {}
+        self.history: list[dict] = []
+
+    # ------------------------------------------------------------------
+    def reset(self, environment_ids=None):
+        ids = None if environment_ids is None else list(environment_ids)
+        if ids is not None and len(set(ids)) != len(ids):
+            raise ValueError('Reset requires unique environment IDs')
+        if ids is None:
+            self.last_certified.clear()
+        else:
+            for env in ids:
+                self.last_certified.pop(env, None)
+
+    def _engine_for(self, problems):
+        keys = [matrix_key(p[0], p[5]) for p in problems]
+        new = [(k, p) for k, p in zip(keys, problems) if k not in self._keys]
+        rebuilt = False
+        if new:
+            seen = set()
+            for k, p in new:
+                if k in seen:
+                    continue
+                seen.add(k)
+                self._keys.append(k)
+                self._matrices.append((p[0], p[5]))
+            if self._engine is not None:
+                self._engine.close()
+            self._engine = LPEngine(self._matrices, options=self.options, device=self.device)
+            rebuilt = True
+        index = {k: i for i, k in enumerate(self._keys)}
+        return np.array([index[k] for k in keys], dtype=np.int32), rebuilt
+
+    def solve_batch(self, requests, *, environment_ids=None):
+        started = time.perf_counter()
+        ids = list(range(len(requests))) if environment_ids is None else list(environment_ids)
+        if not requests or len(ids) != len(requests) or len(set(ids)) != len(ids):
+            raise ValueError('Nonempty requests and unique environment IDs required')
+        problems = [normalize(c, kw) for c, kw in requests]
+        if self.stage is not None and any(kw.get('_stage', self.stage) != self.stage for _, kw in requests):
+            raise ValueError('Use a separate backend and history for each LP stage')
+        prep = time.perf_counter()
+        species, rebuilt = self._engine_for(problems)
+        eng = self._engine
+        lower = np.concatenate([p[2] for p in problems])
+        upper = np.concatenate([p[3] for p in problems])
+        cost = np.concatenate([p[4] for p in problems])
+        rhs = np.concatenate([p[1] for p in problems])
+        co, ro, tc, tr = eng.layout(species)
+        warm_x = warm_y = warm_o = None
+        if self.mode == 'previous':
+            wx = np.zeros(tc)
+            wy = np.zeros(tr)
+            wo = np.ones(len(ids))
+            for i, env in enumerate(ids):
+                prev = self.last_certified.get(env)
+                if prev is not None and prev[0] == species[i]:
+                    n = eng.shapes[species[i]][1]
+                    m = eng.shapes[species[i]][0]
+                    wx[co[i]:co[i] + n] = prev[1]
+                    wy[ro[i]:ro[i] + m] = prev[2]
+                    wo[i] = prev[3]
+            warm_x, warm_y, warm_o = wx, wy, wo
+        elif self.mode == 'mlp':
+            warm_x, warm_y, warm_o = self.model.propose(ids, problems, species, eng)
+        dev = self.device
+        t = lambda a: torch.as_tensor(a, dtype=torch.float64).pin_memory().to(dev, non_blocking=True)
+        eng.set_instances(species, t(lower), t(upper), t(cost), t(rhs) if tr else None)
+        res = eng.solve(warm_x=None if warm_x is None else t(warm_x),
+                        warm_y=None if warm_y is None or not tr else t(warm_y),
+                        warm_omega=None if warm_o is None else t(warm_o), config=self.config)
+        status = res.status.cpu().numpy()
+        iters = res.iterations.cpu().numpy()
+        metrics = res.metrics.cpu().numpy()
+        x = res.x.cpu().numpy()
+        y = res.y.cpu().numpy()
+        solved = time.perf_counter()
+        rows = []
+        certified = {}
+        for i, env in enumerate(ids):
+            n = eng.shapes[species[i]][1]
+            m = eng.shapes[species[i]][0]
+            mt = metrics[i]
+            gate = bool(status[i] == N.STATUS_OPTIMAL and mt[0] <= PRIMAL_GATE and mt[1] <= DUAL_GATE
+                        and mt[2] <= GAP_GATE)
+            xi = x[co[i]:co[i] + n].copy()
+            yi = y[ro[i]:ro[i] + m].copy()
+            diag = dict(primal_residual=float(mt[0]), dual_violation=float(mt[1]),
+                        relative_kkt_gap=float(mt[2]), objective=float(mt[3]),
+                        dual_objective=float(mt[4]), relative_gap=float(mt[5]),
+                        certificate_passed=gate, accepted_iteration=int(iters[i]) if gate else -1,
+                        iterations=int(iters[i]), status=N.STATUS_NAMES.get(int(status[i]), 'unknown'),
+                        environment_id=env, stage=self.stage, success=gate, cpu_lp_calls=0,
+                        mode=self.mode, solver=self.name)
+            if gate:
+                certified[env] = (species[i], xi, yi, float(mt[7]))
+            rows.append(SimpleNamespace(
+                success=gate, x=xi if gate else None, y=yi if gate else None,
+                fun=float(problems[i][4] @ xi) if gate else None, status=int(status[i]),
+                message=('Original-LP certified GPU solution' if gate else
+                         f'GPU solve not certified ({diag["status"]}); no CPU fallback'),
+                diagnostics=diag))
+        # commit per-environment state only after every row is built
+        for env in ids:
+            if env in certified:
+                self.last_certified[env] = certified[env]
+            else:
+                self.last_certified.pop(env, None)
+        if self.mode == 'mlp' and hasattr(self.model, 'commit'):
+            self.model.commit(ids)
+        self.history.append(dict(stage=self.stage, mode=self.mode, batch=len(ids), environment_ids=ids,
+                                 accepted=sum(r.success for r in rows), cpu_lp_calls=0,
+                                 engine_rebuilt=rebuilt, iterations=iters.tolist(),
+                                 host_preparation_seconds=prep - started,
+                                 solve_seconds=solved - prep,
+                                 total_seconds=time.perf_counter() - started,
+                                 rows=[r.diagnostics for r in rows]))
+        return rows
+
+    def close(self):
+        if self._engine is not None:
+            self._engine.close()
+            self._engine = None

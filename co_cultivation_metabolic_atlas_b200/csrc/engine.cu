@@ -1,0 +1,501 @@
+// Host engine and C ABI (include/fbalp.h).
+//
+// The engine owns the per-species preprocessed matrices (device, SELL-32
+// slices of A and A^T in FP32 and FP64, scalings, permutations, warp
+// schedules) and a small workspace (work queue counter, FP32->FP64 hand-off
+// iterates, spill slabs).  Instance data and outputs stay caller-owned.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/fbalp.h"
+#include "fbalp_internal.h"
+#include "prepare.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+struct CudaError : std::exception {
+    std::string msg;
+    explicit CudaError(std::string m) : msg(std::move(m)) {}
+    const char* what() const noexcept override { return msg.c_str(); }
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T> T* dev_upload(const std::vector<T>& h, std::vector<void*>& owned) {
+    T* d = nullptr;
+    size_t bytes = std::max<size_t>(1, h.size()) * sizeof(T);
+    check(cudaMalloc(&d, bytes), "cudaMalloc");
+    owned.push_back(d);
+    if (!h.empty()) check(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy");
+    return d;
+}
+
+struct SpeciesHost {
+    int32_t m = 0, n = 0, neq = 0;
+    fbalp::Scaling scaling;
+    std::vector<int32_t> row_perm, col_perm;  // new -> old
+    fbalp::Sell A, AT;
+    std::vector<int32_t> a_sched_off, a_sched, at_sched_off, at_sched;
+};
+
+struct Buffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t want) {
+        if (want <= bytes) return;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        check(cudaMalloc(&ptr, std::max<size_t>(want, 256)), "cudaMalloc workspace");
+        bytes = std::max<size_t>(want, 256);
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+}  // namespace
+
+struct fbalp_engine {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+    int smem_optin = 0;
+    fbalp_options opt{};
+    std::vector<SpeciesHost> species;
+    std::vector<fbalp::DevSpecies> dev_species_host;
+    fbalp::DevSpecies* dev_species = nullptr;
+    std::vector<void*> owned;  // species allocations
+    // bound batch
+    int64_t count = 0, total_cols = 0, total_rows = 0;
+    std::vector<int32_t> h_species;
+    std::vector<int64_t> h_coloff, h_rowoff;
+    const double *lower = nullptr, *upper = nullptr, *cost = nullptr, *rhs = nullptr;
+    Buffer inst_species, col_off, row_off, order;
+    bool bound = false;
+    // workspace
+    Buffer queue, mid_x, mid_y, mid_omega, mid_iters, mid_status, mid_obj, mid_metrics, spill;
+    ~fbalp_engine() {
+        for (void* p : owned) cudaFree(p);
+        for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
+                          &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill})
+            b->release();
+    }
+};
+
+extern "C" {
+
+void fbalp_default_options(fbalp_options* o) {
+    if (!o) return;
+    o->ruiz_iterations = 10;
+    o->power_iterations = 256;
+    o->step_safety = 0.99;
+    o->warps_per_block = 16;
+    o->blocks_per_sm = 0;
+    o->max_dynamic_smem = 0;
+}
+
+void fbalp_default_solve_params(fbalp_solve_params* p) {
+    if (!p) return;
+    p->precision = FBALP_PRECISION_MIXED;
+    p->max_iterations = 20000;
+    p->fp32_max_iterations = 20000;
+    p->check_every = 64;
+    p->tol_primal = 1e-9;
+    p->tol_dual = 1e-9;
+    p->tol_gap = 1e-9;
+    p->fp32_tol_primal = 1e-6;
+    p->fp32_tol_dual = 1e-6;
+    p->fp32_tol_gap = 1e-4;
+    p->reflection = 1.0;
+    p->restarts = 1;
+}
+
+const char* fbalp_last_error(void) { return g_last_error.c_str(); }
+
+static bool valid_options(const fbalp_options& o, std::string* err) {
+    if (o.ruiz_iterations < 0 || o.ruiz_iterations > 100) return *err = "ruiz_iterations out of [0,100]", false;
+    if (o.power_iterations < 1 || o.power_iterations > 100000) return *err = "power_iterations out of range", false;
+    if (!(o.step_safety > 0.0 && o.step_safety < 1.0)) return *err = "step_safety must be in (0,1)", false;
+    if (o.warps_per_block < 1 || o.warps_per_block * 32 > fbalp::kMaxThreads)
+        return *err = "warps_per_block must be in [1,16]", false;
+    if (o.blocks_per_sm < 0 || o.blocks_per_sm > 32) return *err = "blocks_per_sm out of range", false;
+    if (o.max_dynamic_smem < 0) return *err = "max_dynamic_smem must be non-negative", false;
+    return true;
+}
+
+int fbalp_prepare_matrix(int32_t rows, int32_t cols, const int64_t* indptr, const int32_t* indices,
+                         const double* values, const fbalp_options* options, double* dr, double* dc,
+                         double* sigma_max, double* eta) {
+    try {
+        fbalp_options o;
+        fbalp_default_options(&o);
+        if (options) o = *options;
+        std::string err;
+        if (!valid_options(o, &err)) return fail(FBALP_ERR_INVALID, err);
+        fbalp::Csr a;
+        if (!fbalp::canonical_csr(rows, cols, indptr, indices, values, &a, &err))
+            return fail(FBALP_ERR_INVALID, err);
+        fbalp::Scaling s = fbalp::scale_matrix(a, o.ruiz_iterations, o.power_iterations, o.step_safety);
+        if (dr) std::copy(s.dr.begin(), s.dr.end(), dr);
+        if (dc) std::copy(s.dc.begin(), s.dc.end(), dc);
+        if (sigma_max) *sigma_max = s.sigma_max;
+        if (eta) *eta = s.eta;
+        return FBALP_OK;
+    } catch (const std::exception& e) {
+        return fail(FBALP_ERR_ALLOC, e.what());
+    }
+}
+
+int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t* cols,
+                        const int32_t* neq, const int64_t* const* indptr,
+                        const int32_t* const* indices, const double* const* values,
+                        const fbalp_options* options, void* stream, fbalp_engine** out) {
+    if (!out) return fail(FBALP_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (num_species < 1 || !rows || !cols || !neq || !indptr || !indices || !values)
+        return fail(FBALP_ERR_INVALID, "num_species >= 1 and non-NULL matrix arrays are required");
+    fbalp_options o;
+    fbalp_default_options(&o);
+    if (options) o = *options;
+    std::string err;
+    if (!valid_options(o, &err)) return fail(FBALP_ERR_INVALID, err);
+    std::unique_ptr<fbalp_engine> E(new fbalp_engine());
+    E->opt = o;
+    E->stream = static_cast<cudaStream_t>(stream);
+    try {
+        // --- host preprocessing (validates every matrix before any device work) ---
+        for (int s = 0; s < num_species; ++s) {
+            SpeciesHost sh;
+            if (neq[s] < 0 || neq[s] > rows[s])
+                return fail(FBALP_ERR_INVALID, "neq must identify an initial block of equality rows");
+            fbalp::Csr a;
+            if (!fbalp::canonical_csr(rows[s], cols[s], indptr[s], indices[s], values[s], &a, &err))
+                return fail(FBALP_ERR_INVALID, "species " + std::to_string(s) + ": " + err);
+            sh.m = a.rows;
+            sh.n = a.cols;
+            sh.neq = neq[s];
+            sh.scaling = fbalp::scale_matrix(a, o.ruiz_iterations, o.power_iterations, o.step_safety);
+            fbalp::Csr at = fbalp::transpose(a);
+            // rows: equalities then inequalities, each by decreasing length
+            sh.row_perm.resize(sh.m);
+            std::iota(sh.row_perm.begin(), sh.row_perm.end(), 0);
+            auto rlen = [&](int32_t i) { return a.ptr[i + 1] - a.ptr[i]; };
+            std::stable_sort(sh.row_perm.begin(), sh.row_perm.begin() + sh.neq,
+                             [&](int32_t x, int32_t y) { return rlen(x) > rlen(y); });
+            std::stable_sort(sh.row_perm.begin() + sh.neq, sh.row_perm.end(),
+                             [&](int32_t x, int32_t y) { return rlen(x) > rlen(y); });
+            sh.col_perm.resize(sh.n);
+            std::iota(sh.col_perm.begin(), sh.col_perm.end(), 0);
+            auto clen = [&](int32_t j) { return at.ptr[j + 1] - at.ptr[j]; };
+            std::stable_sort(sh.col_perm.begin(), sh.col_perm.end(),
+                             [&](int32_t x, int32_t y) { return clen(x) > clen(y); });
+            std::vector<int32_t> row_new(sh.m), col_new(sh.n);
+            for (int32_t i = 0; i < sh.m; ++i) row_new[sh.row_perm[i]] = i;
+            for (int32_t j = 0; j < sh.n; ++j) col_new[sh.col_perm[j]] = j;
+            sh.A = fbalp::build_sell(a, sh.row_perm, col_new, sh.scaling.dr, sh.scaling.dc, sh.n);
+            sh.AT = fbalp::build_sell(at, sh.col_perm, row_new, sh.scaling.dc, sh.scaling.dr, sh.m);
+            fbalp::warp_schedule(sh.A, o.warps_per_block, &sh.a_sched_off, &sh.a_sched);
+            fbalp::warp_schedule(sh.AT, o.warps_per_block, &sh.at_sched_off, &sh.at_sched);
+            E->species.push_back(std::move(sh));
+        }
+        // --- device ---
+        check(cudaGetDevice(&E->device), "cudaGetDevice");
+        check(cudaDeviceGetAttribute(&E->sm_count, cudaDevAttrMultiProcessorCount, E->device), "attr");
+        check(cudaDeviceGetAttribute(&E->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E->device),
+              "attr");
+        for (SpeciesHost& sh : E->species) {
+            fbalp::DevSpecies d{};
+            d.m = sh.m;
+            d.n = sh.n;
+            d.neq = sh.neq;
+            d.a_nslices = sh.A.nslices;
+            d.at_nslices = sh.AT.nslices;
+            std::vector<float> a32(sh.A.val.begin(), sh.A.val.end()), at32(sh.AT.val.begin(), sh.AT.val.end());
+            d.a_off = dev_upload(sh.A.off, E->owned);
+            d.a_idx = dev_upload(sh.A.idx, E->owned);
+            d.a_v32 = dev_upload(a32, E->owned);
+            d.a_v64 = dev_upload(sh.A.val, E->owned);
+            d.at_off = dev_upload(sh.AT.off, E->owned);
+            d.at_idx = dev_upload(sh.AT.idx, E->owned);
+            d.at_v32 = dev_upload(at32, E->owned);
+            d.at_v64 = dev_upload(sh.AT.val, E->owned);
+            d.a_sched_off = dev_upload(sh.a_sched_off, E->owned);
+            d.a_sched = dev_upload(sh.a_sched, E->owned);
+            d.at_sched_off = dev_upload(sh.at_sched_off, E->owned);
+            d.at_sched = dev_upload(sh.at_sched, E->owned);
+            d.row_perm = dev_upload(sh.row_perm, E->owned);
+            d.col_perm = dev_upload(sh.col_perm, E->owned);
+            std::vector<double> drn(sh.m), dcn(sh.n);
+            for (int32_t i = 0; i < sh.m; ++i) drn[i] = sh.scaling.dr[sh.row_perm[i]];
+            for (int32_t j = 0; j < sh.n; ++j) dcn[j] = sh.scaling.dc[sh.col_perm[j]];
+            d.dr = dev_upload(drn, E->owned);
+            d.dc = dev_upload(dcn, E->owned);
+            d.eta = sh.scaling.eta;
+            E->dev_species_host.push_back(d);
+        }
+        E->dev_species = dev_upload(E->dev_species_host, E->owned);
+        E->queue.ensure(16 * sizeof(int32_t));
+    } catch (const CudaError& e) {
+        return fail(FBALP_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(FBALP_ERR_ALLOC, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(FBALP_ERR_ALLOC, e.what());
+    }
+    *out = E.release();
+    return FBALP_OK;
+}
+
+int fbalp_engine_destroy(fbalp_engine* e) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    delete e;
+    return FBALP_OK;
+}
+
+int fbalp_engine_set_stream(fbalp_engine* e, void* stream) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    e->stream = static_cast<cudaStream_t>(stream);
+    return FBALP_OK;
+}
+
+int fbalp_engine_set_instances(fbalp_engine* e, int64_t count, const int32_t* species_id,
+                               const double* lower, const double* upper, const double* cost,
+                               const double* rhs) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (count < 1 || count > INT32_MAX || !species_id || !lower || !upper || !cost)
+        return fail(FBALP_ERR_INVALID, "count >= 1, species_id and lower/upper/cost are required");
+    std::vector<int32_t> hs(species_id, species_id + count);
+    std::vector<int64_t> co(count), ro(count);
+    int64_t tc = 0, tr = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        if (hs[i] < 0 || hs[i] >= static_cast<int32_t>(e->species.size()))
+            return fail(FBALP_ERR_INVALID, "species id out of range");
+        co[i] = tc;
+        ro[i] = tr;
+        tc += e->species[hs[i]].n;
+        tr += e->species[hs[i]].m;
+    }
+    // longest instances first: better balance for the persistent queue
+    std::vector<int32_t> ord(count);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) {
+        const SpeciesHost &a = e->species[hs[x]], &b = e->species[hs[y]];
+        return (a.A.off.back() + a.AT.off.back()) > (b.A.off.back() + b.AT.off.back());
+    });
+    try {
+        e->inst_species.ensure(count * sizeof(int32_t));
+        e->col_off.ensure(count * sizeof(int64_t));
+        e->row_off.ensure(count * sizeof(int64_t));
+        e->order.ensure(count * sizeof(int32_t));
+        check(cudaMemcpyAsync(e->inst_species.ptr, hs.data(), count * sizeof(int32_t), cudaMemcpyHostToDevice, e->stream), "copy");
+        check(cudaMemcpyAsync(e->col_off.ptr, co.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, e->stream), "copy");
+        check(cudaMemcpyAsync(e->row_off.ptr, ro.data(), count * sizeof(int64_t), cudaMemcpyHostToDevice, e->stream), "copy");
+        check(cudaMemcpyAsync(e->order.ptr, ord.data(), count * sizeof(int32_t), cudaMemcpyHostToDevice, e->stream), "copy");
+        // pageable sources: complete the copies before the host vectors die
+        check(cudaStreamSynchronize(e->stream), "sync");
+    } catch (const CudaError& ex) {
+        e->bound = false;
+        return fail(FBALP_ERR_CUDA, ex.what());
+    }
+    e->count = count;
+    e->total_cols = tc;
+    e->total_rows = tr;
+    e->h_species = std::move(hs);
+    e->h_coloff = std::move(co);
+    e->h_rowoff = std::move(ro);
+    e->lower = lower;
+    e->upper = upper;
+    e->cost = cost;
+    e->rhs = rhs;
+    e->bound = true;
+    return FBALP_OK;
+}
+
+int fbalp_engine_layout(const fbalp_engine* e, int64_t* total_cols, int64_t* total_rows,
+                        int64_t* col_offsets, int64_t* row_offsets) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (!e->bound) return fail(FBALP_ERR_STATE, "no instances are bound");
+    if (total_cols) *total_cols = e->total_cols;
+    if (total_rows) *total_rows = e->total_rows;
+    if (col_offsets) std::copy(e->h_coloff.begin(), e->h_coloff.end(), col_offsets);
+    if (row_offsets) std::copy(e->h_rowoff.begin(), e->h_rowoff.end(), row_offsets);
+    return FBALP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Launch one precision phase over the bound batch.
+void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
+    const size_t esz = fp64 ? sizeof(double) : sizeof(float);
+    const int threads = e->opt.warps_per_block * 32;
+    int64_t need = 0;
+    std::vector<char> used(e->species.size(), 0);
+    for (int32_t s : e->h_species) used[s] = 1;
+    for (size_t s = 0; s < e->species.size(); ++s)
+        if (used[s]) need = std::max(need, fbalp::total_elems(e->species[s].n, e->species[s].m));
+    const size_t static_smem = sizeof(double) * (fbalp::kMaxWarps * fbalp::kRed + fbalp::kRed) + 64;
+    const size_t cap = static_cast<size_t>(e->smem_optin) > static_smem + 1024 ? e->smem_optin - static_smem - 1024 : 0;
+    size_t dyn = std::min<size_t>(need * esz, cap);
+    if (e->opt.max_dynamic_smem > 0) dyn = std::min<size_t>(dyn, static_cast<size_t>(e->opt.max_dynamic_smem));
+    dyn = dyn / 16 * 16;
+    const void* k = fbalp::kernel_symbol(fp64);
+    check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
+          "cudaFuncSetAttribute");
+    int per_sm = 0;
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, dyn), "occupancy");
+    if (e->opt.blocks_per_sm > 0) per_sm = std::min(per_sm, e->opt.blocks_per_sm);
+    if (per_sm < 1) throw CudaError("kernel does not fit on an SM with this configuration");
+    const int grid = static_cast<int>(std::min<int64_t>(e->count, static_cast<int64_t>(per_sm) * e->sm_count));
+    p.smem_elems = static_cast<int64_t>(dyn / esz);
+    int64_t spill = 0;
+    for (size_t s = 0; s < e->species.size(); ++s)
+        if (used[s]) spill = std::max(spill, fbalp::spill_elems(e->species[s].n, e->species[s].m, p.smem_elems));
+    if (spill > 0) {
+        e->spill.ensure(static_cast<size_t>(spill) * grid * esz);
+        p.spill = e->spill.ptr;
+        p.spill_stride = spill;
+    } else {
+        p.spill = nullptr;
+        p.spill_stride = 0;
+    }
+    p.queue = static_cast<int32_t*>(e->queue.ptr);
+    check(cudaMemsetAsync(e->queue.ptr, 0, sizeof(int32_t), e->stream), "memset queue");
+    check(fbalp::launch_pdhg(fp64, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
+}
+
+bool valid_params(const fbalp_solve_params& q, std::string* err) {
+    if (q.precision < 0 || q.precision > 2) return *err = "precision must be FP64, MIXED or FP32", false;
+    if (q.max_iterations < 0 || q.fp32_max_iterations < 0) return *err = "iteration budgets must be non-negative", false;
+    if (q.check_every < 1) return *err = "check_every must be positive", false;
+    for (double t : {q.tol_primal, q.tol_dual, q.tol_gap, q.fp32_tol_primal, q.fp32_tol_dual, q.fp32_tol_gap})
+        if (!(t >= 0.0) || !std::isfinite(t)) return *err = "tolerances must be finite and non-negative", false;
+    if (!(q.reflection >= 0.0 && q.reflection <= 1.0)) return *err = "reflection must be in [0,1]", false;
+    if (q.restarts != 0 && q.restarts != 1) return *err = "restarts must be 0 or 1", false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const double* warm_y,
+                                  const double* warm_omega, const fbalp_solve_params* params,
+                                  int32_t* out_status, double* out_objective, double* out_x,
+                                  double* out_y, int32_t* out_iterations, double* out_metrics,
+                                  double* out_omega) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (!e->bound) return fail(FBALP_ERR_STATE, "set_instances must be called before solve");
+    if (!out_status || !out_objective || !out_x || !out_y || !out_iterations || !out_metrics)
+        return fail(FBALP_ERR_INVALID, "output arrays are required");
+    fbalp_solve_params q;
+    fbalp_default_solve_params(&q);
+    if (params) q = *params;
+    std::string err;
+    if (!valid_params(q, &err)) return fail(FBALP_ERR_INVALID, err);
+    try {
+        fbalp::KernelParams p{};
+        p.species = e->dev_species;
+        p.count = static_cast<int32_t>(e->count);
+        p.order = static_cast<const int32_t*>(e->order.ptr);
+        p.inst_species = static_cast<const int32_t*>(e->inst_species.ptr);
+        p.col_off = static_cast<const int64_t*>(e->col_off.ptr);
+        p.row_off = static_cast<const int64_t*>(e->row_off.ptr);
+        p.lower = e->lower;
+        p.upper = e->upper;
+        p.cost = e->cost;
+        p.rhs = e->rhs;
+        p.check_every = q.check_every;
+        p.rho = q.reflection;
+        p.restarts = q.restarts;
+        if (q.precision == FBALP_PRECISION_FP64 || q.precision == FBALP_PRECISION_FP32) {
+            const bool fp64 = q.precision == FBALP_PRECISION_FP64;
+            p.warm_x = warm_x;
+            p.warm_y = warm_y;
+            p.warm_omega = warm_omega;
+            p.prior_iters = nullptr;
+            p.out_x = out_x;
+            p.out_y = out_y;
+            p.out_obj = out_objective;
+            p.out_metrics = out_metrics;
+            p.out_omega = out_omega;
+            p.out_status = out_status;
+            p.out_iters = out_iterations;
+            p.max_iters = fp64 ? q.max_iterations : q.fp32_max_iterations;
+            p.tol_p = fp64 ? q.tol_primal : q.fp32_tol_primal;
+            p.tol_d = fp64 ? q.tol_dual : q.fp32_tol_dual;
+            p.tol_g = fp64 ? q.tol_gap : q.fp32_tol_gap;
+            p.final_status = fp64 ? fbalp::kStatusOptimal : fbalp::kStatusHandoff;
+            p.clip_output = 1;
+            run_phase(e, fp64, p);
+        } else {
+            e->mid_x.ensure(e->total_cols * sizeof(double));
+            e->mid_y.ensure(std::max<int64_t>(1, e->total_rows) * sizeof(double));
+            e->mid_omega.ensure(e->count * sizeof(double));
+            e->mid_iters.ensure(e->count * sizeof(int32_t));
+            e->mid_status.ensure(e->count * sizeof(int32_t));
+            e->mid_obj.ensure(e->count * sizeof(double));
+            e->mid_metrics.ensure(e->count * fbalp::kMetrics * sizeof(double));
+            fbalp::KernelParams p32 = p;
+            p32.warm_x = warm_x;
+            p32.warm_y = warm_y;
+            p32.warm_omega = warm_omega;
+            p32.prior_iters = nullptr;
+            p32.out_x = static_cast<double*>(e->mid_x.ptr);
+            p32.out_y = static_cast<double*>(e->mid_y.ptr);
+            p32.out_obj = static_cast<double*>(e->mid_obj.ptr);
+            p32.out_metrics = static_cast<double*>(e->mid_metrics.ptr);
+            p32.out_omega = static_cast<double*>(e->mid_omega.ptr);
+            p32.out_status = static_cast<int32_t*>(e->mid_status.ptr);
+            p32.out_iters = static_cast<int32_t*>(e->mid_iters.ptr);
+            p32.max_iters = q.fp32_max_iterations;
+            p32.tol_p = q.fp32_tol_primal;
+            p32.tol_d = q.fp32_tol_dual;
+            p32.tol_g = q.fp32_tol_gap;
+            p32.final_status = fbalp::kStatusHandoff;
+            p32.clip_output = 0;
+            run_phase(e, false, p32);
+            fbalp::KernelParams p64 = p;
+            p64.warm_x = static_cast<const double*>(e->mid_x.ptr);
+            p64.warm_y = static_cast<const double*>(e->mid_y.ptr);
+            p64.warm_omega = static_cast<const double*>(e->mid_omega.ptr);
+            p64.prior_iters = static_cast<const int32_t*>(e->mid_iters.ptr);
+            p64.out_x = out_x;
+            p64.out_y = out_y;
+            p64.out_obj = out_objective;
+            p64.out_metrics = out_metrics;
+            p64.out_omega = out_omega;
+            p64.out_status = out_status;
+            p64.out_iters = out_iterations;
+            p64.max_iters = q.max_iterations;
+            p64.tol_p = q.tol_primal;
+            p64.tol_d = q.tol_dual;
+            p64.tol_g = q.tol_gap;
+            p64.final_status = fbalp::kStatusOptimal;
+            p64.clip_output = 1;
+            run_phase(e, true, p64);
+        }
+    } catch (const CudaError& ex) {
+        return fail(FBALP_ERR_CUDA, ex.what());
+    } catch (const std::exception& ex) {
+        return fail(FBALP_ERR_ALLOC, ex.what());
+    }
+    return FBALP_OK;
+}

@@ -1,0 +1,90 @@
+// Persistent, instance-resident restarted Halpern PDHG for batches of LPs
+// that share one matrix per species (sm_100a).
+//
+// One CTA owns one LP instance at a time: its iterates, anchors and scaled
+// bounds live in shared memory (spilling to a per-CTA global slab only for
+// species too large for the CTA's shared memory), the species matrix and its
+// transpose are streamed from L2 in SELL-32 slices, and every convergence
+// test, restart decision and primal-weight update happens inside the kernel.
+// When an instance finishes (certified, budget exhausted, or invalid) the CTA
+// writes its results and pulls the next instance from an atomic work queue,
+// so instances of different species and different iteration counts share one
+// launch without host round trips.
+//
+// Arithmetic (per instance, scaled space; see oracle/pdhg.py for the
+// restatement used as the parity reference):
+//   xn = clip(x - tau (c - A^T y), l, u)             tau = eta/omega
+//   yn = P_Y(y + sigma (b - A (2 xn - x)))          sigma = eta*omega
+//   x  = w ((1+rho) xn - rho x) + (1-w) xa          w = (k+1)/(k+2)
+//   y  = w ((1+rho) yn - rho y) + (1-w) ya
+// The reference iterates plain PDHG with a fixed diagonal metric
+// (`src/gpu_pdhg_corrector.py:334-358`, `src/gpu_pdhg_workspace.py:122-134`);
+// the projections keep its NaN-preserving form (a NaN is never clipped).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fbalp {
+
+constexpr int kMaxWarps = 16;
+constexpr int kRed = 16;  // reduced quantities per convergence check
+
+struct DevSpecies {
+    int32_t m, n, neq, pad_;
+    int32_t a_nslices, at_nslices;
+    const int32_t* a_off;
+    const int32_t* a_idx;
+    const float* a_v32;
+    const double* a_v64;
+    const int32_t* at_off;
+    const int32_t* at_idx;
+    const float* at_v32;
+    const double* at_v64;
+    const int32_t* a_sched_off;   // [warps + 1]
+    const int32_t* a_sched;
+    const int32_t* at_sched_off;
+    const int32_t* at_sched;
+    const int32_t* row_perm;      // new -> original row
+    const int32_t* col_perm;      // new -> original column
+    const double* dr;             // new order
+    const double* dc;             // new order
+    double eta;
+};
+
+struct KernelParams {
+    const DevSpecies* species;
+    int32_t count;
+    const int32_t* order;         // work order (instance ids)
+    const int32_t* inst_species;
+    const int64_t* col_off;
+    const int64_t* row_off;
+    const double* lower;
+    const double* upper;
+    const double* cost;
+    const double* rhs;            // may be null (zero)
+    const double* warm_x;         // may be null
+    const double* warm_y;         // may be null
+    const double* warm_omega;     // may be null
+    const int32_t* prior_iters;   // may be null: added to the reported count
+    double* out_x;
+    double* out_y;
+    double* out_obj;
+    double* out_metrics;
+    double* out_omega;            // may be null
+    int32_t* out_status;
+    int32_t* out_iters;
+    int32_t* queue;
+    void* spill;                  // per-CTA global slabs (may be null)
+    int64_t spill_stride;         // elements of T per CTA
+    int64_t smem_elems;           // elements of T available in dynamic smem
+    int32_t max_iters;
+    int32_t check_every;
+    double tol_p, tol_d, tol_g;
+    double rho;
+    int32_t restarts;
+    int32_t final_status;
+    int32_t clip_output;          // clip reported x to the original bounds
+};
+
+}  // namespace fbalp

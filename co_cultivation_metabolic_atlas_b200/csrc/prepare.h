@@ -1,0 +1,53 @@
+// Host-side preprocessing of one species matrix: canonical CSR, Ruiz +
+// Pock-Chambolle scaling, spectral step, SELL-32 slicing, warp schedules.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace fbalp {
+
+struct Csr {
+    int32_t rows = 0, cols = 0;
+    std::vector<int64_t> ptr;
+    std::vector<int32_t> idx;
+    std::vector<double> val;
+};
+
+// Canonicalise: sort columns inside every row, sum duplicates, drop zeros.
+// Returns false (with a message) on out-of-range indices, a non-monotone row
+// pointer or non-finite values.
+bool canonical_csr(int32_t rows, int32_t cols, const int64_t* indptr, const int32_t* indices,
+                   const double* values, Csr* out, std::string* err);
+
+Csr transpose(const Csr& a);
+
+struct Scaling {
+    std::vector<double> dr, dc;  // original row / column order
+    double sigma_max = 0.0;      // ||Dr A Dc||_2 estimate
+    double eta = 1.0;            // step size
+};
+
+Scaling scale_matrix(const Csr& a, int ruiz_iterations, int power_iterations, double step_safety);
+
+// SELL-32 slices of a matrix whose rows are visited in `row_order` (new ->
+// old) and whose column indices are renamed by `col_rename` (old -> new).
+// Padding entries point at `pad_index` with value 0.
+struct Sell {
+    int32_t nslices = 0;
+    std::vector<int32_t> off;    // nslices + 1, in elements
+    std::vector<int32_t> idx;
+    std::vector<double> val;
+    std::vector<int32_t> length; // slice lengths
+};
+
+Sell build_sell(const Csr& a, const std::vector<int32_t>& row_order,
+                const std::vector<int32_t>& col_rename, const std::vector<double>& row_scale,
+                const std::vector<double>& col_scale, int32_t pad_index);
+
+// Greedy longest-first assignment of slices to `warps` warps.
+void warp_schedule(const Sell& s, int warps, std::vector<int32_t>* sched_off,
+                   std::vector<int32_t>* sched);
+
+}  // namespace fbalp

@@ -1,0 +1,240 @@
+"""Batched LP engine over the C ABI (device tensors via PyTorch).
+
+``LPEngine`` is the tensor-level interface: species matrices are registered
+once; a batch binds flat per-instance bound/objective tensors; ``solve`` runs
+the persistent CUDA kernels and returns device tensors.  The reference's
+equivalent is ``GpuPdhgCorrector`` + ``GpuPdhgWorkspace``
+(``src/gpu_pdhg_corrector.py:75-438``, ``src/gpu_pdhg_workspace.py:55-384``),
+which rebuild a block-diagonal copy of every matrix per call; here each
+species matrix is stored once and shared by all of its instances.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+from scipy.sparse import csr_matrix
+
+from . import _native as N
+
+
+def _ptr(t):
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+@dataclass
+class SolveResult:
+    status: torch.Tensor       # int32 [count]
+    objective: torch.Tensor    # float64 [count]
+    x: torch.Tensor            # float64 [total_cols]
+    y: torch.Tensor            # float64 [total_rows]
+    iterations: torch.Tensor   # int32 [count]
+    metrics: torch.Tensor      # float64 [count, 8]
+    omega: torch.Tensor        # float64 [count]
+
+
+@dataclass
+class SolveConfig:
+    precision: str = "mixed"           # "fp64" | "mixed" | "fp32"
+    max_iterations: int = 20000
+    fp32_max_iterations: int = 20000
+    check_every: int = 64
+    tol_primal: float = 1e-9
+    tol_dual: float = 1e-9
+    tol_gap: float = 1e-9
+    fp32_tol_primal: float = 1e-6
+    fp32_tol_dual: float = 1e-6
+    fp32_tol_gap: float = 1e-4
+    reflection: float = 1.0
+    restarts: bool = True
+
+    def native(self) -> N.SolveParams:
+        p = N.default_solve_params()
+        prec = {"fp64": N.PRECISION_FP64, "mixed": N.PRECISION_MIXED, "fp32": N.PRECISION_FP32}
+        if self.precision not in prec:
+            raise ValueError("precision must be 'fp64', 'mixed' or 'fp32'")
+        p.precision = prec[self.precision]
+        for name in ("max_iterations", "fp32_max_iterations", "check_every"):
+            value = getattr(self, name)
+            if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)):
+                raise ValueError(f"{name} must be an integer")
+            setattr(p, name, int(value))
+        for name in ("tol_primal", "tol_dual", "tol_gap", "fp32_tol_primal", "fp32_tol_dual",
+                     "fp32_tol_gap", "reflection"):
+            setattr(p, name, float(getattr(self, name)))
+        p.restarts = 1 if self.restarts else 0
+        return p
+
+
+@dataclass
+class EngineOptions:
+    ruiz_iterations: int = 10
+    power_iterations: int = 256
+    step_safety: float = 0.99
+    warps_per_block: int = 16
+    blocks_per_sm: int = 0
+    max_dynamic_smem: int = 0
+
+    def native(self) -> N.Options:
+        o = N.default_options()
+        o.ruiz_iterations = int(self.ruiz_iterations)
+        o.power_iterations = int(self.power_iterations)
+        o.step_safety = float(self.step_safety)
+        o.warps_per_block = int(self.warps_per_block)
+        o.blocks_per_sm = int(self.blocks_per_sm)
+        o.max_dynamic_smem = int(self.max_dynamic_smem)
+        return o
+
+
+def _host_csr(a):
+    a = csr_matrix(a, dtype=np.float64)
+    indptr = np.ascontiguousarray(a.indptr, dtype=np.int64)
+    indices = np.ascontiguousarray(a.indices, dtype=np.int32)
+    data = np.ascontiguousarray(a.data, dtype=np.float64)
+    return a.shape, indptr, indices, data
+
+
+def prepare_matrix(a, options: EngineOptions | None = None):
+    """Host-only preprocessing (scalings, spectral norm, step); no GPU."""
+    lib = N.load()
+    (m, n), indptr, indices, data = _host_csr(a)
+    dr = np.empty(m)
+    dc = np.empty(n)
+    smax = ctypes.c_double()
+    eta = ctypes.c_double()
+    opt = (options or EngineOptions()).native()
+    N.check(lib.fbalp_prepare_matrix(
+        m, n, indptr.ctypes.data_as(N.c_int64_p), indices.ctypes.data_as(N.c_int32_p),
+        data.ctypes.data_as(N.c_double_p), ctypes.byref(opt), dr.ctypes.data_as(N.c_double_p),
+        dc.ctypes.data_as(N.c_double_p), ctypes.byref(smax), ctypes.byref(eta)))
+    return dict(dr=dr, dc=dc, sigma_max=smax.value, eta=eta.value)
+
+
+class LPEngine:
+    """Species-shared batched LP engine on one CUDA device.
+
+    ``matrices`` is a sequence of ``(A, neq)`` pairs (SciPy sparse or dense);
+    rows ``[0, neq)`` are equalities and the rest ``<=`` inequalities.
+    """
+
+    def __init__(self, matrices, *, options: EngineOptions | None = None, device=None,
+                 stream: torch.cuda.Stream | None = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("a CUDA device is required (no CPU fallback)")
+        self.lib = N.load()
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.options = options or EngineOptions()
+        mats = [(_host_csr(a), int(neq)) for a, neq in matrices]
+        if not mats:
+            raise ValueError("at least one species matrix is required")
+        k = len(mats)
+        self.shapes = [(s[0][0], s[0][1]) for s, _ in mats]
+        self.neq = [q for _, q in mats]
+        rows = (ctypes.c_int32 * k)(*[s[0] for s in self.shapes])
+        cols = (ctypes.c_int32 * k)(*[s[1] for s in self.shapes])
+        neqs = (ctypes.c_int32 * k)(*self.neq)
+        self._keep = [m for m, _ in mats]
+        ip = (N.c_int64_p * k)(*[m[1].ctypes.data_as(N.c_int64_p) for m in self._keep])
+        ix = (N.c_int32_p * k)(*[m[2].ctypes.data_as(N.c_int32_p) for m in self._keep])
+        vv = (N.c_double_p * k)(*[m[3].ctypes.data_as(N.c_double_p) for m in self._keep])
+        self.stream = stream or torch.cuda.current_stream(self.device)
+        handle = ctypes.c_void_p()
+        opt = self.options.native()
+        with torch.cuda.device(self.device):
+            N.check(self.lib.fbalp_engine_create(k, rows, cols, neqs, ip, ix, vv, ctypes.byref(opt),
+                                                 ctypes.c_void_p(self.stream.cuda_stream),
+                                                 ctypes.byref(handle)))
+        self.handle = handle
+        self.count = 0
+        self._bound = None
+        self.species_id = None
+        self.col_offsets = None
+        self.row_offsets = None
+        self.total_cols = 0
+        self.total_rows = 0
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            self.lib.fbalp_engine_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream: torch.cuda.Stream):
+        self.stream = stream
+        N.check(self.lib.fbalp_engine_set_stream(self.handle, ctypes.c_void_p(stream.cuda_stream)))
+
+    # -- batch -------------------------------------------------------------
+    def layout(self, species_id):
+        """Column/row offsets of a batch (host numpy), same rule as the C ABI."""
+        sid = np.asarray(species_id, dtype=np.int64)
+        n = np.array([s[1] for s in self.shapes])[sid]
+        m = np.array([s[0] for s in self.shapes])[sid]
+        co = np.concatenate([[0], np.cumsum(n)[:-1]]) if len(sid) else np.empty(0, np.int64)
+        ro = np.concatenate([[0], np.cumsum(m)[:-1]]) if len(sid) else np.empty(0, np.int64)
+        return co.astype(np.int64), ro.astype(np.int64), int(n.sum()), int(m.sum())
+
+    def _dev(self, t, size, name, dtype=torch.float64):
+        if t is None:
+            return None
+        if not isinstance(t, torch.Tensor):
+            t = torch.as_tensor(np.asarray(t, dtype=np.float64))
+        if t.numel() != size:
+            raise ValueError(f"{name} must have {size} elements")
+        return t.to(device=self.device, dtype=dtype).contiguous().reshape(-1)
+
+    def set_instances(self, species_id, lower, upper, cost, rhs=None):
+        sid = np.ascontiguousarray(np.asarray(species_id, dtype=np.int32).reshape(-1))
+        if sid.size < 1:
+            raise ValueError("at least one instance is required")
+        if sid.min() < 0 or sid.max() >= len(self.shapes):
+            raise ValueError("species id out of range")
+        co, ro, tc, tr = self.layout(sid)
+        lower = self._dev(lower, tc, "lower")
+        upper = self._dev(upper, tc, "upper")
+        cost = self._dev(cost, tc, "cost")
+        rhs = self._dev(rhs, tr, "rhs")
+        N.check(self.lib.fbalp_engine_set_instances(self.handle, int(sid.size), sid.ctypes.data_as(N.c_int32_p),
+                                                    _ptr(lower), _ptr(upper), _ptr(cost), _ptr(rhs)))
+        self._bound = (lower, upper, cost, rhs)  # the engine keeps raw pointers
+        self.species_id = sid
+        self.count = int(sid.size)
+        self.col_offsets, self.row_offsets = co, ro
+        self.total_cols, self.total_rows = tc, tr
+
+    def allocate_result(self) -> SolveResult:
+        dev = self.device
+        c = self.count
+        return SolveResult(
+            status=torch.empty(c, dtype=torch.int32, device=dev),
+            objective=torch.empty(c, dtype=torch.float64, device=dev),
+            x=torch.empty(max(1, self.total_cols), dtype=torch.float64, device=dev),
+            y=torch.empty(max(1, self.total_rows), dtype=torch.float64, device=dev),
+            iterations=torch.empty(c, dtype=torch.int32, device=dev),
+            metrics=torch.empty((c, N.METRICS), dtype=torch.float64, device=dev),
+            omega=torch.empty(c, dtype=torch.float64, device=dev))
+
+    def solve(self, *, warm_x=None, warm_y=None, warm_omega=None, config: SolveConfig | None = None,
+              out: SolveResult | None = None) -> SolveResult:
+        if self._bound is None:
+            raise RuntimeError("set_instances must be called before solve")
+        cfg = config or SolveConfig()
+        params = cfg.native()
+        wx = self._dev(warm_x, self.total_cols, "warm_x")
+        wy = self._dev(warm_y, self.total_rows, "warm_y") if self.total_rows else None
+        wo = self._dev(warm_omega, self.count, "warm_omega")
+        res = out or self.allocate_result()
+        N.check(self.lib.fbalp_engine_solve(
+            self.handle, _ptr(wx), _ptr(wy), _ptr(wo), ctypes.byref(params), _ptr(res.status),
+            _ptr(res.objective), _ptr(res.x), _ptr(res.y), _ptr(res.iterations), _ptr(res.metrics),
+            _ptr(res.omega)))
+        self._warm_keep = (wx, wy, wo)
+        return res

@@ -1,0 +1,175 @@
+/*
+ * fbalp.h -- C ABI of the B200 batched flux-balance LP engine.
+ *
+ * The engine solves batches of independent LPs
+ *
+ *     minimize    c.x
+ *     subject to  A[:neq] x  = b[:neq]
+ *                 A[neq:] x <= b[neq:]
+ *                 l <= x <= u
+ *
+ * where every instance of a "species" shares that species' matrix A (the
+ * stoichiometric matrix S of a flux-balance model) and carries its own
+ * bounds l, u, objective c and right-hand side b.  Row duals follow the HiGHS
+ * convention (inequality duals <= 0, reduced cost c - A^T y).
+ *
+ * It replaces the reference project's batched GPU LP backend call (the
+ * `solve_batch` service used by the dFBA rollout):
+ *   - `src/temporal_gpu_lp.py:86-199`  TemporalGpuLPBackend.solve_batch
+ *   - `src/gpu_pdhg_corrector.py:99-218`  GpuPdhgCorrector.__init__ (setup)
+ *   - `src/gpu_pdhg_corrector.py:273-438` GpuPdhgCorrector.solve (iterations)
+ *   - `src/gpu_pdhg_workspace.py:55-384`  GpuPdhgWorkspace (resident loop)
+ *   - `src/gpu_block_lp.py:52-132`        certify_blocks_device (certificate)
+ *
+ * Conventions: all functions return FBALP_OK (0) or an FBALP_ERR_* code;
+ * fbalp_last_error() gives the message of the calling thread's last failure.
+ * Invalid arguments are rejected before any state changes.  Species matrices
+ * are HOST arrays (copied at creation); instance data, warm starts and
+ * outputs are caller-owned DEVICE arrays.  One engine has one owner: calls on
+ * the same engine must be serialised (as `src/gpu_pdhg_workspace.py:11-12`
+ * and `src/cpu_repeated_lp.py:7` require of the reference services).
+ */
+#ifndef FBALP_H
+#define FBALP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes */
+#define FBALP_OK 0
+#define FBALP_ERR_INVALID 1   /* invalid argument; nothing was changed       */
+#define FBALP_ERR_CUDA 2      /* CUDA runtime error                          */
+#define FBALP_ERR_ALLOC 3     /* device or host allocation failed            */
+#define FBALP_ERR_STATE 4     /* call out of order (e.g. solve before set)   */
+
+/* per-instance solver status */
+#define FBALP_STATUS_OPTIMAL 0          /* FP64 certificate tolerances met    */
+#define FBALP_STATUS_ITERATION_LIMIT 1  /* budget exhausted; fails closed     */
+#define FBALP_STATUS_NUMERICAL 2        /* NaN/Inf met in the iteration       */
+#define FBALP_STATUS_INVALID_INPUT 3    /* l > u, NaN bound, non-finite c / b */
+#define FBALP_STATUS_NOT_RUN 4
+#define FBALP_STATUS_HANDOFF 5          /* FP32 phase met its tolerances      */
+
+/* precision schedules */
+#define FBALP_PRECISION_FP64 0   /* FP64 iterates throughout                  */
+#define FBALP_PRECISION_MIXED 1  /* FP32 iterates, then FP64 refinement phase */
+#define FBALP_PRECISION_FP32 2   /* FP32 phase only (diagnostic)              */
+
+/* out_metrics row layout (FBALP_METRICS doubles per instance) */
+#define FBALP_METRICS 8
+#define FBALP_M_PRIMAL_RESIDUAL 0   /* max |A_eq x-b|, (A_ub x-b)+, bound viol. */
+#define FBALP_M_DUAL_VIOLATION 1    /* y_ub+, reduced-cost sign on inf. bounds  */
+#define FBALP_M_RELATIVE_KKT_GAP 2  /* complementarity / max(1,|c.x|)           */
+#define FBALP_M_OBJECTIVE 3         /* c.x                                      */
+#define FBALP_M_DUAL_OBJECTIVE 4    /* b.y + sum_j min_{[l_j,u_j]} r_j x_j      */
+#define FBALP_M_RELATIVE_GAP 5      /* |c.x - dual| / (1 + |c.x| + |dual|)      */
+#define FBALP_M_X_INF 6             /* max |x_j|                                */
+#define FBALP_M_OMEGA 7             /* final primal weight                      */
+
+typedef struct fbalp_engine fbalp_engine;
+
+/* Setup options (per engine).  Replaces the constructor arguments of
+ * `src/gpu_pdhg_corrector.py:92-99` (step_safety, primal_weight); the
+ * diagonal metric of `:183-200` becomes Ruiz + Pock-Chambolle scaling with a
+ * spectral step. */
+typedef struct fbalp_options {
+    int32_t ruiz_iterations;   /* default 10                                 */
+    int32_t power_iterations;  /* default 256 (||A~||_2 estimate)            */
+    double step_safety;        /* default 0.99 (eta = safety / ||A~||_2)     */
+    int32_t warps_per_block;   /* default 16                                 */
+    int32_t blocks_per_sm;     /* default 0 = derive from occupancy          */
+    int32_t max_dynamic_smem;  /* bytes of shared memory per CTA for instance
+                                  arrays; 0 = device limit.  Arrays that do not
+                                  fit live in a per-CTA global slab.        */
+} fbalp_options;
+
+/* Solve parameters.  Replaces `iterations` / `check_interval` of
+ * `src/gpu_pdhg_corrector.py:273-281`; the acceptance gate of
+ * `src/gpu_block_lp.py:84` is evaluated on the returned metrics. */
+typedef struct fbalp_solve_params {
+    int32_t precision;           /* FBALP_PRECISION_*                         */
+    int32_t max_iterations;      /* FP64 phase budget per instance            */
+    int32_t fp32_max_iterations; /* FP32 phase budget (MIXED / FP32)          */
+    int32_t check_every;         /* convergence / restart test period         */
+    double tol_primal;           /* primal <= tol*(1+|x|_inf)   (FP64 phase)  */
+    double tol_dual;             /* dual viol. <= tol*(1+|c|_inf)             */
+    double tol_gap;              /* relative gap and relative KKT gap         */
+    double fp32_tol_primal;      /* hand-off tolerances of the FP32 phase     */
+    double fp32_tol_dual;
+    double fp32_tol_gap;
+    double reflection;           /* Halpern reflection rho in [0,1], default 1 */
+    int32_t restarts;            /* 1 = adaptive restarts, 0 = none           */
+} fbalp_solve_params;
+
+void fbalp_default_options(fbalp_options* options);
+void fbalp_default_solve_params(fbalp_solve_params* params);
+
+/* Create an engine for `num_species` matrices (HOST CSR arrays; int64 row
+ * pointers, int32 column indices, double values; duplicates are summed and
+ * zeros dropped, as `_problem` does at `src/cpu_repeated_lp.py:141`).
+ * `stream` is a cudaStream_t (NULL = legacy default stream).
+ * Replaces: GpuPdhgCorrector.__init__ (`src/gpu_pdhg_corrector.py:99-218`)
+ * and GpuPdhgWorkspace.__init__ (`src/gpu_pdhg_workspace.py:55-155`). */
+int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t* cols,
+                        const int32_t* neq, const int64_t* const* indptr,
+                        const int32_t* const* indices, const double* const* values,
+                        const fbalp_options* options, void* stream, fbalp_engine** out);
+
+/* Bind a batch of `count` instances.  `species_id` is a HOST array.  The
+ * DEVICE arrays `lower`, `upper`, `cost` (and `rhs`, NULL = zero) are flat:
+ * instance i occupies columns [col_offset[i], col_offset[i] + n_{species[i]})
+ * and rows [row_offset[i], row_offset[i] + m_{species[i]}), offsets being the
+ * prefix sums in instance order.  The pointers are kept (not copied) and must
+ * stay valid until the next set_instances / destroy.
+ * Replaces: the per-call host assembly and copies of
+ * `src/gpu_pdhg_corrector.py:140-184` and GpuPdhgWorkspace.update_problem
+ * (`src/gpu_pdhg_workspace.py:209-267`). */
+int fbalp_engine_set_instances(fbalp_engine* engine, int64_t count, const int32_t* species_id,
+                               const double* lower, const double* upper, const double* cost,
+                               const double* rhs);
+
+/* Solve every bound instance.  Warm starts (`warm_x`, `warm_y`: flat DEVICE,
+ * original units; `warm_omega`: per instance) may be NULL (cold start).
+ * Outputs are DEVICE arrays: status[count], objective[count],
+ * x[total columns], y[total rows], iterations[count],
+ * metrics[count * FBALP_METRICS]; `out_omega` (may be NULL) receives the
+ * final primal weight per instance.  Asynchronous on the engine's stream.
+ * Replaces: GpuPdhgCorrector.solve (`src/gpu_pdhg_corrector.py:273-438`),
+ * GpuPdhgWorkspace.run / set_accepted (`src/gpu_pdhg_workspace.py:295-367`)
+ * and certify_blocks_device (`src/gpu_block_lp.py:52-132`). */
+int fbalp_engine_solve(fbalp_engine* engine, const double* warm_x, const double* warm_y,
+                       const double* warm_omega, const fbalp_solve_params* params,
+                       int32_t* out_status, double* out_objective, double* out_x, double* out_y,
+                       int32_t* out_iterations, double* out_metrics, double* out_omega);
+
+/* Release the engine's device memory.  Replaces the reference services'
+ * close()/release paths (`src/cpu_repeated_lp.py:820-831`). */
+int fbalp_engine_destroy(fbalp_engine* engine);
+
+/* Change the stream later calls are queued on (cudaStream_t). */
+int fbalp_engine_set_stream(fbalp_engine* engine, void* stream);
+
+/* HOST query: total columns/rows of the bound batch and the per-instance
+ * offsets (arrays of `count` int64, may be NULL). */
+int fbalp_engine_layout(const fbalp_engine* engine, int64_t* total_cols, int64_t* total_rows,
+                        int64_t* col_offsets, int64_t* row_offsets);
+
+/* HOST-only preprocessing of one matrix, for inspection and tests: the Ruiz +
+ * Pock-Chambolle scalings (dr[rows], dc[cols], original order), the spectral
+ * norm estimate of the scaled matrix and the step size.  Replaces the metric
+ * computed at `src/gpu_pdhg_corrector.py:183-200`. */
+int fbalp_prepare_matrix(int32_t rows, int32_t cols, const int64_t* indptr,
+                         const int32_t* indices, const double* values,
+                         const fbalp_options* options, double* dr, double* dc,
+                         double* sigma_max, double* eta);
+
+const char* fbalp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FBALP_H */

@@ -1,0 +1,244 @@
+"""NumPy restatement of the engine's restarted Halpern PDHG (test
+infrastructure only; the parity reference for the CUDA kernels).
+
+Problem (minimisation form, HiGHS dual signs, as in
+``src/gpu_pdhg_corrector.py:1-15``)::
+
+    min c.x  s.t.  A[:neq] x = b[:neq],  A[neq:] x <= b[neq:],  l <= x <= u
+
+Preprocessing (per species, shared by every instance of that species):
+  * ``ruiz_iters`` rounds of Ruiz equilibration (row/column infinity norms,
+    square-root updates), then one Pock-Chambolle step (alpha = 1: row/column
+    absolute sums, square roots).  ``A~ = Dr A Dc``, ``x = Dc x~``,
+    ``y = Dr y~``.  The reference uses only the Pock-Chambolle diagonal metric
+    (``src/gpu_pdhg_corrector.py:183-200``); Ruiz scaling is this engine's
+    addition.
+  * ``eta = step_safety / ||A~||_2`` with ``||A~||_2`` from ``power_iters``
+    power iterations on ``A~^T A~`` from a fixed deterministic start vector.
+
+Iteration (primal-first PDHG operator ``T``, reflected Halpern anchoring;
+Lu & Yang "restarted Halpern PDHG", cuPDLPx 2025), ``tau = eta/omega``,
+``sigma = eta*omega``::
+
+    xn = clip(x - tau (c - A^T y), l, u)
+    yn = P_Y(y + sigma (b - A (2 xn - x)))      P_Y: y_i <= 0 on rows >= neq
+    w  = (k+1)/(k+2)
+    x  = w ((1+rho) xn - rho x) + (1-w) xa
+    y  = w ((1+rho) yn - rho y) + (1-w) ya
+
+Every ``check_every`` iterations, at the candidate ``(xn, yn)``: FP64 KKT
+metrics in original units; stop when converged; otherwise the restart rule on
+the fixed-point residual ``r = sqrt(omega |xn-x|^2 + |yn-y|^2/omega)``::
+
+    restart if r <= 0.2 r_restart
+            or (r <= 0.8 r_restart and r > r_prev)
+            or k >= 0.36 * it
+
+On restart the primal weight becomes
+``exp(0.5 log(|yn-ya|/|xn-xa|) + 0.5 log omega)`` (when both distances exceed
+1e-10) and ``x = xa = xn``, ``y = ya = yn``, ``k = 0``.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+from scipy.sparse import csr_matrix, diags
+
+BETA_SUFFICIENT = 0.2
+BETA_NECESSARY = 0.8
+BETA_ARTIFICIAL = 0.36
+OMEGA_SMOOTHING = 0.5
+
+STATUS_OPTIMAL = 0
+STATUS_ITERATION_LIMIT = 1
+STATUS_NUMERICAL = 2
+STATUS_HANDOFF = 5
+
+
+def power_start(n):
+    """Deterministic start vector: a multiplicative hash of the index mapped
+    to [0.5, 1.5) (identical integer arithmetic in the C++ preprocessor)."""
+    j = np.arange(n, dtype=np.uint64)
+    h = (j * np.uint64(2654435761)) % np.uint64(1 << 32)
+    return h.astype(np.float64) / 4294967296.0 + 0.5
+
+
+@dataclass
+class Prepared:
+    A: csr_matrix          # scaled matrix A~ (FP64)
+    dr: np.ndarray
+    dc: np.ndarray
+    eta: float
+    sigma_max: float
+    neq: int
+
+
+def prepare(S, neq=None, *, ruiz_iters=10, power_iters=256, step_safety=0.99):
+    S = csr_matrix(S, dtype=np.float64)
+    S.sum_duplicates()
+    S.sort_indices()
+    m, n = S.shape
+    neq = m if neq is None else int(neq)
+    dr = np.ones(m)
+    dc = np.ones(n)
+    rows = np.repeat(np.arange(m), np.diff(S.indptr))
+    cols = S.indices
+    av = np.abs(S.data)
+    for _ in range(ruiz_iters):
+        cur = av * dr[rows] * dc[cols]
+        rmax = np.zeros(m)
+        np.maximum.at(rmax, rows, cur)
+        cmax = np.zeros(n)
+        np.maximum.at(cmax, cols, cur)
+        fr = np.where(rmax > 0, np.sqrt(rmax), 1.0)
+        fc = np.where(cmax > 0, np.sqrt(cmax), 1.0)
+        dr = dr / fr
+        dc = dc / fc
+    cur = av * dr[rows] * dc[cols]
+    rsum = np.zeros(m)
+    np.add.at(rsum, rows, cur)
+    csum = np.zeros(n)
+    np.add.at(csum, cols, cur)
+    dr = dr / np.where(rsum > 0, np.sqrt(rsum), 1.0)
+    dc = dc / np.where(csum > 0, np.sqrt(csum), 1.0)
+    A = csr_matrix((S.data * dr[rows] * dc[cols], S.indices.copy(), S.indptr.copy()), shape=(m, n))
+    v = power_start(n)
+    v /= np.linalg.norm(v)
+    lam = 0.0
+    AT = A.T.tocsr()
+    for _ in range(power_iters):
+        wv = AT @ (A @ v)
+        lam = np.linalg.norm(wv)
+        if lam <= 0:
+            break
+        v = wv / lam
+    smax = float(np.sqrt(lam)) if lam > 0 else 0.0
+    eta = step_safety / smax if smax > 0 else 1.0
+    return Prepared(A=A, dr=dr, dc=dc, eta=eta, sigma_max=smax, neq=neq)
+
+
+def kkt_metrics(P: Prepared, cs, bs, ls, us, xn, yn):
+    """FP64 metrics at a scaled point (original units where they differ)."""
+    A, dr, dc, neq = P.A, P.dr, P.dc, P.neq
+    rho = A @ xn - bs
+    ro = rho / dr
+    pr_eq = np.max(np.abs(ro[:neq]), initial=0.0)
+    pr_ub = np.max(ro[neq:], initial=0.0)
+    bviol = max(np.max((ls - xn) * dc, initial=0.0), np.max((xn - us) * dc, initial=0.0))
+    primal = max(0.0, pr_eq, pr_ub, bviol)
+    rt = cs - A.T @ yn
+    ro_c = rt / dc
+    finl = np.isfinite(ls)
+    finu = np.isfinite(us)
+    dual = max(0.0, np.max(yn[neq:] * dr[neq:], initial=0.0),
+               np.max(np.where(~finl, ro_c, 0.0), initial=0.0),
+               np.max(np.where(~finu, -ro_c, 0.0), initial=0.0))
+    pobj = float(cs @ xn)
+    term = np.where(rt > 0, np.where(finl, rt * np.where(finl, ls, 0.0), 0.0),
+                    np.where(rt < 0, np.where(finu, rt * np.where(finu, us, 0.0), 0.0), 0.0))
+    dobj = float(bs @ yn + term.sum())
+    target = np.where(rt >= 0, ls, us)
+    bgap = np.abs(rt * (xn - np.where(np.isfinite(target), target, xn))).sum()
+    rgap = np.abs(yn[neq:] * rho[neq:]).sum()
+    kgap = (bgap + rgap) / max(1.0, abs(pobj))
+    rel_gap = abs(pobj - dobj) / (1.0 + abs(pobj) + abs(dobj))
+    xinf = float(np.max(np.abs(xn * dc), initial=0.0))
+    cinf = float(np.max(np.abs(cs / dc), initial=0.0))
+    return dict(primal_residual=primal, dual_violation=dual, relative_kkt_gap=kgap,
+                objective=pobj, dual_objective=dobj, relative_gap=rel_gap, x_inf=xinf, c_inf=cinf)
+
+
+def converged(mt, tol_primal, tol_dual, tol_gap):
+    return (mt["primal_residual"] <= tol_primal * (1.0 + mt["x_inf"])
+            and mt["dual_violation"] <= tol_dual * (1.0 + mt["c_inf"])
+            and mt["relative_gap"] <= tol_gap and mt["relative_kkt_gap"] <= tol_gap)
+
+
+def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0=1.0,
+          dtype=np.float64, max_iters=100000, check_every=64, tol_primal=1e-9, tol_dual=1e-9,
+          tol_gap=1e-9, rho=1.0, restarts=True, stop_on_converge=True, final_status=STATUS_OPTIMAL,
+          trace=None):
+    """Run the engine's algorithm for one instance; return dict with scaled
+    and original-unit iterates, status, iterations and metrics."""
+    A, dr, dc = P.A, P.dr, P.dc
+    m, n = A.shape
+    rhs = np.zeros(m) if rhs is None else np.asarray(rhs, float)
+    ls = lower / dc
+    us = upper / dc
+    cs = cost * dc
+    bs = rhs * dr
+    Af = A.astype(dtype)
+    ATf = A.T.tocsr().astype(dtype)
+    lsf, usf, csf, bsf = (v.astype(dtype) for v in (ls, us, cs, bs))
+    ineq = np.arange(m) >= P.neq
+    x = np.zeros(n) if x0 is None else np.asarray(x0, float) / dc
+    y = np.zeros(m) if y0 is None else np.asarray(y0, float) / dr
+    x = np.clip(x.astype(dtype), lsf, usf)
+    y = np.where(ineq, np.minimum(y, 0.0), y).astype(dtype)
+    xa, ya = x.copy(), y.copy()
+    omega = float(omega0)
+    k = 0
+    r_restart = np.inf
+    r_prev = np.inf
+    status = STATUS_ITERATION_LIMIT
+    mt = None
+    it = 0
+    xn, yn = x, y
+    if max_iters == 0:
+        mt = kkt_metrics(P, cs, bs, ls, us, x.astype(float), y.astype(float))
+    for it in range(1, max_iters + 1):
+        tau = dtype(P.eta / omega)
+        sig = dtype(P.eta * omega)
+        g = ATf @ y
+        xn = np.clip(x - tau * (csf - g), lsf, usf).astype(dtype)
+        xb = (xn + xn - x).astype(dtype)
+        h = Af @ xb
+        yn = (y + sig * (bsf - h)).astype(dtype)
+        yn = np.where(ineq, np.minimum(yn, 0), yn).astype(dtype)
+        w = dtype((k + 1.0) / (k + 2.0))
+        if rho == 1.0:
+            xnew = (w * xb + (1 - w) * xa).astype(dtype)
+            ynew = (w * (yn + yn - y) + (1 - w) * ya).astype(dtype)
+        else:
+            xnew = (w * ((1 + rho) * xn - rho * x) + (1 - w) * xa).astype(dtype)
+            ynew = (w * ((1 + rho) * yn - rho * y) + (1 - w) * ya).astype(dtype)
+        k += 1
+        is_check = (it % check_every == 0) or it == max_iters
+        if is_check:
+            dx = (xn.astype(float) - x.astype(float))
+            dy = (yn.astype(float) - y.astype(float))
+            r = np.sqrt(omega * (dx @ dx) + (dy @ dy) / omega)
+            mt = kkt_metrics(P, cs, bs, ls, us, xn.astype(float), yn.astype(float))
+            if trace is not None:
+                trace.append(dict(it=it, r=r, omega=omega, **mt))
+            if not np.isfinite(r) or not all(np.isfinite(v) for v in mt.values()):
+                status = STATUS_NUMERICAL
+                break
+            if stop_on_converge and converged(mt, tol_primal, tol_dual, tol_gap):
+                status = final_status
+                break
+            if it == max_iters:
+                break
+            if restarts and (r <= BETA_SUFFICIENT * r_restart
+                             or (r <= BETA_NECESSARY * r_restart and r > r_prev)
+                             or k >= BETA_ARTIFICIAL * it):
+                ddx = xn.astype(float) - xa.astype(float)
+                ddy = yn.astype(float) - ya.astype(float)
+                nx = np.sqrt(ddx @ ddx)
+                ny = np.sqrt(ddy @ ddy)
+                if nx > 1e-10 and ny > 1e-10:
+                    omega = float(np.exp(OMEGA_SMOOTHING * np.log(ny / nx)
+                                         + (1 - OMEGA_SMOOTHING) * np.log(omega)))
+                xnew, ynew = xn.copy(), yn.copy()
+                xa, ya = xn.copy(), yn.copy()
+                k = 0
+                r_restart = r
+                r_prev = np.inf
+            else:
+                r_prev = r
+        x, y = xnew, ynew
+    xo = xn.astype(float) * dc
+    yo = yn.astype(float) * dr
+    return dict(x=xo, y=yo, xs=xn, ys=yn, status=status, iterations=it, metrics=mt, omega=omega)

@@ -1,0 +1,181 @@
+"""GPU parity of the engine (through the C ABI) against the CPU oracle and
+HiGHS golden optima."""
+import numpy as np
+import pytest
+from scipy.sparse import csr_matrix
+
+from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+from oracle import certificate, dfba, pdhg
+from tests.conftest import cuda_available
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not cuda_available(), reason="CUDA device required")]
+
+OBJ_TOL = 1e-6  # relative objective tolerance against HiGHS
+
+
+def engine(mats, **opt):
+    import torch  # noqa: F401
+    from co_cultivation_metabolic_atlas_b200.engine import EngineOptions, LPEngine
+    return LPEngine(mats, options=EngineOptions(**opt))
+
+
+def cfg(**kw):
+    from co_cultivation_metabolic_atlas_b200.engine import SolveConfig
+    return SolveConfig(**kw)
+
+
+def flat(rows):
+    return np.concatenate([np.asarray(r, float).ravel() for r in rows])
+
+
+def run_single(a, neq, lowers, uppers, costs, rhss=None, config=None, **opt):
+    eng = engine([(csr_matrix(np.asarray(a, float)) if not hasattr(a, "tocsr") else a, neq)], **opt)
+    k = len(lowers)
+    eng.set_instances(np.zeros(k, np.int32), flat(lowers), flat(uppers), flat(costs),
+                      None if rhss is None else flat(rhss))
+    res = eng.solve(config=config or cfg())
+    n = eng.shapes[0][1]
+    m = eng.shapes[0][0]
+    out = dict(status=res.status.cpu().numpy(), obj=res.objective.cpu().numpy(),
+               x=res.x.cpu().numpy()[:k * n].reshape(k, n),
+               y=res.y.cpu().numpy()[:k * m].reshape(k, m) if m else np.zeros((k, 0)),
+               iters=res.iterations.cpu().numpy(), metrics=res.metrics.cpu().numpy(),
+               omega=res.omega.cpu().numpy())
+    eng.close()
+    return out
+
+
+# --- the reference's known-answer LPs, through the C ABI ---
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_kat_inequality_dual_sign(precision):
+    r = run_single([[1.0]], 0, [[0.0]], [[2.0]], [[-1.0]], [[1.0]], config=cfg(precision=precision))
+    assert r["status"].tolist() == [0]
+    np.testing.assert_allclose(r["x"], [[1.0]], atol=1e-8)
+    np.testing.assert_allclose(r["y"], [[-1.0]], atol=1e-8)
+
+
+def test_kat_independent_instances():
+    r = run_single([[1.0]], 0, [[0.0], [0.0]], [[2.0], [2.0]], [[-1.0], [-1.0]], [[1.0], [0.5]],
+                   config=cfg(precision="fp64"))
+    assert r["status"].tolist() == [0, 0]
+    np.testing.assert_allclose(r["x"].ravel(), [1.0, 0.5], atol=1e-8)
+    np.testing.assert_allclose(r["y"].ravel(), [-1.0, -1.0], atol=3e-7)
+
+
+def test_kat_box_only_infinite_bound():
+    r = run_single([[0.0, 1.0]], 1, [[-np.inf, 0.0]], [[2.0, np.inf]], [[-1.0, 0.0]], [[0.0]],
+                   config=cfg(precision="fp64"))
+    assert r["status"].tolist() == [0]
+    np.testing.assert_allclose(r["x"], [[2.0, 0.0]], atol=1e-10)
+
+
+def test_kat_infeasible_fails_closed():
+    r = run_single([[1.0], [-1.0]], 0, [[-np.inf]], [[np.inf]], [[0.0]], [[0.0, -1.0]],
+                   config=cfg(precision="fp64", max_iterations=40, check_every=5))
+    assert r["status"].tolist() == [1]
+    assert r["iters"].tolist() == [40]
+
+
+def test_warm_start_at_optimum_needs_no_iterations():
+    import torch
+    eng = engine([(csr_matrix([[1.0]]), 1)])
+    eng.set_instances([0, 0], np.zeros(2), np.full(2, 3.0), np.ones(2), np.array([1.0, 2.0]))
+    res = eng.solve(warm_x=np.array([1.0, 2.0]), warm_y=np.array([1.0, 1.0]), config=cfg(precision="fp64"))
+    torch.cuda.synchronize()
+    assert res.status.cpu().tolist() == [0, 0]
+    assert res.iterations.cpu().tolist() == [0, 0]
+    eng.close()
+
+
+def test_invalid_instance_is_flagged_and_others_solve():
+    lo = [[0.0], [3.0], [np.nan]]
+    up = [[2.0], [2.0], [1.0]]
+    r = run_single([[1.0]], 0, lo, up, [[-1.0]] * 3, [[1.0]] * 3, config=cfg(precision="fp64"))
+    assert r["status"].tolist() == [0, 3, 3]
+    assert np.isnan(r["obj"][1]) and np.isnan(r["x"][2]).all()
+
+
+# --- iterate parity with the oracle restatement ---
+
+@pytest.mark.parametrize("restarts,iters", [(False, 37), (False, 200), (True, 640)])
+def test_fp64_iterates_match_oracle(restarts, iters):
+    model, lower, upper = syn.single_species_workload(3, m=120, n=260)
+    P = pdhg.prepare(model.S)
+    config = cfg(precision="fp64", max_iterations=iters, check_every=64, tol_primal=0.0,
+                 tol_dual=0.0, tol_gap=0.0, restarts=restarts)
+    r = run_single(model.S, 120, lower, upper, [model.cost] * 3, config=config)
+    for i in range(3):
+        ref = pdhg.solve(P, lower[i], upper[i], model.cost, max_iters=iters, check_every=64,
+                         tol_primal=0.0, tol_dual=0.0, tol_gap=0.0, restarts=restarts)
+        assert r["status"][i] == 1 and r["iters"][i] == iters
+        scale = max(1.0, np.abs(ref["x"]).max())
+        np.testing.assert_allclose(r["x"][i], np.clip(ref["x"], lower[i], upper[i]), rtol=0,
+                                   atol=1e-9 * scale)
+        np.testing.assert_allclose(r["y"][i], ref["y"], rtol=0, atol=1e-9 * max(1.0, np.abs(ref["y"]).max()))
+        assert r["omega"][i] == pytest.approx(ref["omega"], rel=1e-9)
+
+
+# --- the seeded workloads against HiGHS ---
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_single_species_batch_matches_highs(golden_dir, precision):
+    g = np.load(golden_dir / "highs_single.npz")
+    model, lower, upper = syn.single_species_workload(8)
+    r = run_single(model.S, 1200, lower, upper, [model.cost] * 8, config=cfg(precision=precision))
+    assert (r["status"] == 0).all(), r["status"]
+    fun = g["fun"]
+    assert np.all(np.abs(r["obj"] - fun) <= OBJ_TOL * np.maximum(1.0, np.abs(fun)))
+    for i in range(8):
+        cert = certificate.certificate(model.S, np.zeros(1200), lower[i], upper[i], model.cost, 1200,
+                                       r["x"][i], r["y"][i])
+        assert cert["certificate_passed"], cert
+        assert cert["objective"] == pytest.approx(fun[i], rel=OBJ_TOL, abs=OBJ_TOL)
+
+
+def test_uneven_three_species_batch_in_one_launch(golden_dir):
+    g = np.load(golden_dir / "highs_community.npz")
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(4)
+    eng = engine([(m.S, m.S.shape[0]) for m in models])
+    order = [(s, e) for e in range(4) for s in range(3)]  # species interleaved
+    lows = {s: dfba.uptake_lower_bounds(models[s], medium, biomass, 0.05) for s in range(3)}
+    sid = np.array([s for s, _ in order], np.int32)
+    eng.set_instances(sid, flat([lows[s][e] for s, e in order]),
+                      flat([models[s].upper for s, _ in order]), flat([models[s].cost for s, _ in order]))
+    res = eng.solve(config=cfg(precision="mixed"))
+    status = res.status.cpu().numpy()
+    obj = res.objective.cpu().numpy()
+    x = res.x.cpu().numpy()
+    co, ro, _, _ = eng.layout(sid)
+    y = res.y.cpu().numpy()
+    assert (status == 0).all(), status
+    for i, (s, e) in enumerate(order):
+        fun = float(g[f"s{s}_fun"][e])
+        assert abs(obj[i] - fun) <= OBJ_TOL * max(1.0, abs(fun))
+        mdl = models[s]
+        n, m = mdl.S.shape[1], mdl.S.shape[0]
+        cert = certificate.certificate(mdl.S, np.zeros(m), lows[s][e], mdl.upper, mdl.cost, m,
+                                       x[co[i]:co[i] + n], y[ro[i]:ro[i] + m])
+        assert cert["certificate_passed"], cert
+    eng.close()
+
+
+def test_spilled_arrays_give_identical_results():
+    model, lower, upper = syn.single_species_workload(4, m=300, n=650)
+    config = cfg(precision="mixed")
+    a = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config)
+    b = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config, max_dynamic_smem=8192)
+    np.testing.assert_array_equal(a["x"], b["x"])
+    np.testing.assert_array_equal(a["y"], b["y"])
+    np.testing.assert_array_equal(a["iters"], b["iters"])
+    assert (a["status"] == 0).all()
+
+
+def test_repeat_solves_are_deterministic():
+    model, lower, upper = syn.single_species_workload(6, m=300, n=650)
+    a = run_single(model.S, 300, lower, upper, [model.cost] * 6)
+    b = run_single(model.S, 300, lower, upper, [model.cost] * 6)
+    np.testing.assert_array_equal(a["x"], b["x"])
+    np.testing.assert_array_equal(a["iters"], b["iters"])

@@ -1,0 +1,107 @@
+"""The C-ABI library loads, exports every declared symbol, and its host-only
+preprocessing matches the oracle -- no GPU needed."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+from scipy.sparse import csr_matrix
+
+from tests.conftest import ROOT
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "fbalp.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fbalp_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_symbols()
+    for required in ("fbalp_engine_create", "fbalp_engine_set_instances", "fbalp_engine_solve",
+                     "fbalp_engine_destroy", "fbalp_last_error"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol(native_built):
+    lib = ctypes.CDLL(str(native_built))
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert missing == []
+
+
+def test_defaults(native_built):
+    from co_cultivation_metabolic_atlas_b200 import _native as N
+    o = N.default_options()
+    p = N.default_solve_params()
+    assert (o.ruiz_iterations, o.power_iterations, o.warps_per_block) == (10, 256, 16)
+    assert o.step_safety == pytest.approx(0.99)
+    assert p.precision == N.PRECISION_MIXED and p.check_every == 64
+    assert p.tol_gap == pytest.approx(1e-9) and p.fp32_tol_gap == pytest.approx(1e-4)
+
+
+def test_host_preprocessing_matches_oracle(native_built):
+    from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+    from co_cultivation_metabolic_atlas_b200.engine import prepare_matrix
+    from oracle import pdhg
+    model, _, _ = syn.single_species_workload(1, m=300, n=650)
+    got = prepare_matrix(model.S)
+    ref = pdhg.prepare(model.S)
+    np.testing.assert_allclose(got["dr"], ref.dr, rtol=1e-14, atol=0)
+    np.testing.assert_allclose(got["dc"], ref.dc, rtol=1e-14, atol=0)
+    assert got["sigma_max"] == pytest.approx(ref.sigma_max, rel=1e-12)
+    assert got["eta"] == pytest.approx(ref.eta, rel=1e-12)
+    # Pock-Chambolle scaling bounds the spectral norm by one
+    assert got["sigma_max"] <= 1.0 + 1e-12
+
+
+def test_preprocessing_of_duplicates_equals_summed_matrix(native_built):
+    from co_cultivation_metabolic_atlas_b200.engine import prepare_matrix
+    dup = csr_matrix((np.array([1.0, 2.0, -1.0, 0.0, 4.0]), np.array([0, 0, 2, 1, 1]),
+                      np.array([0, 2, 4, 5])), shape=(3, 3))
+    summed = csr_matrix(np.array([[3.0, 0, 0], [0, 0, -1.0], [0, 4.0, 0]]))
+    a = prepare_matrix(dup)
+    b = prepare_matrix(summed)
+    np.testing.assert_array_equal(a["dr"], b["dr"])
+    np.testing.assert_array_equal(a["dc"], b["dc"])
+
+
+@pytest.mark.parametrize("case,match", [
+    ("index", "column index out of range"),
+    ("nan", "finite"),
+    ("ptr", "monotone"),
+])
+def test_invalid_matrices_are_rejected(native_built, case, match):
+    from co_cultivation_metabolic_atlas_b200 import _native as N
+    lib = N.load()
+    indptr = np.array([0, 2, 3], dtype=np.int64)
+    indices = np.array([0, 1, 1], dtype=np.int32)
+    values = np.array([1.0, 2.0, 3.0])
+    if case == "index":
+        indices[2] = 7
+    elif case == "nan":
+        values[1] = np.nan
+    else:
+        indptr = np.array([0, 3, 2], dtype=np.int64)
+    dr = np.empty(2)
+    dc = np.empty(2)
+    code = lib.fbalp_prepare_matrix(2, 2, indptr.ctypes.data_as(N.c_int64_p),
+                                    indices.ctypes.data_as(N.c_int32_p),
+                                    values.ctypes.data_as(N.c_double_p), None,
+                                    dr.ctypes.data_as(N.c_double_p), dc.ctypes.data_as(N.c_double_p),
+                                    None, None)
+    assert code == N.FBALP_ERR_INVALID
+    assert match in lib.fbalp_last_error().decode()
+
+
+def test_engine_entry_points_reject_null_handles(native_built):
+    from co_cultivation_metabolic_atlas_b200 import _native as N
+    lib = N.load()
+    assert lib.fbalp_engine_destroy(None) == N.FBALP_ERR_INVALID
+    assert lib.fbalp_engine_set_instances(None, 1, None, None, None, None, None) == N.FBALP_ERR_INVALID
+    p = N.default_solve_params()
+    assert lib.fbalp_engine_solve(None, None, None, None, ctypes.byref(p), None, None, None, None,
+                                  None, None, None) == N.FBALP_ERR_INVALID
+    out = ctypes.c_void_p()
+    assert lib.fbalp_engine_create(0, None, None, None, None, None, None, None, None,
+                                   ctypes.byref(out)) == N.FBALP_ERR_INVALID
+    assert out.value is None

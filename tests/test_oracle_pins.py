@@ -1,0 +1,166 @@
+"""Pin the CPU oracle before trusting it: the reference's own known-answer
+LPs, golden certificates produced by the reference's ``_certificate``, and
+HiGHS optima of the seeded workloads."""
+import json
+
+import numpy as np
+import pytest
+from scipy.sparse import csr_matrix
+
+from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+from oracle import certificate, dfba, highs, pdhg, reference_pdhg
+
+
+def solve_small(a, rhs, lo, up, c, neq, **kw):
+    P = pdhg.prepare(csr_matrix(np.asarray(a, float)), neq)
+    return pdhg.solve(P, np.asarray(lo, float), np.asarray(up, float), np.asarray(c, float),
+                      np.asarray(rhs, float), check_every=kw.pop("check_every", 8), **kw)
+
+
+# --- the reference's known-answer tests (tests/test_gpu_pdhg_corrector.py) ---
+
+def test_kat_inequality_dual_sign():
+    # :29-42  min -x, x <= 1, 0 <= x <= 2 -> x = 1, HiGHS-style y = -1
+    r = solve_small([[1.0]], [1.0], [0.0], [2.0], [-1.0], 0)
+    assert r["status"] == pdhg.STATUS_OPTIMAL
+    np.testing.assert_allclose(r["x"], [1.0], atol=1e-8)
+    np.testing.assert_allclose(r["y"], [-1.0], atol=1e-8)
+    cert = certificate.certificate(csr_matrix([[1.0]]), np.array([1.0]), np.array([0.0]),
+                                   np.array([2.0]), np.array([-1.0]), 0, r["x"], r["y"])
+    assert cert["certificate_passed"]
+
+
+def test_kat_independent_blocks():
+    # :66-82  two independent LPs -> x = [1, 0.5], y = [-1, -1]
+    for rhs, want in ((1.0, 1.0), (0.5, 0.5)):
+        r = solve_small([[1.0]], [rhs], [0.0], [2.0], [-1.0], 0)
+        np.testing.assert_allclose(r["x"], [want], atol=1e-8)
+        np.testing.assert_allclose(r["y"], [-1.0], atol=3e-7)
+
+
+def test_kat_box_only_with_infinite_bound():
+    # :85-95  the first variable has no matrix coefficient -> its upper bound
+    r = solve_small([[0.0, 1.0]], [0.0], [-np.inf, 0.0], [2.0, np.inf], [-1.0, 0.0], 1)
+    assert r["status"] == pdhg.STATUS_OPTIMAL
+    np.testing.assert_allclose(r["x"], [2.0, 0.0], atol=1e-10)
+
+
+def test_kat_infeasible_fails_closed():
+    # :98-112  x <= 0 and -x <= -1: never accepted, budget exhausted
+    r = solve_small([[1.0], [-1.0]], [0.0, -1.0], [-np.inf], [np.inf], [0.0], 0, max_iters=40,
+                    check_every=5)
+    assert r["status"] == pdhg.STATUS_ITERATION_LIMIT
+    assert r["iterations"] == 40
+
+
+def test_kat_warm_start_certified_at_iteration_zero():
+    # :45-63  warm starts at the optimum are accepted without iterating
+    r = solve_small([[1.0]], [2.0], [0.0], [3.0], [1.0], 1, x0=np.array([2.0]),
+                    y0=np.array([1.0]), max_iters=0)
+    assert pdhg.converged(r["metrics"], 1e-9, 1e-9, 1e-9)
+
+
+def test_reference_metric_and_primal_weight():
+    # :115-120 and :140-164
+    a = csr_matrix(np.array([[2.0, -1.0]]))
+    tau, sigma = reference_pdhg.metric(a, 0.9)
+    np.testing.assert_allclose(sigma, [0.3])
+    np.testing.assert_allclose(tau, [0.45, 0.9])
+    tau2, sigma2 = reference_pdhg.metric(a, 0.9, primal_weight=2.0)
+    np.testing.assert_allclose(sigma2, 2 * sigma)
+    np.testing.assert_allclose(tau2, tau / 2)
+
+
+def test_reference_operator_reaches_kat_optimum():
+    x, y = reference_pdhg.iterate(csr_matrix([[1.0]]), np.array([1.0]), np.array([0.0]),
+                                  np.array([2.0]), np.array([-1.0]), 0, 200, step_safety=0.9)
+    np.testing.assert_allclose(x, [1.0], atol=1e-8)
+    np.testing.assert_allclose(y, [-1.0], atol=1e-8)
+
+
+# --- golden certificates from the reference's _certificate ---
+
+def test_certificate_matches_reference_golden(golden_dir):
+    g = np.load(golden_dir / "certificate_golden.npz", allow_pickle=False)
+    rows = json.loads(str(g["rows"]))
+    model, lower, upper = syn.single_species_workload(4, m=120, n=260)
+    a_ineq = csr_matrix(np.array([[1.0, 1.0], [1.0, -1.0], [-1.0, 2.0]]))
+    for row in rows:
+        key = row["key"]
+        x, y = g[f"{key}__x"], g[f"{key}__y"]
+        if row["instance"] >= 0:
+            i = row["instance"]
+            got = certificate.certificate(model.S, np.zeros(model.S.shape[0]), lower[i], upper[i],
+                                          model.cost, model.S.shape[0], x, y)
+        else:
+            got = certificate.certificate(a_ineq, np.array([1.0, 0.5, 2.0]), np.array([0.0, -np.inf]),
+                                          np.array([np.inf, 3.0]), np.array([-1.0, -0.5]), 1, x, y)
+        for name in ("primal_residual", "dual_violation", "relative_kkt_gap",
+                     "bound_complementarity_gap", "row_complementarity_gap"):
+            assert got[name] == pytest.approx(row[name], rel=1e-12, abs=1e-15), (key, name)
+        assert got["certificate_passed"] == row["certificate_passed"], key
+
+
+# --- HiGHS and the engine restatement on the seeded workload ---
+
+def test_highs_oracle_reproduces_golden(golden_dir):
+    g = np.load(golden_dir / "highs_single.npz")
+    model, lower, upper = syn.single_species_workload(8)
+    np.testing.assert_array_equal(lower[:, :model.n_exchange], g["exchange_lower"])
+    st, fun, x, y = highs.solve_one(model.S, lower[0], upper[0], model.cost)
+    assert st == 0 and fun == pytest.approx(float(g["fun"][0]), rel=1e-9)
+
+
+def test_engine_restatement_matches_highs(golden_dir):
+    g = np.load(golden_dir / "highs_single.npz")
+    model, lower, upper = syn.single_species_workload(8)
+    P = pdhg.prepare(model.S)
+    for i in range(2):
+        r = pdhg.solve(P, lower[i], upper[i], model.cost)
+        assert r["status"] == pdhg.STATUS_OPTIMAL
+        fun = float(g["fun"][i])
+        assert abs(r["metrics"]["objective"] - fun) <= 1e-6 * max(1.0, abs(fun))
+        cert = certificate.certificate(model.S, np.zeros(model.S.shape[0]), lower[i], upper[i],
+                                       model.cost, model.S.shape[0], r["x"], r["y"])
+        assert cert["certificate_passed"]
+
+
+def test_mixed_precision_restatement_matches_highs(golden_dir):
+    g = np.load(golden_dir / "highs_single.npz")
+    model, lower, upper = syn.single_species_workload(8)
+    P = pdhg.prepare(model.S)
+    r32 = pdhg.solve(P, lower[3], upper[3], model.cost, dtype=np.float32, tol_primal=1e-6,
+                     tol_dual=1e-6, tol_gap=1e-4, final_status=pdhg.STATUS_HANDOFF)
+    assert r32["status"] == pdhg.STATUS_HANDOFF
+    r = pdhg.solve(P, lower[3], upper[3], model.cost, x0=r32["x"], y0=r32["y"], omega0=r32["omega"])
+    assert r["status"] == pdhg.STATUS_OPTIMAL
+    fun = float(g["fun"][3])
+    assert abs(r["metrics"]["objective"] - fun) <= 1e-6 * max(1.0, abs(fun))
+
+
+def test_community_restatement_matches_highs(golden_dir):
+    g = np.load(golden_dir / "highs_community.npz")
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(4)
+    for k, mdl in enumerate(models):
+        lo = dfba.uptake_lower_bounds(mdl, medium, biomass, 0.05)
+        P = pdhg.prepare(mdl.S)
+        r = pdhg.solve(P, lo[0], mdl.upper, mdl.cost)
+        fun = float(g[f"s{k}_fun"][0])
+        assert r["status"] == pdhg.STATUS_OPTIMAL
+        assert abs(r["metrics"]["objective"] - fun) <= 1e-6 * max(1.0, abs(fun))
+
+
+def test_uptake_bounds_follow_michaelis_menten():
+    models = syn.community_models()
+    mdl = models[1]
+    medium = np.full((1, syn.MEDIUM_SIZE), 0.5)
+    biomass = np.array([[0.05, 0.02, 0.03]])
+    lo = dfba.uptake_lower_bounds(mdl, medium, biomass, 0.05)
+    k = 3
+    c = 0.5
+    v_kin = mdl.vmax[k] * c / (mdl.km[k] + c)
+    v_phys = min(c / (0.1 * 0.05), 10 * mdl.vmax[k])
+    assert lo[0, mdl.medium_columns[k]] == pytest.approx(round(-min(v_kin, v_phys), 6))
+    others = np.setdiff1d(np.arange(mdl.S.shape[1]), mdl.medium_columns)
+    np.testing.assert_array_equal(lo[0, others], mdl.lower[others])
