@@ -1,0 +1,428 @@
+"""Benchmark: HiGHS-certified FBA LPs/s on the 4,096-environment three-species
+dFBA workload (one step = 12,288 LPs of uneven size, solved in one persistent
+launch per precision phase, then the Euler update), warm start vs cold.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
+
+Prints one JSON line (rank 0).  See DESIGN.md for the roofline model.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "HiGHS-certified FBA LPs/s (1e-6 rel obj); warm-start vs cold PDHG, same B200"
+UNIT = "LPs/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("product", "reference"), default="product")
+    ap.add_argument("--envs", type=int, default=4096, help="environments per GPU")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64", "fp32"))
+    ap.add_argument("--cpu-sample", type=int, default=48, help="LPs per species in the CPU baseline sample")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cold", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args, lps):
+    from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+    return {"workload": f"community dFBA step: {args.envs} envs x 3 species "
+                        f"({', '.join(f'{m}x{n}' for m, n in syn.COMMUNITY_SIZES)}), {lps} LPs/step, dt=0.05 h",
+            "envs_per_gpu": args.envs, "lps_per_step": lps, "seed": args.seed,
+            "precision": args.precision,
+            "l2": "inputs larger than L2 (bounds+objective of one step > 600 MB), no flush"}
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or not self.path:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(parts)
+            except ValueError:
+                pass
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- peaks
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per FP32-phase instance-iteration from the committed ncu
+    summary (profiles/pdhg_fp32_community.txt), if present."""
+    p = ROOT / "profiles" / "pdhg_fp32_community.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_instance_iteration:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ----------------------------------------------------------------------------- CPU HiGHS
+def cpu_highs_sample(models, lowers, per_species, seed, cores=None):
+    """HiGHS (scipy linprog highs-ds, one thread per LP) over all host cores on
+    a seeded sample of ``per_species`` LPs per species.  Returns (LPs/s, cores,
+    wall seconds, [(species, env, fun)])."""
+    from oracle import highs
+    cores = cores or len(os.sched_getaffinity(0))
+    rng = np.random.default_rng(seed + 99)
+    S_list, lo, up, c, tags = [], [], [], [], []
+    for s, mdl in enumerate(models):
+        envs = rng.choice(lowers[s].shape[0], min(per_species, lowers[s].shape[0]), replace=False)
+        for e in envs:
+            S_list.append(mdl.S)
+            lo.append(lowers[s][e])
+            up.append(mdl.upper)
+            c.append(mdl.cost)
+            tags.append((s, int(e)))
+    res, wall = highs.solve_batch(S_list, lo, up, c, workers=cores)
+    funs = [(t[0], t[1], r[1] if r[0] == 0 else None) for t, r in zip(tags, res)]
+    return len(res) / wall, cores, wall, funs
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+    from oracle import dfba
+    models = syn.community_models(seed=args.seed)
+    medium, biomass = syn.initial_environments(args.envs, seed=args.seed)
+    lowers = [dfba.uptake_lower_bounds(m, medium, biomass, 0.05) for m in models]
+    per = max(4, args.cpu_sample // 3)
+    rates = []
+    cores = None
+    for k in range(args.warmup + args.steps):
+        rate, cores, wall, _ = cpu_highs_sample(models, lowers, per, args.seed + k)
+        if k >= args.warmup:
+            rates.append(rate)
+    value = statistics.mean(rates)
+    lps = args.envs * len(models)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * lps / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(args, lps),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{3 * per} LPs per step (seeded, {per} per species) of the step's "
+                                       f"{lps} LPs; scipy.optimize.linprog(method='highs-ds'), one HiGHS "
+                                       f"thread per LP, thread pool over all cores (the reference's "
+                                       f"ParallelCpuLP pattern)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- product arm
+def run_product(args):
+    import torch
+    import torch.distributed as dist
+
+    from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+    from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
+    from co_cultivation_metabolic_atlas_b200.engine import SolveConfig
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    models = syn.community_models(seed=args.seed)
+    medium, biomass = syn.initial_environments(args.envs, seed=args.seed + 1000 * rank)
+    cfg = SolveConfig(precision=args.precision)
+    lps = args.envs * len(models)
+
+    def trajectory(warm):
+        com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, device=dev)
+        for _ in range(args.warmup):
+            com.step()
+        torch.cuda.synchronize()
+        barrier()
+        stream = torch.cuda.current_stream()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        certified = []
+        iters = []
+        fp32_ms = 0.0
+        fp32_units = 0
+        fp32_bytes = 0.0
+        launches = 0
+        start.record(stream)
+        for _ in range(args.steps):
+            st = com.step()
+            certified.append(st.certified)
+            iters.append(st.iterations.clone())
+            launches += 2 if args.precision == "mixed" else 1
+        stop.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = start.elapsed_time(stop)
+        cert = int(sum(int(c.item()) for c in certified))
+        it = torch.cat(iters).cpu().numpy()
+        return com, ms, cert, it, launches
+
+    with ClockSampler(local) as clocks:
+        com, ms, cert, it, launches = trajectory("previous")
+    clock_summary = clocks.summary()
+    ms_max = max_over_ranks(ms)
+    cert_all = sum_over_ranks(cert)
+    value = cert_all / (ms_max / 1e3)
+
+    # --- roofline of the dominant kernel (FP32 phase of one extra solve) ---
+    peak, peak_kind = hbm_peak()
+    com.uptake_bounds()
+    res = com.solve()
+    torch.cuda.synchronize()
+    t32, t64 = com.engine.phase_times()
+    dom_ms = t32 if args.precision != "fp64" else t64
+    w = 4 if args.precision != "fp64" else 8
+    if args.precision == "mixed":
+        it32 = com.engine.phase_iterations().cpu().numpy().astype(np.int64)
+    else:
+        it32 = res.iterations.cpu().numpy().astype(np.int64)
+    sid = com.species_id
+    per_inst = np.array([w * (3 * m.S.shape[1] + 3 * m.S.shape[0] + 2 * len(m.medium_columns))
+                         for m in models], dtype=np.float64)
+    inst_bytes = float(np.sum(it32 * per_inst[sid]))
+    mat_bytes = 0.0
+    for s, m in enumerate(models):
+        its = it32[sid == s]
+        mat_bytes += float(its.max() if its.size else 0) * 2 * (m.S.nnz * (w + 4) + 4 * (m.S.shape[0] + 1))
+    alg_bytes = inst_bytes + mat_bytes
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    tpi = profiled_traffic()
+    traffic = None if tpi is None else tpi * float(it32.sum())
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} copy bandwidth",
+                "kernel": f"pdhg_persistent<{'float' if w == 4 else 'double'}>",
+                "algorithmic_bytes": alg_bytes, "kernel_ms": dom_ms,
+                "instance_iterations": int(it32.sum())}
+
+    # --- CPU baseline on a sample of this step's LPs + HiGHS objective check ---
+    cpu = None
+    highs_check = None
+    if rank == 0 and world >= 1:
+        lower = com.lower.cpu().numpy()
+        co = com.col_offsets.cpu().numpy()
+        lowers = []
+        for s, m in enumerate(models):
+            n = m.S.shape[1]
+            base = int(co[s * args.envs])
+            lowers.append(lower[base:base + args.envs * n].reshape(args.envs, n))
+        per = max(4, args.cpu_sample // 3)
+        rate, cores, wall, funs = cpu_highs_sample(models, lowers, per, args.seed)
+        obj = res.objective.cpu().numpy()
+        status = res.status.cpu().numpy()
+        errs = []
+        agree = 0
+        for s, e, fun in funs:
+            i = s * args.envs + e
+            if fun is None or status[i] != 0:
+                continue
+            err = abs(obj[i] - fun) / max(1.0, abs(fun))
+            errs.append(err)
+            agree += err <= 1e-6
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{len(funs)} LPs ({per} per species, seeded) of one step's {lps}; "
+                         f"scipy.optimize.linprog(method='highs-ds'), one HiGHS thread per LP, thread "
+                         f"pool over all cores (ParallelCpuLP pattern); {wall:.1f} s wall"}
+        highs_check = {"sampled": len(funs), "within_1e-6": int(agree),
+                       "max_rel_obj_err": max(errs) if errs else None}
+
+    # --- cold PDHG on its own trajectory (same seeds) ---
+    cold = None
+    if not args.no_cold:
+        com.close()
+        com_c, ms_c, cert_c, it_c, _ = trajectory("cold")
+        cold = sum_over_ranks(cert_c) / (max_over_ranks(ms_c) / 1e3)
+        cold_iters = float(np.mean(it_c))
+        com_c.close()
+        com = None
+    # --- e2e through the public engine API with host buffers ---
+    e2e = run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64" if args.precision == "mixed" else args.precision,
+                "data": "synthetic (seeded generator; no public dataset)",
+                "config": dict(workload_config(args, lps), warm_start="previous-step solution",
+                               parallelism=f"env-sharded x{world}"),
+                "certified_fraction": cert / (lps * args.steps),
+                "env_steps_per_s": world * args.envs * args.steps / (ms_max / 1e3),
+                "iterations": {"mean": float(np.mean(it)), "p50": float(np.median(it)),
+                               "p99": float(np.percentile(it, 99)), "max": int(np.max(it))},
+                "cold_value": cold, "warm_vs_cold": (value / cold) if cold else None,
+                "cold_mean_iterations": cold_iters if cold else None,
+                "roofline": roofline, "cpu_baseline": cpu, "highs_check": highs_check, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clock_summary}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks):
+    """Same metric through the public ``LPEngine`` API with HOST inputs: every
+    step copies that step's bounds/objective from pinned host memory and reads
+    status, objectives and fluxes back."""
+    import torch
+
+    from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
+    com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start="previous", device=dev)
+    K = max(1, args.e2e_steps)
+    host_lower = []
+    for _ in range(args.warmup + K):
+        com.uptake_bounds()
+        host_lower.append(com.lower.cpu().pin_memory())
+        res = com.solve()
+        com.integrate(res)
+    up_h = com.upper.cpu().pin_memory()
+    c_h = com.cost.cpu().pin_memory()
+    eng = com.engine
+    lo_d, up_d, c_d = eng._bound[0], eng._bound[1], eng._bound[2]
+    out = [eng.allocate_result(), eng.allocate_result()]
+    x_h = torch.empty(eng.total_cols, dtype=torch.float64).pin_memory()
+    st_h = torch.empty(eng.count, dtype=torch.int32).pin_memory()
+    ob_h = torch.empty(eng.count, dtype=torch.float64).pin_memory()
+    mt_h = torch.empty((eng.count, 8), dtype=torch.float64).pin_memory()
+    prev = None
+
+    def one(k, o):
+        lo_d.copy_(host_lower[k], non_blocking=True)
+        up_d.copy_(up_h, non_blocking=True)
+        c_d.copy_(c_h, non_blocking=True)
+        r = eng.solve(warm_x=None if prev is None else prev.x[:eng.total_cols],
+                      warm_y=None if prev is None else prev.y[:eng.total_rows],
+                      warm_omega=None if prev is None else prev.omega, config=cfg, out=o)
+        x_h.copy_(r.x[:eng.total_cols], non_blocking=True)
+        st_h.copy_(r.status, non_blocking=True)
+        ob_h.copy_(r.objective, non_blocking=True)
+        mt_h.copy_(r.metrics, non_blocking=True)
+        return r
+
+    for k in range(args.warmup):
+        prev = one(k, out[k % 2])
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    cert = 0
+    for k in range(args.warmup, args.warmup + K):
+        prev = one(k, out[k % 2])
+        torch.cuda.synchronize()
+        st = st_h.numpy()
+        mt = mt_h.numpy()
+        cert += int(np.sum((st == 0) & (mt[:, 0] <= 1e-5) & (mt[:, 1] <= 1e-7) & (mt[:, 2] <= 1e-7)))
+    wall = time.perf_counter() - t0
+    barrier()
+    com.close()
+    value = sum_over_ranks(cert) / max_over_ranks(wall)
+    h2d = 3 * eng.total_cols * 8
+    d2h = eng.total_cols * 8 + eng.count * (4 + 8 + 64)
+    return {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "steps": K, "api": "LPEngine.solve over the C ABI (fbalp_engine_solve) with pinned host buffers"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_product(args)
+
+
+if __name__ == "__main__":
+    main()

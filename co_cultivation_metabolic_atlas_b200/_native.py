@@ -44,7 +44,8 @@ c_double_p = ctypes.POINTER(ctypes.c_double)
 class Options(ctypes.Structure):
     _fields_ = [("ruiz_iterations", ctypes.c_int32), ("power_iterations", ctypes.c_int32),
                 ("step_safety", ctypes.c_double), ("warps_per_block", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("max_dynamic_smem", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("max_dynamic_smem", ctypes.c_int32),
+                ("stage_matrix", ctypes.c_int32)]
 
 
 class SolveParams(ctypes.Structure):
@@ -53,7 +54,8 @@ class SolveParams(ctypes.Structure):
                 ("tol_primal", ctypes.c_double), ("tol_dual", ctypes.c_double),
                 ("tol_gap", ctypes.c_double), ("fp32_tol_primal", ctypes.c_double),
                 ("fp32_tol_dual", ctypes.c_double), ("fp32_tol_gap", ctypes.c_double),
-                ("reflection", ctypes.c_double), ("restarts", ctypes.c_int32)]
+                ("reflection", ctypes.c_double), ("restarts", ctypes.c_int32),
+                ("fp32_stall_checks", ctypes.c_int32)]
 
 
 class NativeError(RuntimeError):
@@ -91,6 +93,9 @@ def load(path: os.PathLike | None = None):
         "fbalp_prepare_matrix": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int64_p, c_int32_p,
                                                 c_double_p, ctypes.POINTER(Options), c_double_p,
                                                 c_double_p, c_double_p, c_double_p]),
+        "fbalp_engine_phase_times": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_float),
+                                                    ctypes.POINTER(ctypes.c_float)]),
+        "fbalp_engine_phase_iterations": (ctypes.c_int, [vp, vp]),
         "fbalp_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():

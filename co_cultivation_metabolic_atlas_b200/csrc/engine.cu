@@ -92,10 +92,19 @@ struct fbalp_engine {
     bool bound = false;
     // workspace
     Buffer queue, mid_x, mid_y, mid_omega, mid_iters, mid_status, mid_obj, mid_metrics, spill;
+    Buffer layout32_buf, layout64_buf;
+    std::vector<fbalp::Layout> layouts32, layouts64;
+    int last_grid[2] = {0, 0};
+    int64_t last_smem[2] = {0, 0};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase start/stop: fp32, fp64
+    bool ran[2] = {false, false};
     ~fbalp_engine() {
+        for (cudaEvent_t& v : ev)
+            if (v) cudaEventDestroy(v);
         for (void* p : owned) cudaFree(p);
         for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
-                          &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill})
+                          &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill, &layout32_buf,
+                          &layout64_buf})
             b->release();
     }
 };
@@ -110,6 +119,7 @@ void fbalp_default_options(fbalp_options* o) {
     o->warps_per_block = 16;
     o->blocks_per_sm = 0;
     o->max_dynamic_smem = 0;
+    o->stage_matrix = 1;
 }
 
 void fbalp_default_solve_params(fbalp_solve_params* p) {
@@ -126,6 +136,7 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->fp32_tol_gap = 1e-4;
     p->reflection = 1.0;
     p->restarts = 1;
+    p->fp32_stall_checks = 6;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -135,9 +146,10 @@ static bool valid_options(const fbalp_options& o, std::string* err) {
     if (o.power_iterations < 1 || o.power_iterations > 100000) return *err = "power_iterations out of range", false;
     if (!(o.step_safety > 0.0 && o.step_safety < 1.0)) return *err = "step_safety must be in (0,1)", false;
     if (o.warps_per_block < 1 || o.warps_per_block * 32 > fbalp::kMaxThreads)
-        return *err = "warps_per_block must be in [1,16]", false;
+        return *err = "warps_per_block must be in [1,32]", false;
     if (o.blocks_per_sm < 0 || o.blocks_per_sm > 32) return *err = "blocks_per_sm out of range", false;
     if (o.max_dynamic_smem < 0) return *err = "max_dynamic_smem must be non-negative", false;
+    if (o.stage_matrix != 0 && o.stage_matrix != 1) return *err = "stage_matrix must be 0 or 1", false;
     return true;
 }
 
@@ -229,18 +241,23 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             d.a_nslices = sh.A.nslices;
             d.at_nslices = sh.AT.nslices;
             std::vector<float> a32(sh.A.val.begin(), sh.A.val.end()), at32(sh.AT.val.begin(), sh.AT.val.end());
-            d.a_off = dev_upload(sh.A.off, E->owned);
+            d.a_elems = sh.A.off.back();
+            d.at_elems = sh.AT.off.back();
+            std::vector<int4> alist, atlist;
+            for (int32_t sl : sh.a_sched)
+                alist.push_back(make_int4(sl, sh.A.off[sl], sh.A.length[sl], 0));
+            for (int32_t sl : sh.at_sched)
+                atlist.push_back(make_int4(sl, sh.AT.off[sl], sh.AT.length[sl], 0));
+            d.a_list = dev_upload(alist, E->owned);
+            d.at_list = dev_upload(atlist, E->owned);
             d.a_idx = dev_upload(sh.A.idx, E->owned);
             d.a_v32 = dev_upload(a32, E->owned);
             d.a_v64 = dev_upload(sh.A.val, E->owned);
-            d.at_off = dev_upload(sh.AT.off, E->owned);
             d.at_idx = dev_upload(sh.AT.idx, E->owned);
             d.at_v32 = dev_upload(at32, E->owned);
             d.at_v64 = dev_upload(sh.AT.val, E->owned);
             d.a_sched_off = dev_upload(sh.a_sched_off, E->owned);
-            d.a_sched = dev_upload(sh.a_sched, E->owned);
             d.at_sched_off = dev_upload(sh.at_sched_off, E->owned);
-            d.at_sched = dev_upload(sh.at_sched, E->owned);
             d.row_perm = dev_upload(sh.row_perm, E->owned);
             d.col_perm = dev_upload(sh.col_perm, E->owned);
             std::vector<double> drn(sh.m), dcn(sh.n);
@@ -253,6 +270,7 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
         }
         E->dev_species = dev_upload(E->dev_species_host, E->owned);
         E->queue.ensure(16 * sizeof(int32_t));
+        for (cudaEvent_t& v : E->ev) check(cudaEventCreate(&v), "cudaEventCreate");
     } catch (const CudaError& e) {
         return fail(FBALP_ERR_CUDA, e.what());
     } catch (const std::bad_alloc&) {
@@ -346,19 +364,35 @@ namespace {
 
 // Launch one precision phase over the bound batch.
 void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
-    const size_t esz = fp64 ? sizeof(double) : sizeof(float);
+    const int esz = fp64 ? static_cast<int>(sizeof(double)) : static_cast<int>(sizeof(float));
     const int threads = e->opt.warps_per_block * 32;
-    int64_t need = 0;
+    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
+                      ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
+    if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
     std::vector<char> used(e->species.size(), 0);
     for (int32_t s : e->h_species) used[s] = 1;
-    for (size_t s = 0; s < e->species.size(); ++s)
-        if (used[s]) need = std::max(need, fbalp::total_elems(e->species[s].n, e->species[s].m));
-    const size_t static_smem = sizeof(double) * (fbalp::kMaxWarps * fbalp::kRed + fbalp::kRed) + 64;
-    const size_t cap = static_cast<size_t>(e->smem_optin) > static_smem + 1024 ? e->smem_optin - static_smem - 1024 : 0;
-    size_t dyn = std::min<size_t>(need * esz, cap);
-    if (e->opt.max_dynamic_smem > 0) dyn = std::min<size_t>(dyn, static_cast<size_t>(e->opt.max_dynamic_smem));
-    dyn = dyn / 16 * 16;
-    const void* k = fbalp::kernel_symbol(fp64);
+    std::vector<fbalp::Layout>& layouts = fp64 ? e->layouts64 : e->layouts32;
+    layouts.assign(e->species.size(), fbalp::Layout{});
+    int64_t dyn = 0, slab = 0;
+    for (size_t s = 0; s < e->species.size(); ++s) {
+        if (!used[s]) continue;
+        const SpeciesHost& sh = e->species[s];
+        fbalp::LayoutPlan P = fbalp::plan_layout(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices,
+                                                 sh.AT.nslices, sh.A.off.back(), sh.AT.off.back(),
+                                                 esz, cap, e->opt.stage_matrix != 0);
+        if (P.smem_bytes > cap) throw CudaError("species schedule does not fit into shared memory");
+        if (!fbalp::layout_aligned(P.layout)) throw CudaError("internal error: misaligned shared-memory layout");
+        layouts[s] = P.layout;
+        dyn = std::max(dyn, P.smem_bytes);
+        slab = std::max(slab, P.slab_bytes);
+    }
+    dyn = fbalp::align_up(std::max<int64_t>(dyn, 16), 16);
+    Buffer& dl = fp64 ? e->layout64_buf : e->layout32_buf;
+    dl.ensure(layouts.size() * sizeof(fbalp::Layout));
+    check(cudaMemcpyAsync(dl.ptr, layouts.data(), layouts.size() * sizeof(fbalp::Layout),
+                          cudaMemcpyHostToDevice, e->stream), "copy layouts");
+    const void* k = fbalp::kernel_symbol(fp64, threads);
     check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
           "cudaFuncSetAttribute");
     int per_sm = 0;
@@ -366,21 +400,24 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     if (e->opt.blocks_per_sm > 0) per_sm = std::min(per_sm, e->opt.blocks_per_sm);
     if (per_sm < 1) throw CudaError("kernel does not fit on an SM with this configuration");
     const int grid = static_cast<int>(std::min<int64_t>(e->count, static_cast<int64_t>(per_sm) * e->sm_count));
-    p.smem_elems = static_cast<int64_t>(dyn / esz);
-    int64_t spill = 0;
-    for (size_t s = 0; s < e->species.size(); ++s)
-        if (used[s]) spill = std::max(spill, fbalp::spill_elems(e->species[s].n, e->species[s].m, p.smem_elems));
-    if (spill > 0) {
-        e->spill.ensure(static_cast<size_t>(spill) * grid * esz);
-        p.spill = e->spill.ptr;
-        p.spill_stride = spill;
+    p.layouts = static_cast<const fbalp::Layout*>(dl.ptr);
+    if (slab > 0) {
+        e->spill.ensure(static_cast<size_t>(slab) * grid);
+        p.spill = static_cast<unsigned char*>(e->spill.ptr);
+        p.spill_stride = slab;
     } else {
         p.spill = nullptr;
         p.spill_stride = 0;
     }
-    p.queue = static_cast<int32_t*>(e->queue.ptr);
-    check(cudaMemsetAsync(e->queue.ptr, 0, sizeof(int32_t), e->stream), "memset queue");
+    p.queue = static_cast<int32_t*>(e->queue.ptr) + (fp64 ? 1 : 0);
+    check(cudaMemsetAsync(p.queue, 0, sizeof(int32_t), e->stream), "memset queue");
+    const int ph = fp64 ? 1 : 0;
+    check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
     check(fbalp::launch_pdhg(fp64, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
+    check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
+    e->ran[ph] = true;
+    e->last_grid[fp64 ? 1 : 0] = grid;
+    e->last_smem[fp64 ? 1 : 0] = dyn;
 }
 
 bool valid_params(const fbalp_solve_params& q, std::string* err) {
@@ -391,6 +428,7 @@ bool valid_params(const fbalp_solve_params& q, std::string* err) {
         if (!(t >= 0.0) || !std::isfinite(t)) return *err = "tolerances must be finite and non-negative", false;
     if (!(q.reflection >= 0.0 && q.reflection <= 1.0)) return *err = "reflection must be in [0,1]", false;
     if (q.restarts != 0 && q.restarts != 1) return *err = "restarts must be 0 or 1", false;
+    if (q.fp32_stall_checks < 0) return *err = "fp32_stall_checks must be non-negative", false;
     return true;
 }
 
@@ -411,6 +449,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
     std::string err;
     if (!valid_params(q, &err)) return fail(FBALP_ERR_INVALID, err);
     try {
+        e->ran[0] = e->ran[1] = false;
         fbalp::KernelParams p{};
         p.species = e->dev_species;
         p.count = static_cast<int32_t>(e->count);
@@ -444,6 +483,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p.tol_g = fp64 ? q.tol_gap : q.fp32_tol_gap;
             p.final_status = fp64 ? fbalp::kStatusOptimal : fbalp::kStatusHandoff;
             p.clip_output = 1;
+            p.stall_checks = fp64 ? 0 : q.fp32_stall_checks;
             run_phase(e, fp64, p);
         } else {
             e->mid_x.ensure(e->total_cols * sizeof(double));
@@ -471,6 +511,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p32.tol_g = q.fp32_tol_gap;
             p32.final_status = fbalp::kStatusHandoff;
             p32.clip_output = 0;
+            p32.stall_checks = q.fp32_stall_checks;
             run_phase(e, false, p32);
             fbalp::KernelParams p64 = p;
             p64.warm_x = static_cast<const double*>(e->mid_x.ptr);
@@ -490,6 +531,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p64.tol_g = q.tol_gap;
             p64.final_status = fbalp::kStatusOptimal;
             p64.clip_output = 1;
+            p64.stall_checks = 0;
             run_phase(e, true, p64);
         }
     } catch (const CudaError& ex) {
@@ -497,5 +539,29 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
     } catch (const std::exception& ex) {
         return fail(FBALP_ERR_ALLOC, ex.what());
     }
+    return FBALP_OK;
+}
+
+extern "C" int fbalp_engine_phase_times(fbalp_engine* e, float* ms_fp32, float* ms_fp64) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    float* outs[2] = {ms_fp32, ms_fp64};
+    for (int ph = 0; ph < 2; ++ph) {
+        if (!outs[ph]) continue;
+        *outs[ph] = 0.0f;
+        if (!e->ran[ph]) continue;
+        cudaError_t err = cudaEventSynchronize(e->ev[2 * ph + 1]);
+        if (err == cudaSuccess) err = cudaEventElapsedTime(outs[ph], e->ev[2 * ph], e->ev[2 * ph + 1]);
+        if (err != cudaSuccess) return fail(FBALP_ERR_CUDA, cudaGetErrorString(err));
+    }
+    return FBALP_OK;
+}
+
+extern "C" int fbalp_engine_phase_iterations(fbalp_engine* e, int32_t* out_fp32_iterations) {
+    if (!e || !out_fp32_iterations) return fail(FBALP_ERR_INVALID, "engine and output are required");
+    if (!e->bound) return fail(FBALP_ERR_STATE, "no instances are bound");
+    if (!e->ran[0] || !e->ran[1]) return fail(FBALP_ERR_STATE, "the last solve was not a mixed-precision solve");
+    cudaError_t err = cudaMemcpyAsync(out_fp32_iterations, e->mid_iters.ptr, e->count * sizeof(int32_t),
+                                      cudaMemcpyDeviceToDevice, e->stream);
+    if (err != cudaSuccess) return fail(FBALP_ERR_CUDA, cudaGetErrorString(err));
     return FBALP_OK;
 }

@@ -10,8 +10,7 @@ namespace fbalp {
 
 constexpr int kMetrics = 8;
 constexpr int kRedSums = 10;
-constexpr int kArrayCount = 11;
-constexpr int kMaxThreads = 512;
+constexpr int kMaxThreads = 1024;
 
 constexpr int kStatusOptimal = 0;
 constexpr int kStatusIterationLimit = 1;
@@ -26,36 +25,93 @@ constexpr double kBetaSufficient = 0.2;
 constexpr double kBetaNecessary = 0.8;
 constexpr double kBetaArtificial = 0.36;
 constexpr double kOmegaSmoothing = 0.5;
+// the FP32 phase only hands off on a stall once its error is below this
+constexpr double kStallFloor = 1.0;
 
-// Per-instance arrays in placement priority order:
-// xbar, y, x, xa, ya, c, l, u, b, xs, ys  (gather targets carry a zero slot).
-__host__ __device__ inline void array_sizes(int n, int m, int64_t* s) {
-    const int64_t cols[kArrayCount] = {n + 1, 0, n, n, 0, n, n, n, 0, n + 1, 0};
-    const int64_t rows[kArrayCount] = {0, m + 1, 0, 0, m, 0, 0, 0, m, 0, m + 1};
-    for (int a = 0; a < kArrayCount; ++a) s[a] = ((cols[a] + rows[a]) + 3) & ~int64_t(3);
+// Element counts of the per-instance arrays (gather targets carry a zero
+// slot at index n / m), in shared-memory priority order.
+inline void array_elems(int n, int m, int64_t* s) {
+    const int64_t v[kArrayCount] = {n + 1, m + 1, n, n, m, n, n, n, m, n + 1, m + 1};
+    for (int a = 0; a < kArrayCount; ++a) s[a] = v[a];
 }
 
-// Elements that do not fit into `smem_elems` (first-fit in priority order).
-__host__ __device__ inline int64_t spill_elems(int n, int m, int64_t smem_elems) {
-    int64_t s[kArrayCount];
-    array_sizes(n, m, s);
-    int64_t so = 0, go = 0;
-    for (int a = 0; a < kArrayCount; ++a) {
-        if (so + s[a] <= smem_elems) so += s[a];
-        else go += s[a];
+inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+// Host-side layout planner: decide, for one species and one precision, what
+// lives in the CTA's shared memory (schedule lists always; the two gather
+// targets; then the matrix slices with 16-bit indices; then the remaining
+// arrays in priority order) and what spills to the CTA's global slab.
+struct LayoutPlan {
+    Layout layout;
+    int64_t smem_bytes;  // dynamic shared memory used
+    int64_t slab_bytes;  // per-CTA global slab bytes
+};
+
+inline LayoutPlan plan_layout(int n, int m, int warps, int a_nslices, int at_nslices,
+                              int64_t a_elems, int64_t at_elems, int esz, int64_t smem_cap,
+                              bool allow_matrix) {
+    LayoutPlan P{};
+    Layout& L = P.layout;
+    int64_t off = 0;
+    L.sched_a_off = off;
+    off += 4 * (warps + 1);
+    L.sched_at_off = off;
+    off += 4 * (warps + 1);
+    off = align_up(off, 16);  // int4 slice lists need 16-byte alignment
+    L.list_a = off;
+    off += static_cast<int64_t>(sizeof(int4)) * a_nslices;
+    L.list_at = off;
+    off += static_cast<int64_t>(sizeof(int4)) * at_nslices;
+    off = align_up(off, 16);
+    int64_t slab = 0;
+    int64_t e[kArrayCount];
+    array_elems(n, m, e);
+    L.smem_mask = 0;
+    auto place = [&](int a) {
+        const int64_t bytes = align_up(e[a] * esz, 16);
+        if (off + bytes <= smem_cap) {
+            L.arr[a] = off;
+            L.smem_mask |= 1 << a;
+            off += bytes;
+        } else {
+            L.arr[a] = slab;
+            slab += bytes;
+        }
+    };
+    place(0);  // xbar
+    place(1);  // y
+    const int64_t mat = align_up(2 * a_elems, 16) + align_up(2 * at_elems, 16) +
+                        align_up(esz * a_elems, 16) + align_up(esz * at_elems, 16);
+    L.mat_smem = 0;
+    if (allow_matrix && n + 1 < 65536 && m + 1 < 65536 && off + mat <= smem_cap) {
+        L.mat_smem = 1;
+        L.mat_a_idx = off;
+        off += align_up(2 * a_elems, 16);
+        L.mat_at_idx = off;
+        off += align_up(2 * at_elems, 16);
+        L.mat_a_val = off;
+        off += align_up(esz * a_elems, 16);
+        L.mat_at_val = off;
+        off += align_up(esz * at_elems, 16);
     }
-    return go;
+    for (int a = 2; a < kArrayCount; ++a) place(a);
+    P.smem_bytes = off;
+    P.slab_bytes = slab;
+    return P;
 }
 
-__host__ __device__ inline int64_t total_elems(int n, int m) {
-    int64_t s[kArrayCount];
-    array_sizes(n, m, s);
-    int64_t t = 0;
-    for (int a = 0; a < kArrayCount; ++a) t += s[a];
-    return t;
+// Every region must start on a 16-byte boundary (int4 lists, FP64 arrays).
+inline bool layout_aligned(const Layout& L) {
+    const int64_t offs[] = {L.sched_a_off, L.sched_at_off, L.list_a, L.list_at, L.mat_a_idx,
+                            L.mat_at_idx, L.mat_a_val, L.mat_at_val};
+    for (int64_t o : offs)
+        if (o % 16 != 0 && o != L.sched_at_off) return false;
+    for (int a = 0; a < kArrayCount; ++a)
+        if (L.arr[a] % 16 != 0) return false;
+    return L.sched_a_off % 4 == 0 && L.sched_at_off % 4 == 0;
 }
 
-const void* kernel_symbol(bool fp64);
+const void* kernel_symbol(bool fp64, int threads);
 cudaError_t launch_pdhg(bool fp64, int grid, int threads, size_t smem, cudaStream_t stream,
                         const KernelParams& p);
 

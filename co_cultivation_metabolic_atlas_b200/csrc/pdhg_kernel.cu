@@ -22,38 +22,65 @@ template <typename T> __device__ __forceinline__ T clampT(T v, T l, T u) {
     return v < l ? l : (v > u ? u : v);
 }
 
-// One SELL-32 slice row product: lane `lane` of the warp owns row
-// (slice*32 + lane); element k of that row sits at base + 32*k + lane, so
-// every step of the loop is one coalesced load of 32 indices and 32 values.
-template <typename T, typename V>
-__device__ __forceinline__ T slice_dot(const int32_t* __restrict__ idx, const V* __restrict__ val,
+// One SELL-32 slice row product: lane `lane` owns row (slice*32 + lane) and
+// element k of that row sits at base + 32*k + lane, so every step is one
+// coalesced load of 32 indices and 32 values.  Loads are issued in batches
+// of U before any is used (one memory round trip per batch).
+template <typename T, typename V, typename I, bool GLOBAL>
+__device__ __forceinline__ T slice_dot(const I* __restrict__ idx, const V* __restrict__ val,
                                        int base, int len, int lane, const T* g) {
-    const int32_t* ip = idx + base + lane;
+    constexpr int U = GLOBAL ? (sizeof(V) == 4 ? 8 : 4) : 4;
+    const I* ip = idx + base + lane;
     const V* vp = val + base + lane;
-    T acc0 = T(0), acc1 = T(0);
-    int k = 0;
-    for (; k + 1 < len; k += 2) {
-        const int i0 = __ldg(ip + (k << 5));
-        const int i1 = __ldg(ip + ((k + 1) << 5));
-        const V v0 = __ldg(vp + (k << 5));
-        const V v1 = __ldg(vp + ((k + 1) << 5));
-        acc0 = fma(static_cast<T>(v0), g[i0], acc0);
-        acc1 = fma(static_cast<T>(v1), g[i1], acc1);
+    T acc = T(0);
+    for (int k0 = 0; k0 < len; k0 += U) {
+        int ii[U];
+        V vv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            if (k < len) {
+                if (GLOBAL) {
+                    ii[u] = __ldg(reinterpret_cast<const int32_t*>(ip) + (k << 5));
+                    vv[u] = __ldg(vp + (k << 5));
+                } else {
+                    ii[u] = ip[k << 5];
+                    vv[u] = vp[k << 5];
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u < len) acc = fma(static_cast<T>(vv[u]), g[ii[u]], acc);
     }
-    if (k < len) acc0 = fma(static_cast<T>(__ldg(vp + (k << 5))), g[__ldg(ip + (k << 5))], acc0);
-    return acc0 + acc1;
+    return acc;
 }
 
-// FP64 product for the convergence test, whatever the iterate precision.
+// FP64 product for the convergence test, whatever the iterate precision
+// (always the global FP64 slices).
 template <typename T>
 __device__ __forceinline__ double slice_dot64(const int32_t* __restrict__ idx,
                                               const double* __restrict__ val, int base, int len,
                                               int lane, const T* g) {
+    constexpr int U = 4;
     const int32_t* ip = idx + base + lane;
     const double* vp = val + base + lane;
     double acc = 0.0;
-    for (int k = 0; k < len; ++k)
-        acc = fma(__ldg(vp + (k << 5)), static_cast<double>(g[__ldg(ip + (k << 5))]), acc);
+    for (int k0 = 0; k0 < len; k0 += U) {
+        int ii[U];
+        double vv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            if (k < len) {
+                ii[u] = __ldg(ip + (k << 5));
+                vv[u] = __ldg(vp + (k << 5));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u < len) acc = fma(vv[u], static_cast<double>(g[ii[u]]), acc);
+    }
     return acc;
 }
 
@@ -61,27 +88,8 @@ template <typename T> struct Arrays {
     T *xbar, *y, *x, *xa, *ya, *cs, *ls, *us, *bs, *xs, *ys;
 };
 
-template <typename T>
-__device__ void place_arrays(Arrays<T>& A, T* smem, int64_t smem_elems, T* slab, int n, int m) {
-    int64_t sizes[kArrayCount];
-    array_sizes(n, m, sizes);
-    T** ptrs[kArrayCount] = {&A.xbar, &A.y, &A.x, &A.xa, &A.ya, &A.cs, &A.ls, &A.us, &A.bs, &A.xs, &A.ys};
-    int64_t so = 0, go = 0;
-#pragma unroll
-    for (int a = 0; a < kArrayCount; ++a) {
-        const int64_t sz = sizes[a];
-        if (so + sz <= smem_elems) {
-            *ptrs[a] = smem + so;
-            so += sz;
-        } else {
-            *ptrs[a] = slab + go;
-            go += sz;
-        }
-    }
-}
-
 // Sums for q < kRedSums, maxima above.  Deterministic order.
-__device__ void block_reduce(double* v, double (*s_red)[kRed], double* s_tot) {
+__device__ __noinline__ void block_reduce(double* v, double (*s_red)[kRed], double* s_tot) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int q = 0; q < kRed; ++q) {
@@ -107,60 +115,62 @@ __device__ void block_reduce(double* v, double (*s_red)[kRed], double* s_tot) {
     __syncthreads();
 }
 
-// FP64 KKT quantities at the candidate (xs, ys); partial sums / maxima of
-// this thread are added to v.  Index map of v (see also oracle/pdhg.py
-// kkt_metrics):
+// FP64 KKT quantities at the candidate (xs, ys), in ORIGINAL units and with
+// the caller's exact FP64 bounds, objective and right-hand side (the scaled
+// copies in shared memory may be FP32).  Partial sums / maxima of this thread
+// are added to v.  Index map of v (oracle/pdhg.py kkt_metrics is the twin):
 //  0 c.x   1 b.y   2 sum bound-dual terms   3 bound complementarity
 //  4 row complementarity   5 |xn-x|^2  6 |yn-y|^2  7 |xn-xa|^2  8 |yn-ya|^2
 //  10 max primal row residual  11 max dual violation  12 max bound violation
 //  13 |x|_inf  14 |c|_inf  15 NaN flag
 template <typename T>
-__device__ void kkt_partials(const DevSpecies* sp, const Arrays<T>& A, int warp, int lane,
-                             double* v) {
+__device__ __noinline__ void kkt_partials(const DevSpecies* sp, const int4* alist, const int4* atlist,
+                                          int a0, int a1, int t0, int t1, const T* xs, const T* ys,
+                                          const double* lower, const double* upper,
+                                          const double* cost, const double* rhs, int lane,
+                                          double* v) {
     const int n = sp->n, m = sp->m, neq = sp->neq;
-    for (int t = sp->at_sched_off[warp]; t < sp->at_sched_off[warp + 1]; ++t) {
-        const int s = sp->at_sched[t];
-        const int base = sp->at_off[s];
-        const int len = (sp->at_off[s + 1] - base) >> 5;
-        const double g = slice_dot64<T>(sp->at_idx, sp->at_v64, base, len, lane, A.ys);
-        const int j = (s << 5) + lane;
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = atlist[t];
+        const double g = slice_dot64<T>(sp->at_idx, sp->at_v64, sl.y, sl.z, lane, ys);
+        const int j = (sl.x << 5) + lane;
         if (j < n) {
+            const int jo = sp->col_perm[j];
             const double dcj = sp->dc[j];
-            const double c = A.cs[j], l = A.ls[j], u = A.us[j], xv = A.xs[j];
-            const double r = c - g;
+            const double c = cost[jo], l = lower[jo], u = upper[jo];
+            const double xv = static_cast<double>(xs[j]) * dcj;
+            const double r = c - g / dcj;  // c - A^T y in original units
             v[0] += c * xv;
             if (r > 0.0) {
                 if (isfinite(l)) v[2] += r * l;
-                else v[11] = fmax(v[11], r / dcj);
+                else v[11] = fmax(v[11], r);
             } else if (r < 0.0) {
                 if (isfinite(u)) v[2] += r * u;
-                else v[11] = fmax(v[11], -r / dcj);
+                else v[11] = fmax(v[11], -r);
             }
             const double tg = (r >= 0.0) ? l : u;
             if (isfinite(tg)) v[3] += fabs(r * (xv - tg));
-            v[12] = fmax(v[12], fmax((l - xv) * dcj, (xv - u) * dcj));
-            v[13] = fmax(v[13], fabs(xv * dcj));
-            v[14] = fmax(v[14], fabs(c / dcj));
+            v[12] = fmax(v[12], fmax(l - xv, xv - u));
+            v[13] = fmax(v[13], fabs(xv));
+            v[14] = fmax(v[14], fabs(c));
             if (isnan(g) || isnan(xv)) v[15] = 1.0;
         }
     }
-    for (int t = sp->a_sched_off[warp]; t < sp->a_sched_off[warp + 1]; ++t) {
-        const int s = sp->a_sched[t];
-        const int base = sp->a_off[s];
-        const int len = (sp->a_off[s + 1] - base) >> 5;
-        const double h = slice_dot64<T>(sp->a_idx, sp->a_v64, base, len, lane, A.xs);
-        const int i = (s << 5) + lane;
+    for (int t = a0; t < a1; ++t) {
+        const int4 sl = alist[t];
+        const double h = slice_dot64<T>(sp->a_idx, sp->a_v64, sl.y, sl.z, lane, xs);
+        const int i = (sl.x << 5) + lane;
         if (i < m) {
             const double dri = sp->dr[i];
-            const double b = A.bs[i], yv = A.ys[i];
-            const double rt = h - b;
-            const double ro = rt / dri;
+            const double b = rhs ? rhs[sp->row_perm[i]] : 0.0;
+            const double yv = static_cast<double>(ys[i]) * dri;
+            const double ro = h / dri - b;  // A x - b in original units
             if (i < neq) {
                 v[10] = fmax(v[10], fabs(ro));
             } else {
                 v[10] = fmax(v[10], ro);
-                v[4] += fabs(yv * rt);
-                v[11] = fmax(v[11], yv * dri);
+                v[4] += fabs(yv * ro);
+                v[11] = fmax(v[11], yv);
             }
             v[1] += b * yv;
             if (isnan(h) || isnan(yv)) v[15] = 1.0;
@@ -192,17 +202,51 @@ __device__ Metrics evaluate(const double* s_tot, double omega, double tol_p, dou
     return M;
 }
 
+// Stage one species' warp schedule (and, when the layout says so, its matrix
+// slices with 16-bit indices) into shared memory.
 template <typename T>
-__global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParams p) {
+__device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned char* sm, int warps) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int32_t* soa = reinterpret_cast<int32_t*>(sm + L.sched_a_off);
+    int32_t* sot = reinterpret_cast<int32_t*>(sm + L.sched_at_off);
+    for (int w = tid; w <= warps; w += nt) {
+        soa[w] = sp->a_sched_off[w];
+        sot[w] = sp->at_sched_off[w];
+    }
+    int4* la = reinterpret_cast<int4*>(sm + L.list_a);
+    int4* lt = reinterpret_cast<int4*>(sm + L.list_at);
+    for (int t = tid; t < sp->a_nslices; t += nt) la[t] = sp->a_list[t];
+    for (int t = tid; t < sp->at_nslices; t += nt) lt[t] = sp->at_list[t];
+    if (L.mat_smem) {
+        uint16_t* ai = reinterpret_cast<uint16_t*>(sm + L.mat_a_idx);
+        uint16_t* ti = reinterpret_cast<uint16_t*>(sm + L.mat_at_idx);
+        T* av = reinterpret_cast<T*>(sm + L.mat_a_val);
+        T* tv = reinterpret_cast<T*>(sm + L.mat_at_val);
+        const T* ga = Vals<T>::a(sp);
+        const T* gt = Vals<T>::at(sp);
+        for (int64_t e = tid; e < sp->a_elems; e += nt) {
+            ai[e] = static_cast<uint16_t>(sp->a_idx[e]);
+            av[e] = ga[e];
+        }
+        for (int64_t e = tid; e < sp->at_elems; e += nt) {
+            ti[e] = static_cast<uint16_t>(sp->at_idx[e]);
+            tv[e] = gt[e];
+        }
+    }
+}
+
+template <typename T, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    __shared__ double s_red[kMaxWarps][kRed];
+    __shared__ double s_red[MAXT / 32][kRed];
     __shared__ double s_tot[kRed];
     __shared__ int s_inst;
-    T* smem = reinterpret_cast<T*>(dyn_smem);
+    __shared__ int s_loaded;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthreads = blockDim.x;
-    T* slab = p.spill ? reinterpret_cast<T*>(p.spill) + static_cast<int64_t>(blockIdx.x) * p.spill_stride
-                      : nullptr;
+    const int warps = nthreads >> 5;
+    unsigned char* slab = p.spill ? p.spill + static_cast<int64_t>(blockIdx.x) * p.spill_stride : nullptr;
     const T rho = static_cast<T>(p.rho);
+    if (tid == 0) s_loaded = -1;
 
     for (;;) {
         if (tid == 0) s_inst = atomicAdd(p.queue, 1);
@@ -210,11 +254,37 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParam
         const int q = s_inst;
         if (q >= p.count) break;
         const int inst = p.order[q];
-        const DevSpecies* __restrict__ sp = p.species + p.inst_species[inst];
+        const int species = p.inst_species[inst];
+        const DevSpecies* __restrict__ sp = p.species + species;
+        const Layout& L = p.layouts[species];
         const int n = sp->n, m = sp->m, neq = sp->neq;
         const int64_t coff = p.col_off[inst], roff = p.row_off[inst];
+        if (s_loaded != species) {  // block-uniform
+            stage_species<T>(sp, L, dyn_smem, warps);
+            __syncthreads();
+            if (tid == 0) s_loaded = species;
+        }
         Arrays<T> A;
-        place_arrays<T>(A, smem, p.smem_elems, slab, n, m);
+        {
+            T** ptrs[kArrayCount] = {&A.xbar, &A.y, &A.x, &A.xa, &A.ya, &A.cs, &A.ls, &A.us, &A.bs, &A.xs, &A.ys};
+            const int mask = L.smem_mask;
+#pragma unroll
+            for (int a = 0; a < kArrayCount; ++a)
+                *ptrs[a] = reinterpret_cast<T*>(((mask >> a) & 1) ? dyn_smem + L.arr[a] : slab + L.arr[a]);
+        }
+        const int4* alist = reinterpret_cast<const int4*>(dyn_smem + L.list_a);
+        const int4* atlist = reinterpret_cast<const int4*>(dyn_smem + L.list_at);
+        const int32_t* soa = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_a_off);
+        const int32_t* sot = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_at_off);
+        const int aw0 = soa[warp], aw1 = soa[warp + 1];
+        const int tw0 = sot[warp], tw1 = sot[warp + 1];
+        const bool mat_smem = L.mat_smem != 0;
+        const uint16_t* s_aidx = reinterpret_cast<const uint16_t*>(dyn_smem + L.mat_a_idx);
+        const uint16_t* s_tidx = reinterpret_cast<const uint16_t*>(dyn_smem + L.mat_at_idx);
+        const T* s_aval = reinterpret_cast<const T*>(dyn_smem + L.mat_a_val);
+        const T* s_tval = reinterpret_cast<const T*>(dyn_smem + L.mat_at_val);
+        const T* __restrict__ g_aval = Vals<T>::a(sp);
+        const T* __restrict__ g_tval = Vals<T>::at(sp);
 
         // ---- load the instance (scaled, in the species' permuted order) ----
         int bad = 0;
@@ -274,27 +344,28 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParam
             continue;
         }
 
-        // ---- iteration-0 test of the (projected) starting point ----
         const double eta = sp->eta;
+        const double* lo_i = p.lower + coff;
+        const double* up_i = p.upper + coff;
+        const double* c_i = p.cost + coff;
+        const double* b_i = p.rhs ? p.rhs + roff : nullptr;
         int status = -1;
         Metrics M;
+        // ---- iteration-0 test of the (projected) starting point ----
         {
             double v[kRed];
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-            kkt_partials<T>(sp, A, warp, lane, v);
+            kkt_partials<T>(sp, alist, atlist, aw0, aw1, tw0, tw1, A.xs, A.ys, lo_i, up_i, c_i, b_i,
+                            lane, v);
             block_reduce(v, s_red, s_tot);
             M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
             if (M.conv) status = p.final_status;
             else if (p.max_iters <= 0) status = M.nan ? kStatusNumerical : kStatusIterationLimit;
         }
 
-        int k = 0, it = 0;
-        double r_restart = INFINITY, r_prev = INFINITY;
-        const int aw0 = sp->a_sched_off[warp], aw1 = sp->a_sched_off[warp + 1];
-        const int tw0 = sp->at_sched_off[warp], tw1 = sp->at_sched_off[warp + 1];
-        const T* __restrict__ atv = Vals<T>::at(sp);
-        const T* __restrict__ av = Vals<T>::a(sp);
+        int k = 0, it = 0, stall = 0;
+        double r_restart = INFINITY, r_prev = INFINITY, best_err = INFINITY;
         while (status < 0) {
             ++it;
             const bool check = (it % p.check_every == 0) || (it >= p.max_iters);
@@ -304,11 +375,10 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParam
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
             // primal pass: g = A^T y, projected step, extrapolation, Halpern
             for (int t = tw0; t < tw1; ++t) {
-                const int s = sp->at_sched[t];
-                const int base = sp->at_off[s];
-                const int len = (sp->at_off[s + 1] - base) >> 5;
-                const T g = slice_dot<T>(sp->at_idx, atv, base, len, lane, A.y);
-                const int j = (s << 5) + lane;
+                const int4 sl = atlist[t];
+                const T g = mat_smem ? slice_dot<T, T, uint16_t, false>(s_tidx, s_tval, sl.y, sl.z, lane, A.y)
+                                     : slice_dot<T, T, int32_t, true>(sp->at_idx, g_tval, sl.y, sl.z, lane, A.y);
+                const int j = (sl.x << 5) + lane;
                 if (j < n) {
                     const T xo = A.x[j];
                     const T xn = clampT(xo - tau * (A.cs[j] - g), A.ls[j], A.us[j]);
@@ -329,11 +399,10 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParam
             __syncthreads();
             // dual pass: h = A xbar, projected dual step, Halpern
             for (int t = aw0; t < aw1; ++t) {
-                const int s = sp->a_sched[t];
-                const int base = sp->a_off[s];
-                const int len = (sp->a_off[s + 1] - base) >> 5;
-                const T h = slice_dot<T>(sp->a_idx, av, base, len, lane, A.xbar);
-                const int i = (s << 5) + lane;
+                const int4 sl = alist[t];
+                const T h = mat_smem ? slice_dot<T, T, uint16_t, false>(s_aidx, s_aval, sl.y, sl.z, lane, A.xbar)
+                                     : slice_dot<T, T, int32_t, true>(sp->a_idx, g_aval, sl.y, sl.z, lane, A.xbar);
+                const int i = (sl.x << 5) + lane;
                 if (i < m) {
                     const T yo = A.y[i];
                     T yn = yo + sigma * (A.bs[i] - h);
@@ -361,7 +430,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParam
             v[6] = pdy2;
             v[7] = pdxa2;
             v[8] = pdya2;
-            kkt_partials<T>(sp, A, warp, lane, v);
+            kkt_partials<T>(sp, alist, atlist, aw0, aw1, tw0, tw1, A.xs, A.ys, lo_i, up_i, c_i, b_i,
+                            lane, v);
             block_reduce(v, s_red, s_tot);
             M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
             if (M.nan || !isfinite(M.r)) {
@@ -375,6 +445,22 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParam
             if (it >= p.max_iters) {
                 status = kStatusIterationLimit;
                 break;
+            }
+            // precision floor: the FP32 phase hands off once its KKT error has
+            // stopped halving for `stall_checks` consecutive tests.
+            {
+                const double e = fmax(fmax(M.primal / (1.0 + M.xinf), M.dual / (1.0 + M.cinf)),
+                                      fmax(M.rgap, M.kgap));
+                if (e < 0.5 * best_err) {
+                    best_err = e;
+                    stall = 0;
+                } else {
+                    ++stall;
+                }
+                if (p.stall_checks > 0 && stall >= p.stall_checks && best_err <= kStallFloor) {
+                    status = p.final_status;
+                    break;
+                }
             }
             if (p.restarts && (M.r <= kBetaSufficient * r_restart ||
                                (M.r <= kBetaNecessary * r_restart && M.r > r_prev) ||
@@ -431,18 +517,30 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 2) pdhg_persistent(KernelParam
     }
 }
 
-template __global__ void pdhg_persistent<float>(KernelParams);
-template __global__ void pdhg_persistent<double>(KernelParams);
+template __global__ void pdhg_persistent<float, 512>(KernelParams);
+template __global__ void pdhg_persistent<double, 512>(KernelParams);
+template __global__ void pdhg_persistent<float, 1024>(KernelParams);
+template __global__ void pdhg_persistent<double, 1024>(KernelParams);
 
-const void* kernel_symbol(bool fp64) {
-    return fp64 ? reinterpret_cast<const void*>(&pdhg_persistent<double>)
-                : reinterpret_cast<const void*>(&pdhg_persistent<float>);
+// Blocks of up to 512 threads use the variant with a 128-register budget;
+// larger blocks the 64-register one.
+const void* kernel_symbol(bool fp64, int threads) {
+    if (threads <= 512)
+        return fp64 ? reinterpret_cast<const void*>(&pdhg_persistent<double, 512>)
+                    : reinterpret_cast<const void*>(&pdhg_persistent<float, 512>);
+    return fp64 ? reinterpret_cast<const void*>(&pdhg_persistent<double, 1024>)
+                : reinterpret_cast<const void*>(&pdhg_persistent<float, 1024>);
 }
 
 cudaError_t launch_pdhg(bool fp64, int grid, int threads, size_t smem, cudaStream_t stream,
                         const KernelParams& p) {
-    if (fp64) pdhg_persistent<double><<<grid, threads, smem, stream>>>(p);
-    else pdhg_persistent<float><<<grid, threads, smem, stream>>>(p);
+    if (threads <= 512) {
+        if (fp64) pdhg_persistent<double, 512><<<grid, threads, smem, stream>>>(p);
+        else pdhg_persistent<float, 512><<<grid, threads, smem, stream>>>(p);
+    } else {
+        if (fp64) pdhg_persistent<double, 1024><<<grid, threads, smem, stream>>>(p);
+        else pdhg_persistent<float, 1024><<<grid, threads, smem, stream>>>(p);
+    }
     return cudaGetLastError();
 }
 

@@ -1,18 +1,18 @@
 // Persistent, instance-resident restarted Halpern PDHG for batches of LPs
 // that share one matrix per species (sm_100a).
 //
-// One CTA owns one LP instance at a time: its iterates, anchors and scaled
-// bounds live in shared memory (spilling to a per-CTA global slab only for
-// species too large for the CTA's shared memory), the species matrix and its
-// transpose are streamed from L2 in SELL-32 slices, and every convergence
-// test, restart decision and primal-weight update happens inside the kernel.
-// When an instance finishes (certified, budget exhausted, or invalid) the CTA
-// writes its results and pulls the next instance from an atomic work queue,
-// so instances of different species and different iteration counts share one
-// launch without host round trips.
+// One CTA owns one LP instance at a time.  Its iterates, anchors and scaled
+// bounds live in shared memory; so do the species' SELL-32 matrix slices
+// (16-bit indices) whenever they fit beside them, otherwise the slices are
+// streamed from L2.  Arrays that do not fit spill to a per-CTA global slab.
+// Every convergence test, restart decision and primal-weight update happens
+// inside the kernel.  When an instance finishes (certified, budget exhausted,
+// or invalid) the CTA writes its results and pulls the next instance from an
+// atomic work queue, so instances of different species and different
+// iteration counts share one launch without host round trips.  Consecutive
+// instances of the same species reuse the staged matrix.
 //
-// Arithmetic (per instance, scaled space; see oracle/pdhg.py for the
-// restatement used as the parity reference):
+// Arithmetic (per instance, scaled space; oracle/pdhg.py restates it):
 //   xn = clip(x - tau (c - A^T y), l, u)             tau = eta/omega
 //   yn = P_Y(y + sigma (b - A (2 xn - x)))          sigma = eta*omega
 //   x  = w ((1+rho) xn - rho x) + (1-w) xa          w = (k+1)/(k+2)
@@ -27,24 +27,27 @@
 
 namespace fbalp {
 
-constexpr int kMaxWarps = 16;
+constexpr int kMaxWarps = 32;
 constexpr int kRed = 16;  // reduced quantities per convergence check
+constexpr int kArrayCount = 11;
+
+// Array order: xbar, y, x, xa, ya, c, l, u, b, xs, ys.
+enum ArrayId { kXbar = 0, kY, kX, kXa, kYa, kC, kL, kU, kB, kXs, kYs };
 
 struct DevSpecies {
     int32_t m, n, neq, pad_;
     int32_t a_nslices, at_nslices;
-    const int32_t* a_off;
-    const int32_t* a_idx;
+    int64_t a_elems, at_elems;
+    const int4* a_list;           // per slice in warp-schedule order: {slice, base, len, 0}
+    const int4* at_list;
+    const int32_t* a_sched_off;   // [warps + 1] ranges of a_list per warp
+    const int32_t* at_sched_off;
+    const int32_t* a_idx;         // SELL-32 column indices (new numbering); pad -> n
     const float* a_v32;
     const double* a_v64;
-    const int32_t* at_off;
-    const int32_t* at_idx;
+    const int32_t* at_idx;        // pad -> m
     const float* at_v32;
     const double* at_v64;
-    const int32_t* a_sched_off;   // [warps + 1]
-    const int32_t* a_sched;
-    const int32_t* at_sched_off;
-    const int32_t* at_sched;
     const int32_t* row_perm;      // new -> original row
     const int32_t* col_perm;      // new -> original column
     const double* dr;             // new order
@@ -52,8 +55,18 @@ struct DevSpecies {
     double eta;
 };
 
+// Byte offsets of one species' working set inside the CTA's dynamic shared
+// memory (or its global slab for arrays whose bit in smem_mask is clear).
+struct Layout {
+    int64_t sched_a_off, sched_at_off, list_a, list_at;
+    int32_t mat_smem, smem_mask;
+    int64_t mat_a_idx, mat_at_idx, mat_a_val, mat_at_val;
+    int64_t arr[kArrayCount];
+};
+
 struct KernelParams {
     const DevSpecies* species;
+    const Layout* layouts;        // per species, for this launch's precision
     int32_t count;
     const int32_t* order;         // work order (instance ids)
     const int32_t* inst_species;
@@ -75,9 +88,8 @@ struct KernelParams {
     int32_t* out_status;
     int32_t* out_iters;
     int32_t* queue;
-    void* spill;                  // per-CTA global slabs (may be null)
-    int64_t spill_stride;         // elements of T per CTA
-    int64_t smem_elems;           // elements of T available in dynamic smem
+    unsigned char* spill;         // per-CTA global slabs (may be null)
+    int64_t spill_stride;         // bytes per CTA
     int32_t max_iters;
     int32_t check_every;
     double tol_p, tol_d, tol_g;
@@ -85,6 +97,8 @@ struct KernelParams {
     int32_t restarts;
     int32_t final_status;
     int32_t clip_output;          // clip reported x to the original bounds
+    int32_t stall_checks;         // >0: stop (final_status) after this many
+                                  // non-improving convergence tests
 };
 
 }  // namespace fbalp

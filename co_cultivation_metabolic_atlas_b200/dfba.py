@@ -1,0 +1,154 @@
+"""Device-resident dynamic FBA for the synthetic three-species community.
+
+One ``DeviceCommunity.step`` is the reference simulator's step
+(``src/dfba_simulator.py:1757-1797``) for every environment at once:
+
+1. uptake bounds from the current medium (Michaelis-Menten with the
+   physical-inventory cap, ``set_uptake_constraints`` ``:640-667``);
+2. one batched LP solve of every (environment, species) FBA problem through
+   the C ABI engine (all species in one persistent launch);
+3. biomass Euler step (``update_biomass`` ``:1294-1324``, without the pH
+   model, which the synthetic medium does not carry);
+4. medium Euler step with the beginning-of-step biomass
+   (``_update_environment`` ``:1326-1435``, ``integration_biomass`` ``:1680``).
+
+Everything stays on the GPU; the LP batch is laid out species-major
+(all environments of species 0, then species 1, then species 2).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from .engine import EngineOptions, LPEngine, SolveConfig, SolveResult
+
+CARRYING_CAPACITY = 20.0
+
+
+@dataclass
+class StepStats:
+    lps: int
+    certified: torch.Tensor      # scalar int64 (device)
+    iterations: torch.Tensor     # int32 [lps] (device)
+    status: torch.Tensor
+
+
+class DeviceCommunity:
+    """All environments of a synthetic community on one GPU."""
+
+    def __init__(self, models, medium, biomass, *, dt=0.05, capacity=CARRYING_CAPACITY,
+                 options: EngineOptions | None = None, config: SolveConfig | None = None,
+                 warm_start: str = "previous", device=None):
+        if warm_start not in ("cold", "previous"):
+            raise ValueError("warm_start must be 'cold' or 'previous'")
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        dev = self.device
+        self.models = models
+        self.dt = float(dt)
+        self.capacity = float(capacity)
+        self.config = config or SolveConfig()
+        self.warm_start = warm_start
+        E = medium.shape[0]
+        self.E = E
+        self.S = len(models)
+        self.medium = torch.as_tensor(medium, dtype=torch.float64, device=dev).clone()
+        self.biomass = torch.as_tensor(biomass, dtype=torch.float64, device=dev).clone()
+        self.engine = LPEngine([(m.S, m.S.shape[0]) for m in models], options=options, device=dev)
+        sid = np.repeat(np.arange(self.S, dtype=np.int32), E)
+        co, ro, tc, tr = self.engine.layout(sid)
+        self.species_id = sid
+        self.col_offsets = torch.as_tensor(co, device=dev)
+        self.total_cols, self.total_rows = tc, tr
+        lower, upper, cost = [], [], []
+        self.mm = []          # per species: flat column index tensor (E, k), medium ids, vmax, km, orig lb/ub
+        self.bio_index = []   # flat index of every instance's biomass column
+        base = 0
+        for s, mdl in enumerate(models):
+            n = mdl.S.shape[1]
+            lower.append(np.tile(mdl.lower, E))
+            upper.append(np.tile(mdl.upper, E))
+            cost.append(np.tile(mdl.cost, E))
+            starts = base + np.arange(E, dtype=np.int64) * n
+            flat = starts[:, None] + mdl.medium_columns[None, :]
+            self.mm.append(dict(
+                flat=torch.as_tensor(flat, device=dev),
+                ids=torch.as_tensor(mdl.medium_ids, device=dev),
+                vmax=torch.as_tensor(mdl.vmax, device=dev)[None, :],
+                km=torch.as_tensor(mdl.km, device=dev)[None, :],
+                orig=torch.as_tensor(mdl.lower[mdl.medium_columns], device=dev)[None, :],
+                ub=torch.as_tensor(mdl.upper[mdl.medium_columns], device=dev)[None, :]))
+            self.bio_index.append(torch.as_tensor(starts + mdl.biomass, device=dev))
+            base += E * n
+        self.lower = torch.as_tensor(np.concatenate(lower), device=dev)
+        self.upper = torch.as_tensor(np.concatenate(upper), device=dev)
+        self.cost = torch.as_tensor(np.concatenate(cost), device=dev)
+        self.engine.set_instances(sid, self.lower, self.upper, self.cost)
+        self.result: SolveResult | None = None
+        self.prev: SolveResult | None = None
+        self._bufs = [self.engine.allocate_result(), self.engine.allocate_result()]
+        self._which = 0
+
+    # -- pieces of one step --------------------------------------------------
+    def uptake_bounds(self):
+        """Write Michaelis-Menten uptake bounds into the bound batch."""
+        total = self.biomass.clamp_min(1e-6).sum(dim=1, keepdim=True)          # (E, 1)
+        for mm in self.mm:
+            conc = self.medium[:, mm["ids"]]                                    # (E, k)
+            v_kin = mm["vmax"] * conc / (mm["km"] + conc)
+            v_phys = torch.minimum(conc / (total * self.dt), mm["vmax"] * 10.0)
+            limit = torch.minimum(v_kin, v_phys)
+            lb = torch.clamp(torch.maximum(-limit, mm["orig"]), max=0.0)
+            lb = torch.minimum(lb, mm["ub"])
+            lb = torch.round(lb * 1e6) / 1e6
+            self.lower.index_put_((mm["flat"].reshape(-1),), lb.reshape(-1))
+
+    def solve(self):
+        out = self._bufs[self._which]
+        warm = self.prev if (self.warm_start == "previous" and self.prev is not None) else None
+        res = self.engine.solve(warm_x=None if warm is None else warm.x[:self.total_cols],
+                                warm_y=None if warm is None else warm.y[:self.total_rows],
+                                warm_omega=None if warm is None else warm.omega,
+                                config=self.config, out=out)
+        self._which ^= 1
+        self.prev = res
+        self.result = res
+        return res
+
+    def integrate(self, res: SolveResult):
+        """Euler biomass and medium updates from the solved fluxes."""
+        x = res.x
+        E = self.E
+        mu = torch.stack([x[idx] for idx in self.bio_index], dim=1)            # (E, S)
+        X0 = self.biomass.clone()
+        mu = mu.clamp(-0.5, 2.0)
+        total = self.biomass.sum(dim=1, keepdim=True)
+        cap = torch.clamp(1.0 - total / self.capacity, min=0.0)
+        dX = mu * self.biomass * torch.where(mu > 0, cap, torch.ones_like(cap)) * self.dt
+        self.biomass = torch.clamp(self.biomass + dX, 0.0, self.capacity)
+        delta = torch.zeros_like(self.medium)
+        for s, mm in enumerate(self.mm):
+            v = x[mm["flat"]]                                                   # (E, k)
+            contrib = v * X0[:, s:s + 1] * self.dt
+            delta.index_add_(1, mm["ids"], contrib)
+        self.medium = torch.clamp(self.medium + delta, min=0.0)
+
+    def certified(self, res: SolveResult):
+        """Count of LPs that meet the engine's FP64 tolerances AND the
+        reference's certificate gate (primal <= 1e-5, dual <= 1e-7, relative
+        KKT gap <= 1e-7, ``src/gpu_block_lp.py:84``) -- on the device."""
+        mt = res.metrics
+        ok = (res.status == 0) & (mt[:, 0] <= 1e-5) & (mt[:, 1] <= 1e-7) & (mt[:, 2] <= 1e-7)
+        return ok.sum()
+
+    def step(self) -> StepStats:
+        self.uptake_bounds()
+        res = self.solve()
+        self.integrate(res)
+        return StepStats(lps=self.E * self.S, certified=self.certified(res),
+                         iterations=res.iterations, status=res.status)
+
+    def close(self):
+        self.engine.close()

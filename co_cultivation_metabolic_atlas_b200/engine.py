@@ -50,6 +50,7 @@ class SolveConfig:
     fp32_tol_gap: float = 1e-4
     reflection: float = 1.0
     restarts: bool = True
+    fp32_stall_checks: int = 6
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -57,7 +58,7 @@ class SolveConfig:
         if self.precision not in prec:
             raise ValueError("precision must be 'fp64', 'mixed' or 'fp32'")
         p.precision = prec[self.precision]
-        for name in ("max_iterations", "fp32_max_iterations", "check_every"):
+        for name in ("max_iterations", "fp32_max_iterations", "check_every", "fp32_stall_checks"):
             value = getattr(self, name)
             if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)):
                 raise ValueError(f"{name} must be an integer")
@@ -77,6 +78,7 @@ class EngineOptions:
     warps_per_block: int = 16
     blocks_per_sm: int = 0
     max_dynamic_smem: int = 0
+    stage_matrix: bool = True
 
     def native(self) -> N.Options:
         o = N.default_options()
@@ -86,6 +88,7 @@ class EngineOptions:
         o.warps_per_block = int(self.warps_per_block)
         o.blocks_per_sm = int(self.blocks_per_sm)
         o.max_dynamic_smem = int(self.max_dynamic_smem)
+        o.stage_matrix = 1 if self.stage_matrix else 0
         return o
 
 
@@ -238,3 +241,16 @@ class LPEngine:
             _ptr(res.omega)))
         self._warm_keep = (wx, wy, wo)
         return res
+
+    def phase_times(self):
+        """Device milliseconds of the last solve's (FP32, FP64) phases."""
+        a = ctypes.c_float()
+        b = ctypes.c_float()
+        N.check(self.lib.fbalp_engine_phase_times(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def phase_iterations(self):
+        """FP32-phase iteration counts of the last mixed solve (device int32)."""
+        out = torch.empty(self.count, dtype=torch.int32, device=self.device)
+        N.check(self.lib.fbalp_engine_phase_iterations(self.handle, _ptr(out)))
+        return out

@@ -79,11 +79,14 @@ typedef struct fbalp_options {
     int32_t ruiz_iterations;   /* default 10                                 */
     int32_t power_iterations;  /* default 256 (||A~||_2 estimate)            */
     double step_safety;        /* default 0.99 (eta = safety / ||A~||_2)     */
-    int32_t warps_per_block;   /* default 16                                 */
+    int32_t warps_per_block;   /* default 16, at most 32                     */
     int32_t blocks_per_sm;     /* default 0 = derive from occupancy          */
     int32_t max_dynamic_smem;  /* bytes of shared memory per CTA for instance
                                   arrays; 0 = device limit.  Arrays that do not
                                   fit live in a per-CTA global slab.        */
+    int32_t stage_matrix;      /* 1 (default): stage the species matrix into
+                                  shared memory when it fits; 0: stream it
+                                  from L2 every iteration                   */
 } fbalp_options;
 
 /* Solve parameters.  Replaces `iterations` / `check_interval` of
@@ -102,6 +105,8 @@ typedef struct fbalp_solve_params {
     double fp32_tol_gap;
     double reflection;           /* Halpern reflection rho in [0,1], default 1 */
     int32_t restarts;            /* 1 = adaptive restarts, 0 = none           */
+    int32_t fp32_stall_checks;   /* FP32 phase hands off after this many tests
+                                    without halving its KKT error (0 = never) */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);
@@ -165,6 +170,16 @@ int fbalp_prepare_matrix(int32_t rows, int32_t cols, const int64_t* indptr,
                          const int32_t* indices, const double* values,
                          const fbalp_options* options, double* dr, double* dc,
                          double* sigma_max, double* eta);
+
+/* Device time (ms) of the last solve's FP32 and FP64 phase launches (0 for a
+ * phase that did not run); waits for the last launch to finish.  Timing
+ * instrumentation for benchmarks; the reference reports per-phase seconds in
+ * its `timing` dicts (`src/gpu_pdhg_corrector.py:392-405`). */
+int fbalp_engine_phase_times(fbalp_engine* engine, float* ms_fp32, float* ms_fp64);
+
+/* After a MIXED solve: copy the per-instance FP32-phase iteration counts into
+ * the DEVICE array `out_fp32_iterations[count]` (asynchronous). */
+int fbalp_engine_phase_iterations(fbalp_engine* engine, int32_t* out_fp32_iterations);
 
 const char* fbalp_last_error(void);
 

@@ -50,6 +50,7 @@ BETA_SUFFICIENT = 0.2
 BETA_NECESSARY = 0.8
 BETA_ARTIFICIAL = 0.36
 OMEGA_SMOOTHING = 0.5
+STALL_FLOOR = 1e-2
 
 STATUS_OPTIMAL = 0
 STATUS_ITERATION_LIMIT = 1
@@ -119,33 +120,34 @@ def prepare(S, neq=None, *, ruiz_iters=10, power_iters=256, step_safety=0.99):
     return Prepared(A=A, dr=dr, dc=dc, eta=eta, sigma_max=smax, neq=neq)
 
 
-def kkt_metrics(P: Prepared, cs, bs, ls, us, xn, yn):
-    """FP64 metrics at a scaled point (original units where they differ)."""
+def kkt_metrics(P: Prepared, lower, upper, cost, rhs, xn, yn):
+    """FP64 metrics at a scaled point, evaluated in ORIGINAL units with the
+    exact FP64 bounds / objective / right-hand side."""
     A, dr, dc, neq = P.A, P.dr, P.dc, P.neq
-    rho = A @ xn - bs
-    ro = rho / dr
+    x = xn * dc
+    y = yn * dr
+    ro = (A @ xn) / dr - rhs                  # A x - b
     pr_eq = np.max(np.abs(ro[:neq]), initial=0.0)
     pr_ub = np.max(ro[neq:], initial=0.0)
-    bviol = max(np.max((ls - xn) * dc, initial=0.0), np.max((xn - us) * dc, initial=0.0))
+    bviol = max(np.max(lower - x, initial=0.0), np.max(x - upper, initial=0.0))
     primal = max(0.0, pr_eq, pr_ub, bviol)
-    rt = cs - A.T @ yn
-    ro_c = rt / dc
-    finl = np.isfinite(ls)
-    finu = np.isfinite(us)
-    dual = max(0.0, np.max(yn[neq:] * dr[neq:], initial=0.0),
-               np.max(np.where(~finl, ro_c, 0.0), initial=0.0),
-               np.max(np.where(~finu, -ro_c, 0.0), initial=0.0))
-    pobj = float(cs @ xn)
-    term = np.where(rt > 0, np.where(finl, rt * np.where(finl, ls, 0.0), 0.0),
-                    np.where(rt < 0, np.where(finu, rt * np.where(finu, us, 0.0), 0.0), 0.0))
-    dobj = float(bs @ yn + term.sum())
-    target = np.where(rt >= 0, ls, us)
-    bgap = np.abs(rt * (xn - np.where(np.isfinite(target), target, xn))).sum()
-    rgap = np.abs(yn[neq:] * rho[neq:]).sum()
+    r = cost - (A.T @ yn) / dc                # c - A^T y
+    finl = np.isfinite(lower)
+    finu = np.isfinite(upper)
+    dual = max(0.0, np.max(y[neq:], initial=0.0),
+               np.max(np.where(~finl, r, 0.0), initial=0.0),
+               np.max(np.where(~finu, -r, 0.0), initial=0.0))
+    pobj = float(cost @ x)
+    term = np.where(r > 0, np.where(finl, r * np.where(finl, lower, 0.0), 0.0),
+                    np.where(r < 0, np.where(finu, r * np.where(finu, upper, 0.0), 0.0), 0.0))
+    dobj = float(rhs @ y + term.sum())
+    target = np.where(r >= 0, lower, upper)
+    bgap = np.abs(r * (x - np.where(np.isfinite(target), target, x))).sum()
+    rgap = np.abs(y[neq:] * ro[neq:]).sum()
     kgap = (bgap + rgap) / max(1.0, abs(pobj))
     rel_gap = abs(pobj - dobj) / (1.0 + abs(pobj) + abs(dobj))
-    xinf = float(np.max(np.abs(xn * dc), initial=0.0))
-    cinf = float(np.max(np.abs(cs / dc), initial=0.0))
+    xinf = float(np.max(np.abs(x), initial=0.0))
+    cinf = float(np.max(np.abs(cost), initial=0.0))
     return dict(primal_residual=primal, dual_violation=dual, relative_kkt_gap=kgap,
                 objective=pobj, dual_objective=dobj, relative_gap=rel_gap, x_inf=xinf, c_inf=cinf)
 
@@ -159,7 +161,7 @@ def converged(mt, tol_primal, tol_dual, tol_gap):
 def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0=1.0,
           dtype=np.float64, max_iters=100000, check_every=64, tol_primal=1e-9, tol_dual=1e-9,
           tol_gap=1e-9, rho=1.0, restarts=True, stop_on_converge=True, final_status=STATUS_OPTIMAL,
-          trace=None):
+          stall_checks=0, trace=None):
     """Run the engine's algorithm for one instance; return dict with scaled
     and original-unit iterates, status, iterations and metrics."""
     A, dr, dc = P.A, P.dr, P.dc
@@ -186,8 +188,13 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
     mt = None
     it = 0
     xn, yn = x, y
-    if max_iters == 0:
-        mt = kkt_metrics(P, cs, bs, ls, us, x.astype(float), y.astype(float))
+    mt = kkt_metrics(P, lower, upper, cost, rhs, x.astype(float), y.astype(float))
+    if converged(mt, tol_primal, tol_dual, tol_gap) or max_iters == 0:
+        status = final_status if converged(mt, tol_primal, tol_dual, tol_gap) else STATUS_ITERATION_LIMIT
+        return dict(x=np.clip(x.astype(float) * dc, lower, upper), y=y.astype(float) * dr, xs=x, ys=y,
+                    status=status, iterations=0, metrics=mt, omega=omega)
+    best_err = np.inf
+    stall = 0
     for it in range(1, max_iters + 1):
         tau = dtype(P.eta / omega)
         sig = dtype(P.eta * omega)
@@ -210,7 +217,7 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
             dx = (xn.astype(float) - x.astype(float))
             dy = (yn.astype(float) - y.astype(float))
             r = np.sqrt(omega * (dx @ dx) + (dy @ dy) / omega)
-            mt = kkt_metrics(P, cs, bs, ls, us, xn.astype(float), yn.astype(float))
+            mt = kkt_metrics(P, lower, upper, cost, rhs, xn.astype(float), yn.astype(float))
             if trace is not None:
                 trace.append(dict(it=it, r=r, omega=omega, **mt))
             if not np.isfinite(r) or not all(np.isfinite(v) for v in mt.values()):
@@ -220,6 +227,15 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
                 status = final_status
                 break
             if it == max_iters:
+                break
+            err = max(mt["primal_residual"] / (1 + mt["x_inf"]), mt["dual_violation"] / (1 + mt["c_inf"]),
+                      mt["relative_gap"], mt["relative_kkt_gap"])
+            if err < 0.5 * best_err:
+                best_err, stall = err, 0
+            else:
+                stall += 1
+            if stall_checks > 0 and stall >= stall_checks and best_err <= STALL_FLOOR:
+                status = final_status
                 break
             if restarts and (r <= BETA_SUFFICIENT * r_restart
                              or (r <= BETA_NECESSARY * r_restart and r > r_prev)
@@ -240,5 +256,7 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
                 r_prev = r
         x, y = xnew, ynew
     xo = xn.astype(float) * dc
+    if final_status == STATUS_OPTIMAL:  # the final FP64 phase reports x inside its bounds
+        xo = np.clip(xo, lower, upper)
     yo = yn.astype(float) * dr
     return dict(x=xo, y=yo, xs=xn, ys=yn, status=status, iterations=it, metrics=mt, omega=omega)

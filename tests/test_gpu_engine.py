@@ -167,10 +167,14 @@ def test_spilled_arrays_give_identical_results():
     config = cfg(precision="mixed")
     a = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config)
     b = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config, max_dynamic_smem=8192)
-    np.testing.assert_array_equal(a["x"], b["x"])
-    np.testing.assert_array_equal(a["y"], b["y"])
-    np.testing.assert_array_equal(a["iters"], b["iters"])
-    assert (a["status"] == 0).all()
+    c = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config, stage_matrix=False)
+    d = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config, warps_per_block=32)
+    for other in (b, c):
+        np.testing.assert_array_equal(a["x"], other["x"])
+        np.testing.assert_array_equal(a["y"], other["y"])
+        np.testing.assert_array_equal(a["iters"], other["iters"])
+    assert (a["status"] == 0).all() and (d["status"] == 0).all()
+    np.testing.assert_allclose(a["obj"], d["obj"], rtol=1e-8)
 
 
 def test_repeat_solves_are_deterministic():
