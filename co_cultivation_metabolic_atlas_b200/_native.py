@@ -55,7 +55,8 @@ class SolveParams(ctypes.Structure):
                 ("tol_gap", ctypes.c_double), ("fp32_tol_primal", ctypes.c_double),
                 ("fp32_tol_dual", ctypes.c_double), ("fp32_tol_gap", ctypes.c_double),
                 ("reflection", ctypes.c_double), ("restarts", ctypes.c_int32),
-                ("fp32_stall_checks", ctypes.c_int32)]
+                ("fp32_stall_checks", ctypes.c_int32), ("fp64_stall_checks", ctypes.c_int32),
+                ("floor_tol", ctypes.c_double)]
 
 
 class NativeError(RuntimeError):
@@ -97,6 +98,18 @@ def load(path: os.PathLike | None = None):
                                                     ctypes.POINTER(ctypes.c_float)]),
         "fbalp_engine_phase_iterations": (ctypes.c_int, [vp, vp]),
         "fbalp_last_error": (ctypes.c_char_p, []),
+        # BF16 tensor-core kernels of the learned warm start (include/fbalp_mlp.h)
+        "fbalp_gemm_bf16": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int,
+                                           ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int,
+                                           ctypes.c_float, vp, vp, ctypes.c_int, vp, ctypes.c_int,
+                                           ctypes.c_int, vp]),
+        "fbalp_mlp_error_flag": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+        "fbalp_gelu_backward": (ctypes.c_int, [ctypes.c_int64, vp, vp, vp, vp, vp]),
+        "fbalp_mse_grad": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_float, vp, vp, vp, vp]),
+        "fbalp_column_sum": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, vp, vp, vp]),
+        "fbalp_adam_step": (ctypes.c_int, [ctypes.c_int64, vp, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float,
+                                           ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float, vp]),
+        "fbalp_to_bf16": (ctypes.c_int, [ctypes.c_int64, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)  # AttributeError if the symbol is missing

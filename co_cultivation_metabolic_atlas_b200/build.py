@@ -13,7 +13,7 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libfbalp.so"
 
-SOURCES = ["prepare.cpp", "engine.cu", "pdhg_kernel.cu"]
+SOURCES = ["prepare.cpp", "engine.cu", "pdhg_kernel.cu", "mlp_kernels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -32,7 +32,7 @@ def stale() -> bool:
     if not LIB.exists():
         return True
     t = LIB.stat().st_mtime
-    deps = list(CSRC.glob("*")) + [PKG.parent / "include" / "fbalp.h"]
+    deps = list(CSRC.glob("*")) + list((PKG.parent / "include").glob("*.h"))
     return any(p.stat().st_mtime > t for p in deps if p.is_file())
 
 

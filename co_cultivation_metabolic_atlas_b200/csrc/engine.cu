@@ -130,13 +130,15 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->check_every = 64;
     p->tol_primal = 1e-9;
     p->tol_dual = 1e-9;
-    p->tol_gap = 1e-9;
+    p->tol_gap = 1e-7;
     p->fp32_tol_primal = 1e-6;
     p->fp32_tol_dual = 1e-6;
     p->fp32_tol_gap = 1e-4;
     p->reflection = 1.0;
     p->restarts = 1;
     p->fp32_stall_checks = 6;
+    p->fp64_stall_checks = 8;
+    p->floor_tol = 1e-7;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -428,7 +430,8 @@ bool valid_params(const fbalp_solve_params& q, std::string* err) {
         if (!(t >= 0.0) || !std::isfinite(t)) return *err = "tolerances must be finite and non-negative", false;
     if (!(q.reflection >= 0.0 && q.reflection <= 1.0)) return *err = "reflection must be in [0,1]", false;
     if (q.restarts != 0 && q.restarts != 1) return *err = "restarts must be 0 or 1", false;
-    if (q.fp32_stall_checks < 0) return *err = "fp32_stall_checks must be non-negative", false;
+    if (q.fp32_stall_checks < 0 || q.fp64_stall_checks < 0) return *err = "stall checks must be non-negative", false;
+    if (!(q.floor_tol >= 0.0) || !std::isfinite(q.floor_tol)) return *err = "floor_tol must be finite and non-negative", false;
     return true;
 }
 
@@ -483,7 +486,8 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p.tol_g = fp64 ? q.tol_gap : q.fp32_tol_gap;
             p.final_status = fp64 ? fbalp::kStatusOptimal : fbalp::kStatusHandoff;
             p.clip_output = 1;
-            p.stall_checks = fp64 ? 0 : q.fp32_stall_checks;
+            p.stall_checks = fp64 ? q.fp64_stall_checks : q.fp32_stall_checks;
+            p.floor_tol = q.floor_tol;
             run_phase(e, fp64, p);
         } else {
             e->mid_x.ensure(e->total_cols * sizeof(double));
@@ -512,6 +516,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p32.final_status = fbalp::kStatusHandoff;
             p32.clip_output = 0;
             p32.stall_checks = q.fp32_stall_checks;
+            p32.floor_tol = q.floor_tol;
             run_phase(e, false, p32);
             fbalp::KernelParams p64 = p;
             p64.warm_x = static_cast<const double*>(e->mid_x.ptr);
@@ -531,7 +536,8 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p64.tol_g = q.tol_gap;
             p64.final_status = fbalp::kStatusOptimal;
             p64.clip_output = 1;
-            p64.stall_checks = 0;
+            p64.stall_checks = q.fp64_stall_checks;
+            p64.floor_tol = q.floor_tol;
             run_phase(e, true, p64);
         }
     } catch (const CudaError& ex) {

@@ -235,6 +235,115 @@ __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned ch
     }
 }
 
+// Element offsets (in units of T, or of uint16 for indices) of one species'
+// working set when EVERYTHING lives in shared memory; the fast passes index
+// the dynamic shared array directly, so the compiler keeps 32-bit shared
+// addresses and the per-element instruction count low.
+struct FastOffsets {
+    int xbar, y, x, xa, ya, c, l, u, b;
+    int a_idx, at_idx, a_val, at_val;  // matrix slices
+};
+
+template <typename T>
+__device__ __forceinline__ FastOffsets fast_offsets(const Layout& L) {
+    FastOffsets o;
+    const int e = sizeof(T);
+    o.xbar = L.arr[kXbar] / e;
+    o.y = L.arr[kY] / e;
+    o.x = L.arr[kX] / e;
+    o.xa = L.arr[kXa] / e;
+    o.ya = L.arr[kYa] / e;
+    o.c = L.arr[kC] / e;
+    o.l = L.arr[kL] / e;
+    o.u = L.arr[kU] / e;
+    o.b = L.arr[kB] / e;
+    o.a_idx = L.mat_a_idx / 2;
+    o.at_idx = L.mat_at_idx / 2;
+    o.a_val = L.mat_a_val / e;
+    o.at_val = L.mat_at_val / e;
+    return o;
+}
+
+// Slice product from shared memory: four coalesced index/value loads and
+// four gathers per step with no bounds guards, then the tail; the
+// accumulation order (k ascending, one accumulator) is the generic path's.
+template <typename T>
+__device__ __forceinline__ T slice_dot_fast(const uint16_t* ip, const T* vp, const T* g, int len) {
+    T acc = T(0);
+    int k = 0;
+    for (; k + 4 <= len; k += 4, ip += 128, vp += 128) {
+        const int i0 = ip[0], i1 = ip[32], i2 = ip[64], i3 = ip[96];
+        const T v0 = vp[0], v1 = vp[32], v2 = vp[64], v3 = vp[96];
+        acc = fma(v0, g[i0], acc);
+        acc = fma(v1, g[i1], acc);
+        acc = fma(v2, g[i2], acc);
+        acc = fma(v3, g[i3], acc);
+    }
+    for (; k < len; ++k, ip += 32, vp += 32) acc = fma(vp[0], g[ip[0]], acc);
+    return acc;
+}
+
+// xs / ys (written only on convergence-test iterations) may live in the
+// global slab, so they come in as generic pointers.
+template <typename T>
+__device__ __forceinline__ void primal_pass_fast(const FastOffsets& o, T* xs, const int4* atlist, int t0,
+                                                 int t1, int n, int lane, T tau, T w, T w1, T rho,
+                                                 bool check, double& pdx2, double& pdxa2) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    T* const S = reinterpret_cast<T*>(dyn_smem);
+    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = atlist[t];
+        const T g = slice_dot_fast<T>(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S + o.y, sl.z);
+        const int j = (sl.x << 5) + lane;
+        if (j < n) {
+            const T xo = S[o.x + j];
+            const T xn = clampT(xo - tau * (S[o.c + j] - g), S[o.l + j], S[o.u + j]);
+            const T xb = xn + xn - xo;
+            S[o.xbar + j] = xb;
+            const T xh = (rho == T(1)) ? xb : (T(1) + rho) * xn - rho * xo;
+            const T xav = S[o.xa + j];
+            S[o.x + j] = w * xh + w1 * xav;
+            if (check) {
+                xs[j] = xn;
+                const double d = static_cast<double>(xn) - static_cast<double>(xo);
+                const double da = static_cast<double>(xn) - static_cast<double>(xav);
+                pdx2 += d * d;
+                pdxa2 += da * da;
+            }
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void dual_pass_fast(const FastOffsets& o, T* ys, const int4* alist, int t0,
+                                               int t1, int m, int neq, int lane, T sigma, T w, T w1,
+                                               T rho, bool check, double& pdy2, double& pdya2) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    T* const S = reinterpret_cast<T*>(dyn_smem);
+    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = alist[t];
+        const T h = slice_dot_fast<T>(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S + o.xbar, sl.z);
+        const int i = (sl.x << 5) + lane;
+        if (i < m) {
+            const T yo = S[o.y + i];
+            T yn = yo + sigma * (S[o.b + i] - h);
+            if (i >= neq && yn > T(0)) yn = T(0);
+            const T yh = (rho == T(1)) ? yn + yn - yo : (T(1) + rho) * yn - rho * yo;
+            const T yav = S[o.ya + i];
+            S[o.y + i] = w * yh + w1 * yav;
+            if (check) {
+                ys[i] = yn;
+                const double d = static_cast<double>(yn) - static_cast<double>(yo);
+                const double da = static_cast<double>(yn) - static_cast<double>(yav);
+                pdy2 += d * d;
+                pdya2 += da * da;
+            }
+        }
+    }
+}
+
 template <typename T, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -285,6 +394,9 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
         const T* s_tval = reinterpret_cast<const T*>(dyn_smem + L.mat_at_val);
         const T* __restrict__ g_aval = Vals<T>::a(sp);
         const T* __restrict__ g_tval = Vals<T>::at(sp);
+        // fast path: matrix and every per-iteration array in shared memory
+        const bool fast = mat_smem && (L.smem_mask & 0x1ff) == 0x1ff;
+        const FastOffsets fo = fast_offsets<T>(L);
 
         // ---- load the instance (scaled, in the species' permuted order) ----
         int bad = 0;
@@ -368,54 +480,65 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
         double r_restart = INFINITY, r_prev = INFINITY, best_err = INFINITY;
         while (status < 0) {
             ++it;
-            const bool check = (it % p.check_every == 0) || (it >= p.max_iters);
+            // full tests (restart rule, stall rule) every check_every iterations;
+            // cheap termination-only tests at 8, 16, 32, ... below that
+            const bool full = (it % p.check_every == 0) || (it >= p.max_iters);
+            const bool check = full || (it >= 8 && it < p.check_every && (it & (it - 1)) == 0);
             const T tau = static_cast<T>(eta / omega), sigma = static_cast<T>(eta * omega);
             const T w = static_cast<T>((k + 1.0) / (k + 2.0));
             const T w1 = T(1) - w;
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
             // primal pass: g = A^T y, projected step, extrapolation, Halpern
-            for (int t = tw0; t < tw1; ++t) {
-                const int4 sl = atlist[t];
-                const T g = mat_smem ? slice_dot<T, T, uint16_t, false>(s_tidx, s_tval, sl.y, sl.z, lane, A.y)
-                                     : slice_dot<T, T, int32_t, true>(sp->at_idx, g_tval, sl.y, sl.z, lane, A.y);
-                const int j = (sl.x << 5) + lane;
-                if (j < n) {
-                    const T xo = A.x[j];
-                    const T xn = clampT(xo - tau * (A.cs[j] - g), A.ls[j], A.us[j]);
-                    const T xb = xn + xn - xo;
-                    A.xbar[j] = xb;
-                    const T xh = (rho == T(1)) ? xb : (T(1) + rho) * xn - rho * xo;
-                    const T xav = A.xa[j];
-                    A.x[j] = w * xh + w1 * xav;
-                    if (check) {
-                        A.xs[j] = xn;
-                        const double d = static_cast<double>(xn) - static_cast<double>(xo);
-                        const double da = static_cast<double>(xn) - static_cast<double>(xav);
-                        pdx2 += d * d;
-                        pdxa2 += da * da;
+            if (fast) {
+                primal_pass_fast<T>(fo, A.xs, atlist, tw0, tw1, n, lane, tau, w, w1, rho, check, pdx2, pdxa2);
+            } else {
+                for (int t = tw0; t < tw1; ++t) {
+                    const int4 sl = atlist[t];
+                    const T g = mat_smem ? slice_dot<T, T, uint16_t, false>(s_tidx, s_tval, sl.y, sl.z, lane, A.y)
+                                         : slice_dot<T, T, int32_t, true>(sp->at_idx, g_tval, sl.y, sl.z, lane, A.y);
+                    const int j = (sl.x << 5) + lane;
+                    if (j < n) {
+                        const T xo = A.x[j];
+                        const T xn = clampT(xo - tau * (A.cs[j] - g), A.ls[j], A.us[j]);
+                        const T xb = xn + xn - xo;
+                        A.xbar[j] = xb;
+                        const T xh = (rho == T(1)) ? xb : (T(1) + rho) * xn - rho * xo;
+                        const T xav = A.xa[j];
+                        A.x[j] = w * xh + w1 * xav;
+                        if (check) {
+                            A.xs[j] = xn;
+                            const double d = static_cast<double>(xn) - static_cast<double>(xo);
+                            const double da = static_cast<double>(xn) - static_cast<double>(xav);
+                            pdx2 += d * d;
+                            pdxa2 += da * da;
+                        }
                     }
                 }
             }
             __syncthreads();
             // dual pass: h = A xbar, projected dual step, Halpern
-            for (int t = aw0; t < aw1; ++t) {
-                const int4 sl = alist[t];
-                const T h = mat_smem ? slice_dot<T, T, uint16_t, false>(s_aidx, s_aval, sl.y, sl.z, lane, A.xbar)
-                                     : slice_dot<T, T, int32_t, true>(sp->a_idx, g_aval, sl.y, sl.z, lane, A.xbar);
-                const int i = (sl.x << 5) + lane;
-                if (i < m) {
-                    const T yo = A.y[i];
-                    T yn = yo + sigma * (A.bs[i] - h);
-                    if (i >= neq && yn > T(0)) yn = T(0);
-                    const T yh = (rho == T(1)) ? yn + yn - yo : (T(1) + rho) * yn - rho * yo;
-                    const T yav = A.ya[i];
-                    A.y[i] = w * yh + w1 * yav;
-                    if (check) {
-                        A.ys[i] = yn;
-                        const double d = static_cast<double>(yn) - static_cast<double>(yo);
-                        const double da = static_cast<double>(yn) - static_cast<double>(yav);
-                        pdy2 += d * d;
-                        pdya2 += da * da;
+            if (fast) {
+                dual_pass_fast<T>(fo, A.ys, alist, aw0, aw1, m, neq, lane, sigma, w, w1, rho, check, pdy2, pdya2);
+            } else {
+                for (int t = aw0; t < aw1; ++t) {
+                    const int4 sl = alist[t];
+                    const T h = mat_smem ? slice_dot<T, T, uint16_t, false>(s_aidx, s_aval, sl.y, sl.z, lane, A.xbar)
+                                         : slice_dot<T, T, int32_t, true>(sp->a_idx, g_aval, sl.y, sl.z, lane, A.xbar);
+                    const int i = (sl.x << 5) + lane;
+                    if (i < m) {
+                        const T yo = A.y[i];
+                        T yn = yo + sigma * (A.bs[i] - h);
+                        if (i >= neq && yn > T(0)) yn = T(0);
+                        const T yh = (rho == T(1)) ? yn + yn - yo : (T(1) + rho) * yn - rho * yo;
+                        const T yav = A.ya[i];
+                        A.y[i] = w * yh + w1 * yav;
+                        if (check) {
+                            A.ys[i] = yn;
+                            const double d = static_cast<double>(yn) - static_cast<double>(yo);
+                            const double da = static_cast<double>(yn) - static_cast<double>(yav);
+                            pdy2 += d * d;
+                            pdya2 += da * da;
+                        }
                     }
                 }
             }
@@ -446,8 +569,11 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
                 status = kStatusIterationLimit;
                 break;
             }
-            // precision floor: the FP32 phase hands off once its KKT error has
-            // stopped halving for `stall_checks` consecutive tests.
+            if (!full) continue;
+            // precision floor: once the KKT error has stopped halving for
+            // `stall_checks` consecutive tests, the FP32 phase hands off, and
+            // the FP64 phase accepts the point if it meets the floor
+            // tolerance (otherwise it keeps iterating to its budget).
             {
                 const double e = fmax(fmax(M.primal / (1.0 + M.xinf), M.dual / (1.0 + M.cinf)),
                                       fmax(M.rgap, M.kgap));
@@ -457,9 +583,16 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
                 } else {
                     ++stall;
                 }
-                if (p.stall_checks > 0 && stall >= p.stall_checks && best_err <= kStallFloor) {
-                    status = p.final_status;
-                    break;
+                if (p.stall_checks > 0 && stall >= p.stall_checks) {
+                    if (p.final_status == kStatusHandoff && best_err <= kStallFloor) {
+                        status = p.final_status;
+                        break;
+                    }
+                    if (p.final_status == kStatusOptimal && e <= p.floor_tol &&
+                        M.primal <= p.floor_tol * (1.0 + M.xinf) && M.dual <= p.floor_tol * (1.0 + M.cinf)) {
+                        status = p.final_status;
+                        break;
+                    }
                 }
             }
             if (p.restarts && (M.r <= kBetaSufficient * r_restart ||

@@ -97,8 +97,9 @@ struct KernelParams {
     int32_t restarts;
     int32_t final_status;
     int32_t clip_output;          // clip reported x to the original bounds
-    int32_t stall_checks;         // >0: stop (final_status) after this many
+    int32_t stall_checks;         // >0: stall rule after this many
                                   // non-improving convergence tests
+    double floor_tol;             // FP64 phase: tolerance accepted after a stall
 };
 
 }  // namespace fbalp

@@ -44,13 +44,15 @@ class SolveConfig:
     check_every: int = 64
     tol_primal: float = 1e-9
     tol_dual: float = 1e-9
-    tol_gap: float = 1e-9
+    tol_gap: float = 1e-7
     fp32_tol_primal: float = 1e-6
     fp32_tol_dual: float = 1e-6
     fp32_tol_gap: float = 1e-4
     reflection: float = 1.0
     restarts: bool = True
     fp32_stall_checks: int = 6
+    fp64_stall_checks: int = 8
+    floor_tol: float = 1e-7
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -58,13 +60,14 @@ class SolveConfig:
         if self.precision not in prec:
             raise ValueError("precision must be 'fp64', 'mixed' or 'fp32'")
         p.precision = prec[self.precision]
-        for name in ("max_iterations", "fp32_max_iterations", "check_every", "fp32_stall_checks"):
+        for name in ("max_iterations", "fp32_max_iterations", "check_every", "fp32_stall_checks",
+                     "fp64_stall_checks"):
             value = getattr(self, name)
             if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)):
                 raise ValueError(f"{name} must be an integer")
             setattr(p, name, int(value))
         for name in ("tol_primal", "tol_dual", "tol_gap", "fp32_tol_primal", "fp32_tol_dual",
-                     "fp32_tol_gap", "reflection"):
+                     "fp32_tol_gap", "reflection", "floor_tol"):
             setattr(p, name, float(getattr(self, name)))
         p.restarts = 1 if self.restarts else 0
         return p

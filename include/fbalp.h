@@ -46,7 +46,8 @@ extern "C" {
 #define FBALP_ERR_STATE 4     /* call out of order (e.g. solve before set)   */
 
 /* per-instance solver status */
-#define FBALP_STATUS_OPTIMAL 0          /* FP64 certificate tolerances met    */
+#define FBALP_STATUS_OPTIMAL 0          /* FP64 tolerances met (tight, or the
+                                           floor tolerance after a stall)    */
 #define FBALP_STATUS_ITERATION_LIMIT 1  /* budget exhausted; fails closed     */
 #define FBALP_STATUS_NUMERICAL 2        /* NaN/Inf met in the iteration       */
 #define FBALP_STATUS_INVALID_INPUT 3    /* l > u, NaN bound, non-finite c / b */
@@ -99,7 +100,8 @@ typedef struct fbalp_solve_params {
     int32_t check_every;         /* convergence / restart test period         */
     double tol_primal;           /* primal <= tol*(1+|x|_inf)   (FP64 phase)  */
     double tol_dual;             /* dual viol. <= tol*(1+|c|_inf)             */
-    double tol_gap;              /* relative gap and relative KKT gap         */
+    double tol_gap;              /* relative gap and relative KKT gap (default
+                                    1e-7, the reference's gate)              */
     double fp32_tol_primal;      /* hand-off tolerances of the FP32 phase     */
     double fp32_tol_dual;
     double fp32_tol_gap;
@@ -107,6 +109,11 @@ typedef struct fbalp_solve_params {
     int32_t restarts;            /* 1 = adaptive restarts, 0 = none           */
     int32_t fp32_stall_checks;   /* FP32 phase hands off after this many tests
                                     without halving its KKT error (0 = never) */
+    int32_t fp64_stall_checks;   /* FP64 phase: after this many such tests a
+                                    point meeting floor_tol is accepted as
+                                    OPTIMAL (an FP64 rounding floor above the
+                                    tight tolerances; 0 = never)             */
+    double floor_tol;            /* default 1e-7 = the reference's gap gate   */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);

@@ -50,7 +50,7 @@ BETA_SUFFICIENT = 0.2
 BETA_NECESSARY = 0.8
 BETA_ARTIFICIAL = 0.36
 OMEGA_SMOOTHING = 0.5
-STALL_FLOOR = 1e-2
+STALL_FLOOR = 1.0
 
 STATUS_OPTIMAL = 0
 STATUS_ITERATION_LIMIT = 1
@@ -160,8 +160,8 @@ def converged(mt, tol_primal, tol_dual, tol_gap):
 
 def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0=1.0,
           dtype=np.float64, max_iters=100000, check_every=64, tol_primal=1e-9, tol_dual=1e-9,
-          tol_gap=1e-9, rho=1.0, restarts=True, stop_on_converge=True, final_status=STATUS_OPTIMAL,
-          stall_checks=0, trace=None):
+          tol_gap=1e-7, rho=1.0, restarts=True, stop_on_converge=True, final_status=STATUS_OPTIMAL,
+          stall_checks=None, floor_tol=1e-7, trace=None):
     """Run the engine's algorithm for one instance; return dict with scaled
     and original-unit iterates, status, iterations and metrics."""
     A, dr, dc = P.A, P.dr, P.dc
@@ -195,6 +195,8 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
                     status=status, iterations=0, metrics=mt, omega=omega)
     best_err = np.inf
     stall = 0
+    if stall_checks is None:
+        stall_checks = 8 if final_status == STATUS_OPTIMAL else 6
     for it in range(1, max_iters + 1):
         tau = dtype(P.eta / omega)
         sig = dtype(P.eta * omega)
@@ -212,7 +214,9 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
             xnew = (w * ((1 + rho) * xn - rho * x) + (1 - w) * xa).astype(dtype)
             ynew = (w * ((1 + rho) * yn - rho * y) + (1 - w) * ya).astype(dtype)
         k += 1
-        is_check = (it % check_every == 0) or it == max_iters
+        full = (it % check_every == 0) or it == max_iters
+        # termination-only tests at 8, 16, 32, ... below check_every
+        is_check = full or (8 <= it < check_every and (it & (it - 1)) == 0)
         if is_check:
             dx = (xn.astype(float) - x.astype(float))
             dy = (yn.astype(float) - y.astype(float))
@@ -228,15 +232,24 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
                 break
             if it == max_iters:
                 break
+            if not full:
+                x, y = xnew, ynew
+                continue
             err = max(mt["primal_residual"] / (1 + mt["x_inf"]), mt["dual_violation"] / (1 + mt["c_inf"]),
                       mt["relative_gap"], mt["relative_kkt_gap"])
             if err < 0.5 * best_err:
                 best_err, stall = err, 0
             else:
                 stall += 1
-            if stall_checks > 0 and stall >= stall_checks and best_err <= STALL_FLOOR:
-                status = final_status
-                break
+            if stall_checks > 0 and stall >= stall_checks:
+                if final_status == STATUS_HANDOFF and best_err <= STALL_FLOOR:
+                    status = final_status
+                    break
+                if (final_status == STATUS_OPTIMAL and err <= floor_tol
+                        and mt["primal_residual"] <= floor_tol * (1 + mt["x_inf"])
+                        and mt["dual_violation"] <= floor_tol * (1 + mt["c_inf"])):
+                    status = final_status
+                    break
             if restarts and (r <= BETA_SUFFICIENT * r_restart
                              or (r <= BETA_NECESSARY * r_restart and r > r_prev)
                              or k >= BETA_ARTIFICIAL * it):

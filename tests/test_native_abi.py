@@ -11,7 +11,7 @@ from tests.conftest import ROOT
 
 
 def declared_symbols():
-    text = (ROOT / "include" / "fbalp.h").read_text()
+    text = "".join(p.read_text() for p in sorted((ROOT / "include").glob("*.h")))
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(fbalp_[a-z_0-9]+)\s*\(", text)))
 
@@ -36,7 +36,8 @@ def test_defaults(native_built):
     assert (o.ruiz_iterations, o.power_iterations, o.warps_per_block) == (10, 256, 16)
     assert o.step_safety == pytest.approx(0.99)
     assert p.precision == N.PRECISION_MIXED and p.check_every == 64
-    assert p.tol_gap == pytest.approx(1e-9) and p.fp32_tol_gap == pytest.approx(1e-4)
+    assert p.tol_gap == pytest.approx(1e-7) and p.fp32_tol_gap == pytest.approx(1e-4)
+    assert p.fp64_stall_checks == 8 and p.floor_tol == pytest.approx(1e-7)
 
 
 def test_host_preprocessing_matches_oracle(native_built):
