@@ -45,7 +45,7 @@ class Options(ctypes.Structure):
     _fields_ = [("ruiz_iterations", ctypes.c_int32), ("power_iterations", ctypes.c_int32),
                 ("step_safety", ctypes.c_double), ("warps_per_block", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("max_dynamic_smem", ctypes.c_int32),
-                ("stage_matrix", ctypes.c_int32)]
+                ("stage_matrix", ctypes.c_int32), ("fp64_max_dynamic_smem", ctypes.c_int32)]
 
 
 class SolveParams(ctypes.Structure):
@@ -56,7 +56,7 @@ class SolveParams(ctypes.Structure):
                 ("fp32_tol_dual", ctypes.c_double), ("fp32_tol_gap", ctypes.c_double),
                 ("reflection", ctypes.c_double), ("restarts", ctypes.c_int32),
                 ("fp32_stall_checks", ctypes.c_int32), ("fp64_stall_checks", ctypes.c_int32),
-                ("floor_tol", ctypes.c_double)]
+                ("floor_tol", ctypes.c_double), ("fp32_passthrough_tol", ctypes.c_double)]
 
 
 class NativeError(RuntimeError):

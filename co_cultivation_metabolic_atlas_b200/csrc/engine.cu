@@ -120,6 +120,7 @@ void fbalp_default_options(fbalp_options* o) {
     o->blocks_per_sm = 0;
     o->max_dynamic_smem = 0;
     o->stage_matrix = 1;
+    o->fp64_max_dynamic_smem = 0;
 }
 
 void fbalp_default_solve_params(fbalp_solve_params* p) {
@@ -139,6 +140,7 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->fp32_stall_checks = 6;
     p->fp64_stall_checks = 8;
     p->floor_tol = 1e-7;
+    p->fp32_passthrough_tol = 1e-3;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -152,6 +154,7 @@ static bool valid_options(const fbalp_options& o, std::string* err) {
     if (o.blocks_per_sm < 0 || o.blocks_per_sm > 32) return *err = "blocks_per_sm out of range", false;
     if (o.max_dynamic_smem < 0) return *err = "max_dynamic_smem must be non-negative", false;
     if (o.stage_matrix != 0 && o.stage_matrix != 1) return *err = "stage_matrix must be 0 or 1", false;
+    if (o.fp64_max_dynamic_smem < 0) return *err = "fp64_max_dynamic_smem must be non-negative", false;
     return true;
 }
 
@@ -372,11 +375,13 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
                       ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
     if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
+    if (fp64 && e->opt.fp64_max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.fp64_max_dynamic_smem);
     std::vector<char> used(e->species.size(), 0);
     for (int32_t s : e->h_species) used[s] = 1;
     std::vector<fbalp::Layout>& layouts = fp64 ? e->layouts64 : e->layouts32;
     layouts.assign(e->species.size(), fbalp::Layout{});
     int64_t dyn = 0, slab = 0;
+    bool all_fast = true;
     for (size_t s = 0; s < e->species.size(); ++s) {
         if (!used[s]) continue;
         const SpeciesHost& sh = e->species[s];
@@ -386,6 +391,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
         if (P.smem_bytes > cap) throw CudaError("species schedule does not fit into shared memory");
         if (!fbalp::layout_aligned(P.layout)) throw CudaError("internal error: misaligned shared-memory layout");
         layouts[s] = P.layout;
+        all_fast = all_fast && P.layout.mat_smem && (P.layout.smem_mask & 0x1ff) == 0x1ff;
         dyn = std::max(dyn, P.smem_bytes);
         slab = std::max(slab, P.slab_bytes);
     }
@@ -394,7 +400,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     dl.ensure(layouts.size() * sizeof(fbalp::Layout));
     check(cudaMemcpyAsync(dl.ptr, layouts.data(), layouts.size() * sizeof(fbalp::Layout),
                           cudaMemcpyHostToDevice, e->stream), "copy layouts");
-    const void* k = fbalp::kernel_symbol(fp64, threads);
+    const void* k = fbalp::kernel_symbol(fp64, threads, all_fast);
     check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
           "cudaFuncSetAttribute");
     int per_sm = 0;
@@ -415,7 +421,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     check(cudaMemsetAsync(p.queue, 0, sizeof(int32_t), e->stream), "memset queue");
     const int ph = fp64 ? 1 : 0;
     check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
-    check(fbalp::launch_pdhg(fp64, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
+    check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
     check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
     e->ran[ph] = true;
     e->last_grid[fp64 ? 1 : 0] = grid;
@@ -432,6 +438,8 @@ bool valid_params(const fbalp_solve_params& q, std::string* err) {
     if (q.restarts != 0 && q.restarts != 1) return *err = "restarts must be 0 or 1", false;
     if (q.fp32_stall_checks < 0 || q.fp64_stall_checks < 0) return *err = "stall checks must be non-negative", false;
     if (!(q.floor_tol >= 0.0) || !std::isfinite(q.floor_tol)) return *err = "floor_tol must be finite and non-negative", false;
+    if (!(q.fp32_passthrough_tol >= 0.0) || !std::isfinite(q.fp32_passthrough_tol))
+        return *err = "fp32_passthrough_tol must be finite and non-negative", false;
     return true;
 }
 
@@ -488,6 +496,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p.clip_output = 1;
             p.stall_checks = fp64 ? q.fp64_stall_checks : q.fp32_stall_checks;
             p.floor_tol = q.floor_tol;
+            p.passthrough_tol = 0.0;
             run_phase(e, fp64, p);
         } else {
             e->mid_x.ensure(e->total_cols * sizeof(double));
@@ -517,6 +526,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p32.clip_output = 0;
             p32.stall_checks = q.fp32_stall_checks;
             p32.floor_tol = q.floor_tol;
+            p32.passthrough_tol = q.fp32_passthrough_tol;
             run_phase(e, false, p32);
             fbalp::KernelParams p64 = p;
             p64.warm_x = static_cast<const double*>(e->mid_x.ptr);
@@ -538,6 +548,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p64.clip_output = 1;
             p64.stall_checks = q.fp64_stall_checks;
             p64.floor_tol = q.floor_tol;
+            p64.passthrough_tol = 0.0;
             run_phase(e, true, p64);
         }
     } catch (const CudaError& ex) {

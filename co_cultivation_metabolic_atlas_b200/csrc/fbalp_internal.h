@@ -111,8 +111,8 @@ inline bool layout_aligned(const Layout& L) {
     return L.sched_a_off % 4 == 0 && L.sched_at_off % 4 == 0;
 }
 
-const void* kernel_symbol(bool fp64, int threads);
-cudaError_t launch_pdhg(bool fp64, int grid, int threads, size_t smem, cudaStream_t stream,
+const void* kernel_symbol(bool fp64, int threads, bool fast);
+cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
                         const KernelParams& p);
 
 }  // namespace fbalp

@@ -205,6 +205,14 @@ __device__ Metrics evaluate(const double* s_tot, double omega, double tol_p, dou
 // Stage one species' warp schedule (and, when the layout says so, its matrix
 // slices with 16-bit indices) into shared memory.
 template <typename T>
+__device__ __forceinline__ bool layout_is_fast(const Layout& L) {
+    return L.mat_smem && (L.smem_mask & 0x1ff) == 0x1ff;
+}
+
+// For fast layouts the staged 16-bit indices are ELEMENT offsets from the
+// start of dynamic shared memory (the gather target's base already added),
+// so a gather is one shared load of S[idx].
+template <typename T>
 __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned char* sm, int warps) {
     const int tid = threadIdx.x, nt = blockDim.x;
     int32_t* soa = reinterpret_cast<int32_t*>(sm + L.sched_a_off);
@@ -224,12 +232,15 @@ __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned ch
         T* tv = reinterpret_cast<T*>(sm + L.mat_at_val);
         const T* ga = Vals<T>::a(sp);
         const T* gt = Vals<T>::at(sp);
+        const bool fast = layout_is_fast<T>(L);
+        const int a_add = fast ? static_cast<int>(L.arr[kXbar] / sizeof(T)) : 0;
+        const int t_add = fast ? static_cast<int>(L.arr[kY] / sizeof(T)) : 0;
         for (int64_t e = tid; e < sp->a_elems; e += nt) {
-            ai[e] = static_cast<uint16_t>(sp->a_idx[e]);
+            ai[e] = static_cast<uint16_t>(sp->a_idx[e] + a_add);
             av[e] = ga[e];
         }
         for (int64_t e = tid; e < sp->at_elems; e += nt) {
-            ti[e] = static_cast<uint16_t>(sp->at_idx[e]);
+            ti[e] = static_cast<uint16_t>(sp->at_idx[e] + t_add);
             tv[e] = gt[e];
         }
     }
@@ -294,7 +305,7 @@ __device__ __forceinline__ void primal_pass_fast(const FastOffsets& o, T* xs, co
     const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
         const int4 sl = atlist[t];
-        const T g = slice_dot_fast<T>(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S + o.y, sl.z);
+        const T g = slice_dot_fast<T>(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S, sl.z);
         const int j = (sl.x << 5) + lane;
         if (j < n) {
             const T xo = S[o.x + j];
@@ -324,7 +335,7 @@ __device__ __forceinline__ void dual_pass_fast(const FastOffsets& o, T* ys, cons
     const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
         const int4 sl = alist[t];
-        const T h = slice_dot_fast<T>(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S + o.xbar, sl.z);
+        const T h = slice_dot_fast<T>(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S, sl.z);
         const int i = (sl.x << 5) + lane;
         if (i < m) {
             const T yo = S[o.y + i];
@@ -344,7 +355,10 @@ __device__ __forceinline__ void dual_pass_fast(const FastOffsets& o, T* ys, cons
     }
 }
 
-template <typename T, int MAXT>
+// FAST = every species of the launch has a fast layout (matrix and all
+// per-iteration arrays in shared memory); that variant carries no code for
+// the generic path, which keeps its register budget small.
+template <typename T, int MAXT, bool FAST>
 __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ double s_red[MAXT / 32][kRed];
@@ -395,7 +409,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
         const T* __restrict__ g_aval = Vals<T>::a(sp);
         const T* __restrict__ g_tval = Vals<T>::at(sp);
         // fast path: matrix and every per-iteration array in shared memory
-        const bool fast = mat_smem && (L.smem_mask & 0x1ff) == 0x1ff;
+        const bool fast = FAST || layout_is_fast<T>(L);
         const FastOffsets fo = fast_offsets<T>(L);
 
         // ---- load the instance (scaled, in the species' permuted order) ----
@@ -474,6 +488,13 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
             M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
             if (M.conv) status = p.final_status;
             else if (p.max_iters <= 0) status = M.nan ? kStatusNumerical : kStatusIterationLimit;
+            // FP32 phase: a warm start already at FP32-floor accuracy gains
+            // nothing from FP32 iterations (their rounding would only lose
+            // digits), so it is handed to the FP64 phase unchanged.
+            if (status < 0 && p.passthrough_tol > 0.0 && p.warm_x && !M.nan &&
+                fmax(fmax(M.primal / (1.0 + M.xinf), M.dual / (1.0 + M.cinf)), fmax(M.rgap, M.kgap)) <=
+                    p.passthrough_tol)
+                status = p.final_status;
         }
 
         int k = 0, it = 0, stall = 0;
@@ -489,9 +510,9 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
             const T w1 = T(1) - w;
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
             // primal pass: g = A^T y, projected step, extrapolation, Halpern
-            if (fast) {
+            if (FAST || fast) {
                 primal_pass_fast<T>(fo, A.xs, atlist, tw0, tw1, n, lane, tau, w, w1, rho, check, pdx2, pdxa2);
-            } else {
+            } else if (!FAST) {
                 for (int t = tw0; t < tw1; ++t) {
                     const int4 sl = atlist[t];
                     const T g = mat_smem ? slice_dot<T, T, uint16_t, false>(s_tidx, s_tval, sl.y, sl.z, lane, A.y)
@@ -517,9 +538,9 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
             }
             __syncthreads();
             // dual pass: h = A xbar, projected dual step, Halpern
-            if (fast) {
+            if (FAST || fast) {
                 dual_pass_fast<T>(fo, A.ys, alist, aw0, aw1, m, neq, lane, sigma, w, w1, rho, check, pdy2, pdya2);
-            } else {
+            } else if (!FAST) {
                 for (int t = aw0; t < aw1; ++t) {
                     const int4 sl = alist[t];
                     const T h = mat_smem ? slice_dot<T, T, uint16_t, false>(s_aidx, s_aval, sl.y, sl.z, lane, A.xbar)
@@ -621,17 +642,22 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
         }
 
         // ---- results in original units and original order ----
+        // (an FP32 phase that stopped at its iteration-0 test passes the FP64
+        // warm start through untouched)
+        const bool pass = p.passthrough_tol > 0.0 && it == 0 && p.warm_x != nullptr;
         for (int j = tid; j < n; j += nthreads) {
             const int jo = sp->col_perm[j];
-            double xv = static_cast<double>(A.xs[j]) * sp->dc[j];
+            double xv = pass ? p.warm_x[coff + jo] : static_cast<double>(A.xs[j]) * sp->dc[j];
             if (p.clip_output) {
                 const double lv = p.lower[coff + jo], uv = p.upper[coff + jo];
                 xv = xv < lv ? lv : (xv > uv ? uv : xv);
             }
             p.out_x[coff + jo] = xv;
         }
-        for (int i = tid; i < m; i += nthreads)
-            p.out_y[roff + sp->row_perm[i]] = static_cast<double>(A.ys[i]) * sp->dr[i];
+        for (int i = tid; i < m; i += nthreads) {
+            const int io = sp->row_perm[i];
+            p.out_y[roff + io] = (pass && p.warm_y) ? p.warm_y[roff + io] : static_cast<double>(A.ys[i]) * sp->dr[i];
+        }
         if (tid == 0) {
             double* mo = p.out_metrics + static_cast<int64_t>(inst) * kMetrics;
             mo[0] = M.primal;
@@ -650,30 +676,47 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
     }
 }
 
-template __global__ void pdhg_persistent<float, 512>(KernelParams);
-template __global__ void pdhg_persistent<double, 512>(KernelParams);
-template __global__ void pdhg_persistent<float, 1024>(KernelParams);
-template __global__ void pdhg_persistent<double, 1024>(KernelParams);
+#define FBALP_INSTANTIATE(T, MAXT)                                         \
+    template __global__ void pdhg_persistent<T, MAXT, false>(KernelParams); \
+    template __global__ void pdhg_persistent<T, MAXT, true>(KernelParams);
+FBALP_INSTANTIATE(float, 512)
+FBALP_INSTANTIATE(double, 512)
+FBALP_INSTANTIATE(float, 1024)
+FBALP_INSTANTIATE(double, 1024)
+#undef FBALP_INSTANTIATE
 
-// Blocks of up to 512 threads use the variant with a 128-register budget;
-// larger blocks the 64-register one.
-const void* kernel_symbol(bool fp64, int threads) {
-    if (threads <= 512)
-        return fp64 ? reinterpret_cast<const void*>(&pdhg_persistent<double, 512>)
-                    : reinterpret_cast<const void*>(&pdhg_persistent<float, 512>);
-    return fp64 ? reinterpret_cast<const void*>(&pdhg_persistent<double, 1024>)
-                : reinterpret_cast<const void*>(&pdhg_persistent<float, 1024>);
+// Blocks of up to 512 threads use the variant with a 128-register budget,
+// larger blocks the 64-register one; `fast` selects the shared-memory-only
+// variant.
+template <int MAXT>
+static const void* symbol_for(bool fp64, bool fast) {
+    if (fp64)
+        return fast ? reinterpret_cast<const void*>(&pdhg_persistent<double, MAXT, true>)
+                    : reinterpret_cast<const void*>(&pdhg_persistent<double, MAXT, false>);
+    return fast ? reinterpret_cast<const void*>(&pdhg_persistent<float, MAXT, true>)
+                : reinterpret_cast<const void*>(&pdhg_persistent<float, MAXT, false>);
 }
 
-cudaError_t launch_pdhg(bool fp64, int grid, int threads, size_t smem, cudaStream_t stream,
-                        const KernelParams& p) {
-    if (threads <= 512) {
-        if (fp64) pdhg_persistent<double, 512><<<grid, threads, smem, stream>>>(p);
-        else pdhg_persistent<float, 512><<<grid, threads, smem, stream>>>(p);
+const void* kernel_symbol(bool fp64, int threads, bool fast) {
+    return threads <= 512 ? symbol_for<512>(fp64, fast) : symbol_for<1024>(fp64, fast);
+}
+
+template <int MAXT>
+static void launch_for(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
+                       const KernelParams& p) {
+    if (fp64) {
+        if (fast) pdhg_persistent<double, MAXT, true><<<grid, threads, smem, stream>>>(p);
+        else pdhg_persistent<double, MAXT, false><<<grid, threads, smem, stream>>>(p);
     } else {
-        if (fp64) pdhg_persistent<double, 1024><<<grid, threads, smem, stream>>>(p);
-        else pdhg_persistent<float, 1024><<<grid, threads, smem, stream>>>(p);
+        if (fast) pdhg_persistent<float, MAXT, true><<<grid, threads, smem, stream>>>(p);
+        else pdhg_persistent<float, MAXT, false><<<grid, threads, smem, stream>>>(p);
     }
+}
+
+cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
+                        const KernelParams& p) {
+    if (threads <= 512) launch_for<512>(fp64, fast, grid, threads, smem, stream, p);
+    else launch_for<1024>(fp64, fast, grid, threads, smem, stream, p);
     return cudaGetLastError();
 }
 

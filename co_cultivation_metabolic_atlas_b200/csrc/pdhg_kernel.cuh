@@ -100,6 +100,8 @@ struct KernelParams {
     int32_t stall_checks;         // >0: stall rule after this many
                                   // non-improving convergence tests
     double floor_tol;             // FP64 phase: tolerance accepted after a stall
+    double passthrough_tol;       // FP32 phase: warm starts with error <= this
+                                  // skip the phase unchanged (0 = never)
 };
 
 }  // namespace fbalp

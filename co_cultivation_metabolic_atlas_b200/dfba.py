@@ -41,9 +41,14 @@ class DeviceCommunity:
 
     def __init__(self, models, medium, biomass, *, dt=0.05, capacity=CARRYING_CAPACITY,
                  options: EngineOptions | None = None, config: SolveConfig | None = None,
-                 warm_start: str = "previous", device=None):
-        if warm_start not in ("cold", "previous"):
-            raise ValueError("warm_start must be 'cold' or 'previous'")
+                 warm_start: str = "previous", learned=None, horizon_steps: int = 960, device=None):
+        if warm_start not in ("cold", "previous", "learned"):
+            raise ValueError("warm_start must be 'cold', 'previous' or 'learned'")
+        if warm_start == "learned" and learned is None:
+            raise ValueError("warm_start='learned' needs a LearnedWarmStart")
+        self.learned = learned
+        self.horizon_steps = int(horizon_steps)
+        self.step_index = 0
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         dev = self.device
         self.models = models
@@ -107,11 +112,15 @@ class DeviceCommunity:
 
     def solve(self):
         out = self._bufs[self._which]
-        warm = self.prev if (self.warm_start == "previous" and self.prev is not None) else None
-        res = self.engine.solve(warm_x=None if warm is None else warm.x[:self.total_cols],
-                                warm_y=None if warm is None else warm.y[:self.total_rows],
-                                warm_omega=None if warm is None else warm.omega,
-                                config=self.config, out=out)
+        if self.warm_start == "learned":
+            wx, wy, wo = self.learned.propose(self, self.step_index / self.horizon_steps)
+            res = self.engine.solve(warm_x=wx, warm_y=wy, warm_omega=wo, config=self.config, out=out)
+        else:
+            warm = self.prev if (self.warm_start == "previous" and self.prev is not None) else None
+            res = self.engine.solve(warm_x=None if warm is None else warm.x[:self.total_cols],
+                                    warm_y=None if warm is None else warm.y[:self.total_rows],
+                                    warm_omega=None if warm is None else warm.omega,
+                                    config=self.config, out=out)
         self._which ^= 1
         self.prev = res
         self.result = res
@@ -134,6 +143,7 @@ class DeviceCommunity:
             contrib = v * X0[:, s:s + 1] * self.dt
             delta.index_add_(1, mm["ids"], contrib)
         self.medium = torch.clamp(self.medium + delta, min=0.0)
+        self.step_index += 1
 
     def certified(self, res: SolveResult):
         """Count of LPs that meet the engine's FP64 tolerances AND the

@@ -53,6 +53,7 @@ class SolveConfig:
     fp32_stall_checks: int = 6
     fp64_stall_checks: int = 8
     floor_tol: float = 1e-7
+    fp32_passthrough_tol: float = 1e-3
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -67,7 +68,7 @@ class SolveConfig:
                 raise ValueError(f"{name} must be an integer")
             setattr(p, name, int(value))
         for name in ("tol_primal", "tol_dual", "tol_gap", "fp32_tol_primal", "fp32_tol_dual",
-                     "fp32_tol_gap", "reflection", "floor_tol"):
+                     "fp32_tol_gap", "reflection", "floor_tol", "fp32_passthrough_tol"):
             setattr(p, name, float(getattr(self, name)))
         p.restarts = 1 if self.restarts else 0
         return p
@@ -82,6 +83,7 @@ class EngineOptions:
     blocks_per_sm: int = 0
     max_dynamic_smem: int = 0
     stage_matrix: bool = True
+    fp64_max_dynamic_smem: int = 0
 
     def native(self) -> N.Options:
         o = N.default_options()
@@ -92,6 +94,7 @@ class EngineOptions:
         o.blocks_per_sm = int(self.blocks_per_sm)
         o.max_dynamic_smem = int(self.max_dynamic_smem)
         o.stage_matrix = 1 if self.stage_matrix else 0
+        o.fp64_max_dynamic_smem = int(self.fp64_max_dynamic_smem)
         return o
 
 

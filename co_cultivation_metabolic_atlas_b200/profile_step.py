@@ -1,0 +1,37 @@
+"""Profiling driver: run a few warm-started dFBA steps of the synthetic
+community so that an external profiler can capture the PDHG phase kernels.
+
+    python -m co_cultivation_metabolic_atlas_b200.profile_step --envs 512 --steps 3
+"""
+
+from __future__ import annotations
+
+import argparse
+
+import torch
+
+from . import synthetic as syn
+from .dfba import DeviceCommunity
+from .engine import EngineOptions, SolveConfig
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--envs", type=int, default=512)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--precision", default="mixed")
+    ap.add_argument("--warps", type=int, default=16)
+    args = ap.parse_args()
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(args.envs)
+    com = DeviceCommunity(models, medium, biomass, config=SolveConfig(precision=args.precision),
+                          options=EngineOptions(warps_per_block=args.warps), warm_start="previous")
+    for _ in range(args.steps):
+        st = com.step()
+    torch.cuda.synchronize()
+    print("certified", int(st.certified.item()), "of", st.lps)
+    com.close()
+
+
+if __name__ == "__main__":
+    main()

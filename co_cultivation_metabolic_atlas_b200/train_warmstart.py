@@ -1,0 +1,96 @@
+"""Train the learned warm start on the engine's own dFBA rollouts.
+
+    python -m co_cultivation_metabolic_atlas_b200.train_warmstart --out PATH
+        [--envs 4096] [--steps 48] [--seeds 1 2 ...] [--epochs 20]
+
+Data: for each training seed, ``--envs`` environments are rolled forward
+``--steps`` dFBA steps with previous-step warm starts; every certified
+(environment, step) contributes one (state features -> concatenated x, y of
+the three species) pair.  The seeds must differ from the evaluation seeds.
+The artifact holds the network weights, the codec, the architecture and a
+hash of the species matrices it was trained for.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import time
+
+import numpy as np
+import torch
+
+from . import synthetic as syn
+from .engine import SolveConfig
+from .warmstart import MLP, Codec, LearnedWarmStart, collect, solution_layout, train
+
+HIDDEN = (512, 512, 512, 512)
+N_FEATURES = 44
+
+
+def models_digest(models):
+    h = hashlib.sha256()
+    for m in models:
+        for a in (m.S.data, m.S.indices, m.S.indptr, m.lower, m.upper, m.cost, m.medium_columns, m.medium_ids,
+                  m.vmax, m.km):
+            h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def build_dataset(models, *, envs, steps, seeds, config=None, device=None, log=print):
+    F, T, OM = [], [], []
+    for sd in seeds:
+        t0 = time.perf_counter()
+        f, t, ok, om = collect(models, envs=envs, steps=steps, seed=sd, config=config, device=device)
+        F.append(f[ok])
+        T.append(t[ok])
+        OM.append(om[ok])
+        log(f"seed {sd}: {int(ok.sum())}/{len(ok)} certified pairs in {time.perf_counter() - t0:.1f} s")
+    return torch.cat(F), torch.cat(T), torch.cat(OM)
+
+
+def fit(models, F, T, OM, *, epochs=20, batch=4096, lr=1e-3, lr_final=5e-5, seed=0, device=None, log=print):
+    omega = OM.median(dim=0).values
+    codec = Codec.fit(F, T, omega)
+    width = T.shape[1]
+    net = MLP([N_FEATURES, *HIDDEN, width], device=device, seed=seed)
+    losses = train(net, codec.features(F), codec.targets(T), epochs=epochs, batch=min(batch, F.shape[0]), lr=lr,
+                   lr_final=lr_final, seed=seed, log=log)
+    return LearnedWarmStart(net, codec, models), losses
+
+
+def save(path, ws: LearnedWarmStart, models, meta):
+    torch.save({"mlp": ws.mlp.state_dict(), "codec": ws.codec.state_dict(), "digest": models_digest(models),
+                "meta": meta}, path)
+
+
+def load(path, models, device=None):
+    blob = torch.load(path, map_location="cpu", weights_only=True)
+    if blob["digest"] != models_digest(models):
+        raise ValueError("warm-start artifact was trained for different species matrices")
+    dev = torch.device(device) if device is not None else torch.device("cuda")
+    sd = blob["mlp"]
+    net = MLP(sd["dims"], device=dev)
+    net.load_state_dict(sd)
+    codec = Codec.from_state(blob["codec"], dev)
+    return LearnedWarmStart(net, codec, models), blob.get("meta", {})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--envs", type=int, default=4096)
+    ap.add_argument("--steps", type=int, default=48)
+    ap.add_argument("--seeds", type=int, nargs="+", default=[101, 102])
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--model-seed", type=int, default=0)
+    args = ap.parse_args()
+    models = syn.community_models(seed=args.model_seed)
+    F, T, OM = build_dataset(models, envs=args.envs, steps=args.steps, seeds=args.seeds, config=SolveConfig())
+    ws, losses = fit(models, F, T, OM, epochs=args.epochs)
+    save(args.out, ws, models, {"pairs": int(F.shape[0]), "losses": losses, "seeds": args.seeds})
+    print(f"saved {args.out}: {F.shape[0]} pairs, final mse {losses[-1]:.4e}")
+
+
+if __name__ == "__main__":
+    main()

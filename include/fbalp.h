@@ -88,6 +88,9 @@ typedef struct fbalp_options {
     int32_t stage_matrix;      /* 1 (default): stage the species matrix into
                                   shared memory when it fits; 0: stream it
                                   from L2 every iteration                   */
+    int32_t fp64_max_dynamic_smem; /* cap for the FP64 phase (0 = same as
+                                  max_dynamic_smem); a smaller cap spills the
+                                  cold arrays and fits more CTAs per SM     */
 } fbalp_options;
 
 /* Solve parameters.  Replaces `iterations` / `check_interval` of
@@ -114,6 +117,9 @@ typedef struct fbalp_solve_params {
                                     OPTIMAL (an FP64 rounding floor above the
                                     tight tolerances; 0 = never)             */
     double floor_tol;            /* default 1e-7 = the reference's gap gate   */
+    double fp32_passthrough_tol; /* MIXED: a warm start whose FP64 KKT error is
+                                    already <= this skips the FP32 phase
+                                    unchanged (default 1e-3; 0 = never)      */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);

@@ -183,3 +183,20 @@ def test_repeat_solves_are_deterministic():
     b = run_single(model.S, 300, lower, upper, [model.cost] * 6)
     np.testing.assert_array_equal(a["x"], b["x"])
     np.testing.assert_array_equal(a["iters"], b["iters"])
+
+
+def test_mixed_precision_keeps_an_accurate_fp64_warm_start():
+    """A warm start already at FP32-floor accuracy skips the FP32 phase and
+    reaches the FP64 phase unrounded: re-solving from a certified solution
+    takes no iterations and returns it bit for bit."""
+    model, lower, upper = syn.single_species_workload(3, m=300, n=650)
+    eng = engine([(model.S, 300)])
+    eng.set_instances(np.zeros(3, np.int32), flat(lower), flat(upper), flat([model.cost] * 3))
+    first = eng.solve(config=cfg(precision="mixed"))
+    x0 = first.x[:eng.total_cols].clone()
+    y0 = first.y[:eng.total_rows].clone()
+    again = eng.solve(warm_x=x0, warm_y=y0, warm_omega=first.omega, config=cfg(precision="mixed"))
+    assert again.status.cpu().tolist() == [0, 0, 0]
+    assert again.iterations.cpu().tolist() == [0, 0, 0]
+    np.testing.assert_array_equal(again.x[:eng.total_cols].cpu().numpy(), x0.cpu().numpy())
+    eng.close()
