@@ -50,8 +50,44 @@ struct SpeciesHost {
     fbalp::Scaling scaling;
     std::vector<int32_t> row_perm, col_perm;  // new -> old
     fbalp::Sell A, AT;
+    fbalp::Sell Araw, ATraw;  // same slices, unscaled values
     std::vector<int32_t> a_sched_off, a_sched, at_sched_off, at_sched;
 };
+
+// FP32 "hi" copy of unscaled SELL values plus, per (new-numbered) row, the
+// list of FP64 "lo" remainders of the entries FP32 cannot represent exactly.
+struct HiLo {
+    std::vector<float> hi;
+    std::vector<int32_t> lo_ptr, lo_idx;
+    std::vector<double> lo_val;
+};
+
+static HiLo split_hi_lo(const fbalp::Sell& raw, int32_t rows) {
+    HiLo h;
+    h.hi.resize(raw.val.size());
+    h.lo_ptr.assign(rows + 1, 0);
+    std::vector<std::vector<std::pair<int32_t, double>>> per(rows);
+    for (int32_t sl = 0; sl < raw.nslices; ++sl) {
+        const int32_t len = raw.length[sl];
+        for (int32_t k = 0; k < len; ++k)
+            for (int32_t lane = 0; lane < 32; ++lane) {
+                const int32_t e = raw.off[sl] + k * 32 + lane;
+                const float f = static_cast<float>(raw.val[e]);
+                h.hi[e] = f;
+                const double lo = raw.val[e] - static_cast<double>(f);
+                const int32_t r = sl * 32 + lane;
+                if (lo != 0.0 && r < rows) per[r].emplace_back(raw.idx[e], lo);
+            }
+    }
+    for (int32_t r = 0; r < rows; ++r) {
+        for (auto& pr : per[r]) {
+            h.lo_idx.push_back(pr.first);
+            h.lo_val.push_back(pr.second);
+        }
+        h.lo_ptr[r + 1] = static_cast<int32_t>(h.lo_idx.size());
+    }
+    return h;
+}
 
 struct Buffer {
     void* ptr = nullptr;
@@ -229,6 +265,9 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             for (int32_t j = 0; j < sh.n; ++j) col_new[sh.col_perm[j]] = j;
             sh.A = fbalp::build_sell(a, sh.row_perm, col_new, sh.scaling.dr, sh.scaling.dc, sh.n);
             sh.AT = fbalp::build_sell(at, sh.col_perm, row_new, sh.scaling.dc, sh.scaling.dr, sh.m);
+            const std::vector<double> ones_m(sh.m, 1.0), ones_n(sh.n, 1.0);
+            sh.Araw = fbalp::build_sell(a, sh.row_perm, col_new, ones_m, ones_n, sh.n);
+            sh.ATraw = fbalp::build_sell(at, sh.col_perm, row_new, ones_n, ones_m, sh.m);
             fbalp::warp_schedule(sh.A, o.warps_per_block, &sh.a_sched_off, &sh.a_sched);
             fbalp::warp_schedule(sh.AT, o.warps_per_block, &sh.at_sched_off, &sh.at_sched);
             E->species.push_back(std::move(sh));
@@ -269,6 +308,15 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             for (int32_t i = 0; i < sh.m; ++i) drn[i] = sh.scaling.dr[sh.row_perm[i]];
             for (int32_t j = 0; j < sh.n; ++j) dcn[j] = sh.scaling.dc[sh.col_perm[j]];
             d.dr = dev_upload(drn, E->owned);
+            HiLo ha = split_hi_lo(sh.Araw, sh.m), ht = split_hi_lo(sh.ATraw, sh.n);
+            d.a_hi = dev_upload(ha.hi, E->owned);
+            d.at_hi = dev_upload(ht.hi, E->owned);
+            d.lo_a_ptr = dev_upload(ha.lo_ptr, E->owned);
+            d.lo_a_idx = dev_upload(ha.lo_idx, E->owned);
+            d.lo_a_val = dev_upload(ha.lo_val, E->owned);
+            d.lo_at_ptr = dev_upload(ht.lo_ptr, E->owned);
+            d.lo_at_idx = dev_upload(ht.lo_idx, E->owned);
+            d.lo_at_val = dev_upload(ht.lo_val, E->owned);
             d.dc = dev_upload(dcn, E->owned);
             d.eta = sh.scaling.eta;
             E->dev_species_host.push_back(d);
@@ -382,16 +430,30 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     layouts.assign(e->species.size(), fbalp::Layout{});
     int64_t dyn = 0, slab = 0;
     bool all_fast = true;
+    // FP64: the unscaled staged layout is used only when every species of
+    // the batch fits it (one kernel variant per launch)
+    bool unscaled = fp64 && e->opt.stage_matrix != 0;
+    if (unscaled)
+        for (size_t s = 0; s < e->species.size(); ++s) {
+            if (!used[s]) continue;
+            const SpeciesHost& sh = e->species[s];
+            if (!fbalp::plan_layout_unscaled(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                             sh.A.off.back(), sh.AT.off.back(), cap).layout.unscaled)
+                unscaled = false;
+        }
     for (size_t s = 0; s < e->species.size(); ++s) {
         if (!used[s]) continue;
         const SpeciesHost& sh = e->species[s];
-        fbalp::LayoutPlan P = fbalp::plan_layout(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices,
-                                                 sh.AT.nslices, sh.A.off.back(), sh.AT.off.back(),
-                                                 esz, cap, e->opt.stage_matrix != 0);
+        fbalp::LayoutPlan P = unscaled
+            ? fbalp::plan_layout_unscaled(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                          sh.A.off.back(), sh.AT.off.back(), cap)
+            : fbalp::plan_layout(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                 sh.A.off.back(), sh.AT.off.back(), esz, cap, !fp64 && e->opt.stage_matrix != 0);
         if (P.smem_bytes > cap) throw CudaError("species schedule does not fit into shared memory");
         if (!fbalp::layout_aligned(P.layout)) throw CudaError("internal error: misaligned shared-memory layout");
         layouts[s] = P.layout;
-        all_fast = all_fast && P.layout.mat_smem && (P.layout.smem_mask & 0x1ff) == 0x1ff;
+        all_fast = all_fast && (fp64 ? unscaled
+                                     : (P.layout.mat_smem && (P.layout.smem_mask & 0x1ff) == 0x1ff));
         dyn = std::max(dyn, P.smem_bytes);
         slab = std::max(slab, P.slab_bytes);
     }

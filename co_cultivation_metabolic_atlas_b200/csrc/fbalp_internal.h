@@ -31,7 +31,7 @@ constexpr double kStallFloor = 1.0;
 // Element counts of the per-instance arrays (gather targets carry a zero
 // slot at index n / m), in shared-memory priority order.
 inline void array_elems(int n, int m, int64_t* s) {
-    const int64_t v[kArrayCount] = {n + 1, m + 1, n, n, m, n, n, n, m, n + 1, m + 1};
+    const int64_t v[kArrayCount] = {n + 1, m + 1, n, n, m, n, n, n, m, n + 1, m + 1, 0};
     for (int a = 0; a < kArrayCount; ++a) s[a] = v[a];
 }
 
@@ -95,6 +95,70 @@ inline LayoutPlan plan_layout(int n, int m, int warps, int a_nslices, int at_nsl
         off += align_up(esz * at_elems, 16);
     }
     for (int a = 2; a < kArrayCount; ++a) place(a);
+    P.smem_bytes = off;
+    P.slab_bytes = slab;
+    return P;
+}
+
+// FP64 layout with the unscaled FP32 matrix staged: schedule lists, the two
+// FP64 gather targets z (n+1) and w (m+1), the matrix slices (16-bit indices,
+// FP32 values), then x, xa and the remaining arrays while they fit.  Returns
+// a plan with unscaled = 0 when the targets and the matrix do not fit.
+inline LayoutPlan plan_layout_unscaled(int n, int m, int warps, int a_nslices, int at_nslices,
+                                       int64_t a_elems, int64_t at_elems, int64_t smem_cap) {
+    LayoutPlan P{};
+    Layout& L = P.layout;
+    int64_t off = 0;
+    L.sched_a_off = off;
+    off += 4 * (warps + 1);
+    L.sched_at_off = off;
+    off += 4 * (warps + 1);
+    off = align_up(off, 16);
+    L.list_a = off;
+    off += static_cast<int64_t>(sizeof(int4)) * a_nslices;
+    L.list_at = off;
+    off += static_cast<int64_t>(sizeof(int4)) * at_nslices;
+    off = align_up(off, 16);
+    const int esz = 8;
+    const int64_t need = align_up((int64_t(n) + 1) * esz, 16) + align_up((int64_t(m) + 1) * esz, 16) +
+                         align_up(2 * a_elems, 16) + align_up(2 * at_elems, 16) + align_up(4 * a_elems, 16) +
+                         align_up(4 * at_elems, 16);
+    const int64_t max_word = (int64_t(1) << 16) - 1;
+    if (off + need > smem_cap || (off + need) / esz > max_word) return P;  // unscaled stays 0
+    L.unscaled = 1;
+    L.mat_smem = 1;
+    L.smem_mask = 0;
+    int64_t e[kArrayCount];
+    array_elems(n, m, e);
+    e[kW] = m + 1;
+    auto put = [&](int a) {
+        L.arr[a] = off;
+        L.smem_mask |= 1 << a;
+        off += align_up(e[a] * esz, 16);
+    };
+    put(kXbar);
+    put(kW);
+    L.mat_a_idx = off;
+    off += align_up(2 * a_elems, 16);
+    L.mat_at_idx = off;
+    off += align_up(2 * at_elems, 16);
+    L.mat_a_val = off;
+    off += align_up(4 * a_elems, 16);
+    L.mat_at_val = off;
+    off += align_up(4 * at_elems, 16);
+    int64_t slab = 0;
+    const int order[] = {kX, kXa, kY, kYa, kC, kL, kU, kB, kXs, kYs};
+    for (int a : order) {
+        const int64_t bytes = align_up(e[a] * esz, 16);
+        if (off + bytes <= smem_cap) {
+            L.arr[a] = off;
+            L.smem_mask |= 1 << a;
+            off += bytes;
+        } else {
+            L.arr[a] = slab;
+            slab += bytes;
+        }
+    }
     P.smem_bytes = off;
     P.slab_bytes = slab;
     return P;

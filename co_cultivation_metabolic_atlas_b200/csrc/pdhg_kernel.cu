@@ -85,7 +85,7 @@ __device__ __forceinline__ double slice_dot64(const int32_t* __restrict__ idx,
 }
 
 template <typename T> struct Arrays {
-    T *xbar, *y, *x, *xa, *ya, *cs, *ls, *us, *bs, *xs, *ys;
+    T *xbar, *y, *x, *xa, *ya, *cs, *ls, *us, *bs, *xs, *ys, *w;
 };
 
 // Sums for q < kRedSums, maxima above.  Deterministic order.
@@ -225,7 +225,23 @@ __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned ch
     int4* lt = reinterpret_cast<int4*>(sm + L.list_at);
     for (int t = tid; t < sp->a_nslices; t += nt) la[t] = sp->a_list[t];
     for (int t = tid; t < sp->at_nslices; t += nt) lt[t] = sp->at_list[t];
-    if (L.mat_smem) {
+    if (L.unscaled) {
+        // unscaled FP32 values; indices pre-offset to the FP64 gather targets
+        // z (A pass) and w (A^T pass)
+        uint16_t* ai = reinterpret_cast<uint16_t*>(sm + L.mat_a_idx);
+        uint16_t* ti = reinterpret_cast<uint16_t*>(sm + L.mat_at_idx);
+        float* av = reinterpret_cast<float*>(sm + L.mat_a_val);
+        float* tv = reinterpret_cast<float*>(sm + L.mat_at_val);
+        const int a_add = static_cast<int>(L.arr[kXbar] / 8), t_add = static_cast<int>(L.arr[kW] / 8);
+        for (int64_t e = tid; e < sp->a_elems; e += nt) {
+            ai[e] = static_cast<uint16_t>(sp->a_idx[e] + a_add);
+            av[e] = sp->a_hi[e];
+        }
+        for (int64_t e = tid; e < sp->at_elems; e += nt) {
+            ti[e] = static_cast<uint16_t>(sp->at_idx[e] + t_add);
+            tv[e] = sp->at_hi[e];
+        }
+    } else if (L.mat_smem) {
         uint16_t* ai = reinterpret_cast<uint16_t*>(sm + L.mat_a_idx);
         uint16_t* ti = reinterpret_cast<uint16_t*>(sm + L.mat_at_idx);
         T* av = reinterpret_cast<T*>(sm + L.mat_a_val);
@@ -355,11 +371,123 @@ __device__ __forceinline__ void dual_pass_fast(const FastOffsets& o, T* ys, cons
     }
 }
 
+// ---- unscaled FP64 passes (matrix staged as FP32 + FP64 remainders) ----
+// The A^T pass computes (A~^T y)_j = dc_j * sum_i A_ij w_i with w = dr * y,
+// the A pass (A~ xbar)_i = dr_i * sum_j A_ij z_j with z = dc * xbar; the
+// staged A_ij are the FP32 parts and the per-row remainder lists restore
+// the FP64 products.  Owned data (c, l, u, y, ...) may live in the global
+// slab; it is loaded before the slice's dot product so that its latency
+// overlaps the shared-memory work.
+__device__ __forceinline__ double slice_dot_hi(const uint16_t* ip, const float* vp, const double* S, int len) {
+    double acc = 0.0;
+    int k = 0;
+    for (; k + 4 <= len; k += 4, ip += 128, vp += 128) {
+        const int i0 = ip[0], i1 = ip[32], i2 = ip[64], i3 = ip[96];
+        const float v0 = vp[0], v1 = vp[32], v2 = vp[64], v3 = vp[96];
+        acc = fma(static_cast<double>(v0), S[i0], acc);
+        acc = fma(static_cast<double>(v1), S[i1], acc);
+        acc = fma(static_cast<double>(v2), S[i2], acc);
+        acc = fma(static_cast<double>(v3), S[i3], acc);
+    }
+    for (; k < len; ++k, ip += 32, vp += 32) acc = fma(static_cast<double>(vp[0]), S[ip[0]], acc);
+    return acc;
+}
+
+__device__ __forceinline__ void primal_pass_unscaled(const DevSpecies* sp, const Layout& L, Arrays<double>& A,
+                                                     const int4* atlist, int t0, int t1, int n, int lane,
+                                                     double tau, double w, double w1, double rho, bool check,
+                                                     double& pdx2, double& pdxa2) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const double* const S = reinterpret_cast<const double*>(dyn_smem);
+    const uint16_t* const TI = reinterpret_cast<const uint16_t*>(dyn_smem + L.mat_at_idx);
+    const float* const TV = reinterpret_cast<const float*>(dyn_smem + L.mat_at_val);
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = atlist[t];
+        const int j = (sl.x << 5) + lane;
+        const bool own = j < n;
+        double cj = 0, lj = 0, uj = 0, xo = 0, xav = 0, dcj = 0;
+        int lb = 0, le = 0;
+        if (own) {
+            cj = A.cs[j];
+            lj = A.ls[j];
+            uj = A.us[j];
+            xo = A.x[j];
+            xav = A.xa[j];
+            dcj = sp->dc[j];
+            lb = sp->lo_at_ptr[j];
+            le = sp->lo_at_ptr[j + 1];
+        }
+        double acc = slice_dot_hi(TI + sl.y + lane, TV + sl.y + lane, S, sl.z);
+        if (own) {
+            for (int k = lb; k < le; ++k) acc = fma(sp->lo_at_val[k], A.w[sp->lo_at_idx[k]], acc);
+            const double g = dcj * acc;
+            const double xn = clampT(xo - tau * (cj - g), lj, uj);
+            const double xb = xn + xn - xo;
+            A.xbar[j] = dcj * xb;  // z
+            const double xh = (rho == 1.0) ? xb : (1.0 + rho) * xn - rho * xo;
+            A.x[j] = w * xh + w1 * xav;
+            if (check) {
+                A.xs[j] = xn;
+                const double d = xn - xo, da = xn - xav;
+                pdx2 += d * d;
+                pdxa2 += da * da;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void dual_pass_unscaled(const DevSpecies* sp, const Layout& L, Arrays<double>& A,
+                                                   const int4* alist, int t0, int t1, int m, int neq, int lane,
+                                                   double sigma, double w, double w1, double rho, bool check,
+                                                   double& pdy2, double& pdya2) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const double* const S = reinterpret_cast<const double*>(dyn_smem);
+    const uint16_t* const AI = reinterpret_cast<const uint16_t*>(dyn_smem + L.mat_a_idx);
+    const float* const AV = reinterpret_cast<const float*>(dyn_smem + L.mat_a_val);
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = alist[t];
+        const int i = (sl.x << 5) + lane;
+        const bool own = i < m;
+        double yo = 0, yav = 0, bi = 0, dri = 0;
+        int lb = 0, le = 0;
+        if (own) {
+            yo = A.y[i];
+            yav = A.ya[i];
+            bi = A.bs[i];
+            dri = sp->dr[i];
+            lb = sp->lo_a_ptr[i];
+            le = sp->lo_a_ptr[i + 1];
+        }
+        double acc = slice_dot_hi(AI + sl.y + lane, AV + sl.y + lane, S, sl.z);
+        if (own) {
+            for (int k = lb; k < le; ++k) acc = fma(sp->lo_a_val[k], A.xbar[sp->lo_a_idx[k]], acc);
+            const double h = dri * acc;
+            double yn = yo + sigma * (bi - h);
+            if (i >= neq && yn > 0.0) yn = 0.0;
+            const double yh = (rho == 1.0) ? yn + yn - yo : (1.0 + rho) * yn - rho * yo;
+            const double ynew = w * yh + w1 * yav;
+            A.y[i] = ynew;
+            A.w[i] = dri * ynew;
+            if (check) {
+                A.ys[i] = yn;
+                const double d = yn - yo, da = yn - yav;
+                pdy2 += d * d;
+                pdya2 += da * da;
+            }
+        }
+    }
+}
+
 // FAST = every species of the launch has a fast layout (matrix and all
 // per-iteration arrays in shared memory); that variant carries no code for
 // the generic path, which keeps its register budget small.
-template <typename T, int MAXT, bool FAST>
+// MODE 0: generic; 1 (FAST): matrix and every per-iteration array in shared
+// memory, scaled values; 2 (UNSCALED, FP64 only): unscaled FP32 matrix with
+// FP64 remainders staged, FP64 gather targets in shared memory.
+template <typename T, int MAXT, int MODE>
 __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
+    constexpr bool FAST = MODE == 1;
+    constexpr bool UNS = MODE == 2;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ double s_red[MAXT / 32][kRed];
     __shared__ double s_tot[kRed];
@@ -389,7 +517,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
         }
         Arrays<T> A;
         {
-            T** ptrs[kArrayCount] = {&A.xbar, &A.y, &A.x, &A.xa, &A.ya, &A.cs, &A.ls, &A.us, &A.bs, &A.xs, &A.ys};
+            T** ptrs[kArrayCount] = {&A.xbar, &A.y, &A.x, &A.xa, &A.ya, &A.cs, &A.ls, &A.us, &A.bs, &A.xs, &A.ys, &A.w};
             const int mask = L.smem_mask;
 #pragma unroll
             for (int a = 0; a < kArrayCount; ++a)
@@ -409,7 +537,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
         const T* __restrict__ g_aval = Vals<T>::a(sp);
         const T* __restrict__ g_tval = Vals<T>::at(sp);
         // fast path: matrix and every per-iteration array in shared memory
-        const bool fast = FAST || layout_is_fast<T>(L);
+        const bool fast = FAST || (!UNS && layout_is_fast<T>(L));
         const FastOffsets fo = fast_offsets<T>(L);
 
         // ---- load the instance (scaled, in the species' permuted order) ----
@@ -443,12 +571,14 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
             A.y[i] = static_cast<T>(y0);
             A.ya[i] = static_cast<T>(y0);
             A.ys[i] = static_cast<T>(y0);
+            if (UNS) A.w[i] = static_cast<T>(dri * static_cast<T>(y0));
         }
         if (tid == 0) {
             A.xbar[n] = T(0);
             A.xs[n] = T(0);
             A.y[m] = T(0);
             A.ys[m] = T(0);
+            if (UNS) A.w[m] = T(0);
         }
         bad = __syncthreads_or(bad);
         double omega = 1.0;
@@ -510,7 +640,9 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
             const T w1 = T(1) - w;
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
             // primal pass: g = A^T y, projected step, extrapolation, Halpern
-            if (FAST || fast) {
+            if constexpr (UNS) {
+                primal_pass_unscaled(sp, L, A, atlist, tw0, tw1, n, lane, tau, w, w1, rho, check, pdx2, pdxa2);
+            } else if (FAST || fast) {
                 primal_pass_fast<T>(fo, A.xs, atlist, tw0, tw1, n, lane, tau, w, w1, rho, check, pdx2, pdxa2);
             } else if (!FAST) {
                 for (int t = tw0; t < tw1; ++t) {
@@ -538,7 +670,9 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
             }
             __syncthreads();
             // dual pass: h = A xbar, projected dual step, Halpern
-            if (FAST || fast) {
+            if constexpr (UNS) {
+                dual_pass_unscaled(sp, L, A, alist, aw0, aw1, m, neq, lane, sigma, w, w1, rho, check, pdy2, pdya2);
+            } else if (FAST || fast) {
                 dual_pass_fast<T>(fo, A.ys, alist, aw0, aw1, m, neq, lane, sigma, w, w1, rho, check, pdy2, pdya2);
             } else if (!FAST) {
                 for (int t = aw0; t < aw1; ++t) {
@@ -631,6 +765,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
                     const T yv = A.ys[i];
                     A.y[i] = yv;
                     A.ya[i] = yv;
+                    if (UNS) A.w[i] = static_cast<T>(sp->dr[i] * yv);
                 }
                 k = 0;
                 r_restart = M.r;
@@ -676,25 +811,26 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
     }
 }
 
-#define FBALP_INSTANTIATE(T, MAXT)                                         \
-    template __global__ void pdhg_persistent<T, MAXT, false>(KernelParams); \
-    template __global__ void pdhg_persistent<T, MAXT, true>(KernelParams);
-FBALP_INSTANTIATE(float, 512)
-FBALP_INSTANTIATE(double, 512)
-FBALP_INSTANTIATE(float, 1024)
-FBALP_INSTANTIATE(double, 1024)
+#define FBALP_INSTANTIATE(MAXT)                                               \
+    template __global__ void pdhg_persistent<float, MAXT, 0>(KernelParams);   \
+    template __global__ void pdhg_persistent<float, MAXT, 1>(KernelParams);   \
+    template __global__ void pdhg_persistent<double, MAXT, 0>(KernelParams);  \
+    template __global__ void pdhg_persistent<double, MAXT, 1>(KernelParams);  \
+    template __global__ void pdhg_persistent<double, MAXT, 2>(KernelParams);
+FBALP_INSTANTIATE(512)
+FBALP_INSTANTIATE(1024)
 #undef FBALP_INSTANTIATE
 
 // Blocks of up to 512 threads use the variant with a 128-register budget,
-// larger blocks the 64-register one; `fast` selects the shared-memory-only
-// variant.
+// larger blocks the 64-register one.  `fast`: FP32 launches take the
+// shared-memory-only variant, FP64 launches the unscaled staged one.
 template <int MAXT>
 static const void* symbol_for(bool fp64, bool fast) {
     if (fp64)
-        return fast ? reinterpret_cast<const void*>(&pdhg_persistent<double, MAXT, true>)
-                    : reinterpret_cast<const void*>(&pdhg_persistent<double, MAXT, false>);
-    return fast ? reinterpret_cast<const void*>(&pdhg_persistent<float, MAXT, true>)
-                : reinterpret_cast<const void*>(&pdhg_persistent<float, MAXT, false>);
+        return fast ? reinterpret_cast<const void*>(&pdhg_persistent<double, MAXT, 2>)
+                    : reinterpret_cast<const void*>(&pdhg_persistent<double, MAXT, 0>);
+    return fast ? reinterpret_cast<const void*>(&pdhg_persistent<float, MAXT, 1>)
+                : reinterpret_cast<const void*>(&pdhg_persistent<float, MAXT, 0>);
 }
 
 const void* kernel_symbol(bool fp64, int threads, bool fast) {
@@ -705,11 +841,11 @@ template <int MAXT>
 static void launch_for(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
                        const KernelParams& p) {
     if (fp64) {
-        if (fast) pdhg_persistent<double, MAXT, true><<<grid, threads, smem, stream>>>(p);
-        else pdhg_persistent<double, MAXT, false><<<grid, threads, smem, stream>>>(p);
+        if (fast) pdhg_persistent<double, MAXT, 2><<<grid, threads, smem, stream>>>(p);
+        else pdhg_persistent<double, MAXT, 0><<<grid, threads, smem, stream>>>(p);
     } else {
-        if (fast) pdhg_persistent<float, MAXT, true><<<grid, threads, smem, stream>>>(p);
-        else pdhg_persistent<float, MAXT, false><<<grid, threads, smem, stream>>>(p);
+        if (fast) pdhg_persistent<float, MAXT, 1><<<grid, threads, smem, stream>>>(p);
+        else pdhg_persistent<float, MAXT, 0><<<grid, threads, smem, stream>>>(p);
     }
 }
 

@@ -29,10 +29,12 @@ namespace fbalp {
 
 constexpr int kMaxWarps = 32;
 constexpr int kRed = 16;  // reduced quantities per convergence check
-constexpr int kArrayCount = 11;
+constexpr int kArrayCount = 12;
 
-// Array order: xbar, y, x, xa, ya, c, l, u, b, xs, ys.
-enum ArrayId { kXbar = 0, kY, kX, kXa, kYa, kC, kL, kU, kB, kXs, kYs };
+// Array order: xbar, y, x, xa, ya, c, l, u, b, xs, ys, w.  In the unscaled
+// FP64 layout xbar holds z = dc * xbar (the gather target of the A pass) and
+// w = dr * y is the gather target of the A^T pass.
+enum ArrayId { kXbar = 0, kY, kX, kXa, kYa, kC, kL, kU, kB, kXs, kYs, kW };
 
 struct DevSpecies {
     int32_t m, n, neq, pad_;
@@ -53,6 +55,17 @@ struct DevSpecies {
     const double* dr;             // new order
     const double* dc;             // new order
     double eta;
+    // unscaled values in the same SELL slices: FP32 part (exact for the
+    // usual stoichiometric coefficients) and, per new-numbered row of A /
+    // A^T, the FP64 remainders of entries FP32 cannot hold exactly
+    const float* a_hi;
+    const float* at_hi;
+    const int32_t* lo_a_ptr;
+    const int32_t* lo_a_idx;
+    const double* lo_a_val;
+    const int32_t* lo_at_ptr;
+    const int32_t* lo_at_idx;
+    const double* lo_at_val;
 };
 
 // Byte offsets of one species' working set inside the CTA's dynamic shared
@@ -60,6 +73,7 @@ struct DevSpecies {
 struct Layout {
     int64_t sched_a_off, sched_at_off, list_a, list_at;
     int32_t mat_smem, smem_mask;
+    int32_t unscaled, pad_;
     int64_t mat_a_idx, mat_at_idx, mat_a_val, mat_at_val;
     int64_t arr[kArrayCount];
 };

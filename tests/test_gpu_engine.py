@@ -99,13 +99,14 @@ def test_invalid_instance_is_flagged_and_others_solve():
 
 # --- iterate parity with the oracle restatement ---
 
-@pytest.mark.parametrize("restarts,iters", [(False, 37), (False, 200), (True, 640)])
-def test_fp64_iterates_match_oracle(restarts, iters):
+@pytest.mark.parametrize("restarts,iters,staged", [(False, 37, True), (False, 200, True), (True, 640, True),
+                                                   (True, 640, False)])
+def test_fp64_iterates_match_oracle(restarts, iters, staged):
     model, lower, upper = syn.single_species_workload(3, m=120, n=260)
     P = pdhg.prepare(model.S)
     config = cfg(precision="fp64", max_iterations=iters, check_every=64, tol_primal=0.0,
                  tol_dual=0.0, tol_gap=0.0, restarts=restarts)
-    r = run_single(model.S, 120, lower, upper, [model.cost] * 3, config=config)
+    r = run_single(model.S, 120, lower, upper, [model.cost] * 3, config=config, stage_matrix=staged)
     for i in range(3):
         ref = pdhg.solve(P, lower[i], upper[i], model.cost, max_iters=iters, check_every=64,
                          tol_primal=0.0, tol_dual=0.0, tol_gap=0.0, restarts=restarts)
@@ -163,18 +164,29 @@ def test_uneven_three_species_batch_in_one_launch(golden_dir):
 
 
 def test_spilled_arrays_give_identical_results():
+    """Array placement (shared memory, global slab) and matrix staging do not
+    change the FP32 arithmetic: the FP32 phase is bit for bit the same."""
     model, lower, upper = syn.single_species_workload(4, m=300, n=650)
-    config = cfg(precision="mixed")
+    config = cfg(precision="fp32", fp32_tol_gap=1e-5)
     a = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config)
     b = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config, max_dynamic_smem=8192)
     c = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config, stage_matrix=False)
-    d = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=config, warps_per_block=32)
     for other in (b, c):
         np.testing.assert_array_equal(a["x"], other["x"])
         np.testing.assert_array_equal(a["y"], other["y"])
         np.testing.assert_array_equal(a["iters"], other["iters"])
+    assert (a["status"] == 5).all()
+
+
+@pytest.mark.parametrize("opt", [dict(max_dynamic_smem=8192), dict(stage_matrix=False), dict(warps_per_block=32)])
+def test_fp64_layouts_agree(opt):
+    """The staged unscaled FP64 path (default), the generic path (global
+    matrix, spilled arrays) and 32-warp blocks reach the same optima."""
+    model, lower, upper = syn.single_species_workload(4, m=300, n=650)
+    a = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=cfg(precision="mixed"))
+    d = run_single(model.S, 300, lower, upper, [model.cost] * 4, config=cfg(precision="mixed"), **opt)
     assert (a["status"] == 0).all() and (d["status"] == 0).all()
-    np.testing.assert_allclose(a["obj"], d["obj"], rtol=1e-8)
+    np.testing.assert_allclose(a["obj"], d["obj"], rtol=1e-8, atol=1e-8)
 
 
 def test_repeat_solves_are_deterministic():
