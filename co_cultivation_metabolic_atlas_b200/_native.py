@@ -89,6 +89,8 @@ def load(path: os.PathLike | None = None):
         "fbalp_engine_solve": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(SolveParams), vp, vp, vp, vp,
                                               vp, vp, vp]),
         "fbalp_engine_destroy": (ctypes.c_int, [vp]),
+        "fbalp_engine_solve_noalloc": (ctypes.c_int, [vp, ctypes.c_int64, vp, vp, vp, vp, vp, vp, vp,
+                                                      ctypes.POINTER(SolveParams), vp, vp, vp, vp, vp, vp, vp]),
         "fbalp_engine_set_stream": (ctypes.c_int, [vp, vp]),
         "fbalp_engine_layout": (ctypes.c_int, [vp, c_int64_p, c_int64_p, c_int64_p, c_int64_p]),
         "fbalp_prepare_matrix": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, c_int64_p, c_int32_p,

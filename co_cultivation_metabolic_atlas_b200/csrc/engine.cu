@@ -17,42 +17,9 @@
 #include "fbalp_internal.h"
 #include "prepare.h"
 
+#include "engine_state.h"
+
 namespace {
-
-thread_local std::string g_last_error;
-
-int fail(int code, const std::string& msg) {
-    g_last_error = msg;
-    return code;
-}
-
-struct CudaError : std::exception {
-    std::string msg;
-    explicit CudaError(std::string m) : msg(std::move(m)) {}
-    const char* what() const noexcept override { return msg.c_str(); }
-};
-
-void check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <typename T> T* dev_upload(const std::vector<T>& h, std::vector<void*>& owned) {
-    T* d = nullptr;
-    size_t bytes = std::max<size_t>(1, h.size()) * sizeof(T);
-    check(cudaMalloc(&d, bytes), "cudaMalloc");
-    owned.push_back(d);
-    if (!h.empty()) check(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy");
-    return d;
-}
-
-struct SpeciesHost {
-    int32_t m = 0, n = 0, neq = 0;
-    fbalp::Scaling scaling;
-    std::vector<int32_t> row_perm, col_perm;  // new -> old
-    fbalp::Sell A, AT;
-    fbalp::Sell Araw, ATraw;  // same slices, unscaled values
-    std::vector<int32_t> a_sched_off, a_sched, at_sched_off, at_sched;
-};
 
 // FP32 "hi" copy of unscaled SELL values plus, per (new-numbered) row, the
 // list of FP64 "lo" remainders of the entries FP32 cannot represent exactly.
@@ -89,61 +56,7 @@ static HiLo split_hi_lo(const fbalp::Sell& raw, int32_t rows) {
     return h;
 }
 
-struct Buffer {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    void ensure(size_t want) {
-        if (want <= bytes) return;
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-        check(cudaMalloc(&ptr, std::max<size_t>(want, 256)), "cudaMalloc workspace");
-        bytes = std::max<size_t>(want, 256);
-    }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-    }
-};
-
 }  // namespace
-
-struct fbalp_engine {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int sm_count = 0;
-    int smem_optin = 0;
-    fbalp_options opt{};
-    std::vector<SpeciesHost> species;
-    std::vector<fbalp::DevSpecies> dev_species_host;
-    fbalp::DevSpecies* dev_species = nullptr;
-    std::vector<void*> owned;  // species allocations
-    // bound batch
-    int64_t count = 0, total_cols = 0, total_rows = 0;
-    std::vector<int32_t> h_species;
-    std::vector<int64_t> h_coloff, h_rowoff;
-    const double *lower = nullptr, *upper = nullptr, *cost = nullptr, *rhs = nullptr;
-    Buffer inst_species, col_off, row_off, order;
-    bool bound = false;
-    // workspace
-    Buffer queue, mid_x, mid_y, mid_omega, mid_iters, mid_status, mid_obj, mid_metrics, spill;
-    Buffer layout32_buf, layout64_buf;
-    std::vector<fbalp::Layout> layouts32, layouts64;
-    int last_grid[2] = {0, 0};
-    int64_t last_smem[2] = {0, 0};
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase start/stop: fp32, fp64
-    bool ran[2] = {false, false};
-    ~fbalp_engine() {
-        for (cudaEvent_t& v : ev)
-            if (v) cudaEventDestroy(v);
-        for (void* p : owned) cudaFree(p);
-        for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
-                          &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill, &layout32_buf,
-                          &layout64_buf})
-            b->release();
-    }
-};
 
 extern "C" {
 

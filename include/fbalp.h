@@ -163,6 +163,31 @@ int fbalp_engine_solve(fbalp_engine* engine, const double* warm_x, const double*
                        int32_t* out_status, double* out_objective, double* out_x, double* out_y,
                        int32_t* out_iterations, double* out_metrics, double* out_omega);
 
+/* Allocation-free solve.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory at solve time -- code running
+ * inside a CUDA stream capture (cudaMalloc cannot be captured), real-time
+ * loops that forbid allocator calls after start-up, hosts whose device
+ * memory is budgeted by another allocator.  They create the engine (which
+ * allocates its species data) up front; this call then allocates nothing:
+ * besides the caller's inputs and outputs it uses one library-wide scratch
+ * array of 32 MiB in device memory (held by every GPU that loads the library
+ * until the process exits).
+ * Limits: one-species engine, FP64 precision only (params->precision must be
+ * FBALP_PRECISION_FP64), instances laid out uniformly (instance i at columns
+ * [i*n, (i+1)*n) and rows [i*m, (i+1)*m)), and a batch whose metadata and
+ * per-CTA spill slabs fit in the scratch; larger requests fail with
+ * FBALP_ERR_INVALID before any work is queued.  The first call on each
+ * device (with that device current) looks up the scratch address with
+ * cudaGetSymbolAddress, so make it before any stream capture.  All calls
+ * share the scratch: calls whose kernels overlap on the GPU race.  Outputs
+ * and their meaning are those of fbalp_engine_solve. */
+int fbalp_engine_solve_noalloc(fbalp_engine* engine, int64_t count, const double* lower,
+                               const double* upper, const double* cost, const double* rhs,
+                               const double* warm_x, const double* warm_y, const double* warm_omega,
+                               const fbalp_solve_params* params, int32_t* out_status,
+                               double* out_objective, double* out_x, double* out_y,
+                               int32_t* out_iterations, double* out_metrics, double* out_omega);
+
 /* Release the engine's device memory.  Replaces the reference services'
  * close()/release paths (`src/cpu_repeated_lp.py:820-831`). */
 int fbalp_engine_destroy(fbalp_engine* engine);
