@@ -16,7 +16,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 from pathlib import Path
 
@@ -42,6 +41,12 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=48, help="LPs per species in the CPU baseline sample")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cold", action="store_true")
+    ap.add_argument("--warm", default="extrapolate", choices=("previous", "extrapolate"),
+                    help="warm start of the product arm")
+    ap.add_argument("--learned", type=int, default=1, help="1: also train and measure the learned MLP warm start")
+    ap.add_argument("--learn-seeds", type=int, default=2)
+    ap.add_argument("--learn-steps", type=int, default=16)
+    ap.add_argument("--learn-epochs", type=int, default=10)
     return ap.parse_args()
 
 
@@ -226,8 +231,8 @@ def run_product(args):
     cfg = SolveConfig(precision=args.precision)
     lps = args.envs * len(models)
 
-    def trajectory(warm):
-        com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, device=dev)
+    def trajectory(warm, learned=None):
+        com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, learned=learned, device=dev)
         for _ in range(args.warmup):
             com.step()
         torch.cuda.synchronize()
@@ -256,7 +261,7 @@ def run_product(args):
         return com, ms, cert, it, launches
 
     with ClockSampler(local) as clocks:
-        com, ms, cert, it, launches = trajectory("previous")
+        com, ms, cert, it, launches = trajectory(args.warm)
     clock_summary = clocks.summary()
     ms_max = max_over_ranks(ms)
     cert_all = sum_over_ranks(cert)
@@ -332,6 +337,25 @@ def run_product(args):
         cold_iters = float(np.mean(it_c))
         com_c.close()
         com = None
+    # --- learned warm start: MLP trained on the engine's own rollouts (other seeds) ---
+    learned = None
+    if args.learned:
+        from co_cultivation_metabolic_atlas_b200 import train_warmstart as tw
+        t0 = time.perf_counter()
+        F, T, OM = tw.build_dataset(models, envs=args.envs, steps=args.learn_steps,
+                                    seeds=[args.seed + 1000 + k for k in range(args.learn_seeds)],
+                                    config=cfg, device=dev, log=lambda *_: None)
+        ws, losses = tw.fit(models, F, T, OM, epochs=args.learn_epochs, device=dev, log=lambda *_: None)
+        pairs = int(F.shape[0])
+        del F, T, OM
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        com_l, ms_l, cert_l, it_l, _ = trajectory("learned", learned=ws)
+        com_l.close()
+        learned = {"value": sum_over_ranks(cert_l) / (max_over_ranks(ms_l) / 1e3),
+                   "mean_iterations": float(np.mean(it_l)), "training_pairs": pairs,
+                   "final_train_mse_standardised": losses[-1], "train_seconds": train_s,
+                   "model": "MLP 44 -> 4 x 512 GELU -> x,y of 3 species, BF16 tcgen05 kernels"}
     # --- e2e through the public engine API with host buffers ---
     e2e = run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks)
 
@@ -340,7 +364,9 @@ def run_product(args):
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64" if args.precision == "mixed" else args.precision,
                 "data": "synthetic (seeded generator; no public dataset)",
-                "config": dict(workload_config(args, lps), warm_start="previous-step solution",
+                "config": dict(workload_config(args, lps),
+                               warm_start={"previous": "previous-step solution",
+                                           "extrapolate": "extrapolated from the last two step solutions"}[args.warm],
                                parallelism=f"env-sharded x{world}"),
                 "certified_fraction": cert / (lps * args.steps),
                 "env_steps_per_s": world * args.envs * args.steps / (ms_max / 1e3),
@@ -348,6 +374,7 @@ def run_product(args):
                                "p99": float(np.percentile(it, 99)), "max": int(np.max(it))},
                 "cold_value": cold, "warm_vs_cold": (value / cold) if cold else None,
                 "cold_mean_iterations": cold_iters if cold else None,
+                "learned": learned, "learned_vs_cold": (learned["value"] / cold) if (learned and cold) else None,
                 "roofline": roofline, "cpu_baseline": cpu, "highs_check": highs_check, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clock_summary}
         print(json.dumps(line), flush=True)
@@ -362,7 +389,7 @@ def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, su
     import torch
 
     from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
-    com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start="previous", device=dev)
+    com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=args.warm, device=dev)
     K = max(1, args.e2e_steps)
     host_lower = []
     for _ in range(args.warmup + K):
@@ -374,34 +401,45 @@ def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, su
     c_h = com.cost.cpu().pin_memory()
     eng = com.engine
     lo_d, up_d, c_d = eng._bound[0], eng._bound[1], eng._bound[2]
-    out = [eng.allocate_result(), eng.allocate_result()]
+    out = [eng.allocate_result() for _ in range(3)]
+    wx = torch.empty(eng.total_cols, dtype=torch.float64, device=dev)
+    wy = torch.empty(max(1, eng.total_rows), dtype=torch.float64, device=dev)
     x_h = torch.empty(eng.total_cols, dtype=torch.float64).pin_memory()
     st_h = torch.empty(eng.count, dtype=torch.int32).pin_memory()
     ob_h = torch.empty(eng.count, dtype=torch.float64).pin_memory()
     mt_h = torch.empty((eng.count, 8), dtype=torch.float64).pin_memory()
-    prev = None
+    hist = []
 
     def one(k, o):
         lo_d.copy_(host_lower[k], non_blocking=True)
         up_d.copy_(up_h, non_blocking=True)
         c_d.copy_(c_h, non_blocking=True)
-        r = eng.solve(warm_x=None if prev is None else prev.x[:eng.total_cols],
-                      warm_y=None if prev is None else prev.y[:eng.total_rows],
-                      warm_omega=None if prev is None else prev.omega, config=cfg, out=o)
+        if not hist:
+            kw = {}
+        elif args.warm == "extrapolate" and len(hist) >= 2:
+            torch.sub(hist[-1].x[:eng.total_cols] * 2.0, hist[-2].x[:eng.total_cols], out=wx)
+            torch.sub(hist[-1].y[:eng.total_rows] * 2.0, hist[-2].y[:eng.total_rows], out=wy[:eng.total_rows])
+            kw = dict(warm_x=wx, warm_y=wy[:eng.total_rows], warm_omega=hist[-1].omega)
+        else:
+            kw = dict(warm_x=hist[-1].x[:eng.total_cols], warm_y=hist[-1].y[:eng.total_rows],
+                      warm_omega=hist[-1].omega)
+        r = eng.solve(config=cfg, out=o, **kw)
         x_h.copy_(r.x[:eng.total_cols], non_blocking=True)
         st_h.copy_(r.status, non_blocking=True)
         ob_h.copy_(r.objective, non_blocking=True)
         mt_h.copy_(r.metrics, non_blocking=True)
+        hist.append(r)
+        del hist[:-2]
         return r
 
     for k in range(args.warmup):
-        prev = one(k, out[k % 2])
+        one(k, out[k % 3])
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     cert = 0
     for k in range(args.warmup, args.warmup + K):
-        prev = one(k, out[k % 2])
+        one(k, out[k % 3])
         torch.cuda.synchronize()
         st = st_h.numpy()
         mt = mt_h.numpy()

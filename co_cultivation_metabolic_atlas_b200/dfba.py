@@ -42,8 +42,8 @@ class DeviceCommunity:
     def __init__(self, models, medium, biomass, *, dt=0.05, capacity=CARRYING_CAPACITY,
                  options: EngineOptions | None = None, config: SolveConfig | None = None,
                  warm_start: str = "previous", learned=None, horizon_steps: int = 960, device=None):
-        if warm_start not in ("cold", "previous", "learned"):
-            raise ValueError("warm_start must be 'cold', 'previous' or 'learned'")
+        if warm_start not in ("cold", "previous", "extrapolate", "learned"):
+            raise ValueError("warm_start must be 'cold', 'previous', 'extrapolate' or 'learned'")
         if warm_start == "learned" and learned is None:
             raise ValueError("warm_start='learned' needs a LearnedWarmStart")
         self.learned = learned
@@ -93,8 +93,10 @@ class DeviceCommunity:
         self.engine.set_instances(sid, self.lower, self.upper, self.cost)
         self.result: SolveResult | None = None
         self.prev: SolveResult | None = None
-        self._bufs = [self.engine.allocate_result(), self.engine.allocate_result()]
+        self.prev2: SolveResult | None = None
+        self._bufs = [self.engine.allocate_result() for _ in range(3)]
         self._which = 0
+        self._wx = self._wy = None
 
     # -- pieces of one step --------------------------------------------------
     def uptake_bounds(self):
@@ -115,13 +117,25 @@ class DeviceCommunity:
         if self.warm_start == "learned":
             wx, wy, wo = self.learned.propose(self, self.step_index / self.horizon_steps)
             res = self.engine.solve(warm_x=wx, warm_y=wy, warm_omega=wo, config=self.config, out=out)
+        elif self.warm_start == "extrapolate" and self.prev is not None and self.prev2 is not None:
+            # first-order prediction from the last two certified solutions
+            # (the kernel projects x onto the new bounds and y_ub onto <= 0)
+            if self._wx is None:
+                self._wx = torch.empty(self.total_cols, dtype=torch.float64, device=self.device)
+                self._wy = torch.empty(max(1, self.total_rows), dtype=torch.float64, device=self.device)
+            torch.sub(self.prev.x[:self.total_cols] * 2.0, self.prev2.x[:self.total_cols], out=self._wx)
+            torch.sub(self.prev.y[:self.total_rows] * 2.0, self.prev2.y[:self.total_rows],
+                      out=self._wy[:self.total_rows])
+            res = self.engine.solve(warm_x=self._wx, warm_y=self._wy[:self.total_rows], warm_omega=self.prev.omega,
+                                    config=self.config, out=out)
         else:
-            warm = self.prev if (self.warm_start == "previous" and self.prev is not None) else None
+            warm = self.prev if (self.warm_start in ("previous", "extrapolate") and self.prev is not None) else None
             res = self.engine.solve(warm_x=None if warm is None else warm.x[:self.total_cols],
                                     warm_y=None if warm is None else warm.y[:self.total_rows],
                                     warm_omega=None if warm is None else warm.omega,
                                     config=self.config, out=out)
-        self._which ^= 1
+        self._which = (self._which + 1) % 3
+        self.prev2 = self.prev
         self.prev = res
         self.result = res
         return res
