@@ -39,7 +39,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64", "fp32"))
     ap.add_argument("--cpu-sample", type=int, default=48, help="LPs per species in the CPU baseline sample")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = the same number of steps as the timed region")
     ap.add_argument("--no-cold", action="store_true")
     ap.add_argument("--warm", default="extrapolate", choices=("previous", "extrapolate"),
                     help="warm start of the product arm")
@@ -390,7 +390,7 @@ def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, su
 
     from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
     com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=args.warm, device=dev)
-    K = max(1, args.e2e_steps)
+    K = args.e2e_steps if args.e2e_steps > 0 else args.steps
     host_lower = []
     for _ in range(args.warmup + K):
         com.uptake_bounds()

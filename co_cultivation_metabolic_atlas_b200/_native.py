@@ -56,7 +56,8 @@ class SolveParams(ctypes.Structure):
                 ("fp32_tol_dual", ctypes.c_double), ("fp32_tol_gap", ctypes.c_double),
                 ("reflection", ctypes.c_double), ("restarts", ctypes.c_int32),
                 ("fp32_stall_checks", ctypes.c_int32), ("fp64_stall_checks", ctypes.c_int32),
-                ("floor_tol", ctypes.c_double), ("fp32_passthrough_tol", ctypes.c_double)]
+                ("floor_tol", ctypes.c_double), ("fp32_passthrough_tol", ctypes.c_double),
+                ("fallback_iterations", ctypes.c_int32)]
 
 
 class NativeError(RuntimeError):

@@ -90,6 +90,7 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->fp64_stall_checks = 8;
     p->floor_tol = 1e-7;
     p->fp32_passthrough_tol = 1e-3;
+    p->fallback_iterations = 4096;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -413,6 +414,7 @@ bool valid_params(const fbalp_solve_params& q, std::string* err) {
     if (q.restarts != 0 && q.restarts != 1) return *err = "restarts must be 0 or 1", false;
     if (q.fp32_stall_checks < 0 || q.fp64_stall_checks < 0) return *err = "stall checks must be non-negative", false;
     if (!(q.floor_tol >= 0.0) || !std::isfinite(q.floor_tol)) return *err = "floor_tol must be finite and non-negative", false;
+    if (q.fallback_iterations < 0) return *err = "fallback_iterations must be non-negative", false;
     if (!(q.fp32_passthrough_tol >= 0.0) || !std::isfinite(q.fp32_passthrough_tol))
         return *err = "fp32_passthrough_tol must be finite and non-negative", false;
     return true;
@@ -472,6 +474,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p.stall_checks = fp64 ? q.fp64_stall_checks : q.fp32_stall_checks;
             p.floor_tol = q.floor_tol;
             p.passthrough_tol = 0.0;
+            p.fallback_iters = q.fallback_iterations;
             run_phase(e, fp64, p);
         } else {
             e->mid_x.ensure(e->total_cols * sizeof(double));
@@ -502,6 +505,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p32.stall_checks = q.fp32_stall_checks;
             p32.floor_tol = q.floor_tol;
             p32.passthrough_tol = q.fp32_passthrough_tol;
+            p32.fallback_iters = 0;  // the FP32 phase hands off on a stall instead
             run_phase(e, false, p32);
             fbalp::KernelParams p64 = p;
             p64.warm_x = static_cast<const double*>(e->mid_x.ptr);
@@ -524,6 +528,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p64.stall_checks = q.fp64_stall_checks;
             p64.floor_tol = q.floor_tol;
             p64.passthrough_tol = 0.0;
+            p64.fallback_iters = q.fallback_iterations;
             run_phase(e, true, p64);
         }
     } catch (const CudaError& ex) {

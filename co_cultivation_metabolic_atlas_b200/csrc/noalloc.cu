@@ -186,6 +186,7 @@ extern "C" int fbalp_engine_solve_noalloc(fbalp_engine* e, int64_t count, const 
         p.stall_checks = q.fp64_stall_checks;
         p.floor_tol = q.floor_tol;
         p.passthrough_tol = 0.0;
+        p.fallback_iters = q.fallback_iterations;
 
         check(cudaMemsetAsync(scratch, 0, sizeof(int32_t), e->stream), "clear queue counter");
         const int fill_grid = static_cast<int>(std::min<int64_t>((count + 255) / 256, 1024));

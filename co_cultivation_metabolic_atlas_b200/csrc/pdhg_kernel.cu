@@ -628,6 +628,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
         }
 
         int k = 0, it = 0, stall = 0;
+        bool fell_back = false;
         double r_restart = INFINITY, r_prev = INFINITY, best_err = INFINITY;
         while (status < 0) {
             ++it;
@@ -749,6 +750,31 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
                         break;
                     }
                 }
+            }
+            // cold fallback: a warm-started instance that has not converged
+            // after `fallback_iters` iterations restarts once from the cold
+            // point (x = projection of 0, y = 0, omega = 1)
+            if (p.fallback_iters > 0 && !fell_back && it >= p.fallback_iters &&
+                (p.warm_x != nullptr || p.warm_y != nullptr)) {
+                fell_back = true;
+                omega = 1.0;
+                for (int j = tid; j < n; j += nthreads) {
+                    const T xv = clampT(T(0), A.ls[j], A.us[j]);
+                    A.x[j] = xv;
+                    A.xa[j] = xv;
+                }
+                for (int i = tid; i < m; i += nthreads) {
+                    A.y[i] = T(0);
+                    A.ya[i] = T(0);
+                    if (UNS) A.w[i] = T(0);
+                }
+                k = 0;
+                r_restart = INFINITY;
+                r_prev = INFINITY;
+                best_err = INFINITY;
+                stall = 0;
+                __syncthreads();
+                continue;
             }
             if (p.restarts && (M.r <= kBetaSufficient * r_restart ||
                                (M.r <= kBetaNecessary * r_restart && M.r > r_prev) ||

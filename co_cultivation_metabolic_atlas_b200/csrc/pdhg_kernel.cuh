@@ -116,6 +116,8 @@ struct KernelParams {
     double floor_tol;             // FP64 phase: tolerance accepted after a stall
     double passthrough_tol;       // FP32 phase: warm starts with error <= this
                                   // skip the phase unchanged (0 = never)
+    int32_t fallback_iters;       // warm starts not converged after this many
+                                  // iterations restart once cold (0 = never)
 };
 
 }  // namespace fbalp

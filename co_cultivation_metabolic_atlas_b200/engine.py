@@ -54,6 +54,7 @@ class SolveConfig:
     fp64_stall_checks: int = 8
     floor_tol: float = 1e-7
     fp32_passthrough_tol: float = 1e-3
+    fallback_iterations: int = 4096
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -62,7 +63,7 @@ class SolveConfig:
             raise ValueError("precision must be 'fp64', 'mixed' or 'fp32'")
         p.precision = prec[self.precision]
         for name in ("max_iterations", "fp32_max_iterations", "check_every", "fp32_stall_checks",
-                     "fp64_stall_checks"):
+                     "fp64_stall_checks", "fallback_iterations"):
             value = getattr(self, name)
             if isinstance(value, (bool, np.bool_)) or not isinstance(value, (int, np.integer)):
                 raise ValueError(f"{name} must be an integer")

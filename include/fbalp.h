@@ -120,6 +120,11 @@ typedef struct fbalp_solve_params {
     double fp32_passthrough_tol; /* MIXED: a warm start whose FP64 KKT error is
                                     already <= this skips the FP32 phase
                                     unchanged (default 1e-3; 0 = never)      */
+    int32_t fallback_iterations; /* a warm-started FP64 solve not converged
+                                    after this many iterations restarts once
+                                    from the cold point (default 4096; 0 =
+                                    never): cold PDHG is the fallback of every
+                                    seed                                     */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);

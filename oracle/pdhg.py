@@ -161,7 +161,7 @@ def converged(mt, tol_primal, tol_dual, tol_gap):
 def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0=1.0,
           dtype=np.float64, max_iters=100000, check_every=64, tol_primal=1e-9, tol_dual=1e-9,
           tol_gap=1e-7, rho=1.0, restarts=True, stop_on_converge=True, final_status=STATUS_OPTIMAL,
-          stall_checks=None, floor_tol=1e-7, trace=None):
+          stall_checks=None, floor_tol=1e-7, fallback_iters=0, trace=None):
     """Run the engine's algorithm for one instance; return dict with scaled
     and original-unit iterates, status, iterations and metrics."""
     A, dr, dc = P.A, P.dr, P.dc
@@ -195,6 +195,7 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
                     status=status, iterations=0, metrics=mt, omega=omega)
     best_err = np.inf
     stall = 0
+    fell_back = False
     if stall_checks is None:
         stall_checks = 8 if final_status == STATUS_OPTIMAL else 6
     for it in range(1, max_iters + 1):
@@ -250,6 +251,18 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
                         and mt["dual_violation"] <= floor_tol * (1 + mt["c_inf"])):
                     status = final_status
                     break
+            if (fallback_iters > 0 and not fell_back and it >= fallback_iters
+                    and (x0 is not None or y0 is not None)):
+                # cold fallback of a warm start that has not converged
+                fell_back = True
+                omega = 1.0
+                x = np.clip(np.zeros(n, dtype), lsf, usf).astype(dtype)
+                y = np.zeros(m, dtype)
+                xa, ya = x.copy(), y.copy()
+                k = 0
+                r_restart = r_prev = best_err = np.inf
+                stall = 0
+                continue
             if restarts and (r <= BETA_SUFFICIENT * r_restart
                              or (r <= BETA_NECESSARY * r_restart and r > r_prev)
                              or k >= BETA_ARTIFICIAL * it):
