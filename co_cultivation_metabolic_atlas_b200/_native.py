@@ -57,7 +57,7 @@ class SolveParams(ctypes.Structure):
                 ("reflection", ctypes.c_double), ("restarts", ctypes.c_int32),
                 ("fp32_stall_checks", ctypes.c_int32), ("fp64_stall_checks", ctypes.c_int32),
                 ("floor_tol", ctypes.c_double), ("fp32_passthrough_tol", ctypes.c_double),
-                ("fallback_iterations", ctypes.c_int32)]
+                ("fallback_iterations", ctypes.c_int32), ("fp32_recentre", ctypes.c_int32)]
 
 
 class NativeError(RuntimeError):

@@ -91,6 +91,7 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->floor_tol = 1e-7;
     p->fp32_passthrough_tol = 1e-3;
     p->fallback_iterations = 4096;
+    p->fp32_recentre = 1;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -329,8 +330,30 @@ int fbalp_engine_layout(const fbalp_engine* e, int64_t* total_cols, int64_t* tot
 
 namespace {
 
-// Launch one precision phase over the bound batch.
-void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
+// True when every species of the bound batch fits the re-centred FP32
+// shared-memory layout (the re-centred phase has no streamed-matrix variant).
+bool recentred_fits(fbalp_engine* e) {
+    const int threads = e->opt.warps_per_block * 32;
+    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
+                      ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
+    if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
+    if (e->opt.stage_matrix == 0) return false;
+    std::vector<char> used(e->species.size(), 0);
+    for (int32_t s : e->h_species) used[s] = 1;
+    for (size_t s = 0; s < e->species.size(); ++s) {
+        if (!used[s]) continue;
+        const SpeciesHost& sh = e->species[s];
+        if (!fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                          sh.A.off.back(), sh.AT.off.back(), cap).layout.recentred)
+            return false;
+    }
+    return true;
+}
+
+// Launch one precision phase over the bound batch (`recentred`: the
+// re-centred FP32 kernel).
+void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, bool recentred = false) {
     const int esz = fp64 ? static_cast<int>(sizeof(double)) : static_cast<int>(sizeof(float));
     const int threads = e->opt.warps_per_block * 32;
     const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
@@ -358,16 +381,20 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     for (size_t s = 0; s < e->species.size(); ++s) {
         if (!used[s]) continue;
         const SpeciesHost& sh = e->species[s];
-        fbalp::LayoutPlan P = unscaled
+        fbalp::LayoutPlan P = recentred
+            ? fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                           sh.A.off.back(), sh.AT.off.back(), cap)
+            : unscaled
             ? fbalp::plan_layout_unscaled(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
                                           sh.A.off.back(), sh.AT.off.back(), cap)
             : fbalp::plan_layout(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
                                  sh.A.off.back(), sh.AT.off.back(), esz, cap, !fp64 && e->opt.stage_matrix != 0);
+        if (recentred && !P.layout.recentred) throw CudaError("species does not fit the re-centred layout");
         if (P.smem_bytes > cap) throw CudaError("species schedule does not fit into shared memory");
         if (!fbalp::layout_aligned(P.layout)) throw CudaError("internal error: misaligned shared-memory layout");
         layouts[s] = P.layout;
-        all_fast = all_fast && (fp64 ? unscaled
-                                     : (P.layout.mat_smem && (P.layout.smem_mask & 0x1ff) == 0x1ff));
+        all_fast = all_fast && (recentred || (fp64 ? unscaled
+                                                   : (P.layout.mat_smem && (P.layout.smem_mask & 0x1ff) == 0x1ff)));
         dyn = std::max(dyn, P.smem_bytes);
         slab = std::max(slab, P.slab_bytes);
     }
@@ -376,7 +403,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     dl.ensure(layouts.size() * sizeof(fbalp::Layout));
     check(cudaMemcpyAsync(dl.ptr, layouts.data(), layouts.size() * sizeof(fbalp::Layout),
                           cudaMemcpyHostToDevice, e->stream), "copy layouts");
-    const void* k = fbalp::kernel_symbol(fp64, threads, all_fast);
+    const void* k = recentred ? fbalp::recentred_symbol(threads) : fbalp::kernel_symbol(fp64, threads, all_fast);
     check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
           "cudaFuncSetAttribute");
     int per_sm = 0;
@@ -397,7 +424,10 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p) {
     check(cudaMemsetAsync(p.queue, 0, sizeof(int32_t), e->stream), "memset queue");
     const int ph = fp64 ? 1 : 0;
     check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
-    check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
+    if (recentred)
+        check(fbalp::launch_recentred(grid, threads, dyn, e->stream, p), "re-centred pdhg kernel launch");
+    else
+        check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
     check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
     e->ran[ph] = true;
     e->last_grid[fp64 ? 1 : 0] = grid;
@@ -415,6 +445,7 @@ bool valid_params(const fbalp_solve_params& q, std::string* err) {
     if (q.fp32_stall_checks < 0 || q.fp64_stall_checks < 0) return *err = "stall checks must be non-negative", false;
     if (!(q.floor_tol >= 0.0) || !std::isfinite(q.floor_tol)) return *err = "floor_tol must be finite and non-negative", false;
     if (q.fallback_iterations < 0) return *err = "fallback_iterations must be non-negative", false;
+    if (q.fp32_recentre != 0 && q.fp32_recentre != 1) return *err = "fp32_recentre must be 0 or 1", false;
     if (!(q.fp32_passthrough_tol >= 0.0) || !std::isfinite(q.fp32_passthrough_tol))
         return *err = "fp32_passthrough_tol must be finite and non-negative", false;
     return true;
@@ -476,6 +507,71 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p.passthrough_tol = 0.0;
             p.fallback_iters = q.fallback_iterations;
             run_phase(e, fp64, p);
+        } else if (q.fp32_recentre && recentred_fits(e)) {
+            // re-centred FP32 phase to the FP64 tolerances; what it does not
+            // certify (stalled instances) continues in the FP64 phase
+            e->mid_x.ensure(e->total_cols * sizeof(double));
+            e->mid_y.ensure(std::max<int64_t>(1, e->total_rows) * sizeof(double));
+            e->mid_omega.ensure(e->count * sizeof(double));
+            e->mid_iters.ensure(e->count * sizeof(int32_t));
+            e->hand_list.ensure(e->count * sizeof(int32_t));
+            e->hand_count.ensure(sizeof(int32_t));
+            check(cudaMemsetAsync(e->hand_count.ptr, 0, sizeof(int32_t), e->stream), "memset handoff count");
+            fbalp::KernelParams pr = p;
+            pr.warm_x = warm_x;
+            pr.warm_y = warm_y;
+            pr.warm_omega = warm_omega;
+            pr.prior_iters = nullptr;
+            pr.out_x = out_x;
+            pr.out_y = out_y;
+            pr.out_obj = out_objective;
+            pr.out_metrics = out_metrics;
+            pr.out_omega = out_omega;
+            pr.out_status = out_status;
+            pr.out_iters = out_iterations;
+            pr.max_iters = q.max_iterations;
+            pr.tol_p = q.tol_primal;
+            pr.tol_d = q.tol_dual;
+            pr.tol_g = q.tol_gap;
+            pr.final_status = fbalp::kStatusOptimal;
+            pr.clip_output = 1;
+            pr.stall_checks = q.fp64_stall_checks;
+            pr.floor_tol = q.floor_tol;
+            pr.passthrough_tol = 0.0;
+            pr.fallback_iters = q.fallback_iterations;
+            pr.handoff_list = static_cast<int32_t*>(e->hand_list.ptr);
+            pr.handoff_count = static_cast<int32_t*>(e->hand_count.ptr);
+            pr.hand_x = static_cast<double*>(e->mid_x.ptr);
+            pr.hand_y = static_cast<double*>(e->mid_y.ptr);
+            pr.hand_omega = static_cast<double*>(e->mid_omega.ptr);
+            pr.hand_iters = static_cast<int32_t*>(e->mid_iters.ptr);
+            pr.handoff_on_stall = 4 * q.fp64_stall_checks;
+            run_phase(e, false, pr, true);
+            fbalp::KernelParams p64 = p;
+            p64.order = static_cast<const int32_t*>(e->hand_list.ptr);
+            p64.count_dev = static_cast<const int32_t*>(e->hand_count.ptr);
+            p64.warm_x = static_cast<const double*>(e->mid_x.ptr);
+            p64.warm_y = static_cast<const double*>(e->mid_y.ptr);
+            p64.warm_omega = static_cast<const double*>(e->mid_omega.ptr);
+            p64.prior_iters = static_cast<const int32_t*>(e->mid_iters.ptr);
+            p64.out_x = out_x;
+            p64.out_y = out_y;
+            p64.out_obj = out_objective;
+            p64.out_metrics = out_metrics;
+            p64.out_omega = out_omega;
+            p64.out_status = out_status;
+            p64.out_iters = out_iterations;
+            p64.max_iters = q.max_iterations;
+            p64.tol_p = q.tol_primal;
+            p64.tol_d = q.tol_dual;
+            p64.tol_g = q.tol_gap;
+            p64.final_status = fbalp::kStatusOptimal;
+            p64.clip_output = 1;
+            p64.stall_checks = q.fp64_stall_checks;
+            p64.floor_tol = q.floor_tol;
+            p64.passthrough_tol = 0.0;
+            p64.fallback_iters = q.fallback_iterations;
+            run_phase(e, true, p64);
         } else {
             e->mid_x.ensure(e->total_cols * sizeof(double));
             e->mid_y.ensure(std::max<int64_t>(1, e->total_rows) * sizeof(double));

@@ -92,6 +92,7 @@ struct fbalp_engine {
     bool bound = false;
     // workspace
     Buffer queue, mid_x, mid_y, mid_omega, mid_iters, mid_status, mid_obj, mid_metrics, spill;
+    Buffer hand_list, hand_count;  // re-centred phase -> FP64 phase work list
     Buffer layout32_buf, layout64_buf;
     std::vector<fbalp::Layout> layouts32, layouts64;
     int last_grid[2] = {0, 0};
@@ -104,7 +105,7 @@ struct fbalp_engine {
         for (void* p : owned) cudaFree(p);
         for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
                           &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill, &layout32_buf,
-                          &layout64_buf})
+                          &layout64_buf, &hand_list, &hand_count})
             b->release();
     }
 };

@@ -164,6 +164,67 @@ inline LayoutPlan plan_layout_unscaled(int n, int m, int warps, int a_nslices, i
     return P;
 }
 
+// Re-centred FP32 layout: everything the iteration touches in shared memory
+// (schedule lists; the FP32 gather targets dxbar (n+1) and dy (m+1); the
+// FP32 matrix slices with 16-bit indices; dx, d, l - x^, u - x^ (n each);
+// r and the inequality bound -y^ (m each)), and in the CTA's global slab the
+// two FP64 point buffers of x and y and the FP32 reduced cost / residual of
+// the last evaluated candidate.  Returns recentred = 0 when the shared part
+// does not fit.
+inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, int at_nslices,
+                                        int64_t a_elems, int64_t at_elems, int64_t smem_cap) {
+    LayoutPlan P{};
+    Layout& L = P.layout;
+    int64_t off = 0;
+    L.sched_a_off = off;
+    off += 4 * (warps + 1);
+    L.sched_at_off = off;
+    off += 4 * (warps + 1);
+    off = align_up(off, 16);
+    L.list_a = off;
+    off += static_cast<int64_t>(sizeof(int4)) * a_nslices;
+    L.list_at = off;
+    off += static_cast<int64_t>(sizeof(int4)) * at_nslices;
+    off = align_up(off, 16);
+    if (n + 1 >= 65536 || m + 1 >= 65536) return P;
+    const int64_t e[kArrayCount] = {n + 1, m + 1, n, 0, m, n, n, n, m, 0, 0, 0};
+    L.smem_mask = 0;
+    auto put = [&](int a) {
+        L.arr[a] = off;
+        L.smem_mask |= 1 << a;
+        off += align_up(e[a] * 4, 16);
+    };
+    put(kXbar);
+    put(kY);
+    L.mat_a_idx = off;
+    off += align_up(2 * a_elems, 16);
+    L.mat_at_idx = off;
+    off += align_up(2 * at_elems, 16);
+    L.mat_a_val = off;
+    off += align_up(4 * a_elems, 16);
+    L.mat_at_val = off;
+    off += align_up(4 * at_elems, 16);
+    for (int a : {kX, kC, kL, kU, kB, kYa}) put(a);
+    // every 16-bit index is an element offset from the start of shared memory
+    if (off > smem_cap || off / 4 > (int64_t(1) << 16) - 1) return P;
+    L.mat_smem = 1;
+    L.recentred = 1;
+    int64_t slab = 0;
+    for (int b = 0; b < 2; ++b) {
+        L.pt_x[b] = slab;
+        slab += align_up((int64_t(n) + 1) * 8, 16);
+        L.pt_y[b] = slab;
+        slab += align_up((int64_t(m) + 1) * 8, 16);
+    }
+    L.dcand = slab;
+    slab += align_up(int64_t(n) * 4, 16);
+    L.rcand = slab;
+    slab += align_up(int64_t(m) * 4, 16);
+    P.smem_bytes = off;
+    P.slab_bytes = slab;
+    return P;
+}
+
 // Every region must start on a 16-byte boundary (int4 lists, FP64 arrays).
 inline bool layout_aligned(const Layout& L) {
     const int64_t offs[] = {L.sched_a_off, L.sched_at_off, L.list_a, L.list_at, L.mat_a_idx,
@@ -176,6 +237,8 @@ inline bool layout_aligned(const Layout& L) {
 }
 
 const void* kernel_symbol(bool fp64, int threads, bool fast);
+const void* recentred_symbol(int threads);
+cudaError_t launch_recentred(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p);
 cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
                         const KernelParams& p);
 

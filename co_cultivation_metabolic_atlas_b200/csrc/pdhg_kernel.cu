@@ -248,7 +248,7 @@ __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned ch
         T* tv = reinterpret_cast<T*>(sm + L.mat_at_val);
         const T* ga = Vals<T>::a(sp);
         const T* gt = Vals<T>::at(sp);
-        const bool fast = layout_is_fast<T>(L);
+        const bool fast = layout_is_fast<T>(L) || L.recentred;
         const int a_add = fast ? static_cast<int>(L.arr[kXbar] / sizeof(T)) : 0;
         const int t_add = fast ? static_cast<int>(L.arr[kY] / sizeof(T)) : 0;
         for (int64_t e = tid; e < sp->a_elems; e += nt) {
@@ -497,13 +497,14 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
     const int warps = nthreads >> 5;
     unsigned char* slab = p.spill ? p.spill + static_cast<int64_t>(blockIdx.x) * p.spill_stride : nullptr;
     const T rho = static_cast<T>(p.rho);
+    const int count = p.count_dev ? *p.count_dev : p.count;
     if (tid == 0) s_loaded = -1;
 
     for (;;) {
         if (tid == 0) s_inst = atomicAdd(p.queue, 1);
         __syncthreads();
         const int q = s_inst;
-        if (q >= p.count) break;
+        if (q >= count) break;
         const int inst = p.order[q];
         const int species = p.inst_species[inst];
         const DevSpecies* __restrict__ sp = p.species + species;
@@ -837,12 +838,468 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Re-centred FP32 PDHG (the default first phase of the mixed schedule).
+//
+// The iterates are kept as FP32 differences from an FP64 base point
+// (x^, y^) held in the CTA's global slab:  x = x^ + dx,  y = y^ + dy.  The
+// base moves to the current candidate at every restart (where the Halpern
+// anchor is reset to that candidate anyway), so the anchor is always the
+// base and dx, dy restart from zero.  Per base the FP32 problem is the
+// correction LP
+//     min d.dx  s.t.  A dx = r,  l - x^ <= dx <= u - x^   (y^ + dy <= 0 on
+//     inequality rows)
+// with d = c - A^T y^ and r = b - A x^ evaluated in FP64 and rounded once.
+// In exact arithmetic the sequence equals plain PDHG from the same start;
+// in FP32 the rounding error scales with |dx|, |dy|, d and r, which shrink
+// as the solve converges, so FP32 iterations reach the FP64 tolerances
+// (plain FP32 iterates floor near a 1e-4 relative gap).  Every convergence
+// test evaluates the FP64 candidate x^ + dx_n, y^ + dy_n with the FP64
+// matrix, exactly like the FP64 phase.
+// Shared memory holds dxbar, dy (gather targets), the FP32 matrix slices,
+// dx, d, l - x^, u - x^, r and the inequality-row bound -y^ (in the slots of
+// xbar, y, x, c, l, u, b, ya).
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void primal_pass_recentred(const FastOffsets& o, const int4* atlist, int t0, int t1,
+                                                      int n, int lane, float tau, float w, float rho, bool check,
+                                                      const double* bx, double* cx, double& pdx2,
+                                                      double& pdxa2) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float* const S = reinterpret_cast<float*>(dyn_smem);
+    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = atlist[t];
+        const float g = slice_dot_fast<float>(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S, sl.z);
+        const int j = (sl.x << 5) + lane;
+        if (j < n) {
+            const float xo = S[o.x + j];
+            const float xn = clampT(xo - tau * (S[o.c + j] - g), S[o.l + j], S[o.u + j]);
+            const float xb = xn + xn - xo;
+            S[o.xbar + j] = xb;
+            const float xh = (rho == 1.0f) ? xb : (1.0f + rho) * xn - rho * xo;
+            S[o.x + j] = w * xh;  // the anchor is the base: dx_anchor = 0
+            if (check) {
+                cx[j] = bx[j] + static_cast<double>(xn);
+                const double d = static_cast<double>(xn) - static_cast<double>(xo);
+                pdx2 += d * d;
+                pdxa2 += static_cast<double>(xn) * static_cast<double>(xn);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void dual_pass_recentred(const FastOffsets& o, const int4* alist, int t0, int t1, int m,
+                                                    int neq, int lane, float sigma, float w, float rho, bool check,
+                                                    const double* by, double* cy, double& pdy2, double& pdya2) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float* const S = reinterpret_cast<float*>(dyn_smem);
+    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = alist[t];
+        const float h = slice_dot_fast<float>(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S, sl.z);
+        const int i = (sl.x << 5) + lane;
+        if (i < m) {
+            const float yo = S[o.y + i];
+            float yn = yo + sigma * (S[o.b + i] - h);
+            if (i >= neq) {
+                const float yl = S[o.ya + i];  // y^ + dy <= 0
+                if (yn > yl) yn = yl;
+            }
+            const float yh = (rho == 1.0f) ? yn + yn - yo : (1.0f + rho) * yn - rho * yo;
+            S[o.y + i] = w * yh;
+            if (check) {
+                cy[i] = by[i] + static_cast<double>(yn);
+                const double d = static_cast<double>(yn) - static_cast<double>(yo);
+                pdy2 += d * d;
+                pdya2 += static_cast<double>(yn) * static_cast<double>(yn);
+            }
+        }
+    }
+}
+
+// FP64 KKT partials at the candidate (xc, yc) (scaled, FP64) as kkt_partials
+// computes them; in addition the candidate x is projected onto the exact
+// FP64 bounds (written back: the FP32 bounds l - x^ are rounded), and the
+// scaled reduced cost d = c~ - A~^T yc and primal residual r = b~ - A~ xc are
+// stored in FP32 for a re-centring at this candidate.  All threads call it
+// (it synchronises between the column and the row loops).
+__device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const int4* alist, const int4* atlist,
+                                                    int a0, int a1, int t0, int t1, double* xc, const double* yc,
+                                                    const double* lower, const double* upper, const double* cost,
+                                                    const double* rhs, float* dcand, float* rcand, int lane,
+                                                    double* v) {
+    const int n = sp->n, m = sp->m, neq = sp->neq;
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = atlist[t];
+        const double g = slice_dot64<double>(sp->at_idx, sp->at_v64, sl.y, sl.z, lane, yc);
+        const int j = (sl.x << 5) + lane;
+        if (j < n) {
+            const int jo = sp->col_perm[j];
+            const double dcj = sp->dc[j];
+            const double c = cost[jo], l = lower[jo], u = upper[jo];
+            double xsc = xc[j];
+            const double ls = l / dcj, us = u / dcj;
+            if (xsc < ls || xsc > us) {
+                xsc = xsc < ls ? ls : us;
+                xc[j] = xsc;
+            }
+            const double xv = xsc * dcj;
+            const double r = c - g / dcj;
+            dcand[j] = static_cast<float>(c * dcj - g);
+            v[0] += c * xv;
+            if (r > 0.0) {
+                if (isfinite(l)) v[2] += r * l;
+                else v[11] = fmax(v[11], r);
+            } else if (r < 0.0) {
+                if (isfinite(u)) v[2] += r * u;
+                else v[11] = fmax(v[11], -r);
+            }
+            const double tg = (r >= 0.0) ? l : u;
+            if (isfinite(tg)) v[3] += fabs(r * (xv - tg));
+            v[12] = fmax(v[12], fmax(l - xv, xv - u));
+            v[13] = fmax(v[13], fabs(xv));
+            v[14] = fmax(v[14], fabs(c));
+            if (isnan(g) || isnan(xv)) v[15] = 1.0;
+        }
+    }
+    __syncthreads();  // the projected xc is the gather target below
+    for (int t = a0; t < a1; ++t) {
+        const int4 sl = alist[t];
+        const double h = slice_dot64<double>(sp->a_idx, sp->a_v64, sl.y, sl.z, lane, xc);
+        const int i = (sl.x << 5) + lane;
+        if (i < m) {
+            const double dri = sp->dr[i];
+            const double b = rhs ? rhs[sp->row_perm[i]] : 0.0;
+            const double yv = yc[i] * dri;
+            const double ro = h / dri - b;
+            rcand[i] = static_cast<float>(b * dri - h);
+            if (i < neq) {
+                v[10] = fmax(v[10], fabs(ro));
+            } else {
+                v[10] = fmax(v[10], ro);
+                v[4] += fabs(yv * ro);
+                v[11] = fmax(v[11], yv);
+            }
+            v[1] += b * yv;
+            if (isnan(h) || isnan(yv)) v[15] = 1.0;
+        }
+    }
+}
+
+// Move the base to (bx, by) (the candidate the last kkt_partials_recentred
+// call evaluated): load its reduced cost and residual, shift the bounds and
+// zero the differences.  Callers synchronise afterwards.
+__device__ __forceinline__ void recentre(const DevSpecies* sp, const FastOffsets& o, const double* bx,
+                                         const double* by, const float* dcand, const float* rcand,
+                                         const double* lower, const double* upper) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float* const S = reinterpret_cast<float*>(dyn_smem);
+    const int n = sp->n, m = sp->m, neq = sp->neq;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int jo = sp->col_perm[j];
+        const double dcj = sp->dc[j];
+        const double xb = bx[j];
+        S[o.c + j] = dcand[j];
+        S[o.l + j] = static_cast<float>(lower[jo] / dcj - xb);
+        S[o.u + j] = static_cast<float>(upper[jo] / dcj - xb);
+        S[o.x + j] = 0.0f;
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        S[o.b + i] = rcand[i];
+        S[o.ya + i] = i >= neq ? static_cast<float>(-by[i]) : 0.0f;
+        S[o.y + i] = 0.0f;
+    }
+}
+
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ double s_red[MAXT / 32][kRed];
+    __shared__ double s_tot[kRed];
+    __shared__ int s_inst;
+    __shared__ int s_loaded;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthreads = blockDim.x;
+    const int warps = nthreads >> 5;
+    unsigned char* const slab = p.spill + static_cast<int64_t>(blockIdx.x) * p.spill_stride;
+    const float rho = static_cast<float>(p.rho);
+    const int count = p.count_dev ? *p.count_dev : p.count;
+    if (tid == 0) s_loaded = -1;
+
+    for (;;) {
+        if (tid == 0) s_inst = atomicAdd(p.queue, 1);
+        __syncthreads();
+        const int q = s_inst;
+        if (q >= count) break;
+        const int inst = p.order[q];
+        const int species = p.inst_species[inst];
+        const DevSpecies* __restrict__ sp = p.species + species;
+        const Layout& L = p.layouts[species];
+        const int n = sp->n, m = sp->m, neq = sp->neq;
+        const int64_t coff = p.col_off[inst], roff = p.row_off[inst];
+        if (s_loaded != species) {  // block-uniform
+            stage_species<float>(sp, L, dyn_smem, warps);
+            __syncthreads();
+            if (tid == 0) s_loaded = species;
+        }
+        float* const S = reinterpret_cast<float*>(dyn_smem);
+        const FastOffsets o = fast_offsets<float>(L);
+        // the two point buffers; selected by value (no local-memory array)
+        double* const px0 = reinterpret_cast<double*>(slab + L.pt_x[0]);
+        double* const px1 = reinterpret_cast<double*>(slab + L.pt_x[1]);
+        double* const py0 = reinterpret_cast<double*>(slab + L.pt_y[0]);
+        double* const py1 = reinterpret_cast<double*>(slab + L.pt_y[1]);
+        auto PX = [&](int b) { return b ? px1 : px0; };
+        auto PY = [&](int b) { return b ? py1 : py0; };
+        float* const dcand = reinterpret_cast<float*>(slab + L.dcand);
+        float* const rcand = reinterpret_cast<float*>(slab + L.rcand);
+        const int4* alist = reinterpret_cast<const int4*>(dyn_smem + L.list_a);
+        const int4* atlist = reinterpret_cast<const int4*>(dyn_smem + L.list_at);
+        const int32_t* soa = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_a_off);
+        const int32_t* sot = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_at_off);
+        const int aw0 = soa[warp], aw1 = soa[warp + 1];
+        const int tw0 = sot[warp], tw1 = sot[warp + 1];
+        const double* lo_i = p.lower + coff;
+        const double* up_i = p.upper + coff;
+        const double* c_i = p.cost + coff;
+        const double* b_i = p.rhs ? p.rhs + roff : nullptr;
+
+        // ---- the start point, FP64, projected, becomes buffer 0 ----
+        int bad = 0;
+        for (int j = tid; j < n; j += nthreads) {
+            const int jo = sp->col_perm[j];
+            const double dcj = sp->dc[j];
+            const double lv = lo_i[jo], uv = up_i[jo], cv = c_i[jo];
+            if (isnan(lv) || isnan(uv) || lv > uv || !isfinite(cv) || lv == INFINITY || uv == -INFINITY)
+                bad = 1;
+            double x0 = p.warm_x ? p.warm_x[coff + jo] / dcj : 0.0;
+            if (!isfinite(x0)) x0 = 0.0;
+            const double ls = lv / dcj, us = uv / dcj;
+            PX(0)[j] = x0 < ls ? ls : (x0 > us ? us : x0);
+        }
+        for (int i = tid; i < m; i += nthreads) {
+            const int io = sp->row_perm[i];
+            const double dri = sp->dr[i];
+            if (b_i && !isfinite(b_i[io])) bad = 1;
+            double y0 = p.warm_y ? p.warm_y[roff + io] / dri : 0.0;
+            if (!isfinite(y0)) y0 = 0.0;
+            if (i >= neq && y0 > 0.0) y0 = 0.0;
+            PY(0)[i] = y0;
+        }
+        if (tid == 0) {
+            PX(0)[n] = 0.0;
+            PX(1)[n] = 0.0;
+            PY(0)[m] = 0.0;
+            PY(1)[m] = 0.0;
+            S[o.xbar + n] = 0.0f;
+            S[o.y + m] = 0.0f;
+        }
+        bad = __syncthreads_or(bad);
+        double omega = 1.0;
+        if (p.warm_omega) {
+            const double w0 = p.warm_omega[inst];
+            if (isfinite(w0) && w0 > 0.0) omega = w0;
+        }
+        if (bad) {
+            for (int j = tid; j < n; j += nthreads) p.out_x[coff + sp->col_perm[j]] = NAN;
+            for (int i = tid; i < m; i += nthreads) p.out_y[roff + sp->row_perm[i]] = NAN;
+            if (tid == 0) {
+                p.out_status[inst] = kStatusInvalid;
+                p.out_iters[inst] = 0;
+                if (p.hand_iters) p.hand_iters[inst] = 0;
+                p.out_obj[inst] = NAN;
+                for (int k = 0; k < kMetrics; ++k) p.out_metrics[static_cast<int64_t>(inst) * kMetrics + k] = NAN;
+                if (p.out_omega) p.out_omega[inst] = omega;
+            }
+            continue;
+        }
+
+        const double eta = sp->eta;
+        int status = -1;
+        int cur = 0;   // buffer holding the base
+        int ev = 0;    // buffer holding the last evaluated point
+        Metrics M;
+        {
+            double v[kRed];
+#pragma unroll
+            for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
+            kkt_partials_recentred(sp, alist, atlist, aw0, aw1, tw0, tw1, PX(0), PY(0), lo_i, up_i, c_i, b_i,
+                                   dcand, rcand, lane, v);
+            block_reduce(v, s_red, s_tot);
+            M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
+            if (M.conv) status = p.final_status;
+            else if (p.max_iters <= 0) status = M.nan ? kStatusNumerical : kStatusIterationLimit;
+            if (status < 0) {
+                recentre(sp, o, PX(0), PY(0), dcand, rcand, lo_i, up_i);
+                __syncthreads();
+            }
+        }
+
+        int k = 0, it = 0, stall = 0;
+        bool fell_back = false;
+        double r_restart = INFINITY, r_prev = INFINITY, best_err = INFINITY;
+        while (status < 0) {
+            ++it;
+            const bool full = (it % p.check_every == 0) || (it >= p.max_iters);
+            const bool check = full || (it >= 8 && it < p.check_every && (it & (it - 1)) == 0);
+            const float tau = static_cast<float>(eta / omega), sigma = static_cast<float>(eta * omega);
+            const float w = static_cast<float>((k + 1.0) / (k + 2.0));
+            double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
+            primal_pass_recentred(o, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1), pdx2,
+                                  pdxa2);
+            __syncthreads();
+            dual_pass_recentred(o, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur), PY(cur ^ 1), pdy2,
+                                pdya2);
+            __syncthreads();
+            ++k;
+            if (!check) continue;
+
+            double v[kRed];
+#pragma unroll
+            for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
+            v[5] = pdx2;
+            v[6] = pdy2;
+            v[7] = pdxa2;
+            v[8] = pdya2;
+            kkt_partials_recentred(sp, alist, atlist, aw0, aw1, tw0, tw1, PX(cur ^ 1), PY(cur ^ 1), lo_i, up_i,
+                                   c_i, b_i, dcand, rcand, lane, v);
+            block_reduce(v, s_red, s_tot);
+            M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
+            ev = cur ^ 1;
+            if (M.nan || !isfinite(M.r)) {
+                status = kStatusNumerical;
+                break;
+            }
+            if (M.conv) {
+                status = p.final_status;
+                break;
+            }
+            if (it >= p.max_iters) {
+                status = kStatusIterationLimit;
+                break;
+            }
+            if (!full) continue;
+            {
+                const double e = fmax(fmax(M.primal / (1.0 + M.xinf), M.dual / (1.0 + M.cinf)),
+                                      fmax(M.rgap, M.kgap));
+                if (e < 0.5 * best_err) {
+                    best_err = e;
+                    stall = 0;
+                } else {
+                    ++stall;
+                }
+                if (p.stall_checks > 0 && stall >= p.stall_checks && e <= p.floor_tol &&
+                    M.primal <= p.floor_tol * (1.0 + M.xinf) && M.dual <= p.floor_tol * (1.0 + M.cinf)) {
+                    status = p.final_status;
+                    break;
+                }
+                // a long stall (slow phases of PDHG last a few tests; an FP32
+                // rounding floor does not end) continues in FP64
+                if (p.handoff_on_stall > 0 && stall >= p.handoff_on_stall) {
+                    status = kStatusHandoff;
+                    break;
+                }
+            }
+            if (p.fallback_iters > 0 && !fell_back && it >= p.fallback_iters &&
+                (p.warm_x != nullptr || p.warm_y != nullptr)) {
+                // cold fallback: evaluate the cold point in the candidate
+                // buffer and re-centre there
+                fell_back = true;
+                omega = 1.0;
+                double* cx = PX(cur ^ 1);
+                double* cyv = PY(cur ^ 1);
+                for (int j = tid; j < n; j += nthreads) {
+                    const int jo = sp->col_perm[j];
+                    const double dcj = sp->dc[j];
+                    const double ls = lo_i[jo] / dcj, us = up_i[jo] / dcj;
+                    cx[j] = 0.0 < ls ? ls : (0.0 > us ? us : 0.0);
+                }
+                for (int i = tid; i < m; i += nthreads) cyv[i] = 0.0;
+                __syncthreads();
+                double vv[kRed];
+#pragma unroll
+                for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
+                kkt_partials_recentred(sp, alist, atlist, aw0, aw1, tw0, tw1, cx, cyv, lo_i, up_i, c_i, b_i,
+                                       dcand, rcand, lane, vv);
+                block_reduce(vv, s_red, s_tot);
+                cur ^= 1;
+                ev = cur;
+                recentre(sp, o, PX(cur), PY(cur), dcand, rcand, lo_i, up_i);
+                k = 0;
+                r_restart = INFINITY;
+                r_prev = INFINITY;
+                best_err = INFINITY;
+                stall = 0;
+                __syncthreads();
+                continue;
+            }
+            if (p.restarts && (M.r <= kBetaSufficient * r_restart ||
+                               (M.r <= kBetaNecessary * r_restart && M.r > r_prev) ||
+                               k >= kBetaArtificial * it)) {
+                const double nx = sqrt(s_tot[7]), ny = sqrt(s_tot[8]);
+                if (nx > 1e-10 && ny > 1e-10)
+                    omega = exp(kOmegaSmoothing * log(ny / nx) + (1.0 - kOmegaSmoothing) * log(omega));
+                cur ^= 1;  // the candidate becomes the base
+                recentre(sp, o, PX(cur), PY(cur), dcand, rcand, lo_i, up_i);
+                k = 0;
+                r_restart = M.r;
+                r_prev = INFINITY;
+                __syncthreads();
+            } else {
+                r_prev = M.r;
+            }
+        }
+
+        // ---- results (original units and order) from the last evaluated point ----
+        const bool hand = p.handoff_list != nullptr && status != kStatusOptimal && status != kStatusNumerical &&
+                          status != kStatusIterationLimit;
+        const double* fx = PX(ev);
+        const double* fy = PY(ev);
+        double* ox = hand ? p.hand_x : p.out_x;
+        double* oy = hand ? p.hand_y : p.out_y;
+        for (int j = tid; j < n; j += nthreads) {
+            const int jo = sp->col_perm[j];
+            double xv = fx[j] * sp->dc[j];
+            if (p.clip_output && !hand) {
+                const double lv = lo_i[jo], uv = up_i[jo];
+                xv = xv < lv ? lv : (xv > uv ? uv : xv);
+            }
+            ox[coff + jo] = xv;
+        }
+        for (int i = tid; i < m; i += nthreads) oy[roff + sp->row_perm[i]] = fy[i] * sp->dr[i];
+        if (tid == 0) {
+            if (p.hand_iters) p.hand_iters[inst] = it;
+            if (hand) {
+                p.hand_omega[inst] = omega;
+                p.handoff_list[atomicAdd(p.handoff_count, 1)] = inst;
+            } else {
+                double* mo = p.out_metrics + static_cast<int64_t>(inst) * kMetrics;
+                mo[0] = M.primal;
+                mo[1] = M.dual;
+                mo[2] = M.kgap;
+                mo[3] = M.pobj;
+                mo[4] = M.dobj;
+                mo[5] = M.rgap;
+                mo[6] = M.xinf;
+                mo[7] = omega;
+                p.out_obj[inst] = M.pobj;
+                p.out_status[inst] = status;
+                p.out_iters[inst] = it;
+                if (p.out_omega) p.out_omega[inst] = omega;
+            }
+        }
+        // the next instance reuses the slab and shared memory
+        __syncthreads();
+    }
+}
+
 #define FBALP_INSTANTIATE(MAXT)                                               \
     template __global__ void pdhg_persistent<float, MAXT, 0>(KernelParams);   \
     template __global__ void pdhg_persistent<float, MAXT, 1>(KernelParams);   \
     template __global__ void pdhg_persistent<double, MAXT, 0>(KernelParams);  \
     template __global__ void pdhg_persistent<double, MAXT, 1>(KernelParams);  \
-    template __global__ void pdhg_persistent<double, MAXT, 2>(KernelParams);
+    template __global__ void pdhg_persistent<double, MAXT, 2>(KernelParams);  \
+    template __global__ void pdhg_recentred<MAXT>(KernelParams);
 FBALP_INSTANTIATE(512)
 FBALP_INSTANTIATE(1024)
 #undef FBALP_INSTANTIATE
@@ -879,6 +1336,17 @@ cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem
                         const KernelParams& p) {
     if (threads <= 512) launch_for<512>(fp64, fast, grid, threads, smem, stream, p);
     else launch_for<1024>(fp64, fast, grid, threads, smem, stream, p);
+    return cudaGetLastError();
+}
+
+const void* recentred_symbol(int threads) {
+    return threads <= 512 ? reinterpret_cast<const void*>(&pdhg_recentred<512>)
+                          : reinterpret_cast<const void*>(&pdhg_recentred<1024>);
+}
+
+cudaError_t launch_recentred(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p) {
+    if (threads <= 512) pdhg_recentred<512><<<grid, threads, smem, stream>>>(p);
+    else pdhg_recentred<1024><<<grid, threads, smem, stream>>>(p);
     return cudaGetLastError();
 }
 

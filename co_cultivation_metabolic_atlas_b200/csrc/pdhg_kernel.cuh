@@ -73,9 +73,14 @@ struct DevSpecies {
 struct Layout {
     int64_t sched_a_off, sched_at_off, list_a, list_at;
     int32_t mat_smem, smem_mask;
-    int32_t unscaled, pad_;
+    int32_t unscaled, recentred;
     int64_t mat_a_idx, mat_at_idx, mat_a_val, mat_at_val;
     int64_t arr[kArrayCount];
+    // re-centred FP32 layout only (slab offsets): the two FP64 point buffers
+    // of x (n+1) and y (m+1) -- base and candidate, roles swapped at every
+    // re-centring -- and the FP32 reduced cost / primal residual of the last
+    // evaluated candidate
+    int64_t pt_x[2], pt_y[2], dcand, rcand;
 };
 
 struct KernelParams {
@@ -118,6 +123,21 @@ struct KernelParams {
                                   // skip the phase unchanged (0 = never)
     int32_t fallback_iters;       // warm starts not converged after this many
                                   // iterations restart once cold (0 = never)
+    // re-centred FP32 phase followed by an FP64 phase: instances the first
+    // phase does not certify are appended to `handoff_list` (count in
+    // `handoff_count`) with their point in hand_x / hand_y / hand_omega and
+    // iteration count in hand_iters; certified ones go straight to out_*.
+    // The FP64 phase then reads its work list size from `count_dev`.
+    int32_t* handoff_list;        // may be null: every instance goes to out_*
+    int32_t* handoff_count;
+    double* hand_x;
+    double* hand_y;
+    double* hand_omega;
+    int32_t* hand_iters;          // may be null; iterations of this phase
+    const int32_t* count_dev;     // may be null: use `count`
+    int32_t handoff_on_stall;     // >0: a re-centred solve whose KKT error has
+                                  // not halved for this many full tests hands
+                                  // off to the FP64 phase (0 = never)
 };
 
 }  // namespace fbalp

@@ -55,6 +55,7 @@ class SolveConfig:
     floor_tol: float = 1e-7
     fp32_passthrough_tol: float = 1e-3
     fallback_iterations: int = 4096
+    recentre: bool = True              # MIXED: re-centred FP32 phase (FP64 tolerances)
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -72,6 +73,7 @@ class SolveConfig:
                      "fp32_tol_gap", "reflection", "floor_tol", "fp32_passthrough_tol"):
             setattr(p, name, float(getattr(self, name)))
         p.restarts = 1 if self.restarts else 0
+        p.fp32_recentre = 1 if self.recentre else 0
         return p
 
 

@@ -125,6 +125,16 @@ typedef struct fbalp_solve_params {
                                     from the cold point (default 4096; 0 =
                                     never): cold PDHG is the fallback of every
                                     seed                                     */
+    int32_t fp32_recentre;       /* MIXED (default 1): the FP32 phase iterates
+                                    on differences from an FP64 base point that
+                                    moves to the iterate at every restart, so
+                                    FP32 iterations reach the FP64 tolerances;
+                                    instances it does not certify (a stall)
+                                    continue in the FP64 phase.  Used when the
+                                    batch's species fit the shared-memory
+                                    layout, else the plain schedule below.
+                                    0: plain schedule -- FP32 iterates to the
+                                    fp32_* tolerances, then FP64 iterates    */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);

@@ -286,3 +286,177 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
         xo = np.clip(xo, lower, upper)
     yo = yn.astype(float) * dr
     return dict(x=xo, y=yo, xs=xn, ys=yn, status=status, iterations=it, metrics=mt, omega=omega)
+
+
+def solve_recentred(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0=1.0,
+                    max_iters=20000, check_every=64, tol_primal=1e-9, tol_dual=1e-9, tol_gap=1e-7, rho=1.0,
+                    restarts=True, stall_checks=8, floor_tol=1e-7, fallback_iters=0, handoff_stall_checks=32,
+                    trace=None):
+    """The engine's re-centred FP32 phase (the first phase of its mixed
+    schedule).
+
+    Iterates are FP32 differences from an FP64 base ``(xh, yh)`` (scaled
+    space).  At the start, after every restart and after a cold fallback the
+    base moves to the evaluated candidate and the FP32 problem becomes the
+    correction LP ``min d.dx s.t. A~ dx = r, ls - xh <= dx <= us - xh``
+    (``yh + dy <= 0`` on inequality rows) with ``d = c~ - A~^T yh`` and
+    ``r = b~ - A~ xh`` computed in FP64 and rounded to FP32 once.  The Halpern
+    anchor is the base, so the differences restart from zero.  Convergence
+    tests evaluate the FP64 candidate ``xh + dxn`` (projected onto the exact
+    scaled bounds), ``yh + dyn``.  After ``stall_checks`` full tests without
+    halving the KKT error a point meeting ``floor_tol`` is accepted; after
+    ``handoff_stall_checks`` such tests the solve ends with
+    ``STATUS_HANDOFF`` (the FP64 phase continues; 0 = never).
+    """
+    f32 = np.float32
+    A, dr, dc = P.A, P.dr, P.dc
+    m, n = A.shape
+    rhs = np.zeros(m) if rhs is None else np.asarray(rhs, float)
+    ls, us, cs, bs = lower / dc, upper / dc, cost * dc, rhs * dr
+    AT = A.T.tocsr()
+    Af = A.astype(f32)
+    ATf = AT.astype(f32)
+    ineq = np.arange(m) >= P.neq
+
+    def evaluate(xc, yc):
+        xc = np.minimum(np.maximum(xc, ls), us)
+        mt = kkt_metrics(P, lower, upper, cost, rhs, xc, yc)
+        d = (cs - AT @ yc).astype(f32)
+        r = (bs - A @ xc).astype(f32)
+        return xc, mt, d, r
+
+    def recentre(xh, yh, d, r):
+        lp = (ls - xh).astype(f32)
+        up = (us - xh).astype(f32)
+        yl = np.where(ineq, -yh, 0.0).astype(f32)
+        return d, r, lp, up, yl
+
+    xh = np.zeros(n) if x0 is None else np.asarray(x0, float) / dc
+    xh = np.where(np.isfinite(xh), xh, 0.0)
+    xh = np.minimum(np.maximum(xh, ls), us)
+    yh = np.zeros(m) if y0 is None else np.asarray(y0, float) / dr
+    yh = np.where(np.isfinite(yh), yh, 0.0)
+    yh = np.where(ineq, np.minimum(yh, 0.0), yh)
+    omega = float(omega0)
+    xh, mt, d, r = evaluate(xh, yh)
+    xo, yo = xh, yh
+    if converged(mt, tol_primal, tol_dual, tol_gap) or max_iters == 0:
+        st = STATUS_OPTIMAL if converged(mt, tol_primal, tol_dual, tol_gap) else STATUS_ITERATION_LIMIT
+        return dict(x=np.clip(xo * dc, lower, upper), y=yo * dr, status=st, iterations=0, metrics=mt,
+                    omega=omega)
+    d, r, lp, up, yl = recentre(xh, yh, d, r)
+    dx = np.zeros(n, f32)
+    dy = np.zeros(m, f32)
+    k = 0
+    r_restart = r_prev = best_err = np.inf
+    stall = 0
+    fell_back = False
+    status = STATUS_ITERATION_LIMIT
+    it = 0
+    for it in range(1, max_iters + 1):
+        tau = f32(P.eta / omega)
+        sig = f32(P.eta * omega)
+        w = f32((k + 1.0) / (k + 2.0))
+        g = ATf @ dy
+        dxn = np.minimum(np.maximum(dx - tau * (d - g), lp), up).astype(f32)
+        xb = (dxn + dxn - dx).astype(f32)
+        h = Af @ xb
+        dyn = (dy + sig * (r - h)).astype(f32)
+        dyn = np.where(ineq, np.minimum(dyn, yl), dyn).astype(f32)
+        if rho == 1.0:
+            dxnew = (w * xb).astype(f32)
+            dynew = (w * (dyn + dyn - dy)).astype(f32)
+        else:
+            dxnew = (w * ((1 + f32(rho)) * dxn - f32(rho) * dx)).astype(f32)
+            dynew = (w * ((1 + f32(rho)) * dyn - f32(rho) * dy)).astype(f32)
+        k += 1
+        full = (it % check_every == 0) or it >= max_iters
+        is_check = full or (8 <= it < check_every and (it & (it - 1)) == 0)
+        if not is_check:
+            dx, dy = dxnew, dynew
+            continue
+        ddx = dxn.astype(float) - dx.astype(float)
+        ddy = dyn.astype(float) - dy.astype(float)
+        rr = np.sqrt(omega * (ddx @ ddx) + (ddy @ ddy) / omega)
+        xc, mt, dcand, rcand = evaluate(xh + dxn.astype(float), yh + dyn.astype(float))
+        yc = yh + dyn.astype(float)
+        xo, yo = xc, yc
+        if trace is not None:
+            trace.append(dict(it=it, r=rr, omega=omega, **mt))
+        if not np.isfinite(rr) or not all(np.isfinite(v) for v in mt.values()):
+            status = STATUS_NUMERICAL
+            break
+        if converged(mt, tol_primal, tol_dual, tol_gap):
+            status = STATUS_OPTIMAL
+            break
+        if it >= max_iters:
+            status = STATUS_ITERATION_LIMIT
+            break
+        if not full:
+            dx, dy = dxnew, dynew
+            continue
+        err = max(mt["primal_residual"] / (1 + mt["x_inf"]), mt["dual_violation"] / (1 + mt["c_inf"]),
+                  mt["relative_gap"], mt["relative_kkt_gap"])
+        if err < 0.5 * best_err:
+            best_err, stall = err, 0
+        else:
+            stall += 1
+        if (stall_checks > 0 and stall >= stall_checks and err <= floor_tol
+                and mt["primal_residual"] <= floor_tol * (1 + mt["x_inf"])
+                and mt["dual_violation"] <= floor_tol * (1 + mt["c_inf"])):
+            status = STATUS_OPTIMAL
+            break
+        if handoff_stall_checks > 0 and stall >= handoff_stall_checks:
+            status = STATUS_HANDOFF
+            break
+        if fallback_iters > 0 and not fell_back and it >= fallback_iters and (x0 is not None or y0 is not None):
+            fell_back = True
+            omega = 1.0
+            xh, _, d0, r0 = evaluate(np.minimum(np.maximum(np.zeros(n), ls), us), np.zeros(m))
+            yh = np.zeros(m)
+            xo, yo = xh, yh
+            d, r, lp, up, yl = recentre(xh, yh, d0, r0)
+            dx = np.zeros(n, f32)
+            dy = np.zeros(m, f32)
+            k = 0
+            r_restart = r_prev = best_err = np.inf
+            stall = 0
+            continue
+        if restarts and (rr <= BETA_SUFFICIENT * r_restart or (rr <= BETA_NECESSARY * r_restart and rr > r_prev)
+                         or k >= BETA_ARTIFICIAL * it):
+            nx = np.sqrt(float(dxn.astype(float) @ dxn.astype(float)))
+            ny = np.sqrt(float(dyn.astype(float) @ dyn.astype(float)))
+            if nx > 1e-10 and ny > 1e-10:
+                omega = float(np.exp(OMEGA_SMOOTHING * np.log(ny / nx) + (1 - OMEGA_SMOOTHING) * np.log(omega)))
+            xh, yh = xc, yc
+            d, r, lp, up, yl = recentre(xh, yh, dcand, rcand)
+            dx = np.zeros(n, f32)
+            dy = np.zeros(m, f32)
+            k = 0
+            r_restart = rr
+            r_prev = np.inf
+            continue
+        r_prev = rr
+        dx, dy = dxnew, dynew
+    x_out = xo * dc
+    if status != STATUS_HANDOFF:
+        x_out = np.clip(x_out, lower, upper)
+    return dict(x=x_out, y=yo * dr, status=status, iterations=it, metrics=mt, omega=omega)
+
+
+def solve_mixed(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0=1.0, max_iters=20000,
+                check_every=64, tol_primal=1e-9, tol_dual=1e-9, tol_gap=1e-7, fallback_iters=4096, **kw):
+    """The engine's default mixed schedule: the re-centred FP32 phase; an
+    instance it hands off (a stall above the floor tolerance) continues in
+    FP64 from the handed-off point.  Iterations of both phases are summed."""
+    kw.setdefault("handoff_stall_checks", 4 * kw.get("stall_checks", 8))
+    r = solve_recentred(P, lower, upper, cost, rhs, x0=x0, y0=y0, omega0=omega0, max_iters=max_iters,
+                        check_every=check_every, tol_primal=tol_primal, tol_dual=tol_dual, tol_gap=tol_gap,
+                        fallback_iters=fallback_iters, **kw)
+    if r["status"] != STATUS_HANDOFF:
+        return r
+    r2 = solve(P, lower, upper, cost, rhs, x0=r["x"], y0=r["y"], omega0=r["omega"], max_iters=max_iters,
+               check_every=check_every, tol_primal=tol_primal, tol_dual=tol_dual, tol_gap=tol_gap,
+               fallback_iters=fallback_iters)
+    r2["iterations"] += r["iterations"]
+    return r2

@@ -212,3 +212,82 @@ def test_mixed_precision_keeps_an_accurate_fp64_warm_start():
     assert again.iterations.cpu().tolist() == [0, 0, 0]
     np.testing.assert_array_equal(again.x[:eng.total_cols].cpu().numpy(), x0.cpu().numpy())
     eng.close()
+
+
+# --- the re-centred FP32 phase (default mixed schedule) ---
+
+def test_recentred_iterates_match_oracle():
+    """A fixed number of re-centred FP32 iterations (restarts included)
+    follows the oracle's restatement to FP32 accuracy."""
+    model, lower, upper = syn.single_species_workload(3, m=120, n=260)
+    P = pdhg.prepare(model.S)
+    iters = 320
+    config = cfg(precision="mixed", max_iterations=iters, check_every=64, tol_primal=0.0, tol_dual=0.0,
+                 tol_gap=0.0, fp64_stall_checks=0)
+    r = run_single(model.S, 120, lower, upper, [model.cost] * 3, config=config)
+    for i in range(3):
+        ref = pdhg.solve_recentred(P, lower[i], upper[i], model.cost, max_iters=iters, check_every=64,
+                                   tol_primal=0.0, tol_dual=0.0, tol_gap=0.0, stall_checks=0,
+                                   handoff_stall_checks=0)
+        assert r["status"][i] == 1 and r["iters"][i] == iters
+        scale = max(1.0, np.abs(ref["x"]).max())
+        np.testing.assert_allclose(r["x"][i], ref["x"], rtol=0, atol=1e-5 * scale)
+        np.testing.assert_allclose(r["y"][i], ref["y"], rtol=0, atol=1e-5 * max(1.0, np.abs(ref["y"]).max()))
+
+
+def test_recentred_reaches_fp64_tolerances_in_fp32(golden_dir):
+    """The default mixed schedule certifies the three species' LPs in its
+    FP32 phase (no FP64 iterations) with the oracle's iteration counts."""
+    import torch
+    g = np.load(golden_dir / "highs_community.npz")
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(4)
+    for s, mdl in enumerate(models):
+        lo = dfba.uptake_lower_bounds(mdl, medium, biomass, 0.05)
+        eng = engine([(mdl.S, mdl.S.shape[0])])
+        eng.set_instances(np.zeros(4, np.int32), lo.ravel(), np.tile(mdl.upper, 4), np.tile(mdl.cost, 4))
+        res = eng.solve(config=cfg())
+        it32 = eng.phase_iterations().cpu().numpy()
+        torch.cuda.synchronize()
+        st = res.status.cpu().numpy()
+        it = res.iterations.cpu().numpy()
+        obj = res.objective.cpu().numpy()
+        eng.close()
+        assert (st == 0).all(), st
+        np.testing.assert_array_equal(it, it32)  # nothing was handed to the FP64 phase
+        P = pdhg.prepare(mdl.S)
+        ref = pdhg.solve_recentred(P, lo[0], mdl.upper, mdl.cost)
+        assert abs(int(it[0]) - ref["iterations"]) <= 64
+        fun = g[f"s{s}_fun"]
+        assert np.all(np.abs(obj - fun) <= OBJ_TOL * np.maximum(1.0, np.abs(fun)))
+
+
+def test_recentred_handoff_continues_in_fp64(golden_dir):
+    """Instances the re-centred phase hands off (forced by a one-test stall
+    rule and short test period) finish in the FP64 phase from the compacted
+    work list; every objective still matches HiGHS."""
+    import torch
+    g = np.load(golden_dir / "highs_single.npz")
+    model, lower, upper = syn.single_species_workload(8)
+    eng = engine([(model.S, 1200)])
+    eng.set_instances(np.zeros(8, np.int32), flat(lower), flat(upper), flat([model.cost] * 8))
+    res = eng.solve(config=cfg(fp64_stall_checks=1, check_every=16))
+    it32 = eng.phase_iterations().cpu().numpy()
+    torch.cuda.synchronize()
+    st = res.status.cpu().numpy()
+    it = res.iterations.cpu().numpy()
+    obj = res.objective.cpu().numpy()
+    eng.close()
+    assert (st == 0).all(), st
+    assert (it > it32).any(), "no instance reached the FP64 phase"
+    fun = g["fun"]
+    assert np.all(np.abs(obj - fun) <= OBJ_TOL * np.maximum(1.0, np.abs(fun)))
+
+
+def test_plain_mixed_schedule_still_available(golden_dir):
+    g = np.load(golden_dir / "highs_single.npz")
+    model, lower, upper = syn.single_species_workload(4)
+    r = run_single(model.S, 1200, lower[:4], upper[:4], [model.cost] * 4, config=cfg(recentre=False))
+    assert (r["status"] == 0).all()
+    fun = g["fun"][:4]
+    assert np.all(np.abs(r["obj"] - fun) <= OBJ_TOL * np.maximum(1.0, np.abs(fun)))

@@ -164,3 +164,41 @@ def test_uptake_bounds_follow_michaelis_menten():
     assert lo[0, mdl.medium_columns[k]] == pytest.approx(round(-min(v_kin, v_phys), 6))
     others = np.setdiff1d(np.arange(mdl.S.shape[1]), mdl.medium_columns)
     np.testing.assert_array_equal(lo[0, others], mdl.lower[others])
+
+
+def test_recentred_restatement_matches_highs_and_fp64(golden_dir):
+    """FP32 iterations re-centred on an FP64 base reach the FP64 tolerances in
+    the same number of iterations as FP64 iterates (plain FP32 iterates stall
+    near a 1e-4 gap), and the optimum matches HiGHS."""
+    g = np.load(golden_dir / "highs_community.npz")
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(4)
+    mdl = models[2]
+    lo = dfba.uptake_lower_bounds(mdl, medium, biomass, 0.05)
+    P = pdhg.prepare(mdl.S)
+    r = pdhg.solve_recentred(P, lo[0], mdl.upper, mdl.cost)
+    r64 = pdhg.solve(P, lo[0], mdl.upper, mdl.cost)
+    assert r["status"] == pdhg.STATUS_OPTIMAL and r64["status"] == pdhg.STATUS_OPTIMAL
+    assert abs(r["iterations"] - r64["iterations"]) <= 64
+    fun = float(g["s2_fun"][0])
+    assert abs(r["metrics"]["objective"] - fun) <= 1e-6 * max(1.0, abs(fun))
+    cert = certificate.certificate(mdl.S, np.zeros(mdl.S.shape[0]), lo[0], mdl.upper, mdl.cost,
+                                   mdl.S.shape[0], r["x"], r["y"])
+    assert cert["certificate_passed"]
+    plain = pdhg.solve(P, lo[0], mdl.upper, mdl.cost, dtype=np.float32, max_iters=r["iterations"] + 512,
+                       stall_checks=0)
+    assert plain["status"] == pdhg.STATUS_ITERATION_LIMIT
+
+
+def test_recentred_handoff_finishes_in_fp64(golden_dir):
+    """A re-centred solve that hands off (forced by a short stall limit)
+    continues in FP64 from the handed-off point to the same optimum."""
+    g = np.load(golden_dir / "highs_single.npz")
+    model, lower, upper = syn.single_species_workload(8)
+    P = pdhg.prepare(model.S)
+    first = pdhg.solve_recentred(P, lower[1], upper[1], model.cost, handoff_stall_checks=1)
+    assert first["status"] == pdhg.STATUS_HANDOFF
+    r = pdhg.solve_mixed(P, lower[1], upper[1], model.cost, handoff_stall_checks=1)
+    assert r["status"] == pdhg.STATUS_OPTIMAL and r["iterations"] > first["iterations"]
+    fun = float(g["fun"][1])
+    assert abs(r["metrics"]["objective"] - fun) <= 1e-6 * max(1.0, abs(fun))
