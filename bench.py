@@ -42,8 +42,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = the same number of steps as the timed region")
     ap.add_argument("--no-cold", action="store_true")
     ap.add_argument("--warm", default="extrapolate", choices=("previous", "extrapolate"),
-                    help="warm start of the product arm")
-    ap.add_argument("--learned", type=int, default=1, help="1: also train and measure the learned MLP warm start")
+                    help="temporal base of the warm start (the product arm without --learned)")
+    ap.add_argument("--learned", type=int, default=1,
+                    help="1: train the learned warm start and measure it as the product arm (the temporal base "
+                         "alone and cold PDHG are measured beside it)")
     ap.add_argument("--learn-seeds", type=int, default=2)
     ap.add_argument("--learn-steps", type=int, default=16)
     ap.add_argument("--learn-epochs", type=int, default=10)
@@ -230,6 +232,28 @@ def run_product(args):
     medium, biomass = syn.initial_environments(args.envs, seed=args.seed + 1000 * rank)
     cfg = SolveConfig(precision=args.precision)
     lps = args.envs * len(models)
+    # kernels of this project per step: the PDHG launches (re-centred FP32 +
+    # FP64 hand-off phase in the mixed schedule); the network runs only at an
+    # environment's first step, which is a warm-up step
+    pdhg_launches = 2 if args.precision == "mixed" else 1
+
+    # --- learned warm start: networks trained on the engine's own rollouts
+    # (seeds disjoint from the evaluated environments) ---
+    ws = None
+    learned_info = None
+    if args.learned:
+        from co_cultivation_metabolic_atlas_b200 import train_warmstart as tw
+        t0 = time.perf_counter()
+        data = tw.build_dataset(models, envs=args.envs, steps=args.learn_steps,
+                                seeds=[args.seed + 1000 * (world + 1) + 100 * rank + k for k in range(args.learn_seeds)],
+                                config=cfg, device=dev, log=lambda *_: None)
+        ws, losses = tw.fit(models, data, epochs=args.learn_epochs, device=dev, log=lambda *_: None)
+        torch.cuda.synchronize()
+        learned_info = {"training_pairs": int(data.F.shape[0]), "final_train_mse_standardised": losses[-1],
+                        "train_seconds": time.perf_counter() - t0,
+                        "model": "MLP 44 -> 4 x 512 GELU -> x,y of 3 species, BF16 tcgen05 kernels; seeds an "
+                                 "environment's first solve, the temporal base seeds the later ones"}
+        del data
 
     def trajectory(warm, learned=None):
         com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, learned=learned, device=dev)
@@ -242,16 +266,13 @@ def run_product(args):
         stop = torch.cuda.Event(enable_timing=True)
         certified = []
         iters = []
-        fp32_ms = 0.0
-        fp32_units = 0
-        fp32_bytes = 0.0
         launches = 0
         start.record(stream)
         for _ in range(args.steps):
             st = com.step()
             certified.append(st.certified)
             iters.append(st.iterations.clone())
-            launches += 2 if args.precision == "mixed" else 1
+            launches += pdhg_launches
         stop.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -260,14 +281,16 @@ def run_product(args):
         it = torch.cat(iters).cpu().numpy()
         return com, ms, cert, it, launches
 
+    headline = "learned" if ws is not None else args.warm
     with ClockSampler(local) as clocks:
-        com, ms, cert, it, launches = trajectory(args.warm)
+        com, ms, cert, it, launches = trajectory(headline, learned=ws)
     clock_summary = clocks.summary()
     ms_max = max_over_ranks(ms)
     cert_all = sum_over_ranks(cert)
     value = cert_all / (ms_max / 1e3)
 
-    # --- roofline of the dominant kernel (FP32 phase of one extra solve) ---
+    # --- roofline of the dominant kernel (the re-centred FP32 phase of one
+    # more step of the same trajectory) ---
     peak, peak_kind = hbm_peak()
     com.uptake_bounds()
     res = com.solve()
@@ -291,16 +314,16 @@ def run_product(args):
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9
     tpi = profiled_traffic()
     traffic = None if tpi is None else tpi * float(it32.sum())
+    kname = {"mixed": "pdhg_recentred", "fp32": "pdhg_persistent<float>", "fp64": "pdhg_persistent<double>"}
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} copy bandwidth",
-                "kernel": f"pdhg_persistent<{'float' if w == 4 else 'double'}>",
-                "algorithmic_bytes": alg_bytes, "kernel_ms": dom_ms,
+                "kernel": kname[args.precision], "algorithmic_bytes": alg_bytes, "kernel_ms": dom_ms,
                 "instance_iterations": int(it32.sum())}
 
     # --- CPU baseline on a sample of this step's LPs + HiGHS objective check ---
     cpu = None
     highs_check = None
-    if rank == 0 and world >= 1:
+    if rank == 0:
         lower = com.lower.cpu().numpy()
         co = com.col_offsets.cpu().numpy()
         lowers = []
@@ -327,54 +350,49 @@ def run_product(args):
                          f"pool over all cores (ParallelCpuLP pattern); {wall:.1f} s wall"}
         highs_check = {"sampled": len(funs), "within_1e-6": int(agree),
                        "max_rel_obj_err": max(errs) if errs else None}
+    com.close()
+    com = None
 
-    # --- cold PDHG on its own trajectory (same seeds) ---
+    # --- the same trajectory without the network (temporal base only) and cold ---
+    extrap = None
+    if ws is not None:
+        com_e, ms_e, cert_e, it_e, _ = trajectory(args.warm)
+        com_e.close()
+        extrap = {"value": sum_over_ranks(cert_e) / (max_over_ranks(ms_e) / 1e3),
+                  "mean_iterations": float(np.mean(it_e)), "warm_start": args.warm}
     cold = None
+    cold_iters = None
     if not args.no_cold:
-        com.close()
         com_c, ms_c, cert_c, it_c, _ = trajectory("cold")
         cold = sum_over_ranks(cert_c) / (max_over_ranks(ms_c) / 1e3)
         cold_iters = float(np.mean(it_c))
         com_c.close()
-        com = None
-    # --- learned warm start: MLP trained on the engine's own rollouts (other seeds) ---
-    learned = None
-    if args.learned:
-        from co_cultivation_metabolic_atlas_b200 import train_warmstart as tw
-        t0 = time.perf_counter()
-        F, T, OM = tw.build_dataset(models, envs=args.envs, steps=args.learn_steps,
-                                    seeds=[args.seed + 1000 + k for k in range(args.learn_seeds)],
-                                    config=cfg, device=dev, log=lambda *_: None)
-        ws, losses = tw.fit(models, F, T, OM, epochs=args.learn_epochs, device=dev, log=lambda *_: None)
-        pairs = int(F.shape[0])
-        del F, T, OM
-        torch.cuda.synchronize()
-        train_s = time.perf_counter() - t0
-        com_l, ms_l, cert_l, it_l, _ = trajectory("learned", learned=ws)
-        com_l.close()
-        learned = {"value": sum_over_ranks(cert_l) / (max_over_ranks(ms_l) / 1e3),
-                   "mean_iterations": float(np.mean(it_l)), "training_pairs": pairs,
-                   "final_train_mse_standardised": losses[-1], "train_seconds": train_s,
-                   "model": "MLP 44 -> 4 x 512 GELU -> x,y of 3 species, BF16 tcgen05 kernels"}
     # --- e2e through the public engine API with host buffers ---
-    e2e = run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks)
+    e2e = run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks, ws)
 
     if rank == 0:
+        warm_desc = {"previous": "previous-step solution",
+                     "extrapolate": "extrapolated from the last two step solutions"}[args.warm]
+        if ws is not None:
+            warm_desc = ("learned: MLP prediction from the medium state at an environment's first step, then the "
+                         "temporal base (" + warm_desc + ")")
+        if learned_info is not None:
+            learned_info.update(value=value, mean_iterations=float(np.mean(it)))
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64" if args.precision == "mixed" else args.precision,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "fp32+fp64" if args.precision == "mixed" else args.precision,
                 "data": "synthetic (seeded generator; no public dataset)",
-                "config": dict(workload_config(args, lps),
-                               warm_start={"previous": "previous-step solution",
-                                           "extrapolate": "extrapolated from the last two step solutions"}[args.warm],
+                "config": dict(workload_config(args, lps), warm_start=warm_desc,
                                parallelism=f"env-sharded x{world}"),
                 "certified_fraction": cert / (lps * args.steps),
                 "env_steps_per_s": world * args.envs * args.steps / (ms_max / 1e3),
                 "iterations": {"mean": float(np.mean(it)), "p50": float(np.median(it)),
                                "p99": float(np.percentile(it, 99)), "max": int(np.max(it))},
                 "cold_value": cold, "warm_vs_cold": (value / cold) if cold else None,
-                "cold_mean_iterations": cold_iters if cold else None,
-                "learned": learned, "learned_vs_cold": (learned["value"] / cold) if (learned and cold) else None,
+                "cold_mean_iterations": cold_iters,
+                "without_network": extrap, "network_gain": (value / extrap["value"]) if extrap else None,
+                "learned": learned_info, "learned_vs_cold": (value / cold) if (ws is not None and cold) else None,
                 "roofline": roofline, "cpu_baseline": cpu, "highs_check": highs_check, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clock_summary}
         print(json.dumps(line), flush=True)
@@ -382,17 +400,30 @@ def run_product(args):
         dist.destroy_process_group()
 
 
-def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks):
+class _HostDrivenState:
+    """What a warm-start proposal reads of a community (state and the last
+    two results), fed from host copies in the end-to-end arm."""
+
+    def __init__(self, E, total_cols, total_rows):
+        self.E = E
+        self.total_cols, self.total_rows = total_cols, total_rows
+        self.medium = self.biomass = None
+        self.prev = self.prev2 = None
+
+
+def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks, ws=None):
     """Same metric through the public ``LPEngine`` API with HOST inputs: every
-    step copies that step's bounds/objective from pinned host memory and reads
-    status, objectives and fluxes back."""
+    step copies that step's bounds/objective (and, for the learned warm
+    start, the medium state) from pinned host memory, proposes the warm
+    start, solves, and reads status, objectives, metrics and fluxes back."""
     import torch
 
     from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
     com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=args.warm, device=dev)
     K = args.e2e_steps if args.e2e_steps > 0 else args.steps
-    host_lower = []
+    host_lower, host_state = [], []
     for _ in range(args.warmup + K):
+        host_state.append((com.medium.cpu().pin_memory(), com.biomass.cpu().pin_memory()))
         com.uptake_bounds()
         host_lower.append(com.lower.cpu().pin_memory())
         res = com.solve()
@@ -408,13 +439,24 @@ def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, su
     st_h = torch.empty(eng.count, dtype=torch.int32).pin_memory()
     ob_h = torch.empty(eng.count, dtype=torch.float64).pin_memory()
     mt_h = torch.empty((eng.count, 8), dtype=torch.float64).pin_memory()
+    state = _HostDrivenState(com.E, eng.total_cols, eng.total_rows)
+    med_d = torch.empty_like(com.medium)
+    bio_d = torch.empty_like(com.biomass)
     hist = []
 
     def one(k, o):
         lo_d.copy_(host_lower[k], non_blocking=True)
         up_d.copy_(up_h, non_blocking=True)
         c_d.copy_(c_h, non_blocking=True)
-        if not hist:
+        if ws is not None:
+            med_d.copy_(host_state[k][0], non_blocking=True)
+            bio_d.copy_(host_state[k][1], non_blocking=True)
+            state.medium, state.biomass = med_d, bio_d
+            state.prev = hist[-1] if hist else None
+            state.prev2 = hist[-2] if len(hist) > 1 else None
+            px, py, po = ws.propose(state, k / 960)
+            kw = dict(warm_x=px, warm_y=py, warm_omega=po)
+        elif not hist:
             kw = {}
         elif args.warm == "extrapolate" and len(hist) >= 2:
             torch.sub(hist[-1].x[:eng.total_cols] * 2.0, hist[-2].x[:eng.total_cols], out=wx)
@@ -448,10 +490,11 @@ def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, su
     barrier()
     com.close()
     value = sum_over_ranks(cert) / max_over_ranks(wall)
-    h2d = 3 * eng.total_cols * 8
+    h2d = 3 * eng.total_cols * 8 + (0 if ws is None else (med_d.numel() + bio_d.numel()) * 8)
     d2h = eng.total_cols * 8 + eng.count * (4 + 8 + 64)
     return {"value": value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "steps": K, "api": "LPEngine.solve over the C ABI (fbalp_engine_solve) with pinned host buffers"}
+            "steps": K, "warm_start": "learned" if ws is not None else args.warm,
+            "api": "LPEngine.solve over the C ABI (fbalp_engine_solve) with pinned host buffers"}
 
 
 def main():

@@ -21,11 +21,12 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--warps", type=int, default=16)
+    ap.add_argument("--warm", default="extrapolate", choices=("cold", "previous", "extrapolate"))
     args = ap.parse_args()
     models = syn.community_models()
     medium, biomass = syn.initial_environments(args.envs)
     com = DeviceCommunity(models, medium, biomass, config=SolveConfig(precision=args.precision),
-                          options=EngineOptions(warps_per_block=args.warps), warm_start="previous")
+                          options=EngineOptions(warps_per_block=args.warps), warm_start=args.warm)
     for _ in range(args.steps):
         st = com.step()
     torch.cuda.synchronize()

@@ -4,7 +4,7 @@
         [--envs 4096] [--steps 48] [--seeds 1 2 ...] [--epochs 20]
 
 Data: for each training seed, ``--envs`` environments are rolled forward
-``--steps`` dFBA steps with previous-step warm starts; every certified
+``--steps`` dFBA steps with extrapolated warm starts; every certified
 (environment, step) contributes one (state features -> concatenated x, y of
 the three species) pair.  The seeds must differ from the evaluation seeds.
 The artifact holds the network weights, the codec, the architecture and a
@@ -22,7 +22,7 @@ import torch
 
 from . import synthetic as syn
 from .engine import SolveConfig
-from .warmstart import MLP, Codec, LearnedWarmStart, collect, solution_layout, train
+from .warmstart import MLP, Codec, LearnedWarmStart, Rollouts, collect, solution_layout, train
 
 HIDDEN = (512, 512, 512, 512)
 N_FEATURES = 44
@@ -37,25 +37,27 @@ def models_digest(models):
     return h.hexdigest()
 
 
-def build_dataset(models, *, envs, steps, seeds, config=None, device=None, log=print):
-    F, T, OM = [], [], []
+def build_dataset(models, *, envs, steps, seeds, config=None, device=None, log=print) -> Rollouts:
+    parts = []
     for sd in seeds:
         t0 = time.perf_counter()
-        f, t, ok, om = collect(models, envs=envs, steps=steps, seed=sd, config=config, device=device)
-        F.append(f[ok])
-        T.append(t[ok])
-        OM.append(om[ok])
+        r = collect(models, envs=envs, steps=steps, seed=sd, config=config, device=device)
+        ok = r.ok
+        parts.append(Rollouts(r.F[ok], r.T[ok], ok[ok], r.omega[ok]))
         log(f"seed {sd}: {int(ok.sum())}/{len(ok)} certified pairs in {time.perf_counter() - t0:.1f} s")
-    return torch.cat(F), torch.cat(T), torch.cat(OM)
+    return Rollouts(*(torch.cat([getattr(p, f) for p in parts]) for f in ("F", "T", "ok", "omega")))
 
 
-def fit(models, F, T, OM, *, epochs=20, batch=4096, lr=1e-3, lr_final=5e-5, seed=0, device=None, log=print):
-    omega = OM.median(dim=0).values
-    codec = Codec.fit(F, T, omega)
-    width = T.shape[1]
+def fit(models, data: Rollouts, *, epochs=20, batch=4096, lr=1e-3, lr_final=5e-5, seed=0, device=None,
+        log=print):
+    """Train the network (state -> solution) on standardised targets;
+    returns the warm start and the per-epoch losses."""
+    omega = data.omega.median(dim=0).values
+    codec = Codec.fit(data.F, data.T, omega)
+    width = data.T.shape[1]
     net = MLP([N_FEATURES, *HIDDEN, width], device=device, seed=seed)
-    losses = train(net, codec.features(F), codec.targets(T), epochs=epochs, batch=min(batch, F.shape[0]), lr=lr,
-                   lr_final=lr_final, seed=seed, log=log)
+    losses = train(net, codec.features(data.F), codec.targets(data.T), epochs=epochs,
+                   batch=min(batch, data.F.shape[0]), lr=lr, lr_final=lr_final, seed=seed, log=log)
     return LearnedWarmStart(net, codec, models), losses
 
 
@@ -86,10 +88,10 @@ def main():
     ap.add_argument("--model-seed", type=int, default=0)
     args = ap.parse_args()
     models = syn.community_models(seed=args.model_seed)
-    F, T, OM = build_dataset(models, envs=args.envs, steps=args.steps, seeds=args.seeds, config=SolveConfig())
-    ws, losses = fit(models, F, T, OM, epochs=args.epochs)
-    save(args.out, ws, models, {"pairs": int(F.shape[0]), "losses": losses, "seeds": args.seeds})
-    print(f"saved {args.out}: {F.shape[0]} pairs, final mse {losses[-1]:.4e}")
+    data = build_dataset(models, envs=args.envs, steps=args.steps, seeds=args.seeds, config=SolveConfig())
+    ws, losses = fit(models, data, epochs=args.epochs)
+    save(args.out, ws, models, {"pairs": int(data.F.shape[0]), "losses": losses, "seeds": args.seeds})
+    print(f"saved {args.out}: {data.F.shape[0]} pairs, final mse {losses[-1]:.4e}")
 
 
 if __name__ == "__main__":

@@ -14,6 +14,16 @@ codec, ``scripts/train_temporal_lp.py:23-88`` training).  Here:
   accumulators) -- torch only allocates device memory;
 * training data are (state -> certified solution) pairs produced by the
   engine's own dFBA rollouts (``collect``);
+* the network seeds an environment's first solve (no history); afterwards
+  the proposal is the temporal base -- the previous certified solution,
+  extrapolated linearly from the last two -- as the reference's
+  ``TemporalLPModel`` proposes the previous solution when its residual head
+  is zero (``src/temporal_lp_model.py:58-142``).  A trained residual network
+  over the base was measured to cost PDHG iterations on these degenerate
+  LPs (its corrections move the seed off the optimal face the base sits on),
+  so it is not used; the network's first-step seed, besides cutting that
+  step's iterations about threefold, also leads the trajectory to optimal
+  points from which the later warm-started solves converge faster;
 * ``LearnedWarmStart.propose`` turns a batch of states into warm starts; every
   seed is still driven by PDHG to the same tolerances (cold PDHG remains the
   fallback behaviour of any seed).
@@ -277,29 +287,46 @@ def gather_targets(com, res):
     return torch.cat(cols, dim=1).float()
 
 
+def temporal_base(prev, prev2):
+    """Temporal base of a warm start (any layout, FP64): the previous
+    solution extrapolated linearly from the last two, or the previous one."""
+    return prev if prev2 is None else 2.0 * prev - prev2
+
+
+@dataclass
+class Rollouts:
+    """Training pairs of one or more rollouts (device tensors)."""
+    F: torch.Tensor        # (N, 44) state features
+    T: torch.Tensor        # (N, width) certified solutions (FP32)
+    ok: torch.Tensor       # (N,) every species certified
+    omega: torch.Tensor    # (N, species) final primal weights
+
+
 def collect(models, *, envs, steps, seed, dt=0.05, horizon_steps=960, config=None, device=None):
-    """Roll the community forward with previous-step warm starts and record
-    (features, certified solution, status) for every environment and step."""
+    """Roll the community forward with extrapolated warm starts and record
+    (features, certified solution, status, primal weights) for every
+    environment and step."""
     from .dfba import DeviceCommunity
     from . import synthetic as syn
     medium, biomass = syn.initial_environments(envs, seed=seed)
-    com = DeviceCommunity(models, medium, biomass, config=config, warm_start="previous", device=device)
+    com = DeviceCommunity(models, medium, biomass, config=config, warm_start="extrapolate", device=device)
     F, T, ok, om = [], [], [], []
     for k in range(steps):
         F.append(state_features(com.medium, com.biomass, k / horizon_steps))
         com.uptake_bounds()
         res = com.solve()
         T.append(gather_targets(com, res))
-        good = (res.status == 0).view(len(models), envs).all(dim=0)
-        ok.append(good)
+        ok.append((res.status == 0).view(len(models), envs).all(dim=0))
         om.append(res.omega.view(len(models), envs).float().t())
         com.integrate(res)
     com.close()
-    return torch.cat(F), torch.cat(T), torch.cat(ok), torch.cat(om)
+    return Rollouts(torch.cat(F), torch.cat(T), torch.cat(ok), torch.cat(om))
 
 
 class LearnedWarmStart:
-    """Trained MLP + codec producing flat warm-start arrays for a community."""
+    """Trained network + codec producing flat warm-start arrays for a
+    community: the network's prediction for environments without history,
+    the temporal base of their last certified solutions otherwise."""
 
     def __init__(self, mlp: MLP, codec: Codec, models):
         self.mlp = mlp
@@ -311,17 +338,28 @@ class LearnedWarmStart:
         Y = self.mlp.forward(self.codec.features(features))[:, :self.width]
         return self.codec.decode(Y)
 
-    def propose(self, com, t_frac):
-        """Warm start (x, y, omega) flat device arrays for the community's
-        species-major batch, from its current state."""
-        P = self.predict(state_features(com.medium, com.biomass, t_frac)).double()
-        E = com.E
+    def _flat(self, P):
         xs, ys = [], []
         for s, (xo, n, yo, r) in enumerate(self.layout):
             xs.append(P[:, xo:xo + n].reshape(-1))
             ys.append(P[:, yo:yo + r].reshape(-1))
-        omega = torch.repeat_interleave(self.codec.omega.double(), E)
-        return torch.cat(xs), torch.cat(ys), omega
+        return torch.cat(xs), torch.cat(ys)
+
+    def propose(self, com, t_frac):
+        """Warm start (x, y, omega) flat device arrays for the community's
+        species-major batch, from its current state (``com.medium``,
+        ``com.biomass``) or its last certified solutions (``com.prev``,
+        ``com.prev2``)."""
+        if com.prev is None:
+            feats = state_features(com.medium, com.biomass, t_frac)
+            x, y = self._flat(self.predict(feats).double())
+            omega = torch.repeat_interleave(self.codec.omega.double(), com.E)
+            return x, y, omega
+        nc, nr = com.total_cols, com.total_rows
+        p2 = com.prev2
+        bx = temporal_base(com.prev.x[:nc], None if p2 is None else p2.x[:nc])
+        by = temporal_base(com.prev.y[:nr], None if p2 is None else p2.y[:nr])
+        return bx, by, com.prev.omega
 
 
 def train(mlp: MLP, F, T, *, epochs=20, batch=4096, lr=1e-3, lr_final=1e-4, seed=0, log=None):
