@@ -233,6 +233,11 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             d.lo_at_idx = dev_upload(ht.lo_idx, E->owned);
             d.lo_at_val = dev_upload(ht.lo_val, E->owned);
             d.dc = dev_upload(dcn, E->owned);
+            std::vector<double> idr(sh.m), idc(sh.n);
+            for (int32_t i = 0; i < sh.m; ++i) idr[i] = 1.0 / drn[i];
+            for (int32_t j = 0; j < sh.n; ++j) idc[j] = 1.0 / dcn[j];
+            d.inv_dr = dev_upload(idr, E->owned);
+            d.inv_dc = dev_upload(idc, E->owned);
             d.eta = sh.scaling.eta;
             E->dev_species_host.push_back(d);
         }

@@ -168,8 +168,9 @@ inline LayoutPlan plan_layout_unscaled(int n, int m, int warps, int a_nslices, i
 // (schedule lists; the FP32 gather targets dxbar (n+1) and dy (m+1); the
 // FP32 matrix slices with 16-bit indices; dx, d, l - x^, u - x^ (n each);
 // r and the inequality bound -y^ (m each)), and in the CTA's global slab the
-// two FP64 point buffers of x and y and the FP32 reduced cost / residual of
-// the last evaluated candidate.  Returns recentred = 0 when the shared part
+// two FP64 point buffers of x and y, the FP32 reduced cost / residual of
+// the last evaluated candidate, and the instance's scaled FP64 objective,
+// bounds and right-hand side.  Returns recentred = 0 when the shared part
 // does not fit.
 inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, int at_nslices,
                                         int64_t a_elems, int64_t at_elems, int64_t smem_cap) {
@@ -220,6 +221,12 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, 
     slab += align_up(int64_t(n) * 4, 16);
     L.rcand = slab;
     slab += align_up(int64_t(m) * 4, 16);
+    for (int64_t* o : {&L.sc_c, &L.sc_l, &L.sc_u}) {
+        *o = slab;
+        slab += align_up(int64_t(n) * 8, 16);
+    }
+    L.sc_b = slab;
+    slab += align_up(int64_t(m) * 8, 16);
     P.smem_bytes = off;
     P.slab_bytes = slab;
     return P;

@@ -858,8 +858,36 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
 // matrix, exactly like the FP64 phase.
 // Shared memory holds dxbar, dy (gather targets), the FP32 matrix slices,
 // dx, d, l - x^, u - x^, r and the inequality-row bound -y^ (in the slots of
-// xbar, y, x, c, l, u, b, ya).
+// xbar, y, x, c, l, u, b, ya).  The slab also keeps the instance's scaled
+// FP64 objective and bounds (new column order) and right-hand side, so the
+// convergence test reads them without permutation or division.
 // ---------------------------------------------------------------------------
+
+// Slice product from shared memory with two interleaved accumulators (even
+// and odd k), summed at the end.
+__device__ __forceinline__ float slice_dot_fast2(const uint16_t* ip, const float* vp, const float* g, int len) {
+    float a0 = 0.0f, a1 = 0.0f;
+    int k = 0;
+    for (; k + 4 <= len; k += 4, ip += 128, vp += 128) {
+        const int i0 = ip[0], i1 = ip[32], i2 = ip[64], i3 = ip[96];
+        const float v0 = vp[0], v1 = vp[32], v2 = vp[64], v3 = vp[96];
+        a0 = fmaf(v0, g[i0], a0);
+        a1 = fmaf(v1, g[i1], a1);
+        a0 = fmaf(v2, g[i2], a0);
+        a1 = fmaf(v3, g[i3], a1);
+    }
+    if (k + 2 <= len) {
+        const int i0 = ip[0], i1 = ip[32];
+        const float v0 = vp[0], v1 = vp[32];
+        a0 = fmaf(v0, g[i0], a0);
+        a1 = fmaf(v1, g[i1], a1);
+        k += 2;
+        ip += 64;
+        vp += 64;
+    }
+    if (k < len) a0 = fmaf(vp[0], g[ip[0]], a0);
+    return a0 + a1;
+}
 
 __device__ __forceinline__ void primal_pass_recentred(const FastOffsets& o, const int4* atlist, int t0, int t1,
                                                       int n, int lane, float tau, float w, float rho, bool check,
@@ -870,11 +898,14 @@ __device__ __forceinline__ void primal_pass_recentred(const FastOffsets& o, cons
     const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
         const int4 sl = atlist[t];
-        const float g = slice_dot_fast<float>(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S, sl.z);
         const int j = (sl.x << 5) + lane;
-        if (j < n) {
-            const float xo = S[o.x + j];
-            const float xn = clampT(xo - tau * (S[o.c + j] - g), S[o.l + j], S[o.u + j]);
+        const bool own = j < n;
+        const int jj = own ? j : 0;
+        // the column's operands first: their latency overlaps the product
+        const float xo = S[o.x + jj], dj = S[o.c + jj], lj = S[o.l + jj], uj = S[o.u + jj];
+        const float g = slice_dot_fast2(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S, sl.z);
+        if (own) {
+            const float xn = clampT(xo - tau * (dj - g), lj, uj);
             const float xb = xn + xn - xo;
             S[o.xbar + j] = xb;
             const float xh = (rho == 1.0f) ? xb : (1.0f + rho) * xn - rho * xo;
@@ -897,15 +928,14 @@ __device__ __forceinline__ void dual_pass_recentred(const FastOffsets& o, const 
     const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
         const int4 sl = alist[t];
-        const float h = slice_dot_fast<float>(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S, sl.z);
         const int i = (sl.x << 5) + lane;
-        if (i < m) {
-            const float yo = S[o.y + i];
-            float yn = yo + sigma * (S[o.b + i] - h);
-            if (i >= neq) {
-                const float yl = S[o.ya + i];  // y^ + dy <= 0
-                if (yn > yl) yn = yl;
-            }
+        const bool own = i < m;
+        const int ii = own ? i : 0;
+        const float yo = S[o.y + ii], ri = S[o.b + ii], yl = S[o.ya + ii];
+        const float h = slice_dot_fast2(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S, sl.z);
+        if (own) {
+            float yn = yo + sigma * (ri - h);
+            if (i >= neq && yn > yl) yn = yl;  // y^ + dy <= 0
             const float yh = (rho == 1.0f) ? yn + yn - yo : (1.0f + rho) * yn - rho * yo;
             S[o.y + i] = w * yh;
             if (check) {
@@ -918,71 +948,105 @@ __device__ __forceinline__ void dual_pass_recentred(const FastOffsets& o, const 
     }
 }
 
-// FP64 KKT partials at the candidate (xc, yc) (scaled, FP64) as kkt_partials
-// computes them; in addition the candidate x is projected onto the exact
-// FP64 bounds (written back: the FP32 bounds l - x^ are rounded), and the
-// scaled reduced cost d = c~ - A~^T yc and primal residual r = b~ - A~ xc are
-// stored in FP32 for a re-centring at this candidate.  All threads call it
-// (it synchronises between the column and the row loops).
-__device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const int4* alist, const int4* atlist,
-                                                    int a0, int a1, int t0, int t1, double* xc, const double* yc,
-                                                    const double* lower, const double* upper, const double* cost,
-                                                    const double* rhs, float* dcand, float* rcand, int lane,
-                                                    double* v) {
+// FP64 slice product for the convergence test: the 16-bit column indices
+// come from the staged copy in shared memory (minus the gather-target
+// offset `sub`), the FP64 values from global memory, the FP64 gather
+// target from the slab.  The value loads do not depend on the indices, so
+// one memory round trip serves each batch.
+__device__ __forceinline__ double slice_dot64_staged(const uint16_t* sip, int sub, const double* __restrict__ vp,
+                                                     const double* g, int len) {
+    constexpr int U = 4;
+    double acc0 = 0.0, acc1 = 0.0;
+    for (int k0 = 0; k0 < len; k0 += U) {
+        double vv[U], gg[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            if (k < len) {
+                vv[u] = __ldg(vp + (k << 5));
+                gg[u] = g[static_cast<int>(sip[k << 5]) - sub];
+            } else {
+                vv[u] = 0.0;
+                gg[u] = 0.0;
+            }
+        }
+        acc0 = fma(vv[0], gg[0], acc0);
+        acc1 = fma(vv[1], gg[1], acc1);
+        acc0 = fma(vv[2], gg[2], acc0);
+        acc1 = fma(vv[3], gg[3], acc1);
+    }
+    return acc0 + acc1;
+}
+
+// FP64 KKT partials at the candidate (xc, yc) (scaled, FP64) in the index
+// map of kkt_partials, computed in scaled space with the slab's scaled
+// objective cs, bounds ls/us and right-hand side bs (c.x = cs.xs,
+// r_j l_j = rs_j ls_j with rs = cs - A~^T y the scaled reduced cost, ...).
+// The candidate x is projected onto the exact FP64 bounds (written back: the
+// FP32 bounds l - x^ are rounded), and rs and the scaled primal residual
+// bs - A~ xc are stored in FP32 for a re-centring at this candidate.
+// |c|_inf (v[14]) is accumulated only when `cinf` is set.  All threads call
+// it (it synchronises between the column and the row loops).
+__device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const FastOffsets& o, const int4* alist,
+                                                    const int4* atlist, int a0, int a1, int t0, int t1, int a_sub,
+                                                    int t_sub, double* xc, const double* yc, const double* cs,
+                                                    const double* ls, const double* us, const double* bs,
+                                                    float* dcand, float* rcand, bool cinf, int lane, double* v) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
     const int n = sp->n, m = sp->m, neq = sp->neq;
     for (int t = t0; t < t1; ++t) {
         const int4 sl = atlist[t];
-        const double g = slice_dot64<double>(sp->at_idx, sp->at_v64, sl.y, sl.z, lane, yc);
         const int j = (sl.x << 5) + lane;
-        if (j < n) {
-            const int jo = sp->col_perm[j];
-            const double dcj = sp->dc[j];
-            const double c = cost[jo], l = lower[jo], u = upper[jo];
-            double xsc = xc[j];
-            const double ls = l / dcj, us = u / dcj;
-            if (xsc < ls || xsc > us) {
-                xsc = xsc < ls ? ls : us;
+        const bool own = j < n;
+        const int jj = own ? j : 0;
+        const double cj = cs[jj], lj = ls[jj], uj = us[jj], dcj = __ldg(sp->dc + jj);
+        double xsc = xc[jj];
+        const double g = slice_dot64_staged(SI + o.at_idx + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z);
+        if (own) {
+            if (xsc < lj || xsc > uj) {
+                xsc = xsc < lj ? lj : uj;
                 xc[j] = xsc;
             }
-            const double xv = xsc * dcj;
-            const double r = c - g / dcj;
-            dcand[j] = static_cast<float>(c * dcj - g);
-            v[0] += c * xv;
-            if (r > 0.0) {
-                if (isfinite(l)) v[2] += r * l;
-                else v[11] = fmax(v[11], r);
-            } else if (r < 0.0) {
-                if (isfinite(u)) v[2] += r * u;
-                else v[11] = fmax(v[11], -r);
+            const double rs = cj - g;
+            dcand[j] = static_cast<float>(rs);
+            v[0] += cj * xsc;
+            if (rs > 0.0) {
+                if (isfinite(lj)) v[2] += rs * lj;
+                else v[11] = fmax(v[11], rs * __ldg(sp->inv_dc + j));
+            } else if (rs < 0.0) {
+                if (isfinite(uj)) v[2] += rs * uj;
+                else v[11] = fmax(v[11], -rs * __ldg(sp->inv_dc + j));
             }
-            const double tg = (r >= 0.0) ? l : u;
-            if (isfinite(tg)) v[3] += fabs(r * (xv - tg));
-            v[12] = fmax(v[12], fmax(l - xv, xv - u));
-            v[13] = fmax(v[13], fabs(xv));
-            v[14] = fmax(v[14], fabs(c));
-            if (isnan(g) || isnan(xv)) v[15] = 1.0;
+            const double tg = (rs >= 0.0) ? lj : uj;
+            if (isfinite(tg)) v[3] += fabs(rs * (xsc - tg));
+            v[12] = fmax(v[12], dcj * fmax(lj - xsc, xsc - uj));
+            v[13] = fmax(v[13], fabs(xsc * dcj));
+            if (cinf) v[14] = fmax(v[14], fabs(cj * __ldg(sp->inv_dc + j)));
+            if (isnan(g) || isnan(xsc)) v[15] = 1.0;
         }
     }
     __syncthreads();  // the projected xc is the gather target below
     for (int t = a0; t < a1; ++t) {
         const int4 sl = alist[t];
-        const double h = slice_dot64<double>(sp->a_idx, sp->a_v64, sl.y, sl.z, lane, xc);
         const int i = (sl.x << 5) + lane;
-        if (i < m) {
-            const double dri = sp->dr[i];
-            const double b = rhs ? rhs[sp->row_perm[i]] : 0.0;
-            const double yv = yc[i] * dri;
-            const double ro = h / dri - b;
-            rcand[i] = static_cast<float>(b * dri - h);
+        const bool own = i < m;
+        const int ii = own ? i : 0;
+        const double bi = bs[ii], ysc = yc[ii];
+        const double h = slice_dot64_staged(SI + o.a_idx + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z);
+        if (own) {
+            const double rr = bi - h;                  // scaled b - A x
+            const double ro = -rr * __ldg(sp->inv_dr + i);  // A x - b in original units
+            rcand[i] = static_cast<float>(rr);
             if (i < neq) {
                 v[10] = fmax(v[10], fabs(ro));
             } else {
                 v[10] = fmax(v[10], ro);
-                v[4] += fabs(yv * ro);
-                v[11] = fmax(v[11], yv);
+                v[4] += fabs(ysc * rr);
+                v[11] = fmax(v[11], ysc * __ldg(sp->dr + i));
             }
-            v[1] += b * yv;
-            if (isnan(h) || isnan(yv)) v[15] = 1.0;
+            v[1] += bi * ysc;
+            if (isnan(h) || isnan(ysc)) v[15] = 1.0;
         }
     }
 }
@@ -992,17 +1056,15 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
 // zero the differences.  Callers synchronise afterwards.
 __device__ __forceinline__ void recentre(const DevSpecies* sp, const FastOffsets& o, const double* bx,
                                          const double* by, const float* dcand, const float* rcand,
-                                         const double* lower, const double* upper) {
+                                         const double* ls, const double* us) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
     const int n = sp->n, m = sp->m, neq = sp->neq;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        const int jo = sp->col_perm[j];
-        const double dcj = sp->dc[j];
         const double xb = bx[j];
         S[o.c + j] = dcand[j];
-        S[o.l + j] = static_cast<float>(lower[jo] / dcj - xb);
-        S[o.u + j] = static_cast<float>(upper[jo] / dcj - xb);
+        S[o.l + j] = static_cast<float>(ls[j] - xb);
+        S[o.u + j] = static_cast<float>(us[j] - xb);
         S[o.x + j] = 0.0f;
     }
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -1044,6 +1106,8 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         }
         float* const S = reinterpret_cast<float*>(dyn_smem);
         const FastOffsets o = fast_offsets<float>(L);
+        // the staged 16-bit indices carry the gather-target offsets
+        const int a_sub = static_cast<int>(L.arr[kXbar] / 4), t_sub = static_cast<int>(L.arr[kY] / 4);
         // the two point buffers; selected by value (no local-memory array)
         double* const px0 = reinterpret_cast<double*>(slab + L.pt_x[0]);
         double* const px1 = reinterpret_cast<double*>(slab + L.pt_x[1]);
@@ -1053,6 +1117,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         auto PY = [&](int b) { return b ? py1 : py0; };
         float* const dcand = reinterpret_cast<float*>(slab + L.dcand);
         float* const rcand = reinterpret_cast<float*>(slab + L.rcand);
+        double* const cs = reinterpret_cast<double*>(slab + L.sc_c);
+        double* const ls = reinterpret_cast<double*>(slab + L.sc_l);
+        double* const us = reinterpret_cast<double*>(slab + L.sc_u);
+        double* const bs = reinterpret_cast<double*>(slab + L.sc_b);
         const int4* alist = reinterpret_cast<const int4*>(dyn_smem + L.list_a);
         const int4* atlist = reinterpret_cast<const int4*>(dyn_smem + L.list_at);
         const int32_t* soa = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_a_off);
@@ -1064,7 +1132,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         const double* c_i = p.cost + coff;
         const double* b_i = p.rhs ? p.rhs + roff : nullptr;
 
-        // ---- the start point, FP64, projected, becomes buffer 0 ----
+        // ---- scaled instance data and the start point (FP64, projected) ----
         int bad = 0;
         for (int j = tid; j < n; j += nthreads) {
             const int jo = sp->col_perm[j];
@@ -1072,15 +1140,20 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             const double lv = lo_i[jo], uv = up_i[jo], cv = c_i[jo];
             if (isnan(lv) || isnan(uv) || lv > uv || !isfinite(cv) || lv == INFINITY || uv == -INFINITY)
                 bad = 1;
+            const double lsj = lv / dcj, usj = uv / dcj;
+            cs[j] = cv * dcj;
+            ls[j] = lsj;
+            us[j] = usj;
             double x0 = p.warm_x ? p.warm_x[coff + jo] / dcj : 0.0;
             if (!isfinite(x0)) x0 = 0.0;
-            const double ls = lv / dcj, us = uv / dcj;
-            PX(0)[j] = x0 < ls ? ls : (x0 > us ? us : x0);
+            PX(0)[j] = x0 < lsj ? lsj : (x0 > usj ? usj : x0);
         }
         for (int i = tid; i < m; i += nthreads) {
             const int io = sp->row_perm[i];
             const double dri = sp->dr[i];
-            if (b_i && !isfinite(b_i[io])) bad = 1;
+            const double bv = b_i ? b_i[io] : 0.0;
+            if (!isfinite(bv)) bad = 1;
+            bs[i] = bv * dri;
             double y0 = p.warm_y ? p.warm_y[roff + io] / dri : 0.0;
             if (!isfinite(y0)) y0 = 0.0;
             if (i >= neq && y0 > 0.0) y0 = 0.0;
@@ -1118,19 +1191,21 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         int status = -1;
         int cur = 0;   // buffer holding the base
         int ev = 0;    // buffer holding the last evaluated point
+        double cinf = 0.0;
         Metrics M;
         {
             double v[kRed];
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-            kkt_partials_recentred(sp, alist, atlist, aw0, aw1, tw0, tw1, PX(0), PY(0), lo_i, up_i, c_i, b_i,
-                                   dcand, rcand, lane, v);
+            kkt_partials_recentred(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
+                                   us, bs, dcand, rcand, true, lane, v);
             block_reduce(v, s_red, s_tot);
+            cinf = s_tot[14];
             M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
             if (M.conv) status = p.final_status;
             else if (p.max_iters <= 0) status = M.nan ? kStatusNumerical : kStatusIterationLimit;
             if (status < 0) {
-                recentre(sp, o, PX(0), PY(0), dcand, rcand, lo_i, up_i);
+                recentre(sp, o, PX(0), PY(0), dcand, rcand, ls, us);
                 __syncthreads();
             }
         }
@@ -1161,9 +1236,11 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             v[6] = pdy2;
             v[7] = pdxa2;
             v[8] = pdya2;
-            kkt_partials_recentred(sp, alist, atlist, aw0, aw1, tw0, tw1, PX(cur ^ 1), PY(cur ^ 1), lo_i, up_i,
-                                   c_i, b_i, dcand, rcand, lane, v);
+            kkt_partials_recentred(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
+                                   cs, ls, us, bs, dcand, rcand, false, lane, v);
             block_reduce(v, s_red, s_tot);
+            if (threadIdx.x == 0) s_tot[14] = cinf;
+            __syncthreads();
             M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
             ev = cur ^ 1;
             if (M.nan || !isfinite(M.r)) {
@@ -1208,23 +1285,18 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 omega = 1.0;
                 double* cx = PX(cur ^ 1);
                 double* cyv = PY(cur ^ 1);
-                for (int j = tid; j < n; j += nthreads) {
-                    const int jo = sp->col_perm[j];
-                    const double dcj = sp->dc[j];
-                    const double ls = lo_i[jo] / dcj, us = up_i[jo] / dcj;
-                    cx[j] = 0.0 < ls ? ls : (0.0 > us ? us : 0.0);
-                }
+                for (int j = tid; j < n; j += nthreads) cx[j] = 0.0 < ls[j] ? ls[j] : (0.0 > us[j] ? us[j] : 0.0);
                 for (int i = tid; i < m; i += nthreads) cyv[i] = 0.0;
                 __syncthreads();
                 double vv[kRed];
 #pragma unroll
                 for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-                kkt_partials_recentred(sp, alist, atlist, aw0, aw1, tw0, tw1, cx, cyv, lo_i, up_i, c_i, b_i,
-                                       dcand, rcand, lane, vv);
+                kkt_partials_recentred(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
+                                       bs, dcand, rcand, false, lane, vv);
                 block_reduce(vv, s_red, s_tot);
                 cur ^= 1;
                 ev = cur;
-                recentre(sp, o, PX(cur), PY(cur), dcand, rcand, lo_i, up_i);
+                recentre(sp, o, PX(cur), PY(cur), dcand, rcand, ls, us);
                 k = 0;
                 r_restart = INFINITY;
                 r_prev = INFINITY;
@@ -1240,7 +1312,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 if (nx > 1e-10 && ny > 1e-10)
                     omega = exp(kOmegaSmoothing * log(ny / nx) + (1.0 - kOmegaSmoothing) * log(omega));
                 cur ^= 1;  // the candidate becomes the base
-                recentre(sp, o, PX(cur), PY(cur), dcand, rcand, lo_i, up_i);
+                recentre(sp, o, PX(cur), PY(cur), dcand, rcand, ls, us);
                 k = 0;
                 r_restart = M.r;
                 r_prev = INFINITY;
@@ -1251,8 +1323,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         }
 
         // ---- results (original units and order) from the last evaluated point ----
-        const bool hand = p.handoff_list != nullptr && status != kStatusOptimal && status != kStatusNumerical &&
-                          status != kStatusIterationLimit;
+        const bool hand = p.handoff_list != nullptr && status == kStatusHandoff;
         const double* fx = PX(ev);
         const double* fy = PY(ev);
         double* ox = hand ? p.hand_x : p.out_x;

@@ -66,6 +66,8 @@ struct DevSpecies {
     const int32_t* lo_at_ptr;
     const int32_t* lo_at_idx;
     const double* lo_at_val;
+    const double* inv_dr;         // 1 / dr, new order
+    const double* inv_dc;         // 1 / dc, new order
 };
 
 // Byte offsets of one species' working set inside the CTA's dynamic shared
@@ -81,6 +83,9 @@ struct Layout {
     // re-centring -- and the FP32 reduced cost / primal residual of the last
     // evaluated candidate
     int64_t pt_x[2], pt_y[2], dcand, rcand;
+    // and the instance's scaled FP64 objective and bounds (new column order)
+    // and scaled right-hand side (new row order)
+    int64_t sc_c, sc_l, sc_u, sc_b;
 };
 
 struct KernelParams {
