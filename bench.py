@@ -125,9 +125,10 @@ def hbm_peak():
 
 
 def profiled_traffic():
-    """DRAM bytes per FP32-phase instance-iteration from the committed ncu
-    summary (profiles/pdhg_fp32_community.txt), if present."""
-    p = ROOT / "profiles" / "pdhg_fp32_community.txt"
+    """DRAM bytes per instance-iteration of the re-centred phase from the
+    committed ncu summary of a smaller case of the same step
+    (profiles/pdhg_recentred_community_small.txt), if present."""
+    p = ROOT / "profiles" / "pdhg_recentred_community_small.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():

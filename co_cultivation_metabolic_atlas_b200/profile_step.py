@@ -27,8 +27,13 @@ def main():
     medium, biomass = syn.initial_environments(args.envs)
     com = DeviceCommunity(models, medium, biomass, config=SolveConfig(precision=args.precision),
                           options=EngineOptions(warps_per_block=args.warps), warm_start=args.warm)
-    for _ in range(args.steps):
+    for k in range(args.steps):
         st = com.step()
+        if args.precision == "mixed":
+            phase = com.engine.phase_iterations()
+            t32, t64 = com.engine.phase_times()
+            print(f"step {k}: first-phase instance-iterations {int(phase.sum().item())}, "
+                  f"first phase {t32:.3f} ms, FP64 phase {t64:.3f} ms")
     torch.cuda.synchronize()
     print("certified", int(st.certified.item()), "of", st.lps)
     com.close()

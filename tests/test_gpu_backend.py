@@ -88,3 +88,19 @@ def test_unsolved_rows_fail_closed():
     assert all(r.x is None and r.fun is None for r in rows)
     assert "no CPU fallback" in rows[0].message
     be.close()
+
+
+def test_reference_traces_replay_through_the_backend(golden_dir, tmp_path, forbid_cpu_optimizers):
+    """LP traces written by the reference's trace writer (one with an
+    inequality row) replay through ``solve_batch`` to their HiGHS optima."""
+    import shutil
+    from co_cultivation_metabolic_atlas_b200 import B200LPBackend, lp_trace
+    d = tmp_path / "traces"
+    shutil.copytree(golden_dir / "traces", d)
+    be = B200LPBackend(mode="cold")
+    rows, ref = lp_trace.replay(d, be)
+    be.close()
+    assert len(rows) == 3
+    for r, fun in zip(rows, ref):
+        assert r.success, r.message
+        assert abs(r.fun - fun) <= 1e-6 * max(1.0, abs(fun))

@@ -202,3 +202,42 @@ def test_recentred_handoff_finishes_in_fp64(golden_dir):
     assert r["status"] == pdhg.STATUS_OPTIMAL and r["iterations"] > first["iterations"]
     fun = float(g["fun"][1])
     assert abs(r["metrics"]["objective"] - fun) <= 1e-6 * max(1.0, abs(fun))
+
+
+def test_trajectory_fixture_is_pinned_to_highs_and_the_oracle(golden_dir):
+    """The 48 h fixture's LP objectives agree with HiGHS at the sampled steps,
+    and re-running the oracle's first steps reproduces the fixture."""
+    import importlib.util
+    g = np.load(golden_dir / "trajectory_community.npz")
+    hs = g["highs_steps"]
+    ours = g["objective"][hs]
+    ref = g["highs_objective"]
+    assert np.all(np.isfinite(ref))
+    assert np.all(np.abs(ours - ref) <= 1e-6 * np.maximum(1.0, np.abs(ref)))
+    spec = importlib.util.spec_from_file_location("make_trajectory", golden_dir / "make_trajectory.py")
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    _, states = mk.rollout(0, int(g["envs"]), 3)
+    np.testing.assert_array_equal(np.array(states["objective"]), g["objective"][:3, 0])
+    np.testing.assert_array_equal(states["biomass"][0][1], g["biomass"][0, 0])
+
+
+def test_medium_exchange_fluxes_are_not_determined_by_the_lps():
+    """Flux variability at the optimum: with the growth objective held at its
+    optimum, medium exchange fluxes still span their whole bound range, so a
+    metabolite trajectory depends on which optimal point a solver returns."""
+    from scipy.optimize import linprog
+    from scipy.sparse import csr_matrix
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(4, seed=11)
+    mdl = models[2]
+    lo = dfba.uptake_lower_bounds(mdl, medium, biomass, 0.05)[0]
+    st, fun, _, _ = highs.solve_one(mdl.S, lo, mdl.upper, mdl.cost)
+    kw = dict(A_eq=mdl.S, b_eq=np.zeros(mdl.S.shape[0]), A_ub=csr_matrix(mdl.cost[None, :]),
+              b_ub=[fun + 1e-7 * abs(fun)], bounds=np.column_stack([lo, mdl.upper]), method="highs")
+    col = int(mdl.medium_columns[0])
+    e = np.zeros(mdl.S.shape[1])
+    e[col] = 1.0
+    vmin = linprog(e, **kw).fun
+    vmax = -linprog(-e, **kw).fun
+    assert vmin == pytest.approx(lo[col], abs=1e-6) and vmax == pytest.approx(mdl.upper[col], rel=1e-6)
