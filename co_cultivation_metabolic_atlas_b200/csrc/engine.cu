@@ -335,30 +335,35 @@ int fbalp_engine_layout(const fbalp_engine* e, int64_t* total_cols, int64_t* tot
 
 namespace {
 
-// True when every species of the bound batch fits the re-centred FP32
-// shared-memory layout (the re-centred phase has no streamed-matrix variant).
-bool recentred_fits(fbalp_engine* e) {
+// Re-centred FP32 layout of the bound batch: 1 when every species fits with
+// its matrix staged in shared memory, 2 when every species' vectors fit
+// with the matrix streamed from L2 (one variant per launch), 0 otherwise.
+int recentred_mode(fbalp_engine* e) {
     const int threads = e->opt.warps_per_block * 32;
     const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
     int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
                       ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
     if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
-    if (e->opt.stage_matrix == 0) return false;
     std::vector<char> used(e->species.size(), 0);
     for (int32_t s : e->h_species) used[s] = 1;
+    bool staged = e->opt.stage_matrix != 0, streamed = true;
     for (size_t s = 0; s < e->species.size(); ++s) {
         if (!used[s]) continue;
         const SpeciesHost& sh = e->species[s];
-        if (!fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
-                                          sh.A.off.back(), sh.AT.off.back(), cap).layout.recentred)
-            return false;
+        for (int st = 0; st < 2; ++st) {
+            bool& ok = st ? staged : streamed;
+            if (ok && !fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                                    sh.A.off.back(), sh.AT.off.back(), cap, st != 0)
+                           .layout.recentred)
+                ok = false;
+        }
     }
-    return true;
+    return staged ? 1 : (streamed ? 2 : 0);
 }
 
 // Launch one precision phase over the bound batch (`recentred`: the
-// re-centred FP32 kernel).
-void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, bool recentred = false) {
+// re-centred FP32 kernel in mode 1 (staged matrix) or 2 (streamed)).
+void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred = 0) {
     const int esz = fp64 ? static_cast<int>(sizeof(double)) : static_cast<int>(sizeof(float));
     const int threads = e->opt.warps_per_block * 32;
     const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
@@ -388,7 +393,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, bool recentred
         const SpeciesHost& sh = e->species[s];
         fbalp::LayoutPlan P = recentred
             ? fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
-                                           sh.A.off.back(), sh.AT.off.back(), cap)
+                                           sh.A.off.back(), sh.AT.off.back(), cap, recentred == 1)
             : unscaled
             ? fbalp::plan_layout_unscaled(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
                                           sh.A.off.back(), sh.AT.off.back(), cap)
@@ -408,7 +413,8 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, bool recentred
     dl.ensure(layouts.size() * sizeof(fbalp::Layout));
     check(cudaMemcpyAsync(dl.ptr, layouts.data(), layouts.size() * sizeof(fbalp::Layout),
                           cudaMemcpyHostToDevice, e->stream), "copy layouts");
-    const void* k = recentred ? fbalp::recentred_symbol(threads) : fbalp::kernel_symbol(fp64, threads, all_fast);
+    const void* k = recentred ? fbalp::recentred_symbol(threads, recentred == 1)
+                              : fbalp::kernel_symbol(fp64, threads, all_fast);
     check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
           "cudaFuncSetAttribute");
     int per_sm = 0;
@@ -430,7 +436,8 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, bool recentred
     const int ph = fp64 ? 1 : 0;
     check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
     if (recentred)
-        check(fbalp::launch_recentred(grid, threads, dyn, e->stream, p), "re-centred pdhg kernel launch");
+        check(fbalp::launch_recentred(recentred == 1, grid, threads, dyn, e->stream, p),
+              "re-centred pdhg kernel launch");
     else
         check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
     check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
@@ -512,7 +519,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p.passthrough_tol = 0.0;
             p.fallback_iters = q.fallback_iterations;
             run_phase(e, fp64, p);
-        } else if (q.fp32_recentre && recentred_fits(e)) {
+        } else if (q.fp32_recentre && recentred_mode(e) != 0) {
             // re-centred FP32 phase to the FP64 tolerances; what it does not
             // certify (stalled instances) continues in the FP64 phase
             e->mid_x.ensure(e->total_cols * sizeof(double));
@@ -551,7 +558,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             pr.hand_omega = static_cast<double*>(e->mid_omega.ptr);
             pr.hand_iters = static_cast<int32_t*>(e->mid_iters.ptr);
             pr.handoff_on_stall = 4 * q.fp64_stall_checks;
-            run_phase(e, false, pr, true);
+            run_phase(e, false, pr, recentred_mode(e));
             fbalp::KernelParams p64 = p;
             p64.order = static_cast<const int32_t*>(e->hand_list.ptr);
             p64.count_dev = static_cast<const int32_t*>(e->hand_count.ptr);

@@ -171,9 +171,10 @@ inline LayoutPlan plan_layout_unscaled(int n, int m, int warps, int a_nslices, i
 // two FP64 point buffers of x and y, the FP32 reduced cost / residual of
 // the last evaluated candidate, and the instance's scaled FP64 objective,
 // bounds and right-hand side.  Returns recentred = 0 when the shared part
-// does not fit.
+// does not fit.  With `stage` false the matrix is not staged (it is streamed
+// from L2 every iteration) and only the vectors need to fit.
 inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, int at_nslices,
-                                        int64_t a_elems, int64_t at_elems, int64_t smem_cap) {
+                                        int64_t a_elems, int64_t at_elems, int64_t smem_cap, bool stage = true) {
     LayoutPlan P{};
     Layout& L = P.layout;
     int64_t off = 0;
@@ -197,18 +198,22 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, 
     };
     put(kXbar);
     put(kY);
-    L.mat_a_idx = off;
-    off += align_up(2 * a_elems, 16);
-    L.mat_at_idx = off;
-    off += align_up(2 * at_elems, 16);
-    L.mat_a_val = off;
-    off += align_up(4 * a_elems, 16);
-    L.mat_at_val = off;
-    off += align_up(4 * at_elems, 16);
+    if (stage) {
+        L.mat_a_idx = off;
+        off += align_up(2 * a_elems, 16);
+        L.mat_at_idx = off;
+        off += align_up(2 * at_elems, 16);
+        L.mat_a_val = off;
+        off += align_up(4 * a_elems, 16);
+        L.mat_at_val = off;
+        off += align_up(4 * at_elems, 16);
+    }
     for (int a : {kX, kC, kL, kU, kB, kYa}) put(a);
-    // every 16-bit index is an element offset from the start of shared memory
-    if (off > smem_cap || off / 4 > (int64_t(1) << 16) - 1) return P;
-    L.mat_smem = 1;
+    if (off > smem_cap) return P;
+    // every staged 16-bit index is an element offset from the start of
+    // shared memory
+    if (stage && off / 4 > (int64_t(1) << 16) - 1) return P;
+    L.mat_smem = stage ? 1 : 0;
     L.recentred = 1;
     int64_t slab = 0;
     for (int b = 0; b < 2; ++b) {
@@ -244,8 +249,9 @@ inline bool layout_aligned(const Layout& L) {
 }
 
 const void* kernel_symbol(bool fp64, int threads, bool fast);
-const void* recentred_symbol(int threads);
-cudaError_t launch_recentred(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p);
+const void* recentred_symbol(int threads, bool staged);
+cudaError_t launch_recentred(bool staged, int grid, int threads, size_t smem, cudaStream_t stream,
+                             const KernelParams& p);
 cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
                         const KernelParams& p);
 

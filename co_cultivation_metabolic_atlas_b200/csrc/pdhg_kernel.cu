@@ -889,9 +889,39 @@ __device__ __forceinline__ float slice_dot_fast2(const uint16_t* ip, const float
     return a0 + a1;
 }
 
-__device__ __forceinline__ void primal_pass_recentred(const FastOffsets& o, const int4* atlist, int t0, int t1,
-                                                      int n, int lane, float tau, float w, float rho, bool check,
-                                                      const double* bx, double* cx, double& pdx2,
+// Slice product with the matrix streamed from global memory (L2): int32
+// indices relative to the gather target `g`, FP32 values; batches of eight
+// loads in flight, two accumulators.
+__device__ __forceinline__ float slice_dot_global2(const int32_t* __restrict__ ip, const float* __restrict__ vp,
+                                                   const float* g, int len) {
+    constexpr int U = 8;
+    float a0 = 0.0f, a1 = 0.0f;
+    for (int k0 = 0; k0 < len; k0 += U) {
+        int ii[U];
+        float vv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            if (k < len) {
+                ii[u] = __ldg(ip + (k << 5));
+                vv[u] = __ldg(vp + (k << 5));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u += 2) {
+            if (k0 + u < len) a0 = fmaf(vv[u], g[ii[u]], a0);
+            if (k0 + u + 1 < len) a1 = fmaf(vv[u + 1], g[ii[u + 1]], a1);
+        }
+    }
+    return a0 + a1;
+}
+
+// STAGED: the species' matrix slices are in shared memory (16-bit indices
+// pre-offset to the gather target); otherwise they are streamed from L2.
+template <bool STAGED>
+__device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const int4* atlist,
+                                                      int t0, int t1, int n, int lane, float tau, float w, float rho,
+                                                      bool check, const double* bx, double* cx, double& pdx2,
                                                       double& pdxa2) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
@@ -903,7 +933,9 @@ __device__ __forceinline__ void primal_pass_recentred(const FastOffsets& o, cons
         const int jj = own ? j : 0;
         // the column's operands first: their latency overlaps the product
         const float xo = S[o.x + jj], dj = S[o.c + jj], lj = S[o.l + jj], uj = S[o.u + jj];
-        const float g = slice_dot_fast2(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S, sl.z);
+        const float g = STAGED
+            ? slice_dot_fast2(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S, sl.z)
+            : slice_dot_global2(sp->at_idx + sl.y + lane, sp->at_v32 + sl.y + lane, S + o.y, sl.z);
         if (own) {
             const float xn = clampT(xo - tau * (dj - g), lj, uj);
             const float xb = xn + xn - xo;
@@ -920,9 +952,11 @@ __device__ __forceinline__ void primal_pass_recentred(const FastOffsets& o, cons
     }
 }
 
-__device__ __forceinline__ void dual_pass_recentred(const FastOffsets& o, const int4* alist, int t0, int t1, int m,
-                                                    int neq, int lane, float sigma, float w, float rho, bool check,
-                                                    const double* by, double* cy, double& pdy2, double& pdya2) {
+template <bool STAGED>
+__device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const int4* alist,
+                                                    int t0, int t1, int m, int neq, int lane, float sigma, float w,
+                                                    float rho, bool check, const double* by, double* cy, double& pdy2,
+                                                    double& pdya2) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
     const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
@@ -932,7 +966,9 @@ __device__ __forceinline__ void dual_pass_recentred(const FastOffsets& o, const 
         const bool own = i < m;
         const int ii = own ? i : 0;
         const float yo = S[o.y + ii], ri = S[o.b + ii], yl = S[o.ya + ii];
-        const float h = slice_dot_fast2(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S, sl.z);
+        const float h = STAGED
+            ? slice_dot_fast2(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S, sl.z)
+            : slice_dot_global2(sp->a_idx + sl.y + lane, sp->a_v32 + sl.y + lane, S + o.xbar, sl.z);
         if (own) {
             float yn = yo + sigma * (ri - h);
             if (i >= neq && yn > yl) yn = yl;  // y^ + dy <= 0
@@ -978,6 +1014,34 @@ __device__ __forceinline__ double slice_dot64_staged(const uint16_t* sip, int su
     return acc0 + acc1;
 }
 
+// The same product with the indices streamed from global memory; the
+// accumulation order equals slice_dot64_staged's, so both variants produce
+// identical results.
+__device__ __forceinline__ double slice_dot64_global2(const int32_t* __restrict__ ip, const double* __restrict__ vp,
+                                                      const double* g, int len) {
+    constexpr int U = 4;
+    double acc0 = 0.0, acc1 = 0.0;
+    for (int k0 = 0; k0 < len; k0 += U) {
+        double vv[U], gg[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            if (k < len) {
+                vv[u] = __ldg(vp + (k << 5));
+                gg[u] = g[__ldg(ip + (k << 5))];
+            } else {
+                vv[u] = 0.0;
+                gg[u] = 0.0;
+            }
+        }
+        acc0 = fma(vv[0], gg[0], acc0);
+        acc1 = fma(vv[1], gg[1], acc1);
+        acc0 = fma(vv[2], gg[2], acc0);
+        acc1 = fma(vv[3], gg[3], acc1);
+    }
+    return acc0 + acc1;
+}
+
 // FP64 KKT partials at the candidate (xc, yc) (scaled, FP64) in the index
 // map of kkt_partials, computed in scaled space with the slab's scaled
 // objective cs, bounds ls/us and right-hand side bs (c.x = cs.xs,
@@ -987,6 +1051,7 @@ __device__ __forceinline__ double slice_dot64_staged(const uint16_t* sip, int su
 // bs - A~ xc are stored in FP32 for a re-centring at this candidate.
 // |c|_inf (v[14]) is accumulated only when `cinf` is set.  All threads call
 // it (it synchronises between the column and the row loops).
+template <bool STAGED>
 __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const FastOffsets& o, const int4* alist,
                                                     const int4* atlist, int a0, int a1, int t0, int t1, int a_sub,
                                                     int t_sub, double* xc, const double* yc, const double* cs,
@@ -1002,7 +1067,9 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         const int jj = own ? j : 0;
         const double cj = cs[jj], lj = ls[jj], uj = us[jj], dcj = __ldg(sp->dc + jj);
         double xsc = xc[jj];
-        const double g = slice_dot64_staged(SI + o.at_idx + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z);
+        const double g = STAGED
+            ? slice_dot64_staged(SI + o.at_idx + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z)
+            : slice_dot64_global2(sp->at_idx + sl.y + lane, sp->at_v64 + sl.y + lane, yc, sl.z);
         if (own) {
             if (xsc < lj || xsc > uj) {
                 xsc = xsc < lj ? lj : uj;
@@ -1033,7 +1100,9 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         const bool own = i < m;
         const int ii = own ? i : 0;
         const double bi = bs[ii], ysc = yc[ii];
-        const double h = slice_dot64_staged(SI + o.a_idx + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z);
+        const double h = STAGED
+            ? slice_dot64_staged(SI + o.a_idx + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z)
+            : slice_dot64_global2(sp->a_idx + sl.y + lane, sp->a_v64 + sl.y + lane, xc, sl.z);
         if (own) {
             const double rr = bi - h;                  // scaled b - A x
             const double ro = -rr * __ldg(sp->inv_dr + i);  // A x - b in original units
@@ -1074,7 +1143,7 @@ __device__ __forceinline__ void recentre(const DevSpecies* sp, const FastOffsets
     }
 }
 
-template <int MAXT>
+template <int MAXT, bool STAGED>
 __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ double s_red[MAXT / 32][kRed];
@@ -1197,7 +1266,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             double v[kRed];
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-            kkt_partials_recentred(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
+            kkt_partials_recentred<STAGED>(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
                                    us, bs, dcand, rcand, true, lane, v);
             block_reduce(v, s_red, s_tot);
             cinf = s_tot[14];
@@ -1220,11 +1289,11 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             const float tau = static_cast<float>(eta / omega), sigma = static_cast<float>(eta * omega);
             const float w = static_cast<float>((k + 1.0) / (k + 2.0));
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
-            primal_pass_recentred(o, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1), pdx2,
-                                  pdxa2);
+            primal_pass_recentred<STAGED>(sp, o, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
+                                          pdx2, pdxa2);
             __syncthreads();
-            dual_pass_recentred(o, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur), PY(cur ^ 1), pdy2,
-                                pdya2);
+            dual_pass_recentred<STAGED>(sp, o, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur),
+                                        PY(cur ^ 1), pdy2, pdya2);
             __syncthreads();
             ++k;
             if (!check) continue;
@@ -1236,7 +1305,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             v[6] = pdy2;
             v[7] = pdxa2;
             v[8] = pdya2;
-            kkt_partials_recentred(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
+            kkt_partials_recentred<STAGED>(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
                                    cs, ls, us, bs, dcand, rcand, false, lane, v);
             block_reduce(v, s_red, s_tot);
             if (threadIdx.x == 0) s_tot[14] = cinf;
@@ -1291,7 +1360,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 double vv[kRed];
 #pragma unroll
                 for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-                kkt_partials_recentred(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
+                kkt_partials_recentred<STAGED>(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
                                        bs, dcand, rcand, false, lane, vv);
                 block_reduce(vv, s_red, s_tot);
                 cur ^= 1;
@@ -1370,7 +1439,8 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     template __global__ void pdhg_persistent<double, MAXT, 0>(KernelParams);  \
     template __global__ void pdhg_persistent<double, MAXT, 1>(KernelParams);  \
     template __global__ void pdhg_persistent<double, MAXT, 2>(KernelParams);  \
-    template __global__ void pdhg_recentred<MAXT>(KernelParams);
+    template __global__ void pdhg_recentred<MAXT, true>(KernelParams);        \
+    template __global__ void pdhg_recentred<MAXT, false>(KernelParams);
 FBALP_INSTANTIATE(512)
 FBALP_INSTANTIATE(1024)
 #undef FBALP_INSTANTIATE
@@ -1410,14 +1480,23 @@ cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem
     return cudaGetLastError();
 }
 
-const void* recentred_symbol(int threads) {
-    return threads <= 512 ? reinterpret_cast<const void*>(&pdhg_recentred<512>)
-                          : reinterpret_cast<const void*>(&pdhg_recentred<1024>);
+const void* recentred_symbol(int threads, bool staged) {
+    if (threads <= 512)
+        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<512, true>)
+                      : reinterpret_cast<const void*>(&pdhg_recentred<512, false>);
+    return staged ? reinterpret_cast<const void*>(&pdhg_recentred<1024, true>)
+                  : reinterpret_cast<const void*>(&pdhg_recentred<1024, false>);
 }
 
-cudaError_t launch_recentred(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p) {
-    if (threads <= 512) pdhg_recentred<512><<<grid, threads, smem, stream>>>(p);
-    else pdhg_recentred<1024><<<grid, threads, smem, stream>>>(p);
+cudaError_t launch_recentred(bool staged, int grid, int threads, size_t smem, cudaStream_t stream,
+                             const KernelParams& p) {
+    if (threads <= 512) {
+        if (staged) pdhg_recentred<512, true><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<512, false><<<grid, threads, smem, stream>>>(p);
+    } else {
+        if (staged) pdhg_recentred<1024, true><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<1024, false><<<grid, threads, smem, stream>>>(p);
+    }
     return cudaGetLastError();
 }
 

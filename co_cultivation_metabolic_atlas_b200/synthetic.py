@@ -40,6 +40,7 @@ class SpeciesModel:
     cost: np.ndarray            # minimisation objective (-e_biomass)
     n_exchange: int
     biomass: int                # column index of the biomass reaction
+    anchor: np.ndarray | None = None  # a feasible flux of the default bounds (scale workload)
     medium_columns: np.ndarray = field(default_factory=lambda: np.empty(0, np.int64))
     medium_ids: np.ndarray = field(default_factory=lambda: np.empty(0, np.int64))
     vmax: np.ndarray = field(default_factory=lambda: np.empty(0))
@@ -130,9 +131,19 @@ def community_models(sizes=COMMUNITY_SIZES, *, seed: int = 0, n_medium: int = ME
     subset of the medium metabolites, with Michaelis-Menten parameters
     ``v_max ~ U[5, 20]`` and ``K_m ~ U[0.01, 1]``.  The other exchange columns
     keep the fixed bounds drawn by ``species_matrix``.  ``fixed_fraction`` of
-    the non-medium exchange bounds are fixed (``l = u ~ U[0, 2]``) and
+    the non-medium exchange bounds are fixed (``l = u``) and
     ``duplicate_fraction`` of the reversible internal reactions receive a
     parallel duplicate column (the scale/degeneracy stress workload).
+
+    Fixed exchange values drawn independently (``U[0, 2]``) make most draws
+    infeasible (measured: with secretions fixed two of the three large
+    species have no feasible flux, with uptakes fixed the third), and a
+    batch of infeasible LPs measures nothing.  The fixed values are
+    therefore taken from a feasible flux: ``anchor`` = the optimum of the
+    species' network for a seeded random objective (HiGHS, default bounds),
+    scaled so that its fixed exchange values lie in ``[-2, 2]`` (the scaled
+    flux stays feasible because the bounds contain 0); the value magnitudes
+    keep the ``[0, 2]`` range, their signs are the network's.
     """
     rng = np.random.default_rng(seed + 7919)
     models = []
@@ -167,11 +178,49 @@ def community_models(sizes=COMMUNITY_SIZES, *, seed: int = 0, n_medium: int = ME
         if fixed_fraction > 0:
             others = np.setdiff1d(np.arange(model.n_exchange), cols)
             fixed = rng.choice(others, int(round(fixed_fraction * len(others))), replace=False)
-            value = rng.uniform(0.0, 2.0, len(fixed))
-            model.lower[fixed] = value
-            model.upper[fixed] = value
+            flux = _feasible_flux(model, rng)
+            peak = float(np.abs(flux[fixed]).max(initial=0.0))
+            scale = rng.uniform(0.0, 2.0) / peak if peak > 0 else 0.0
+            model.anchor = flux * min(1.0, scale)
+            model.lower[fixed] = model.anchor[fixed]
+            model.upper[fixed] = model.anchor[fixed]
         models.append(model)
     return models
+
+
+def _feasible_flux(model: SpeciesModel, rng) -> np.ndarray:
+    """A vertex flux of ``S v = 0`` within the model's bounds that optimises
+    a random objective (HiGHS interior point with crossover)."""
+    from scipy.optimize import linprog
+    objective = rng.uniform(-1.0, 1.0, model.S.shape[1])
+    res = linprog(objective, A_eq=model.S, b_eq=np.zeros(model.S.shape[0]),
+                  bounds=np.column_stack([model.lower, model.upper]), method="highs-ipm")
+    if res.status != 0:
+        raise RuntimeError("species network has no feasible flux")
+    return np.clip(np.asarray(res.x), model.lower, model.upper)
+
+
+def scale_batch(models, count: int, *, mix=(0.5, 0.3, 0.2), seed: int = 0):
+    """An uneven batch of the scale workload: ``count`` instances split over
+    the species by ``mix``; each instance draws its free exchange lower
+    bounds ``-u`` with ``u ~ U[0, 20]`` (widened to contain the species'
+    anchor flux, so every instance stays feasible).  Returns the species id
+    of every instance and per-species ``(lower, upper)`` arrays."""
+    rng = np.random.default_rng(seed + 31337)
+    sizes = np.floor(np.asarray(mix, float) / np.sum(mix) * count).astype(int)
+    sizes[0] += count - sizes.sum()
+    species_id = np.repeat(np.arange(len(models), dtype=np.int32), sizes)
+    bounds = []
+    for s, mdl in enumerate(models):
+        k = int(sizes[s])
+        lower = np.repeat(mdl.lower[None, :], k, axis=0)
+        free = np.flatnonzero((mdl.lower[:mdl.n_exchange] < mdl.upper[:mdl.n_exchange]))
+        draw = -rng.uniform(0.0, 20.0, (k, len(free)))
+        if mdl.anchor is not None:
+            draw = np.minimum(draw, mdl.anchor[free][None, :])
+        lower[:, free] = draw
+        bounds.append((lower, np.repeat(mdl.upper[None, :], k, axis=0)))
+    return species_id, bounds
 
 
 def initial_environments(count: int, n_medium: int = MEDIUM_SIZE, n_species: int = 3, *, seed: int = 0):
