@@ -56,6 +56,19 @@ static HiLo split_hi_lo(const fbalp::Sell& raw, int32_t rows) {
     return h;
 }
 
+// Packed matrix words of the re-centred phase: index in the low 16 bits,
+// the FP32 value rounded to nearest-even BF16 in the high 16 bits.
+static std::vector<uint32_t> pack_bf16(const std::vector<int32_t>& idx, const std::vector<float>& val) {
+    std::vector<uint32_t> out(idx.size());
+    for (size_t e = 0; e < idx.size(); ++e) {
+        uint32_t bits;
+        std::memcpy(&bits, &val[e], sizeof(bits));
+        const uint32_t rounded = (bits + 0x7fffu + ((bits >> 16) & 1u)) & 0xffff0000u;
+        out[e] = rounded | static_cast<uint32_t>(idx[e] & 0xffff);
+    }
+    return out;
+}
+
 }  // namespace
 
 extern "C" {
@@ -212,6 +225,10 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             d.a_idx = dev_upload(sh.A.idx, E->owned);
             d.a_v32 = dev_upload(a32, E->owned);
             d.a_v64 = dev_upload(sh.A.val, E->owned);
+            if (sh.n + 1 < 65536 && sh.m + 1 < 65536) {
+                d.a_pk = dev_upload(pack_bf16(sh.A.idx, a32), E->owned);
+                d.at_pk = dev_upload(pack_bf16(sh.AT.idx, at32), E->owned);
+            }
             d.at_idx = dev_upload(sh.AT.idx, E->owned);
             d.at_v32 = dev_upload(at32, E->owned);
             d.at_v64 = dev_upload(sh.AT.val, E->owned);

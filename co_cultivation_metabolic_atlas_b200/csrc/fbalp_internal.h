@@ -166,7 +166,8 @@ inline LayoutPlan plan_layout_unscaled(int n, int m, int warps, int a_nslices, i
 
 // Re-centred FP32 layout: everything the iteration touches in shared memory
 // (schedule lists; the FP32 gather targets dxbar (n+1) and dy (m+1); the
-// FP32 matrix slices with 16-bit indices; dx, d, l - x^, u - x^ (n each);
+// matrix slices as packed words (16-bit index, BF16 value); dx, d, l - x^,
+// u - x^ (n each);
 // r and the inequality bound -y^ (m each)), and in the CTA's global slab the
 // two FP64 point buffers of x and y, the FP32 reduced cost / residual of
 // the last evaluated candidate, and the instance's scaled FP64 objective,
@@ -198,15 +199,13 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, 
     };
     put(kXbar);
     put(kY);
-    if (stage) {
+    if (stage) {  // packed 32-bit words (16-bit index | BF16 value)
         L.mat_a_idx = off;
-        off += align_up(2 * a_elems, 16);
-        L.mat_at_idx = off;
-        off += align_up(2 * at_elems, 16);
-        L.mat_a_val = off;
         off += align_up(4 * a_elems, 16);
-        L.mat_at_val = off;
+        L.mat_at_idx = off;
         off += align_up(4 * at_elems, 16);
+        L.mat_a_val = L.mat_a_idx;
+        L.mat_at_val = L.mat_at_idx;
     }
     for (int a : {kX, kC, kL, kU, kB, kYa}) put(a);
     if (off > smem_cap) return P;

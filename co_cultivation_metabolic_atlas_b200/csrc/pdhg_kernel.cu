@@ -225,7 +225,23 @@ __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned ch
     int4* lt = reinterpret_cast<int4*>(sm + L.list_at);
     for (int t = tid; t < sp->a_nslices; t += nt) la[t] = sp->a_list[t];
     for (int t = tid; t < sp->at_nslices; t += nt) lt[t] = sp->at_list[t];
-    if (L.unscaled) {
+    if (L.recentred) {
+        // packed words (16-bit index | BF16 value) with the index pre-offset
+        // to the FP32 gather targets dxbar (A slices) and dy (A^T slices)
+        if (L.mat_smem) {
+            uint32_t* pa = reinterpret_cast<uint32_t*>(sm + L.mat_a_idx);
+            uint32_t* pt = reinterpret_cast<uint32_t*>(sm + L.mat_at_idx);
+            const uint32_t a_add = static_cast<uint32_t>(L.arr[kXbar] / 4), t_add = static_cast<uint32_t>(L.arr[kY] / 4);
+            for (int64_t e = tid; e < sp->a_elems; e += nt) {
+                const uint32_t w = sp->a_pk[e];
+                pa[e] = (w & 0xffff0000u) | ((w & 0xffffu) + a_add);
+            }
+            for (int64_t e = tid; e < sp->at_elems; e += nt) {
+                const uint32_t w = sp->at_pk[e];
+                pt[e] = (w & 0xffff0000u) | ((w & 0xffffu) + t_add);
+            }
+        }
+    } else if (L.unscaled) {
         // unscaled FP32 values; indices pre-offset to the FP64 gather targets
         // z (A pass) and w (A^T pass)
         uint16_t* ai = reinterpret_cast<uint16_t*>(sm + L.mat_a_idx);
@@ -863,69 +879,61 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
 // convergence test reads them without permutation or division.
 // ---------------------------------------------------------------------------
 
-// Slice product from shared memory with two interleaved accumulators (even
-// and odd k), summed at the end.
-__device__ __forceinline__ float slice_dot_fast2(const uint16_t* ip, const float* vp, const float* g, int len) {
+// Slice product over packed matrix words (16-bit index | BF16 value): one
+// 32-bit shared-memory load per element, two accumulators (even / odd k).
+// The BF16 value is the word with its index bits cleared.
+__device__ __forceinline__ float slice_dot_pk(const uint32_t* wp, const float* g, int len) {
     float a0 = 0.0f, a1 = 0.0f;
     int k = 0;
-    for (; k + 4 <= len; k += 4, ip += 128, vp += 128) {
-        const int i0 = ip[0], i1 = ip[32], i2 = ip[64], i3 = ip[96];
-        const float v0 = vp[0], v1 = vp[32], v2 = vp[64], v3 = vp[96];
-        a0 = fmaf(v0, g[i0], a0);
-        a1 = fmaf(v1, g[i1], a1);
-        a0 = fmaf(v2, g[i2], a0);
-        a1 = fmaf(v3, g[i3], a1);
+    for (; k + 4 <= len; k += 4, wp += 128) {
+        const uint32_t w0 = wp[0], w1 = wp[32], w2 = wp[64], w3 = wp[96];
+        a0 = fmaf(__uint_as_float(w0 & 0xffff0000u), g[w0 & 0xffffu], a0);
+        a1 = fmaf(__uint_as_float(w1 & 0xffff0000u), g[w1 & 0xffffu], a1);
+        a0 = fmaf(__uint_as_float(w2 & 0xffff0000u), g[w2 & 0xffffu], a0);
+        a1 = fmaf(__uint_as_float(w3 & 0xffff0000u), g[w3 & 0xffffu], a1);
     }
     if (k + 2 <= len) {
-        const int i0 = ip[0], i1 = ip[32];
-        const float v0 = vp[0], v1 = vp[32];
-        a0 = fmaf(v0, g[i0], a0);
-        a1 = fmaf(v1, g[i1], a1);
+        const uint32_t w0 = wp[0], w1 = wp[32];
+        a0 = fmaf(__uint_as_float(w0 & 0xffff0000u), g[w0 & 0xffffu], a0);
+        a1 = fmaf(__uint_as_float(w1 & 0xffff0000u), g[w1 & 0xffffu], a1);
         k += 2;
-        ip += 64;
-        vp += 64;
+        wp += 64;
     }
-    if (k < len) a0 = fmaf(vp[0], g[ip[0]], a0);
+    if (k < len) {
+        const uint32_t w0 = wp[0];
+        a0 = fmaf(__uint_as_float(w0 & 0xffff0000u), g[w0 & 0xffffu], a0);
+    }
     return a0 + a1;
 }
 
-// Slice product with the matrix streamed from global memory (L2): int32
-// indices relative to the gather target `g`, FP32 values; batches of eight
-// loads in flight, two accumulators.
-__device__ __forceinline__ float slice_dot_global2(const int32_t* __restrict__ ip, const float* __restrict__ vp,
-                                                   const float* g, int len) {
+// The same product with the packed words streamed from global memory (raw
+// indices relative to the gather target `g`); identical accumulation order.
+__device__ __forceinline__ float slice_dot_pk_global(const uint32_t* __restrict__ wp, const float* g, int len) {
     constexpr int U = 8;
     float a0 = 0.0f, a1 = 0.0f;
     for (int k0 = 0; k0 < len; k0 += U) {
-        int ii[U];
-        float vv[U];
+        uint32_t ww[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int k = k0 + u;
-            if (k < len) {
-                ii[u] = __ldg(ip + (k << 5));
-                vv[u] = __ldg(vp + (k << 5));
-            }
-        }
+        for (int u = 0; u < U; ++u)
+            if (k0 + u < len) ww[u] = __ldg(wp + ((k0 + u) << 5));
 #pragma unroll
         for (int u = 0; u < U; u += 2) {
-            if (k0 + u < len) a0 = fmaf(vv[u], g[ii[u]], a0);
-            if (k0 + u + 1 < len) a1 = fmaf(vv[u + 1], g[ii[u + 1]], a1);
+            if (k0 + u < len) a0 = fmaf(__uint_as_float(ww[u] & 0xffff0000u), g[ww[u] & 0xffffu], a0);
+            if (k0 + u + 1 < len) a1 = fmaf(__uint_as_float(ww[u + 1] & 0xffff0000u), g[ww[u + 1] & 0xffffu], a1);
         }
     }
     return a0 + a1;
 }
 
-// STAGED: the species' matrix slices are in shared memory (16-bit indices
+// STAGED: the species' packed matrix words are in shared memory (indices
 // pre-offset to the gather target); otherwise they are streamed from L2.
 template <bool STAGED>
-__device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const int4* atlist,
-                                                      int t0, int t1, int n, int lane, float tau, float w, float rho,
-                                                      bool check, const double* bx, double* cx, double& pdx2,
-                                                      double& pdxa2) {
+__device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PT,
+                                                      const int4* atlist, int t0, int t1, int n, int lane, float tau,
+                                                      float w, float rho, bool check, const double* bx, double* cx,
+                                                      double& pdx2, double& pdxa2) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
-    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
         const int4 sl = atlist[t];
         const int j = (sl.x << 5) + lane;
@@ -934,8 +942,8 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
         // the column's operands first: their latency overlaps the product
         const float xo = S[o.x + jj], dj = S[o.c + jj], lj = S[o.l + jj], uj = S[o.u + jj];
         const float g = STAGED
-            ? slice_dot_fast2(SI + o.at_idx + sl.y + lane, S + o.at_val + sl.y + lane, S, sl.z)
-            : slice_dot_global2(sp->at_idx + sl.y + lane, sp->at_v32 + sl.y + lane, S + o.y, sl.z);
+            ? slice_dot_pk(PT + sl.y + lane, S, sl.z)
+            : slice_dot_pk_global(sp->at_pk + sl.y + lane, S + o.y, sl.z);
         if (own) {
             const float xn = clampT(xo - tau * (dj - g), lj, uj);
             const float xb = xn + xn - xo;
@@ -953,13 +961,12 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
 }
 
 template <bool STAGED>
-__device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const int4* alist,
-                                                    int t0, int t1, int m, int neq, int lane, float sigma, float w,
-                                                    float rho, bool check, const double* by, double* cy, double& pdy2,
-                                                    double& pdya2) {
+__device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PA,
+                                                    const int4* alist, int t0, int t1, int m, int neq, int lane,
+                                                    float sigma, float w, float rho, bool check, const double* by,
+                                                    double* cy, double& pdy2, double& pdya2) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
-    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
         const int4 sl = alist[t];
         const int i = (sl.x << 5) + lane;
@@ -967,8 +974,8 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
         const int ii = own ? i : 0;
         const float yo = S[o.y + ii], ri = S[o.b + ii], yl = S[o.ya + ii];
         const float h = STAGED
-            ? slice_dot_fast2(SI + o.a_idx + sl.y + lane, S + o.a_val + sl.y + lane, S, sl.z)
-            : slice_dot_global2(sp->a_idx + sl.y + lane, sp->a_v32 + sl.y + lane, S + o.xbar, sl.z);
+            ? slice_dot_pk(PA + sl.y + lane, S, sl.z)
+            : slice_dot_pk_global(sp->a_pk + sl.y + lane, S + o.xbar, sl.z);
         if (own) {
             float yn = yo + sigma * (ri - h);
             if (i >= neq && yn > yl) yn = yl;  // y^ + dy <= 0
@@ -985,11 +992,11 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
 }
 
 // FP64 slice product for the convergence test: the 16-bit column indices
-// come from the staged copy in shared memory (minus the gather-target
-// offset `sub`), the FP64 values from global memory, the FP64 gather
+// come from the staged packed words in shared memory (minus the
+// gather-target offset `sub`), the FP64 values from global memory, the FP64 gather
 // target from the slab.  The value loads do not depend on the indices, so
 // one memory round trip serves each batch.
-__device__ __forceinline__ double slice_dot64_staged(const uint16_t* sip, int sub, const double* __restrict__ vp,
+__device__ __forceinline__ double slice_dot64_staged(const uint32_t* wp, int sub, const double* __restrict__ vp,
                                                      const double* g, int len) {
     constexpr int U = 4;
     double acc0 = 0.0, acc1 = 0.0;
@@ -1000,7 +1007,7 @@ __device__ __forceinline__ double slice_dot64_staged(const uint16_t* sip, int su
             const int k = k0 + u;
             if (k < len) {
                 vv[u] = __ldg(vp + (k << 5));
-                gg[u] = g[static_cast<int>(sip[k << 5]) - sub];
+                gg[u] = g[static_cast<int>(wp[k << 5] & 0xffffu) - sub];
             } else {
                 vv[u] = 0.0;
                 gg[u] = 0.0;
@@ -1052,13 +1059,12 @@ __device__ __forceinline__ double slice_dot64_global2(const int32_t* __restrict_
 // |c|_inf (v[14]) is accumulated only when `cinf` is set.  All threads call
 // it (it synchronises between the column and the row loops).
 template <bool STAGED>
-__device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const FastOffsets& o, const int4* alist,
-                                                    const int4* atlist, int a0, int a1, int t0, int t1, int a_sub,
-                                                    int t_sub, double* xc, const double* yc, const double* cs,
-                                                    const double* ls, const double* us, const double* bs,
-                                                    float* dcand, float* rcand, bool cinf, int lane, double* v) {
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    const uint16_t* const SI = reinterpret_cast<const uint16_t*>(dyn_smem);
+__device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const uint32_t* PA, const uint32_t* PT,
+                                                    const int4* alist, const int4* atlist, int a0, int a1, int t0,
+                                                    int t1, int a_sub, int t_sub, double* xc, const double* yc,
+                                                    const double* cs, const double* ls, const double* us,
+                                                    const double* bs, float* dcand, float* rcand, bool cinf, int lane,
+                                                    double* v) {
     const int n = sp->n, m = sp->m, neq = sp->neq;
     for (int t = t0; t < t1; ++t) {
         const int4 sl = atlist[t];
@@ -1068,7 +1074,7 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         const double cj = cs[jj], lj = ls[jj], uj = us[jj], dcj = __ldg(sp->dc + jj);
         double xsc = xc[jj];
         const double g = STAGED
-            ? slice_dot64_staged(SI + o.at_idx + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z)
+            ? slice_dot64_staged(PT + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z)
             : slice_dot64_global2(sp->at_idx + sl.y + lane, sp->at_v64 + sl.y + lane, yc, sl.z);
         if (own) {
             if (xsc < lj || xsc > uj) {
@@ -1101,7 +1107,7 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         const int ii = own ? i : 0;
         const double bi = bs[ii], ysc = yc[ii];
         const double h = STAGED
-            ? slice_dot64_staged(SI + o.a_idx + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z)
+            ? slice_dot64_staged(PA + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z)
             : slice_dot64_global2(sp->a_idx + sl.y + lane, sp->a_v64 + sl.y + lane, xc, sl.z);
         if (own) {
             const double rr = bi - h;                  // scaled b - A x
@@ -1175,8 +1181,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         }
         float* const S = reinterpret_cast<float*>(dyn_smem);
         const FastOffsets o = fast_offsets<float>(L);
-        // the staged 16-bit indices carry the gather-target offsets
+        // the staged packed words' indices carry the gather-target offsets
         const int a_sub = static_cast<int>(L.arr[kXbar] / 4), t_sub = static_cast<int>(L.arr[kY] / 4);
+        const uint32_t* const PA = reinterpret_cast<const uint32_t*>(dyn_smem + L.mat_a_idx);
+        const uint32_t* const PT = reinterpret_cast<const uint32_t*>(dyn_smem + L.mat_at_idx);
         // the two point buffers; selected by value (no local-memory array)
         double* const px0 = reinterpret_cast<double*>(slab + L.pt_x[0]);
         double* const px1 = reinterpret_cast<double*>(slab + L.pt_x[1]);
@@ -1266,7 +1274,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             double v[kRed];
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-            kkt_partials_recentred<STAGED>(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
+            kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
                                    us, bs, dcand, rcand, true, lane, v);
             block_reduce(v, s_red, s_tot);
             cinf = s_tot[14];
@@ -1289,10 +1297,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             const float tau = static_cast<float>(eta / omega), sigma = static_cast<float>(eta * omega);
             const float w = static_cast<float>((k + 1.0) / (k + 2.0));
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
-            primal_pass_recentred<STAGED>(sp, o, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
+            primal_pass_recentred<STAGED>(sp, o, PT, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
                                           pdx2, pdxa2);
             __syncthreads();
-            dual_pass_recentred<STAGED>(sp, o, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur),
+            dual_pass_recentred<STAGED>(sp, o, PA, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur),
                                         PY(cur ^ 1), pdy2, pdya2);
             __syncthreads();
             ++k;
@@ -1305,7 +1313,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             v[6] = pdy2;
             v[7] = pdxa2;
             v[8] = pdya2;
-            kkt_partials_recentred<STAGED>(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
+            kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
                                    cs, ls, us, bs, dcand, rcand, false, lane, v);
             block_reduce(v, s_red, s_tot);
             if (threadIdx.x == 0) s_tot[14] = cinf;
@@ -1360,7 +1368,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 double vv[kRed];
 #pragma unroll
                 for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-                kkt_partials_recentred<STAGED>(sp, o, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
+                kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
                                        bs, dcand, rcand, false, lane, vv);
                 block_reduce(vv, s_red, s_tot);
                 cur ^= 1;

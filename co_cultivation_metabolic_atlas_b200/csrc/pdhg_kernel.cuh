@@ -68,6 +68,12 @@ struct DevSpecies {
     const double* lo_at_val;
     const double* inv_dr;         // 1 / dr, new order
     const double* inv_dc;         // 1 / dc, new order
+    // the scaled matrix as packed 32-bit words in the SELL slices: the
+    // 16-bit index in the low half, the value rounded to BF16 in the high
+    // half (the re-centred phase's FP32 passes; null when n or m exceeds
+    // 16-bit indices)
+    const uint32_t* a_pk;
+    const uint32_t* at_pk;
 };
 
 // Byte offsets of one species' working set inside the CTA's dynamic shared

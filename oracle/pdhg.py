@@ -288,6 +288,13 @@ def solve(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0
     return dict(x=xo, y=yo, xs=xn, ys=yn, status=status, iterations=it, metrics=mt, omega=omega)
 
 
+def bf16_round(x):
+    """FP32 values rounded to the nearest BF16 (ties to even), as FP32."""
+    b = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    r = (b + np.uint32(0x7FFF) + ((b >> np.uint32(16)) & np.uint32(1))) & np.uint32(0xFFFF0000)
+    return r.view(np.float32)
+
+
 def solve_recentred(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=None, omega0=1.0,
                     max_iters=20000, check_every=64, tol_primal=1e-9, tol_dual=1e-9, tol_gap=1e-7, rho=1.0,
                     restarts=True, stall_checks=8, floor_tol=1e-7, fallback_iters=0, handoff_stall_checks=32,
@@ -300,7 +307,11 @@ def solve_recentred(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=No
     base moves to the evaluated candidate and the FP32 problem becomes the
     correction LP ``min d.dx s.t. A~ dx = r, ls - xh <= dx <= us - xh``
     (``yh + dy <= 0`` on inequality rows) with ``d = c~ - A~^T yh`` and
-    ``r = b~ - A~ xh`` computed in FP64 and rounded to FP32 once.  The Halpern
+    ``r = b~ - A~ xh`` computed in FP64 and rounded to FP32 once.  The FP32
+    passes use the scaled matrix rounded to BF16 (the engine stages it as
+    packed 16-bit index / BF16 value words): the re-centring corrects the
+    rounding of the matrix like the rounding of the iterates, and the
+    convergence tests use the FP64 matrix.  The Halpern
     anchor is the base, so the differences restart from zero.  Convergence
     tests evaluate the FP64 candidate ``xh + dxn`` (projected onto the exact
     scaled bounds), ``yh + dyn``.  After ``stall_checks`` full tests without
@@ -316,6 +327,8 @@ def solve_recentred(P: Prepared, lower, upper, cost, rhs=None, *, x0=None, y0=No
     AT = A.T.tocsr()
     Af = A.astype(f32)
     ATf = AT.astype(f32)
+    Af.data = bf16_round(Af.data)
+    ATf.data = bf16_round(ATf.data)
     ineq = np.arange(m) >= P.neq
 
     def evaluate(xc, yc):
