@@ -87,6 +87,8 @@ def load(path: os.PathLike | None = None):
                                                ctypes.POINTER(c_double_p), ctypes.POINTER(Options), vp,
                                                ctypes.POINTER(vp)]),
         "fbalp_engine_set_instances": (ctypes.c_int, [vp, ctypes.c_int64, c_int32_p, vp, vp, vp, vp]),
+        "fbalp_engine_set_instance_data": (ctypes.c_int, [vp, vp, vp, vp, vp]),
+        "fbalp_engine_set_iteration_hints": (ctypes.c_int, [vp, vp]),
         "fbalp_engine_solve": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(SolveParams), vp, vp, vp, vp,
                                               vp, vp, vp]),
         "fbalp_engine_destroy": (ctypes.c_int, [vp]),

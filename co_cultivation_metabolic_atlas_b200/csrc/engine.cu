@@ -333,7 +333,27 @@ int fbalp_engine_set_instances(fbalp_engine* e, int64_t count, const int32_t* sp
     e->upper = upper;
     e->cost = cost;
     e->rhs = rhs;
+    e->hints = nullptr;
     e->bound = true;
+    return FBALP_OK;
+}
+
+int fbalp_engine_set_instance_data(fbalp_engine* e, const double* lower, const double* upper, const double* cost,
+                                   const double* rhs) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (!e->bound) return fail(FBALP_ERR_STATE, "set_instances must be called first");
+    if (!lower || !upper || !cost) return fail(FBALP_ERR_INVALID, "lower/upper/cost are required");
+    e->lower = lower;
+    e->upper = upper;
+    e->cost = cost;
+    e->rhs = rhs;
+    return FBALP_OK;
+}
+
+int fbalp_engine_set_iteration_hints(fbalp_engine* e, const int32_t* hints) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (!e->bound) return fail(FBALP_ERR_STATE, "set_instances must be called first");
+    e->hints = hints;
     return FBALP_OK;
 }
 
@@ -575,6 +595,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             pr.hand_omega = static_cast<double*>(e->mid_omega.ptr);
             pr.hand_iters = static_cast<int32_t*>(e->mid_iters.ptr);
             pr.handoff_on_stall = 4 * q.fp64_stall_checks;
+            pr.hint_iters = e->hints;
             run_phase(e, false, pr, recentred_mode(e));
             fbalp::KernelParams p64 = p;
             p64.order = static_cast<const int32_t*>(e->hand_list.ptr);

@@ -88,6 +88,7 @@ struct fbalp_engine {
     std::vector<int32_t> h_species;
     std::vector<int64_t> h_coloff, h_rowoff;
     const double *lower = nullptr, *upper = nullptr, *cost = nullptr, *rhs = nullptr;
+    const int32_t* hints = nullptr;  // per-instance iteration hints (device), may be null
     Buffer inst_species, col_off, row_off, order;
     bool bound = false;
     // workspace

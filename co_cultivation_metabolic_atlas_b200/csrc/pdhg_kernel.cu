@@ -1289,11 +1289,13 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
 
         int k = 0, it = 0, stall = 0;
         bool fell_back = false;
+        // early termination tests only for instances expected to finish early
+        const bool early = p.hint_iters == nullptr || p.hint_iters[inst] < p.check_every;
         double r_restart = INFINITY, r_prev = INFINITY, best_err = INFINITY;
         while (status < 0) {
             ++it;
             const bool full = (it % p.check_every == 0) || (it >= p.max_iters);
-            const bool check = full || (it >= 8 && it < p.check_every && (it & (it - 1)) == 0);
+            const bool check = full || (early && it >= 8 && it < p.check_every && (it & (it - 1)) == 0);
             const float tau = static_cast<float>(eta / omega), sigma = static_cast<float>(eta * omega);
             const float w = static_cast<float>((k + 1.0) / (k + 2.0));
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
@@ -1451,6 +1453,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     template __global__ void pdhg_recentred<MAXT, false>(KernelParams);
 FBALP_INSTANTIATE(512)
 FBALP_INSTANTIATE(1024)
+// the re-centred kernel also at 768 threads (an 85-register budget: more
+// warps per scheduler to hide shared-memory latency)
+template __global__ void pdhg_recentred<768, true>(KernelParams);
+template __global__ void pdhg_recentred<768, false>(KernelParams);
 #undef FBALP_INSTANTIATE
 
 // Blocks of up to 512 threads use the variant with a 128-register budget,
@@ -1492,6 +1498,9 @@ const void* recentred_symbol(int threads, bool staged) {
     if (threads <= 512)
         return staged ? reinterpret_cast<const void*>(&pdhg_recentred<512, true>)
                       : reinterpret_cast<const void*>(&pdhg_recentred<512, false>);
+    if (threads <= 768)
+        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<768, true>)
+                      : reinterpret_cast<const void*>(&pdhg_recentred<768, false>);
     return staged ? reinterpret_cast<const void*>(&pdhg_recentred<1024, true>)
                   : reinterpret_cast<const void*>(&pdhg_recentred<1024, false>);
 }
@@ -1501,6 +1510,9 @@ cudaError_t launch_recentred(bool staged, int grid, int threads, size_t smem, cu
     if (threads <= 512) {
         if (staged) pdhg_recentred<512, true><<<grid, threads, smem, stream>>>(p);
         else pdhg_recentred<512, false><<<grid, threads, smem, stream>>>(p);
+    } else if (threads <= 768) {
+        if (staged) pdhg_recentred<768, true><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<768, false><<<grid, threads, smem, stream>>>(p);
     } else {
         if (staged) pdhg_recentred<1024, true><<<grid, threads, smem, stream>>>(p);
         else pdhg_recentred<1024, false><<<grid, threads, smem, stream>>>(p);

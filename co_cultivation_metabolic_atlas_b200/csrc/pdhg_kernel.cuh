@@ -149,6 +149,10 @@ struct KernelParams {
     int32_t handoff_on_stall;     // >0: a re-centred solve whose KKT error has
                                   // not halved for this many full tests hands
                                   // off to the FP64 phase (0 = never)
+    const int32_t* hint_iters;    // may be null: per instance, the iteration
+                                  // count of its previous solve; an instance
+                                  // whose hint is >= check_every skips the
+                                  // early termination tests (8, 16, 32, ...)
 };
 
 }  // namespace fbalp

@@ -114,6 +114,9 @@ class DeviceCommunity:
 
     def solve(self):
         out = self._bufs[self._which]
+        # the previous step's iteration counts tell the kernel which
+        # instances need no early termination tests
+        self.engine.set_iteration_hints(None if self.prev is None else self.prev.iterations)
         if self.warm_start == "learned":
             wx, wy, wo = self.learned.propose(self, self.step_index / self.horizon_steps)
             res = self.engine.solve(warm_x=wx, warm_y=wy, warm_omega=wo, config=self.config, out=out)

@@ -222,6 +222,28 @@ class LPEngine:
         self.col_offsets, self.row_offsets = co, ro
         self.total_cols, self.total_rows = tc, tr
 
+    def set_instance_data(self, lower, upper, cost, rhs=None):
+        """Point the bound batch at new device tensors of the same layout
+        (no layout recomputation, no synchronisation)."""
+        if self._bound is None:
+            raise RuntimeError("set_instances must be called first")
+        lower = self._dev(lower, self.total_cols, "lower")
+        upper = self._dev(upper, self.total_cols, "upper")
+        cost = self._dev(cost, self.total_cols, "cost")
+        rhs = self._dev(rhs, self.total_rows, "rhs")
+        N.check(self.lib.fbalp_engine_set_instance_data(self.handle, _ptr(lower), _ptr(upper), _ptr(cost), _ptr(rhs)))
+        self._bound = (lower, upper, cost, rhs)
+
+    def set_iteration_hints(self, hints):
+        """Per-instance iteration hints (device int32, e.g. the previous
+        solve's iteration counts; None clears): instances expected to take at
+        least one test period skip the early termination tests."""
+        if self._bound is None:
+            raise RuntimeError("set_instances must be called first")
+        h = None if hints is None else self._dev(hints, self.count, "hints", dtype=torch.int32)
+        N.check(self.lib.fbalp_engine_set_iteration_hints(self.handle, _ptr(h)))
+        self._hints = h
+
     def allocate_result(self) -> SolveResult:
         dev = self.device
         c = self.count

@@ -164,6 +164,24 @@ int fbalp_engine_set_instances(fbalp_engine* engine, int64_t count, const int32_
                                const double* lower, const double* upper, const double* cost,
                                const double* rhs);
 
+/* Re-point the bound batch at new DEVICE arrays of the same layout (same
+ * count, species and offsets) without recomputing it: the per-step call of a
+ * caller whose bounds change every step in place or in alternating buffers.
+ * Replaces: GpuPdhgWorkspace.update_problem (`src/gpu_pdhg_workspace.py:
+ * 209-267`), which keeps its pointers and rewrites their values. */
+int fbalp_engine_set_instance_data(fbalp_engine* engine, const double* lower, const double* upper,
+                                   const double* cost, const double* rhs);
+
+/* Optional per-instance iteration hints (DEVICE int32[count], e.g. the
+ * iteration counts of the previous solve; NULL clears): in the re-centred
+ * phase an instance whose hint is >= check_every skips the early
+ * termination-only tests at iterations 8, 16, 32, ... (each costs a few
+ * iterations' time); results are unaffected except that such an instance
+ * cannot stop before its first full test.  The pointer is kept until the next
+ * set_instances / set_iteration_hints.  No counterpart in the reference (its
+ * certificate period is fixed, `src/gpu_pdhg_corrector.py:278-279`). */
+int fbalp_engine_set_iteration_hints(fbalp_engine* engine, const int32_t* hints);
+
 /* Solve every bound instance.  Warm starts (`warm_x`, `warm_y`: flat DEVICE,
  * original units; `warm_omega`: per instance) may be NULL (cold start).
  * Outputs are DEVICE arrays: status[count], objective[count],

@@ -336,3 +336,34 @@ def test_large_species_solve_in_the_streamed_recentred_phase():
             assert hst == 0
             assert abs(obj[k] - fun) <= OBJ_TOL * max(1.0, abs(fun))
             k += 1
+
+
+def test_iteration_hints_and_instance_data_rebinding():
+    """Hints >= the test period skip the early termination tests (an instance
+    that would stop at iteration 8 stops at the first full test instead, with
+    the same optimum); re-pointing the batch at new arrays of the same layout
+    solves exactly what set_instances with those arrays solves."""
+    import torch
+    model, lower, upper = syn.single_species_workload(4, m=300, n=650)
+    eng = engine([(model.S, 300)])
+    eng.set_instances(np.zeros(4, np.int32), flat(lower), flat(upper), flat([model.cost] * 4))
+    first = eng.solve(config=cfg())
+    x0, y0 = first.x[:eng.total_cols].clone(), first.y[:eng.total_rows].clone()
+    lo2 = lower.copy()
+    lo2[:, :model.n_exchange] *= 0.999
+    lo2_d = torch.as_tensor(flat(lo2), device="cuda")
+    eng.set_instance_data(lo2_d, flat(upper), flat([model.cost] * 4))
+    rebound = eng.solve(config=cfg())
+    plain = eng.solve(warm_x=x0, warm_y=y0, warm_omega=first.omega, config=cfg())
+    eng.set_iteration_hints(torch.full((4,), 1000, dtype=torch.int32, device="cuda"))
+    hinted = eng.solve(warm_x=x0, warm_y=y0, warm_omega=first.omega, config=cfg())
+    eng.set_iteration_hints(None)
+    torch.cuda.synchronize()
+    ip, ih = plain.iterations.cpu().numpy(), hinted.iterations.cpu().numpy()
+    assert (plain.status.cpu().numpy() == 0).all() and (hinted.status.cpu().numpy() == 0).all()
+    assert np.all(ih >= np.minimum(ip, 64)) and np.all(ih % 64 == 0)
+    np.testing.assert_allclose(hinted.objective.cpu().numpy(), plain.objective.cpu().numpy(), rtol=1e-7, atol=1e-8)
+    ref = run_single(model.S, 300, lo2, upper, [model.cost] * 4)
+    np.testing.assert_array_equal(rebound.iterations.cpu().numpy(), ref["iters"])
+    np.testing.assert_array_equal(rebound.x[:eng.total_cols].cpu().numpy().reshape(4, -1), ref["x"])
+    eng.close()
