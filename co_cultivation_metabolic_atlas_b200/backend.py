@@ -22,6 +22,13 @@ Success means: the engine's FP64 tolerances are met (status OPTIMAL) AND the
 reference's original-LP certificate gate passes on the returned primal/dual
 pair (``primal <= 1e-5, dual <= 1e-7, relative KKT gap <= 1e-7``,
 ``src/gpu_block_lp.py:84``).
+
+With ``equality_reduction=True`` (the reference's ``equality_reduction``
+option, ``src/temporal_gpu_lp.py:22-52``) each request is presolved by the
+exact homogeneous-equality reduction (``reduction.py``; one plan per
+equality block), the reduced LPs are solved on the GPU, and the primal is
+expanded and the duals lifted back; the row is accepted only when the
+original-LP certificate passes on the lifted pair.
 """
 
 from __future__ import annotations
@@ -34,7 +41,9 @@ import torch
 
 from . import _native as N
 from .engine import EngineOptions, LPEngine, SolveConfig
+from .lp_trace import certificate as original_certificate
 from .problem import matrix_key, normalize
+from .reduction import EqualityReduction
 
 PRIMAL_GATE = 1e-5
 DUAL_GATE = 1e-7
@@ -47,7 +56,8 @@ class B200LPBackend:
 
     def __init__(self, *, mode='previous', precision='mixed', iterations=20000,
                  fp32_iterations=20000, check_interval=64, stage=None,
-                 options: EngineOptions | None = None, warm_start_model=None, device=None):
+                 options: EngineOptions | None = None, warm_start_model=None, device=None,
+                 equality_reduction=False):
         if mode not in ('cold', 'previous', 'mlp'):
             raise ValueError('Unknown warm-start mode')
         if mode == 'mlp' and warm_start_model is None:
@@ -69,6 +79,10 @@ class B200LPBackend:
         self.options = options or EngineOptions()
         self.device = torch.device(device) if device is not None else torch.device('cuda')
         self.model = warm_start_model
+        if mode == 'mlp' and equality_reduction:
+            raise ValueError('the learned warm start proposes original-space points; use equality_reduction=False')
+        self.equality_reduction = bool(equality_reduction)
+        self._plans: dict = {}
         self._keys: list[str] = []
         self._matrices = []
         self._engine: LPEngine | None = None
@@ -110,9 +124,12 @@ class B200LPBackend:
         ids = list(range(len(requests))) if environment_ids is None else list(environment_ids)
         if not requests or len(ids) != len(requests) or len(set(ids)) != len(ids):
             raise ValueError('Nonempty requests and unique environment IDs required')
-        problems = [normalize(c, kw) for c, kw in requests]
+        originals = [normalize(c, kw) for c, kw in requests]
         if self.stage is not None and any(kw.get('_stage', self.stage) != self.stage for _, kw in requests):
             raise ValueError('Use a separate backend and history for each LP stage')
+        reduced = self._reduce(originals) if self.equality_reduction else None
+        problems = originals if reduced is None else [r.problem if r is not None else o
+                                                        for r, o in zip(reduced, originals)]
         prep = time.perf_counter()
         species, rebuilt = self._engine_for(problems)
         eng = self._engine
@@ -131,8 +148,12 @@ class B200LPBackend:
                 if prev is not None and prev[0] == species[i]:
                     n = eng.shapes[species[i]][1]
                     m = eng.shapes[species[i]][0]
-                    wx[co[i]:co[i] + n] = prev[1]
-                    wy[ro[i]:ro[i] + m] = prev[2]
+                    px, py = prev[1], prev[2]
+                    if reduced is not None and reduced[i] is not None:
+                        px = reduced[i].compress_primal(px)
+                        py = py[reduced[i].plan.kept_rows]
+                    wx[co[i]:co[i] + n] = px
+                    wy[ro[i]:ro[i] + m] = py
                     wo[i] = prev[3]
             warm_x, warm_y, warm_o = wx, wy, wo
         elif self.mode == 'mlp':
@@ -159,20 +180,29 @@ class B200LPBackend:
                         and mt[2] <= GAP_GATE)
             xi = x[co[i]:co[i] + n].copy()
             yi = y[ro[i]:ro[i] + m].copy()
-            diag = dict(primal_residual=float(mt[0]), dual_violation=float(mt[1]),
-                        relative_kkt_gap=float(mt[2]), objective=float(mt[3]),
+            cert = dict(primal_residual=float(mt[0]), dual_violation=float(mt[1]),
+                        relative_kkt_gap=float(mt[2]))
+            note = None
+            if reduced is not None:
+                if reduced[i] is None:
+                    gate, note = False, 'bounds infeasible under the eliminated equalities'
+                else:
+                    # expand and lift, then certify the ORIGINAL LP
+                    xi, yi, cert, ok = self._postsolve(reduced[i], originals[i], xi, yi)
+                    gate = gate and ok
+            diag = dict(cert, objective=float(mt[3]),
                         dual_objective=float(mt[4]), relative_gap=float(mt[5]),
                         certificate_passed=gate, accepted_iteration=int(iters[i]) if gate else -1,
                         iterations=int(iters[i]), status=N.STATUS_NAMES.get(int(status[i]), 'unknown'),
                         environment_id=env, stage=self.stage, success=gate, cpu_lp_calls=0,
-                        mode=self.mode, solver=self.name)
+                        mode=self.mode, solver=self.name, equality_reduction=reduced is not None)
             if gate:
                 certified[env] = (species[i], xi, yi, float(mt[7]))
             rows.append(SimpleNamespace(
                 success=gate, x=xi if gate else None, y=yi if gate else None,
-                fun=float(problems[i][4] @ xi) if gate else None, status=int(status[i]),
+                fun=float(originals[i][4] @ xi) if gate else None, status=int(status[i]),
                 message=('Original-LP certified GPU solution' if gate else
-                         f'GPU solve not certified ({diag["status"]}); no CPU fallback'),
+                         f'GPU solve not certified ({note or diag["status"]}); no CPU fallback'),
                 diagnostics=diag))
         # commit per-environment state only after every row is built
         for env in ids:
@@ -190,6 +220,39 @@ class B200LPBackend:
                                  total_seconds=time.perf_counter() - started,
                                  rows=[r.diagnostics for r in rows]))
         return rows
+
+    def _reduce(self, originals):
+        """Reduce every request with the plan of its equality block (built
+        once per block); a request whose bounds are infeasible under the
+        eliminated equalities maps to None (a failed row)."""
+        out = []
+        for p in originals:
+            key = matrix_key(p[0], p[5])
+            plan = self._plans.get(key)
+            if plan is None:
+                plan = self._plans[key] = EqualityReduction(p)
+            try:
+                out.append(plan.reduce(p))
+            except ValueError as exc:
+                if 'infeasible' not in str(exc):
+                    raise
+                out.append(None)
+        return out
+
+    @staticmethod
+    def _postsolve(red, original, z, y_red):
+        """Original-space primal and duals of a reduced solution and the
+        original-LP certificate of the pair."""
+        ra, _, _, _, rc, _ = red.problem
+        x = red.expand_primal(z)
+        try:
+            y = red.lift_dual(y_red, rc - np.asarray(ra.T @ y_red).ravel())
+        except (ValueError, ArithmeticError):
+            return x, np.full(original[0].shape[0], np.nan), dict(primal_residual=np.inf, dual_violation=np.inf,
+                                                                  relative_kkt_gap=np.inf), False
+        cert = original_certificate(original, x, y)
+        ok = cert.pop('certificate_passed')
+        return x, y, cert, ok
 
     def close(self):
         if self._engine is not None:

@@ -104,3 +104,32 @@ def test_reference_traces_replay_through_the_backend(golden_dir, tmp_path, forbi
     for r, fun in zip(rows, ref):
         assert r.success, r.message
         assert abs(r.fun - fun) <= 1e-6 * max(1.0, abs(fun))
+
+
+def test_equality_reduction_presolve_certifies_the_original_lps(golden_dir, forbid_cpu_optimizers):
+    """With the exact homogeneous-equality presolve the GPU solves the
+    reduced LPs; expanded primals and lifted duals pass the ORIGINAL LPs'
+    certificate and reach HiGHS's objectives; a second call warm-starts from
+    the compressed previous solutions."""
+    from co_cultivation_metabolic_atlas_b200 import B200LPBackend
+    from oracle import dfba
+    g = np.load(golden_dir / "highs_community.npz")
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(4)
+    reqs, funs = [], []
+    for s, mdl in enumerate(models):
+        lo = dfba.uptake_lower_bounds(mdl, medium, biomass, 0.05)
+        for e in range(2):
+            reqs.append(request((mdl.S, np.zeros(mdl.S.shape[0]), lo[e], mdl.upper, mdl.cost, mdl.S.shape[0])))
+            funs.append(float(g[f"s{s}_fun"][e]))
+    be = B200LPBackend(mode="previous", equality_reduction=True)
+    rows = be.solve_batch(reqs, environment_ids=list(range(6)))
+    assert all(r.success for r in rows), [r.message for r in rows]
+    for r, fun, (c, kw) in zip(rows, funs, reqs):
+        assert abs(r.fun - fun) <= 1e-6 * max(1.0, abs(fun))
+        assert r.diagnostics["equality_reduction"] and r.diagnostics["certificate_passed"]
+        assert r.x.shape == (kw["A_eq"].shape[1],) and r.y.shape == (kw["A_eq"].shape[0],)
+    again = be.solve_batch(reqs, environment_ids=list(range(6)))
+    assert all(r.success for r in again)
+    assert sum(r.diagnostics["iterations"] for r in again) < sum(r.diagnostics["iterations"] for r in rows)
+    be.close()
