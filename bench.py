@@ -197,40 +197,19 @@ def run_reference(args):
 # ----------------------------------------------------------------------------- product arm
 def run_product(args):
     import torch
-    import torch.distributed as dist
 
     from co_cultivation_metabolic_atlas_b200 import synthetic as syn
     from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
     from co_cultivation_metabolic_atlas_b200.engine import SolveConfig
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
+    from co_cultivation_metabolic_atlas_b200.distributed import Ranks
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    ranks = Ranks("nccl")
+    world, rank, local, dev = ranks.world, ranks.rank, ranks.local_rank, ranks.device
+    barrier, max_over_ranks, sum_over_ranks = ranks.barrier, ranks.max, ranks.sum
 
     models = syn.community_models(seed=args.seed)
-    medium, biomass = syn.initial_environments(args.envs, seed=args.seed + 1000 * rank)
+    medium, biomass = syn.initial_environments(args.envs, seed=ranks.environment_seed(args.seed))
     cfg = SolveConfig(precision=args.precision)
     lps = args.envs * len(models)
     # kernels of this project per step: the PDHG launches (re-centred FP32 +
@@ -246,7 +225,7 @@ def run_product(args):
         from co_cultivation_metabolic_atlas_b200 import train_warmstart as tw
         t0 = time.perf_counter()
         data = tw.build_dataset(models, envs=args.envs, steps=args.learn_steps,
-                                seeds=[args.seed + 1000 * (world + 1) + 100 * rank + k for k in range(args.learn_seeds)],
+                                seeds=ranks.training_seeds(args.seed, args.learn_seeds),
                                 config=cfg, device=dev, log=lambda *_: None)
         ws, losses = tw.fit(models, data, epochs=args.learn_epochs, device=dev, log=lambda *_: None)
         torch.cuda.synchronize()
@@ -397,8 +376,7 @@ def run_product(args):
                 "roofline": roofline, "cpu_baseline": cpu, "highs_check": highs_check, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clock_summary}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 class _HostDrivenState:
