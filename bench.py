@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--learned", type=int, default=1,
                     help="1: train the learned warm start and measure it as the product arm (the temporal base "
                          "alone and cold PDHG are measured beside it)")
+    ap.add_argument("--graphs", type=int, default=1,
+                    help="1: capture the dFBA step in CUDA graphs after the warm-up and replay them when timed")
     ap.add_argument("--learn-seeds", type=int, default=2)
     ap.add_argument("--learn-steps", type=int, default=16)
     ap.add_argument("--learn-epochs", type=int, default=10)
@@ -239,6 +241,8 @@ def run_product(args):
         com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, learned=learned, device=dev)
         for _ in range(args.warmup):
             com.step()
+        if args.graphs and args.warmup >= 2:
+            com.capture()  # the timed steps replay CUDA graphs of whole dFBA steps
         torch.cuda.synchronize()
         barrier()
         stream = torch.cuda.current_stream()
@@ -250,7 +254,7 @@ def run_product(args):
         start.record(stream)
         for _ in range(args.steps):
             st = com.step()
-            certified.append(st.certified)
+            certified.append(st.certified.clone())
             iters.append(st.iterations.clone())
             launches += pdhg_launches
         stop.record(stream)
@@ -359,6 +363,7 @@ def run_product(args):
         if learned_info is not None:
             learned_info.update(value=value, mean_iterations=float(np.mean(it)))
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "cuda_graphs": bool(args.graphs and args.warmup >= 2),
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "fp32+fp64" if args.precision == "mixed" else args.precision,

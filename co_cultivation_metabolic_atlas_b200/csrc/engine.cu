@@ -446,14 +446,29 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
         slab = std::max(slab, P.slab_bytes);
     }
     dyn = fbalp::align_up(std::max<int64_t>(dyn, 16), 16);
-    Buffer& dl = fp64 ? e->layout64_buf : e->layout32_buf;
-    dl.ensure(layouts.size() * sizeof(fbalp::Layout));
-    check(cudaMemcpyAsync(dl.ptr, layouts.data(), layouts.size() * sizeof(fbalp::Layout),
-                          cudaMemcpyHostToDevice, e->stream), "copy layouts");
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    check(cudaStreamIsCapturing(e->stream, &capture), "cudaStreamIsCapturing");
+    const bool capturing = capture != cudaStreamCaptureStatusNone;
+    const int kind = recentred ? 1 + recentred : (fp64 ? 1 : 0);
+    Buffer& dl = e->layout_dev[kind];
+    std::vector<fbalp::Layout>& cached = e->layout_host[kind];
+    const size_t lbytes = layouts.size() * sizeof(fbalp::Layout);
+    if (cached.size() != layouts.size() || std::memcmp(cached.data(), layouts.data(), lbytes) != 0) {
+        if (capturing) throw CudaError("launch layouts changed during stream capture; solve once before capturing");
+        dl.ensure(lbytes);
+        check(cudaMemcpy(dl.ptr, layouts.data(), lbytes, cudaMemcpyHostToDevice), "copy layouts");
+        cached = layouts;
+    }
     const void* k = recentred ? fbalp::recentred_symbol(threads, recentred == 1)
                               : fbalp::kernel_symbol(fp64, threads, all_fast);
-    check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
-          "cudaFuncSetAttribute");
+    auto attr = std::find_if(e->smem_attr.begin(), e->smem_attr.end(),
+                             [&](const std::pair<const void*, int>& a) { return a.first == k; });
+    if (attr == e->smem_attr.end() || attr->second < dyn) {
+        check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
+              "cudaFuncSetAttribute");
+        if (attr == e->smem_attr.end()) e->smem_attr.emplace_back(k, static_cast<int>(dyn));
+        else attr->second = static_cast<int>(dyn);
+    }
     int per_sm = 0;
     check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, dyn), "occupancy");
     if (e->opt.blocks_per_sm > 0) per_sm = std::min(per_sm, e->opt.blocks_per_sm);
@@ -461,6 +476,8 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     const int grid = static_cast<int>(std::min<int64_t>(e->count, static_cast<int64_t>(per_sm) * e->sm_count));
     p.layouts = static_cast<const fbalp::Layout*>(dl.ptr);
     if (slab > 0) {
+        if (capturing && e->spill.bytes < static_cast<size_t>(slab) * grid)
+            throw CudaError("workspace would grow during stream capture; solve once before capturing");
         e->spill.ensure(static_cast<size_t>(slab) * grid);
         p.spill = static_cast<unsigned char*>(e->spill.ptr);
         p.spill_stride = slab;
@@ -471,14 +488,16 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     p.queue = static_cast<int32_t*>(e->queue.ptr) + (fp64 ? 1 : 0);
     check(cudaMemsetAsync(p.queue, 0, sizeof(int32_t), e->stream), "memset queue");
     const int ph = fp64 ? 1 : 0;
-    check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
+    // phase timing events only outside a capture (a graph replay has no
+    // per-phase timing)
+    if (!capturing) check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
     if (recentred)
         check(fbalp::launch_recentred(recentred == 1, grid, threads, dyn, e->stream, p),
               "re-centred pdhg kernel launch");
     else
         check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
-    check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
-    e->ran[ph] = true;
+    if (!capturing) check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
+    e->ran[ph] = !capturing;
     e->last_grid[fp64 ? 1 : 0] = grid;
     e->last_smem[fp64 ? 1 : 0] = dyn;
 }

@@ -95,6 +95,13 @@ struct fbalp_engine {
     Buffer queue, mid_x, mid_y, mid_omega, mid_iters, mid_status, mid_obj, mid_metrics, spill;
     Buffer hand_list, hand_count;  // re-centred phase -> FP64 phase work list
     Buffer layout32_buf, layout64_buf;
+    // device copies of the launch layouts, one per kernel kind (plain FP32,
+    // FP64, re-centred staged, re-centred streamed), uploaded only when their
+    // content changes: a solve that reuses them issues no host-to-device
+    // copy, so it can be captured in a CUDA graph
+    Buffer layout_dev[4];
+    std::vector<fbalp::Layout> layout_host[4];
+    std::vector<std::pair<const void*, int>> smem_attr;  // kernel -> dynamic smem set
     std::vector<fbalp::Layout> layouts32, layouts64;
     int last_grid[2] = {0, 0};
     int64_t last_smem[2] = {0, 0};
@@ -106,7 +113,8 @@ struct fbalp_engine {
         for (void* p : owned) cudaFree(p);
         for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
                           &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill, &layout32_buf,
-                          &layout64_buf, &hand_list, &hand_count})
+                          &layout64_buf, &hand_list, &hand_count, &layout_dev[0], &layout_dev[1],
+                          &layout_dev[2], &layout_dev[3]})
             b->release();
     }
 };

@@ -153,13 +153,15 @@ class DeviceCommunity:
         total = self.biomass.sum(dim=1, keepdim=True)
         cap = torch.clamp(1.0 - total / self.capacity, min=0.0)
         dX = mu * self.biomass * torch.where(mu > 0, cap, torch.ones_like(cap)) * self.dt
-        self.biomass = torch.clamp(self.biomass + dX, 0.0, self.capacity)
+        # state tensors are updated in place: their addresses stay fixed, so
+        # a captured step replays on the current state
+        self.biomass.copy_(torch.clamp(self.biomass + dX, 0.0, self.capacity))
         delta = torch.zeros_like(self.medium)
         for s, mm in enumerate(self.mm):
             v = x[mm["flat"]]                                                   # (E, k)
             contrib = v * X0[:, s:s + 1] * self.dt
             delta.index_add_(1, mm["ids"], contrib)
-        self.medium = torch.clamp(self.medium + delta, min=0.0)
+        self.medium.copy_(torch.clamp(self.medium + delta, min=0.0))
         self.step_index += 1
 
     def certified(self, res: SolveResult):
@@ -171,11 +173,66 @@ class DeviceCommunity:
         return ok.sum()
 
     def step(self) -> StepStats:
+        """One dFBA step: a captured graph's replay after ``capture``,
+        otherwise eager launches."""
+        if getattr(self, "_graphs", None):
+            return self._graph_step()
+        return self._eager_step()
+
+    # -- CUDA-graph-captured steps ---------------------------------------
+    def capture(self):
+        """Capture the next three dFBA steps as CUDA graphs (uptake bounds,
+        the engine's launches, Euler updates, certified count); ``step``
+        then replays them in turn.  Three graphs because a step reads the
+        result buffers of the two previous steps and writes the third, in a
+        rotation of period three; each graph bakes its buffers' addresses.
+        Needs two eager steps first (the warm-start history exists and the
+        engine's workspace is allocated) and a warm start that does not call
+        the network (it runs only at an environment's first step)."""
+        if self.prev is None or self.prev2 is None:
+            raise RuntimeError("run two steps before capturing")
+        if self.warm_start == "learned" and self.prev is None:
+            raise RuntimeError("the network's first-step seed is not captured")
+        if self.warm_start == "extrapolate" and self._wx is None:
+            raise RuntimeError("run a warm-started step before capturing")
+        saved = (self.step_index, self.prev, self.prev2, self.result, self._which)
+        old_stream = self.engine.stream
+        self._graphs, self._graph_stats = [], []
+        torch.cuda.synchronize(self.device)
+        try:
+            for _ in range(3):
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self.engine.set_stream(torch.cuda.current_stream(self.device))
+                    st = self._eager_step()
+                self._graphs.append(g)
+                self._graph_stats.append(st)
+        finally:
+            self.engine.set_stream(old_stream)
+            # capture ran nothing: the state is where it was
+            self.step_index, self.prev, self.prev2, self.result, self._which = saved
+        self._replay = 0
+
+    def release_graphs(self):
+        self._graphs, self._graph_stats = [], []
+
+    def _eager_step(self) -> StepStats:
         self.uptake_bounds()
         res = self.solve()
         self.integrate(res)
         return StepStats(lps=self.E * self.S, certified=self.certified(res),
                          iterations=res.iterations, status=res.status)
 
+    def _graph_step(self) -> StepStats:
+        k = self._replay
+        self._graphs[k].replay()
+        res = self._bufs[self._which]
+        self._which = (self._which + 1) % 3
+        self.prev2, self.prev, self.result = self.prev, res, res
+        self.step_index += 1
+        self._replay = (k + 1) % 3
+        return self._graph_stats[k]
+
     def close(self):
+        self.release_graphs()
         self.engine.close()

@@ -367,3 +367,29 @@ def test_iteration_hints_and_instance_data_rebinding():
     np.testing.assert_array_equal(rebound.iterations.cpu().numpy(), ref["iters"])
     np.testing.assert_array_equal(rebound.x[:eng.total_cols].cpu().numpy().reshape(4, -1), ref["x"])
     eng.close()
+
+
+def test_graph_captured_dfba_steps_equal_eager_steps():
+    """dFBA steps replayed from CUDA graphs (uptake bounds, the engine's
+    launches, Euler updates) give bit-for-bit the states of eager steps."""
+    import torch
+    from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(24, seed=5)
+    a = DeviceCommunity(models, medium, biomass, warm_start="extrapolate")
+    b = DeviceCommunity(models, medium, biomass, warm_start="extrapolate")
+    for _ in range(3):
+        a.step()
+        b.step()
+    b.capture()
+    its_a, its_b = [], []
+    for _ in range(7):
+        its_a.append(a.step().iterations.clone())
+        its_b.append(b.step().iterations.clone())
+    torch.cuda.synchronize()
+    for x, y in zip(its_a, its_b):
+        assert torch.equal(x, y)
+    assert torch.equal(a.medium, b.medium) and torch.equal(a.biomass, b.biomass)
+    assert torch.equal(a.result.x, b.result.x)
+    a.close()
+    b.close()
