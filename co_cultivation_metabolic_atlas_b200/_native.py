@@ -89,6 +89,8 @@ def load(path: os.PathLike | None = None):
         "fbalp_engine_set_instances": (ctypes.c_int, [vp, ctypes.c_int64, c_int32_p, vp, vp, vp, vp]),
         "fbalp_engine_set_instance_data": (ctypes.c_int, [vp, vp, vp, vp, vp]),
         "fbalp_engine_set_iteration_hints": (ctypes.c_int, [vp, vp]),
+        "fbalp_engine_set_patches": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p]),
+        "fbalp_engine_set_patch_values": (ctypes.c_int, [vp, vp, ctypes.c_int32]),
         "fbalp_engine_solve": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(SolveParams), vp, vp, vp, vp,
                                               vp, vp, vp]),
         "fbalp_engine_destroy": (ctypes.c_int, [vp]),

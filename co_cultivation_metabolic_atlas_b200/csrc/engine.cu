@@ -215,13 +215,14 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             std::vector<float> a32(sh.A.val.begin(), sh.A.val.end()), at32(sh.AT.val.begin(), sh.AT.val.end());
             d.a_elems = sh.A.off.back();
             d.at_elems = sh.AT.off.back();
-            std::vector<int4> alist, atlist;
+            std::vector<int4>& alist = sh.alist;
+            std::vector<int4>& atlist = sh.atlist;
             for (int32_t sl : sh.a_sched)
                 alist.push_back(make_int4(sl, sh.A.off[sl], sh.A.length[sl], 0));
             for (int32_t sl : sh.at_sched)
                 atlist.push_back(make_int4(sl, sh.AT.off[sl], sh.AT.length[sl], 0));
-            d.a_list = dev_upload(alist, E->owned);
-            d.at_list = dev_upload(atlist, E->owned);
+            d.a_list = sh.d_alist = dev_upload(alist, E->owned);
+            d.at_list = sh.d_atlist = dev_upload(atlist, E->owned);
             d.a_idx = dev_upload(sh.A.idx, E->owned);
             d.a_v32 = dev_upload(a32, E->owned);
             d.a_v64 = dev_upload(sh.A.val, E->owned);
@@ -256,6 +257,7 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             d.inv_dr = dev_upload(idr, E->owned);
             d.inv_dc = dev_upload(idc, E->owned);
             d.eta = sh.scaling.eta;
+            d.sigma_max = sh.scaling.sigma_max;
             E->dev_species_host.push_back(d);
         }
         E->dev_species = dev_upload(E->dev_species_host, E->owned);
@@ -334,6 +336,8 @@ int fbalp_engine_set_instances(fbalp_engine* e, int64_t count, const int32_t* sp
     e->cost = cost;
     e->rhs = rhs;
     e->hints = nullptr;
+    e->patch_values = nullptr;
+    e->patch_stride = 0;
     e->bound = true;
     return FBALP_OK;
 }
@@ -354,6 +358,63 @@ int fbalp_engine_set_iteration_hints(fbalp_engine* e, const int32_t* hints) {
     if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
     if (!e->bound) return fail(FBALP_ERR_STATE, "set_instances must be called first");
     e->hints = hints;
+    return FBALP_OK;
+}
+
+int fbalp_engine_set_patches(fbalp_engine* e, int32_t species, int32_t count, const int32_t* rows,
+                             const int32_t* cols) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (species < 0 || species >= static_cast<int32_t>(e->species.size()))
+        return fail(FBALP_ERR_INVALID, "species id out of range");
+    if (count < 0 || count > fbalp::kMaxPatches || (count > 0 && (!rows || !cols)))
+        return fail(FBALP_ERR_INVALID, "between 0 and 8 patched entries with row and column indices");
+    SpeciesHost& sh = e->species[species];
+    std::vector<int32_t> row_new(sh.m), col_new(sh.n);
+    for (int32_t i = 0; i < sh.m; ++i) row_new[sh.row_perm[i]] = i;
+    for (int32_t j = 0; j < sh.n; ++j) col_new[sh.col_perm[j]] = j;
+    for (int32_t q = 0; q < count; ++q)
+        if (rows[q] < 0 || rows[q] >= sh.m || cols[q] < 0 || cols[q] >= sh.n)
+            return fail(FBALP_ERR_INVALID, "patched entry outside the species matrix");
+    fbalp::DevSpecies& d = e->dev_species_host[species];
+    d.npatch = count;
+    for (int q = 0; q < fbalp::kMaxPatches; ++q) {
+        d.patch_row[q] = d.patch_col[q] = 0;
+        d.patch_scale[q] = 0.0;
+    }
+    for (auto& v : sh.alist) v.w = 0;
+    for (auto& v : sh.atlist) v.w = 0;
+    for (int32_t q = 0; q < count; ++q) {
+        const int32_t r = row_new[rows[q]], c = col_new[cols[q]];
+        d.patch_row[q] = r;
+        d.patch_col[q] = c;
+        d.patch_scale[q] = sh.scaling.dr[rows[q]] * sh.scaling.dc[cols[q]];
+        for (auto& v : sh.alist)
+            if (v.x == r / 32) v.w = 1;
+        for (auto& v : sh.atlist)
+            if (v.x == c / 32) v.w = 1;
+    }
+    try {
+        check(cudaMemcpy(sh.d_alist, sh.alist.data(), sh.alist.size() * sizeof(int4), cudaMemcpyHostToDevice),
+              "copy schedule");
+        check(cudaMemcpy(sh.d_atlist, sh.atlist.data(), sh.atlist.size() * sizeof(int4), cudaMemcpyHostToDevice),
+              "copy schedule");
+        check(cudaMemcpy(e->dev_species + species, &d, sizeof(d), cudaMemcpyHostToDevice), "copy species");
+    } catch (const CudaError& ex) {
+        return fail(FBALP_ERR_CUDA, ex.what());
+    }
+    return FBALP_OK;
+}
+
+int fbalp_engine_set_patch_values(fbalp_engine* e, const double* values, int32_t stride) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (!e->bound) return fail(FBALP_ERR_STATE, "set_instances must be called first");
+    if (values && (stride < 1 || stride > fbalp::kMaxPatches))
+        return fail(FBALP_ERR_INVALID, "stride must be in [1, 8]");
+    for (int32_t s : e->h_species)
+        if (values && e->dev_species_host[s].npatch > stride)
+            return fail(FBALP_ERR_INVALID, "stride is smaller than a species' number of patched entries");
+    e->patch_values = values;
+    e->patch_stride = values ? stride : 0;
     return FBALP_OK;
 }
 
@@ -551,6 +612,11 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
         p.check_every = q.check_every;
         p.rho = q.reflection;
         p.restarts = q.restarts;
+        bool patched = false;
+        if (e->patch_values)
+            for (int32_t sp_id : e->h_species) patched = patched || e->dev_species_host[sp_id].npatch > 0;
+        if (patched && !(q.precision == FBALP_PRECISION_MIXED && q.fp32_recentre && recentred_mode(e) != 0))
+            return fail(FBALP_ERR_INVALID, "patched entries need the re-centred mixed schedule");
         if (q.precision == FBALP_PRECISION_FP64 || q.precision == FBALP_PRECISION_FP32) {
             const bool fp64 = q.precision == FBALP_PRECISION_FP64;
             p.warm_x = warm_x;
@@ -615,6 +681,9 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             pr.hand_iters = static_cast<int32_t*>(e->mid_iters.ptr);
             pr.handoff_on_stall = 4 * q.fp64_stall_checks;
             pr.hint_iters = e->hints;
+            pr.patch_values = patched ? e->patch_values : nullptr;
+            pr.patch_stride = e->patch_stride;
+            if (patched) pr.handoff_on_stall = 0;  // the FP64 phase has no patched entries
             run_phase(e, false, pr, recentred_mode(e));
             fbalp::KernelParams p64 = p;
             p64.order = static_cast<const int32_t*>(e->hand_list.ptr);

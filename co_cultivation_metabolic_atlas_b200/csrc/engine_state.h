@@ -49,6 +49,9 @@ struct SpeciesHost {
     fbalp::Sell A, AT;
     fbalp::Sell Araw, ATraw;  // same slices, unscaled values
     std::vector<int32_t> a_sched_off, a_sched, at_sched_off, at_sched;
+    std::vector<int4> alist, atlist;  // schedule entries as uploaded (w: patched slice)
+    int4* d_alist = nullptr;           // their device copies
+    int4* d_atlist = nullptr;
 };
 
 struct Buffer {
@@ -89,6 +92,8 @@ struct fbalp_engine {
     std::vector<int64_t> h_coloff, h_rowoff;
     const double *lower = nullptr, *upper = nullptr, *cost = nullptr, *rhs = nullptr;
     const int32_t* hints = nullptr;  // per-instance iteration hints (device), may be null
+    const double* patch_values = nullptr;  // per-instance patched-entry deltas (device), may be null
+    int32_t patch_stride = 0;
     Buffer inst_species, col_off, row_off, order;
     bool bound = false;
     // workspace

@@ -78,6 +78,8 @@ extern "C" int fbalp_engine_solve_noalloc(fbalp_engine* e, int64_t count, const 
                                           double* out_omega) {
     if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
     if (e->species.size() != 1) return fail(FBALP_ERR_INVALID, "the no-allocation solve needs a one-species engine");
+    if (e->dev_species_host[0].npatch > 0)
+        return fail(FBALP_ERR_INVALID, "the no-allocation solve has no per-instance patched entries");
     if (count < 1 || count > INT32_MAX || !lower || !upper || !cost)
         return fail(FBALP_ERR_INVALID, "count >= 1 and lower/upper/cost are required");
     if (!out_status || !out_objective || !out_x || !out_y || !out_iterations || !out_metrics)

@@ -927,11 +927,20 @@ __device__ __forceinline__ float slice_dot_pk_global(const uint32_t* __restrict_
 
 // STAGED: the species' packed matrix words are in shared memory (indices
 // pre-offset to the gather target); otherwise they are streamed from L2.
+// Per-instance patched entries held by the CTA for the current instance.
+struct Patches {
+    int n;
+    const int* row;
+    const int* col;
+    const float* v32;
+    const double* v64;
+};
+
 template <bool STAGED>
 __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PT,
                                                       const int4* atlist, int t0, int t1, int n, int lane, float tau,
                                                       float w, float rho, bool check, const double* bx, double* cx,
-                                                      double& pdx2, double& pdxa2) {
+                                                      double& pdx2, double& pdxa2, const Patches& pt) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
@@ -941,9 +950,12 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
         const int jj = own ? j : 0;
         // the column's operands first: their latency overlaps the product
         const float xo = S[o.x + jj], dj = S[o.c + jj], lj = S[o.l + jj], uj = S[o.u + jj];
-        const float g = STAGED
+        float g = STAGED
             ? slice_dot_pk(PT + sl.y + lane, S, sl.z)
             : slice_dot_pk_global(sp->at_pk + sl.y + lane, S + o.y, sl.z);
+        if (sl.w && pt.n)  // a slice holding a patched column
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.col[q] == j) g = fmaf(pt.v32[q], S[o.y + pt.row[q]], g);
         if (own) {
             const float xn = clampT(xo - tau * (dj - g), lj, uj);
             const float xb = xn + xn - xo;
@@ -964,7 +976,7 @@ template <bool STAGED>
 __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PA,
                                                     const int4* alist, int t0, int t1, int m, int neq, int lane,
                                                     float sigma, float w, float rho, bool check, const double* by,
-                                                    double* cy, double& pdy2, double& pdya2) {
+                                                    double* cy, double& pdy2, double& pdya2, const Patches& pt) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
     for (int t = t0; t < t1; ++t) {
@@ -973,9 +985,12 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
         const bool own = i < m;
         const int ii = own ? i : 0;
         const float yo = S[o.y + ii], ri = S[o.b + ii], yl = S[o.ya + ii];
-        const float h = STAGED
+        float h = STAGED
             ? slice_dot_pk(PA + sl.y + lane, S, sl.z)
             : slice_dot_pk_global(sp->a_pk + sl.y + lane, S + o.xbar, sl.z);
+        if (sl.w && pt.n)  // a slice holding a patched row
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.row[q] == i) h = fmaf(pt.v32[q], S[o.xbar + pt.col[q]], h);
         if (own) {
             float yn = yo + sigma * (ri - h);
             if (i >= neq && yn > yl) yn = yl;  // y^ + dy <= 0
@@ -1064,7 +1079,7 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
                                                     int t1, int a_sub, int t_sub, double* xc, const double* yc,
                                                     const double* cs, const double* ls, const double* us,
                                                     const double* bs, float* dcand, float* rcand, bool cinf, int lane,
-                                                    double* v) {
+                                                    double* v, const Patches& pt) {
     const int n = sp->n, m = sp->m, neq = sp->neq;
     for (int t = t0; t < t1; ++t) {
         const int4 sl = atlist[t];
@@ -1073,9 +1088,12 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         const int jj = own ? j : 0;
         const double cj = cs[jj], lj = ls[jj], uj = us[jj], dcj = __ldg(sp->dc + jj);
         double xsc = xc[jj];
-        const double g = STAGED
+        double g = STAGED
             ? slice_dot64_staged(PT + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z)
             : slice_dot64_global2(sp->at_idx + sl.y + lane, sp->at_v64 + sl.y + lane, yc, sl.z);
+        if (sl.w && pt.n)
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.col[q] == j) g = fma(pt.v64[q], yc[pt.row[q]], g);
         if (own) {
             if (xsc < lj || xsc > uj) {
                 xsc = xsc < lj ? lj : uj;
@@ -1106,9 +1124,12 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         const bool own = i < m;
         const int ii = own ? i : 0;
         const double bi = bs[ii], ysc = yc[ii];
-        const double h = STAGED
+        double h = STAGED
             ? slice_dot64_staged(PA + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z)
             : slice_dot64_global2(sp->a_idx + sl.y + lane, sp->a_v64 + sl.y + lane, xc, sl.z);
+        if (sl.w && pt.n)
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.row[q] == i) h = fma(pt.v64[q], xc[pt.col[q]], h);
         if (own) {
             const double rr = bi - h;                  // scaled b - A x
             const double ro = -rr * __ldg(sp->inv_dr + i);  // A x - b in original units
@@ -1156,6 +1177,9 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     __shared__ double s_tot[kRed];
     __shared__ int s_inst;
     __shared__ int s_loaded;
+    __shared__ int s_prow[kMaxPatches], s_pcol[kMaxPatches];
+    __shared__ float s_pv32[kMaxPatches];
+    __shared__ double s_pv64[kMaxPatches];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthreads = blockDim.x;
     const int warps = nthreads >> 5;
     unsigned char* const slab = p.spill + static_cast<int64_t>(blockIdx.x) * p.spill_stride;
@@ -1209,8 +1233,21 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         const double* c_i = p.cost + coff;
         const double* b_i = p.rhs ? p.rhs + roff : nullptr;
 
-        // ---- scaled instance data and the start point (FP64, projected) ----
+        // ---- this instance's patched entries (scaled deltas) ----
+        const int npatch = (p.patch_values != nullptr) ? sp->npatch : 0;
         int bad = 0;
+        if (tid < npatch) {
+            const double dv = p.patch_values[static_cast<int64_t>(inst) * p.patch_stride + tid];
+            if (!isfinite(dv)) bad = 1;
+            const double sv = dv * sp->patch_scale[tid];
+            s_prow[tid] = sp->patch_row[tid];
+            s_pcol[tid] = sp->patch_col[tid];
+            s_pv64[tid] = sv;
+            s_pv32[tid] = static_cast<float>(sv);
+        }
+        const Patches pt{npatch, s_prow, s_pcol, s_pv32, s_pv64};
+
+        // ---- scaled instance data and the start point (FP64, projected) ----
         for (int j = tid; j < n; j += nthreads) {
             const int jo = sp->col_perm[j];
             const double dcj = sp->dc[j];
@@ -1264,7 +1301,14 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             continue;
         }
 
-        const double eta = sp->eta;
+        // step size: the shared matrix's, shrunk so that it stays below
+        // 1/||A~ + patches|| (||A~|| + ||deltas||_F bounds the latter)
+        double eta = sp->eta;
+        if (npatch) {
+            double f2 = 0.0;
+            for (int q = 0; q < npatch; ++q) f2 += s_pv64[q] * s_pv64[q];
+            eta *= sp->sigma_max / (sp->sigma_max + sqrt(f2));
+        }
         int status = -1;
         int cur = 0;   // buffer holding the base
         int ev = 0;    // buffer holding the last evaluated point
@@ -1275,7 +1319,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
             kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
-                                   us, bs, dcand, rcand, true, lane, v);
+                                   us, bs, dcand, rcand, true, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             cinf = s_tot[14];
             M = evaluate(s_tot, omega, p.tol_p, p.tol_d, p.tol_g);
@@ -1300,10 +1344,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             const float w = static_cast<float>((k + 1.0) / (k + 2.0));
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
             primal_pass_recentred<STAGED>(sp, o, PT, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
-                                          pdx2, pdxa2);
+                                          pdx2, pdxa2, pt);
             __syncthreads();
             dual_pass_recentred<STAGED>(sp, o, PA, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur),
-                                        PY(cur ^ 1), pdy2, pdya2);
+                                        PY(cur ^ 1), pdy2, pdya2, pt);
             __syncthreads();
             ++k;
             if (!check) continue;
@@ -1316,7 +1360,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             v[7] = pdxa2;
             v[8] = pdya2;
             kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
-                                   cs, ls, us, bs, dcand, rcand, false, lane, v);
+                                   cs, ls, us, bs, dcand, rcand, false, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             if (threadIdx.x == 0) s_tot[14] = cinf;
             __syncthreads();
@@ -1371,7 +1415,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
 #pragma unroll
                 for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
                 kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
-                                       bs, dcand, rcand, false, lane, vv);
+                                       bs, dcand, rcand, false, lane, vv, pt);
                 block_reduce(vv, s_red, s_tot);
                 cur ^= 1;
                 ev = cur;

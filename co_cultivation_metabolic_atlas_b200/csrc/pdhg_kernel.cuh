@@ -30,6 +30,7 @@ namespace fbalp {
 constexpr int kMaxWarps = 32;
 constexpr int kRed = 16;  // reduced quantities per convergence check
 constexpr int kArrayCount = 12;
+constexpr int kMaxPatches = 8;  // per-instance matrix entries per species
 
 // Array order: xbar, y, x, xa, ya, c, l, u, b, xs, ys, w.  In the unscaled
 // FP64 layout xbar holds z = dc * xbar (the gather target of the A pass) and
@@ -74,6 +75,15 @@ struct DevSpecies {
     // 16-bit indices)
     const uint32_t* a_pk;
     const uint32_t* at_pk;
+    // per-instance matrix entries: instance i's matrix is A + sum_p
+    // delta_ip e_{row p} e_{col p}^T (new numbering; the slices holding a
+    // patched row / column carry w = 1 in their schedule entries); the scaled
+    // delta is delta * patch_scale (dr_row dc_col)
+    int32_t npatch, pad2_;
+    int32_t patch_row[kMaxPatches];
+    int32_t patch_col[kMaxPatches];
+    double patch_scale[kMaxPatches];
+    double sigma_max;             // ||A~||_2 estimate of the shared matrix
 };
 
 // Byte offsets of one species' working set inside the CTA's dynamic shared
@@ -149,6 +159,9 @@ struct KernelParams {
     int32_t handoff_on_stall;     // >0: a re-centred solve whose KKT error has
                                   // not halved for this many full tests hands
                                   // off to the FP64 phase (0 = never)
+    const double* patch_values;   // may be null: per instance, npatch deltas
+                                  // (original units) at patch_stride apart
+    int32_t patch_stride, pad3_;
     const int32_t* hint_iters;    // may be null: per instance, the iteration
                                   // count of its previous solve; an instance
                                   // whose hint is >= check_every skips the

@@ -244,6 +244,31 @@ class LPEngine:
         N.check(self.lib.fbalp_engine_set_iteration_hints(self.handle, _ptr(h)))
         self._hints = h
 
+    def set_patches(self, species, rows, cols):
+        """Declare up to 8 per-instance matrix entries of one species
+        (original row / column indices)."""
+        rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1))
+        cols = np.ascontiguousarray(np.asarray(cols, dtype=np.int32).reshape(-1))
+        if rows.shape != cols.shape:
+            raise ValueError("rows and cols must have the same length")
+        N.check(self.lib.fbalp_engine_set_patches(self.handle, int(species), int(rows.size),
+                                                  rows.ctypes.data_as(N.c_int32_p), cols.ctypes.data_as(N.c_int32_p)))
+
+    def set_patch_values(self, values):
+        """Per-instance deltas of the patched entries: device (count, stride)
+        float64 (None clears)."""
+        if values is None:
+            N.check(self.lib.fbalp_engine_set_patch_values(self.handle, None, 0))
+            self._patch_values = None
+            return
+        if not isinstance(values, torch.Tensor):
+            values = torch.as_tensor(np.asarray(values, dtype=np.float64))
+        values = values.to(device=self.device, dtype=torch.float64).contiguous()
+        if values.ndim != 2 or values.shape[0] != self.count:
+            raise ValueError("patch values must have shape (count, stride)")
+        N.check(self.lib.fbalp_engine_set_patch_values(self.handle, _ptr(values), int(values.shape[1])))
+        self._patch_values = values
+
     def allocate_result(self) -> SolveResult:
         dev = self.device
         c = self.count

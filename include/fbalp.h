@@ -182,6 +182,24 @@ int fbalp_engine_set_instance_data(fbalp_engine* engine, const double* lower, co
  * certificate period is fixed, `src/gpu_pdhg_corrector.py:278-279`). */
 int fbalp_engine_set_iteration_hints(fbalp_engine* engine, const int32_t* hints);
 
+/* Per-instance matrix entries: declare up to 8 entries (original row and
+ * column indices) of species `species` whose value differs per instance;
+ * instance i's matrix is then A + sum_q delta_iq e_{rows[q]} e_{cols[q]}^T
+ * with the deltas bound by fbalp_engine_set_patch_values.  For LPs whose
+ * coefficients change with the state, e.g. the cooperative community LP's
+ * biomass-weighted rows (`src/community_solver.py:1084-1151`).  Solves of a
+ * batch with patched entries use the re-centred mixed schedule (and have no
+ * FP64 hand-off phase).  count = 0 clears.  The step size of each instance
+ * is shrunk to stay below 1/(||A~|| + ||scaled deltas||_F). */
+int fbalp_engine_set_patches(fbalp_engine* engine, int32_t species, int32_t count, const int32_t* rows,
+                             const int32_t* cols);
+
+/* Bind the per-instance deltas of the patched entries: DEVICE double
+ * [count * stride], instance i's deltas at [i*stride, i*stride + npatch);
+ * NULL clears (every instance uses A).  Kept until the next
+ * set_instances / set_patch_values. */
+int fbalp_engine_set_patch_values(fbalp_engine* engine, const double* values, int32_t stride);
+
 /* Solve every bound instance.  Warm starts (`warm_x`, `warm_y`: flat DEVICE,
  * original units; `warm_omega`: per instance) may be NULL (cold start).
  * Outputs are DEVICE arrays: status[count], objective[count],
