@@ -33,6 +33,7 @@ PRECISION_MIXED = 1
 PRECISION_FP32 = 2
 
 METRICS = 8
+MAX_PATCHES = 8      # FBALP_MAX_PATCHES
 METRIC_NAMES = ("primal_residual", "dual_violation", "relative_kkt_gap", "objective",
                 "dual_objective", "relative_gap", "x_inf", "omega")
 

@@ -19,6 +19,8 @@
 
 #include "engine_state.h"
 
+static_assert(fbalp::kMaxPatches == FBALP_MAX_PATCHES, "patch capacity of the kernel and the C ABI differ");
+
 namespace {
 
 // FP32 "hi" copy of unscaled SELL values plus, per (new-numbered) row, the

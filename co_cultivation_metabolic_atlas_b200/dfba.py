@@ -28,6 +28,31 @@ from .engine import EngineOptions, LPEngine, SolveConfig, SolveResult
 CARRYING_CAPACITY = 20.0
 
 
+def uptake_lower(conc, total, dt, mm):
+    """Michaelis-Menten uptake lower bounds of one species' medium exchanges
+    (``set_uptake_constraints``, ``src/dfba_simulator.py:640-667``):
+    ``conc`` (E, k) concentrations, ``total`` (E, 1) floored total biomass,
+    ``mm`` the species' ``vmax``/``km``/original lower (``orig``)/upper
+    (``ub``) rows; rounded to 6 decimals (``_safe_lb`` ``:553-563``)."""
+    v_kin = mm["vmax"] * conc / (mm["km"] + conc)
+    v_phys = torch.minimum(conc / (total * dt), mm["vmax"] * 10.0)
+    limit = torch.minimum(v_kin, v_phys)
+    lb = torch.clamp(torch.maximum(-limit, mm["orig"]), max=0.0)
+    lb = torch.minimum(lb, mm["ub"])
+    return torch.round(lb * 1e6) / 1e6
+
+
+def euler_biomass(biomass, mu, capacity, dt):
+    """Biomass Euler step (``update_biomass``, ``src/dfba_simulator.py:
+    1294-1324``, without the pH model): growth clipped to [-0.5, 2],
+    logistic capacity factor for positive growth."""
+    mu = mu.clamp(-0.5, 2.0)
+    total = biomass.sum(dim=1, keepdim=True)
+    cap = torch.clamp(1.0 - total / capacity, min=0.0)
+    dX = mu * biomass * torch.where(mu > 0, cap, torch.ones_like(cap)) * dt
+    return torch.clamp(biomass + dX, 0.0, capacity)
+
+
 @dataclass
 class StepStats:
     lps: int
@@ -103,13 +128,7 @@ class DeviceCommunity:
         """Write Michaelis-Menten uptake bounds into the bound batch."""
         total = self.biomass.clamp_min(1e-6).sum(dim=1, keepdim=True)          # (E, 1)
         for mm in self.mm:
-            conc = self.medium[:, mm["ids"]]                                    # (E, k)
-            v_kin = mm["vmax"] * conc / (mm["km"] + conc)
-            v_phys = torch.minimum(conc / (total * self.dt), mm["vmax"] * 10.0)
-            limit = torch.minimum(v_kin, v_phys)
-            lb = torch.clamp(torch.maximum(-limit, mm["orig"]), max=0.0)
-            lb = torch.minimum(lb, mm["ub"])
-            lb = torch.round(lb * 1e6) / 1e6
+            lb = uptake_lower(self.medium[:, mm["ids"]], total, self.dt, mm)
             self.lower.index_put_((mm["flat"].reshape(-1),), lb.reshape(-1))
 
     def solve(self):
@@ -149,13 +168,9 @@ class DeviceCommunity:
         E = self.E
         mu = torch.stack([x[idx] for idx in self.bio_index], dim=1)            # (E, S)
         X0 = self.biomass.clone()
-        mu = mu.clamp(-0.5, 2.0)
-        total = self.biomass.sum(dim=1, keepdim=True)
-        cap = torch.clamp(1.0 - total / self.capacity, min=0.0)
-        dX = mu * self.biomass * torch.where(mu > 0, cap, torch.ones_like(cap)) * self.dt
         # state tensors are updated in place: their addresses stay fixed, so
         # a captured step replays on the current state
-        self.biomass.copy_(torch.clamp(self.biomass + dX, 0.0, self.capacity))
+        self.biomass.copy_(euler_biomass(self.biomass, mu, self.capacity, self.dt))
         delta = torch.zeros_like(self.medium)
         for s, mm in enumerate(self.mm):
             v = x[mm["flat"]]                                                   # (E, k)

@@ -61,6 +61,9 @@ extern "C" {
 
 /* out_metrics row layout (FBALP_METRICS doubles per instance) */
 #define FBALP_METRICS 8
+
+/* most per-instance matrix entries one species may declare */
+#define FBALP_MAX_PATCHES 8
 #define FBALP_M_PRIMAL_RESIDUAL 0   /* max |A_eq x-b|, (A_ub x-b)+, bound viol. */
 #define FBALP_M_DUAL_VIOLATION 1    /* y_ub+, reduced-cost sign on inf. bounds  */
 #define FBALP_M_RELATIVE_KKT_GAP 2  /* complementarity / max(1,|c.x|)           */

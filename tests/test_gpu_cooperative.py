@@ -1,0 +1,150 @@
+"""Cooperative community LP on the GPU against the HiGHS oracle of the
+reference's own formulation (stage optima, certificates of the mapped-back
+solutions in the reference's units)."""
+
+import numpy as np
+import pytest
+import torch
+
+from co_cultivation_metabolic_atlas_b200 import cooperative as co
+from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+from co_cultivation_metabolic_atlas_b200.lp_trace import certificate as host_certificate
+from oracle import cooperative as oc
+from oracle.highs import solve_one
+from tests.test_cooperative import SMALL_SIZES, crossfeeding_members, oracle_args, random_state
+
+pytestmark = pytest.mark.gpu
+
+
+def reference_solution(solver, key, i, optimize, aggregate):
+    """Environment i's last solution of stage ``key`` in the reference's
+    variables and row layout (x_v = x_w / D, y_v = R y_w; empty metabolite
+    rows and an absent performance row get no dual)."""
+    st = solver.structure
+    x, y, _, table, _ = solver._prev[key]
+    x, y, table = x[i].double().cpu().numpy(), y[i].double().cpu().numpy(), table[i].cpu().numpy()
+    stage3 = key == "parsimonious_exchange"
+    rg = st.row_group3 if stage3 else st.row_group1
+    cg = st.col_group3 if stage3 else st.col_group1
+    xv = x / table[cg]
+    yv = y * table[rg]
+    full_k = st.neq + st.n_species + len(st.metabolites)
+    keep1 = np.concatenate([np.arange(st.neq + st.n_species), st.neq + st.n_species + st.medium_rows])
+    rows = np.arange(len(yv))
+    if stage3:
+        n_tail = 2 * st.n_aux
+        perf_present = optimize and aggregate > 1e-9
+        if optimize and not perf_present:
+            rows = np.delete(rows, st.perf_row)
+        ref_rows = np.concatenate([keep1, full_k + np.arange(int(perf_present) + n_tail)])
+        m_ref = full_k + int(perf_present) + n_tail
+    else:
+        ref_rows, m_ref = keep1, full_k
+    y_ref = np.zeros(m_ref)
+    y_ref[ref_rows] = yv[rows]
+    return xv, y_ref
+
+
+def check_against_oracle(solver, members, lower, upper, biomass, medium, dt, res, *, gmax, optimize, envs):
+    st, blocks, growth, exchange, orig = oracle_args(members)
+    for i in envs:
+        bio = dict(enumerate(biomass[i]))
+        med = dict(zip(st.metabolites, medium[i]))
+        full = oc.solve(blocks, growth, exchange, st.global_objective, lower[i], upper[i], bio, med, dt,
+                        original_lower=orig, maximum_coexistence_growth=gmax,
+                        optimize_live_objectives=optimize)
+        assert full.status == "optimal"
+        nu = float(res.coexistence[i])
+        assert nu == pytest.approx(full.coexistence, abs=1e-6 * (1 + abs(full.coexistence)))
+        agg = float(res.aggregate[i])
+        probs = oc.stage_problems(blocks, growth, exchange, st.global_objective, lower[i], upper[i], bio, med, dt,
+                                  coexistence=nu, aggregate=agg, original_lower=orig,
+                                  maximum_coexistence_growth=gmax, optimize_live_objectives=optimize)
+        keys = ["max_min"] + (["aggregate_objective"] if optimize else []) + ["parsimonious_exchange"]
+        for key in keys:
+            prob = probs[key]
+            xv, yv = reference_solution(solver, key, i, optimize, agg)
+            cert = host_certificate(prob, xv, yv)
+            assert cert["certificate_passed"], (key, i, cert)
+            if key != "max_min":
+                status, fun, _, _ = solve_one(prob[0], prob[2], prob[3], prob[4], prob[1], prob[5])
+                assert status == 0
+                mine = float(prob[4] @ xv)
+                assert mine == pytest.approx(fun, rel=1e-6, abs=1e-7), (key, i)
+
+
+def test_crossfeeding_community_on_gpu():
+    members, lower, upper = crossfeeding_members()
+    solver = co.CooperativeSolver(members)
+    st = solver.structure
+    assert st.metabolites == ["carbon_e", "factor_e"]
+    biomass = np.array([[1.0, 1.0], [1.0, 0.7], [0.23, 1.9], [0.5, 0.05]])
+    medium = np.array([[10.0, 0.0], [10.0, 0.0], [2.0, 0.4], [5.0, 1.0]])
+    E = len(biomass)
+    lo, up = np.repeat(lower[None], E, 0), np.repeat(upper[None], E, 0)
+    res = solver.solve(biomass, medium, 0.2, lo, up)
+    torch.cuda.synchronize()
+    assert bool(res.ok.all()), res.stages["max_min"]["status"]
+    assert (res.stage.cpu() == co.STAGE_PARSIMONIOUS).all()
+    v = res.fluxes.cpu().numpy()
+    # without factor in the medium the consumer lives on the producer's
+    # secretion in the same interval
+    produced, consumed = biomass[:2, 0] * v[:2, 4], -biomass[:2, 1] * v[:2, 6]
+    assert (produced > 0).all() and (consumed > 0).all() and (consumed <= produced + 1e-8).all()
+    assert (v[:, 8] > 0).all()
+    check_against_oracle(solver, members, lo, up, biomass, medium, 0.2, res, gmax=None, optimize=False,
+                         envs=range(E))
+    solver.close()
+
+
+@pytest.mark.parametrize("optimize", [False, True])
+def test_synthetic_community_stages_match_oracle(optimize):
+    models = syn.community_models(SMALL_SIZES, seed=0, n_medium=12, per_species=6)
+    members = co.synthetic_members(models)
+    gmax = None if optimize else 0.005
+    solver = co.CooperativeSolver(members, optimize_live_objectives=optimize, maximum_coexistence_growth=gmax)
+    st = solver.structure
+    rng = np.random.default_rng(11)
+    E = 12
+    biomass, medium = random_state(st, E, rng)
+    lower = np.repeat(np.concatenate([m.lower for m in models])[None], E, 0)
+    upper = np.repeat(np.concatenate([m.upper for m in models])[None], E, 0)
+    # uptake-limited medium exchanges, as the dFBA step sets them
+    for s, m in enumerate(models):
+        cols = st.col_start[s] + m.medium_columns
+        lower[:, cols] = -rng.uniform(0.0, 10.0, (E, len(cols)))
+    for call in range(2):
+        res = solver.solve(biomass, medium, 0.1, lower, upper)
+        torch.cuda.synchronize()
+        assert bool(res.ok.all()), {k: v["certified"].cpu() for k, v in res.stages.items()}
+        check_against_oracle(solver, members, lower, upper, biomass, medium, 0.1, res, gmax=gmax,
+                             optimize=optimize, envs=range(0, E, 3))
+        # the next call warm-starts from this one, rescaled to a new biomass
+        biomass = biomass * rng.uniform(0.9, 1.2, biomass.shape)
+        medium = medium * rng.uniform(0.8, 1.0, medium.shape)
+    solver.close()
+
+
+def test_cooperative_rollout_full_size_community():
+    """Three steps of the cooperative dFBA on the full-size synthetic
+    community (one 6,701-column joint LP per environment and stage)."""
+    models = syn.community_models()
+    medium, biomass = syn.initial_environments(16)
+    com = co.CooperativeCommunity(models, medium, biomass, dt=0.05)
+    st = com.solver.structure
+    members = com.solver.structure.members
+    for step in range(3):
+        X = com.biomass.cpu().numpy()
+        C = com.medium[:, com.met_ids].cpu().numpy()
+        lower = com.live_bounds()
+        lo = lower.cpu().numpy()
+        up = com.upper.cpu().numpy()
+        res = com.step()
+        torch.cuda.synchronize()
+        assert bool(res.ok.all())
+        if step in (0, 2):
+            check_against_oracle(com.solver, members, lo, up, X, C, com.dt, res, gmax=0.005, optimize=False,
+                                 envs=(0, 7))
+    assert torch.isfinite(com.biomass).all() and (com.biomass > 0).all()
+    assert st.template1.shape[1] == st.n_fluxes + 1
+    com.close()
