@@ -44,6 +44,7 @@ reference's gate.
 
 from __future__ import annotations
 
+import warnings
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -223,10 +224,15 @@ class CommunityStructure:
 
 def _csr_tensor(a, device):
     a = csr_matrix(a)
-    return torch.sparse_csr_tensor(torch.as_tensor(a.indptr, dtype=torch.int64),
-                                   torch.as_tensor(a.indices, dtype=torch.int64),
-                                   torch.as_tensor(a.data, dtype=torch.float64), size=a.shape, device=device,
-                                   check_invariants=False)
+    a.sort_indices()
+    with warnings.catch_warnings():
+        # torch flags its CSR layout as beta; the arrays come from a
+        # canonical SciPy matrix
+        warnings.simplefilter("ignore", UserWarning)
+        return torch.sparse_csr_tensor(torch.as_tensor(a.indptr, dtype=torch.int64),
+                                       torch.as_tensor(a.indices, dtype=torch.int64),
+                                       torch.as_tensor(a.data, dtype=torch.float64), size=a.shape, device=device,
+                                       check_invariants=False)
 
 
 class _Template:
