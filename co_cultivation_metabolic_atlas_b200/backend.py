@@ -29,6 +29,16 @@ exact homogeneous-equality reduction (``reduction.py``; one plan per
 equality block), the reduced LPs are solved on the GPU, and the primal is
 expanded and the duals lifted back; the row is accepted only when the
 original-LP certificate passes on the lifted pair.
+
+With ``split_rows=L`` (off by default) rows longer than ``L`` (the hub
+metabolites of genome-scale models hold up to ~1,200 reactions) are split
+exactly into segments with auxiliary variables (``rowsplit.py``) before the
+solve, so that no slice of the kernel walks or pads to a thousand-entry row;
+the solution is restricted back and accepted only on the original LP's
+certificate.  Measured on the reference's five consortium models: the split
+solves are ~12x faster, but the restricted duals (one per row where the
+split LP has one per segment) miss the 1e-7 KKT-gap gate on most LPs
+(relative gaps 1.6e-7 to 9.5e-6), so those rows fail closed.
 """
 
 from __future__ import annotations
@@ -44,6 +54,7 @@ from .engine import EngineOptions, LPEngine, SolveConfig
 from .lp_trace import certificate as original_certificate
 from .problem import matrix_key, normalize
 from .reduction import EqualityReduction
+from .rowsplit import RowSplit
 
 PRIMAL_GATE = 1e-5
 DUAL_GATE = 1e-7
@@ -57,7 +68,7 @@ class B200LPBackend:
     def __init__(self, *, mode='previous', precision='mixed', iterations=20000,
                  fp32_iterations=20000, check_interval=64, stage=None,
                  options: EngineOptions | None = None, warm_start_model=None, device=None,
-                 equality_reduction=False):
+                 equality_reduction=False, split_rows=None):
         if mode not in ('cold', 'previous', 'mlp'):
             raise ValueError('Unknown warm-start mode')
         if mode == 'mlp' and warm_start_model is None:
@@ -82,6 +93,11 @@ class B200LPBackend:
         if mode == 'mlp' and equality_reduction:
             raise ValueError('the learned warm start proposes original-space points; use equality_reduction=False')
         self.equality_reduction = bool(equality_reduction)
+        if split_rows is not None and (isinstance(split_rows, (bool, np.bool_)) or
+                                       not isinstance(split_rows, (int, np.integer)) or split_rows < 2):
+            raise ValueError('split_rows must be None or an integer >= 2')
+        self.split_rows = None if split_rows is None else int(split_rows)
+        self._split_plans: dict = {}
         self._plans: dict = {}
         self._keys: list[str] = []
         self._matrices = []
@@ -130,6 +146,8 @@ class B200LPBackend:
         reduced = self._reduce(originals) if self.equality_reduction else None
         problems = originals if reduced is None else [r.problem if r is not None else o
                                                         for r, o in zip(reduced, originals)]
+        splits = self._splits(problems)
+        problems = [sp.split_problem(p) if sp is not None else p for sp, p in zip(splits, problems)]
         prep = time.perf_counter()
         species, rebuilt = self._engine_for(problems)
         eng = self._engine
@@ -152,6 +170,8 @@ class B200LPBackend:
                     if reduced is not None and reduced[i] is not None:
                         px = reduced[i].compress_primal(px)
                         py = py[reduced[i].plan.kept_rows]
+                    if splits[i] is not None:
+                        px, py = splits[i].extend_primal(px), splits[i].extend_dual(py)
                     wx[co[i]:co[i] + n] = px
                     wy[ro[i]:ro[i] + m] = py
                     wo[i] = prev[3]
@@ -183,6 +203,12 @@ class B200LPBackend:
             cert = dict(primal_residual=float(mt[0]), dual_violation=float(mt[1]),
                         relative_kkt_gap=float(mt[2]))
             note = None
+            if splits[i] is not None:
+                # back to the unsplit LP; the kernel's metrics were the split LP's
+                xi, yi = splits[i].restrict(xi, yi)
+                if reduced is None:
+                    cert = original_certificate(originals[i], xi, yi)
+                    gate = gate and cert.pop('certificate_passed')
             if reduced is not None:
                 if reduced[i] is None:
                     gate, note = False, 'bounds infeasible under the eliminated equalities'
@@ -220,6 +246,21 @@ class B200LPBackend:
                                  total_seconds=time.perf_counter() - started,
                                  rows=[r.diagnostics for r in rows]))
         return rows
+
+    def _splits(self, problems):
+        """The long-row split plan of every request's matrix (built once per
+        matrix), or None where no row exceeds ``split_rows``."""
+        if self.split_rows is None or self.mode == 'mlp':
+            # the learned warm start proposes points of the unsplit LPs
+            return [None] * len(problems)
+        out = []
+        for p in problems:
+            key = matrix_key(p[0], p[5])
+            if key not in self._split_plans:
+                plan = RowSplit(p[0], p[5], max_length=self.split_rows)
+                self._split_plans[key] = plan if plan.active else None
+            out.append(self._split_plans[key])
+        return out
 
     def _reduce(self, originals):
         """Reduce every request with the plan of its equality block (built

@@ -32,3 +32,12 @@ def native_built():
     from co_cultivation_metabolic_atlas_b200 import build
     build.build()
     return build.LIB
+
+
+@pytest.fixture
+def forbid_cpu_optimizers(monkeypatch):
+    import scipy.optimize
+
+    def forbidden(*_a, **_k):
+        raise AssertionError("CPU optimizer was called")
+    monkeypatch.setattr(scipy.optimize, "linprog", forbidden)

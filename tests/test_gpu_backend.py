@@ -16,15 +16,6 @@ def requests_for(model, lower, upper):
                      model.S.shape[0])) for i in range(len(lower))]
 
 
-@pytest.fixture
-def forbid_cpu_optimizers(monkeypatch):
-    import scipy.optimize
-
-    def forbidden(*_a, **_k):
-        raise AssertionError("CPU optimizer was called")
-    monkeypatch.setattr(scipy.optimize, "linprog", forbidden)
-
-
 def test_rows_match_highs_without_cpu_optimizer(golden_dir, forbid_cpu_optimizers):
     from co_cultivation_metabolic_atlas_b200 import B200LPBackend
     g = np.load(golden_dir / "highs_single.npz")

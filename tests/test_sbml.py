@@ -1,0 +1,102 @@
+"""SBML reader: known answers from the reference's own tests on its
+consortium models (read when the reference checkout is present), and the
+committed real-model LP fixtures (always)."""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+from scipy.optimize import linprog
+
+from co_cultivation_metabolic_atlas_b200 import lp_trace, sbml
+
+REFERENCE = Path("/root/reference")
+SBML_DIR = Path(__file__).resolve().parent / "golden" / "sbml"
+needs_reference = pytest.mark.skipif(not (REFERENCE / "models" / "sbml").is_dir(),
+                                     reason="reference models not present")
+
+
+def _open_growth(m):
+    """``_fully_open_growth`` of ``tests/test_wcfs1_2022_repair.py:13-19``:
+    every exchange at ``lower <= -20``, ``upper >= 1000``, maximise the
+    objective."""
+    lo, up = m.lower.copy(), m.upper.copy()
+    lo[m.exchanges] = np.minimum(lo[m.exchanges], -20.0)
+    up[m.exchanges] = np.maximum(up[m.exchanges], 1000.0)
+    r = linprog(m.fba_cost(), A_eq=m.S, b_eq=np.zeros(m.S.shape[0]), bounds=np.column_stack([lo, up]),
+                method="highs")
+    return -r.fun if r.status == 0 else 0.0
+
+
+@needs_reference
+def test_wcfs1_repaired_model_pins():
+    """``tests/test_wcfs1_2022_repair.py``: model id, biomass coefficients,
+    no peptido_LPL_c in the repaired biomass, positive open growth; the
+    deposited model's biomass holds peptido_LPL_c and cannot grow."""
+    m = sbml.read_sbml(REFERENCE / "models/sbml/final_consortium/Lactobacillus_plantarum.xml")
+    assert m.id == "WCFS1_Koduru2022_repaired"
+    coef = m.reaction_stoichiometry("biomass")
+    assert coef["PGlac2_c"] == pytest.approx(-0.1462)
+    assert coef["CPS_LPL2_c"] == pytest.approx(-0.1294)
+    assert coef["nad_c"] == pytest.approx(-0.002)
+    assert "peptido_LPL_c" not in coef
+    assert "UGMDDS2" in m.reactions
+    assert _open_growth(m) > 1e-6
+    src = sbml.read_sbml(REFERENCE / "models/sbml/reference/Lactiplantibacillus_plantarum_WCFS1_Koduru2022.xml")
+    assert "peptido_LPL_c" in src.reaction_stoichiometry("biomass")
+    assert "UGMDDS2" not in src.reactions
+    assert _open_growth(src) == pytest.approx(0.0, abs=1e-9)
+    assert len(m.exchanges) == len(src.exchanges)
+    assert len(m.reactions) == len(src.reactions) + 1
+
+
+@needs_reference
+def test_consortium_model_pins():
+    """``tests/test_science_integrity.py``: NS21's PHA unit is cytosolic
+    (compartment ``C_c``); OR16 has no ODTD metabolite and its Lcp reaction
+    ``R_LCP`` is closed; the plantarum model with every exchange at -10
+    solves and secretes no biosurfactant."""
+    base = REFERENCE / "models/sbml/final_consortium"
+    ns21 = sbml.read_sbml(base / "Rhizobacter_gummiphilus_NS21.xml")
+    assert ns21.compartments[ns21.metabolite_index("pha_c")] == "C_c"
+    or16 = sbml.read_sbml(base / "Actinoplanes_sp_OR16_lcp.xml")
+    assert not [x for x in or16.metabolites if "odtd" in x.lower()]
+    j = or16.reaction_index("R_LCP")
+    assert (or16.lower[j], or16.upper[j]) == (0.0, 0.0)
+    lp = sbml.read_sbml(base / "Lactobacillus_plantarum.xml")
+    lo = lp.lower.copy()
+    lo[lp.exchanges] = -10.0
+    r = linprog(lp.fba_cost(), A_eq=lp.S, b_eq=np.zeros(lp.S.shape[0]), bounds=np.column_stack([lo, lp.upper]),
+                method="highs")
+    assert r.status == 0
+    if "EX_biosurfactant_e" in lp.reactions:
+        assert abs(r.x[lp.reaction_index("EX_biosurfactant_e")]) < 1e-12
+
+
+@needs_reference
+def test_reader_on_every_consortium_model():
+    """Every model parses with one objective column, an external
+    compartment and exchange reactions that each touch one external
+    metabolite; the committed fixtures hold exactly these matrices."""
+    meta = json.loads((SBML_DIR / "models.json").read_text())
+    for key, info in meta.items():
+        m = sbml.read_sbml(REFERENCE / info["source"])
+        assert (m.S.shape, m.S.nnz) == ((info["rows"], info["columns"]), info["nonzeros"])
+        assert list(m.exchanges) == info["exchanges"]
+        assert int(np.flatnonzero(m.objective)[0]) == info["objective_column"]
+        for j in m.exchanges[:20]:
+            assert m.compartments[m.metabolite_index(m.exchange_metabolite(j))] == m.external_compartment
+
+
+def test_sbml_fixtures_load_and_certify():
+    """The real-model LPs load through the trace loader (checksums, hashes,
+    certificate of the recorded HiGHS pair) and their objectives are the
+    recorded HiGHS optima."""
+    meta = json.loads((SBML_DIR / "models.json").read_text())
+    entries = lp_trace.read_manifest(SBML_DIR)
+    assert len(entries) == 2 * len(meta)
+    for e in entries:
+        problem, x, y = lp_trace.load_trace_lp(SBML_DIR, e)
+        key, variant = e["filename"][:-4].rsplit("_", 1)
+        assert float(problem[4] @ x) == pytest.approx(meta[key]["highs_objective"][variant], rel=1e-12)
