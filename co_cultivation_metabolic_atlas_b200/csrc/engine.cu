@@ -522,7 +522,8 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
         check(cudaMemcpy(dl.ptr, layouts.data(), lbytes, cudaMemcpyHostToDevice), "copy layouts");
         cached = layouts;
     }
-    const void* k = recentred ? fbalp::recentred_symbol(threads, recentred == 1)
+    const bool patched = recentred && p.patch_values != nullptr;
+    const void* k = recentred ? fbalp::recentred_symbol(threads, recentred == 1, patched)
                               : fbalp::kernel_symbol(fp64, threads, all_fast);
     auto attr = std::find_if(e->smem_attr.begin(), e->smem_attr.end(),
                              [&](const std::pair<const void*, int>& a) { return a.first == k; });
@@ -555,7 +556,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     // per-phase timing)
     if (!capturing) check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
     if (recentred)
-        check(fbalp::launch_recentred(recentred == 1, grid, threads, dyn, e->stream, p),
+        check(fbalp::launch_recentred(recentred == 1, patched, grid, threads, dyn, e->stream, p),
               "re-centred pdhg kernel launch");
     else
         check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");

@@ -248,8 +248,8 @@ inline bool layout_aligned(const Layout& L) {
 }
 
 const void* kernel_symbol(bool fp64, int threads, bool fast);
-const void* recentred_symbol(int threads, bool staged);
-cudaError_t launch_recentred(bool staged, int grid, int threads, size_t smem, cudaStream_t stream,
+const void* recentred_symbol(int threads, bool staged, bool patched);
+cudaError_t launch_recentred(bool staged, bool patched, int grid, int threads, size_t smem, cudaStream_t stream,
                              const KernelParams& p);
 cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
                         const KernelParams& p);

@@ -936,7 +936,7 @@ struct Patches {
     const double* v64;
 };
 
-template <bool STAGED>
+template <bool STAGED, bool PATCHED>
 __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PT,
                                                       const int4* atlist, int t0, int t1, int n, int lane, float tau,
                                                       float w, float rho, bool check, const double* bx, double* cx,
@@ -953,7 +953,7 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
         float g = STAGED
             ? slice_dot_pk(PT + sl.y + lane, S, sl.z)
             : slice_dot_pk_global(sp->at_pk + sl.y + lane, S + o.y, sl.z);
-        if (sl.w && pt.n)  // a slice holding a patched column
+        if (PATCHED && sl.w && pt.n)  // a slice holding a patched column
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fmaf(pt.v32[q], S[o.y + pt.row[q]], g);
         if (own) {
@@ -972,7 +972,7 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
     }
 }
 
-template <bool STAGED>
+template <bool STAGED, bool PATCHED>
 __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PA,
                                                     const int4* alist, int t0, int t1, int m, int neq, int lane,
                                                     float sigma, float w, float rho, bool check, const double* by,
@@ -988,7 +988,7 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
         float h = STAGED
             ? slice_dot_pk(PA + sl.y + lane, S, sl.z)
             : slice_dot_pk_global(sp->a_pk + sl.y + lane, S + o.xbar, sl.z);
-        if (sl.w && pt.n)  // a slice holding a patched row
+        if (PATCHED && sl.w && pt.n)  // a slice holding a patched row
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fmaf(pt.v32[q], S[o.xbar + pt.col[q]], h);
         if (own) {
@@ -1073,7 +1073,7 @@ __device__ __forceinline__ double slice_dot64_global2(const int32_t* __restrict_
 // bs - A~ xc are stored in FP32 for a re-centring at this candidate.
 // |c|_inf (v[14]) is accumulated only when `cinf` is set.  All threads call
 // it (it synchronises between the column and the row loops).
-template <bool STAGED>
+template <bool STAGED, bool PATCHED>
 __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const uint32_t* PA, const uint32_t* PT,
                                                     const int4* alist, const int4* atlist, int a0, int a1, int t0,
                                                     int t1, int a_sub, int t_sub, double* xc, const double* yc,
@@ -1091,7 +1091,7 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         double g = STAGED
             ? slice_dot64_staged(PT + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z)
             : slice_dot64_global2(sp->at_idx + sl.y + lane, sp->at_v64 + sl.y + lane, yc, sl.z);
-        if (sl.w && pt.n)
+        if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fma(pt.v64[q], yc[pt.row[q]], g);
         if (own) {
@@ -1127,7 +1127,7 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
         double h = STAGED
             ? slice_dot64_staged(PA + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z)
             : slice_dot64_global2(sp->a_idx + sl.y + lane, sp->a_v64 + sl.y + lane, xc, sl.z);
-        if (sl.w && pt.n)
+        if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fma(pt.v64[q], xc[pt.col[q]], h);
         if (own) {
@@ -1170,7 +1170,7 @@ __device__ __forceinline__ void recentre(const DevSpecies* sp, const FastOffsets
     }
 }
 
-template <int MAXT, bool STAGED>
+template <int MAXT, bool STAGED, bool PATCHED>
 __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ double s_red[MAXT / 32][kRed];
@@ -1234,7 +1234,8 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         const double* b_i = p.rhs ? p.rhs + roff : nullptr;
 
         // ---- this instance's patched entries (scaled deltas) ----
-        const int npatch = (p.patch_values != nullptr) ? sp->npatch : 0;
+        // (compiled out of the variant for batches without patched entries)
+        const int npatch = (PATCHED && p.patch_values != nullptr) ? sp->npatch : 0;
         int bad = 0;
         if (tid < npatch) {
             const double dv = p.patch_values[static_cast<int64_t>(inst) * p.patch_stride + tid];
@@ -1304,7 +1305,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         // step size: the shared matrix's, shrunk so that it stays below
         // 1/||A~ + patches|| (||A~|| + ||deltas||_F bounds the latter)
         double eta = sp->eta;
-        if (npatch) {
+        if (PATCHED && npatch) {
             double f2 = 0.0;
             for (int q = 0; q < npatch; ++q) f2 += s_pv64[q] * s_pv64[q];
             eta *= sp->sigma_max / (sp->sigma_max + sqrt(f2));
@@ -1318,7 +1319,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             double v[kRed];
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-            kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
+            kkt_partials_recentred<STAGED, PATCHED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
                                    us, bs, dcand, rcand, true, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             cinf = s_tot[14];
@@ -1343,10 +1344,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             const float tau = static_cast<float>(eta / omega), sigma = static_cast<float>(eta * omega);
             const float w = static_cast<float>((k + 1.0) / (k + 2.0));
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
-            primal_pass_recentred<STAGED>(sp, o, PT, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
+            primal_pass_recentred<STAGED, PATCHED>(sp, o, PT, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
                                           pdx2, pdxa2, pt);
             __syncthreads();
-            dual_pass_recentred<STAGED>(sp, o, PA, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur),
+            dual_pass_recentred<STAGED, PATCHED>(sp, o, PA, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur),
                                         PY(cur ^ 1), pdy2, pdya2, pt);
             __syncthreads();
             ++k;
@@ -1359,7 +1360,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             v[6] = pdy2;
             v[7] = pdxa2;
             v[8] = pdya2;
-            kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
+            kkt_partials_recentred<STAGED, PATCHED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
                                    cs, ls, us, bs, dcand, rcand, false, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             if (threadIdx.x == 0) s_tot[14] = cinf;
@@ -1414,7 +1415,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 double vv[kRed];
 #pragma unroll
                 for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-                kkt_partials_recentred<STAGED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
+                kkt_partials_recentred<STAGED, PATCHED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
                                        bs, dcand, rcand, false, lane, vv, pt);
                 block_reduce(vv, s_red, s_tot);
                 cur ^= 1;
@@ -1493,14 +1494,18 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     template __global__ void pdhg_persistent<double, MAXT, 0>(KernelParams);  \
     template __global__ void pdhg_persistent<double, MAXT, 1>(KernelParams);  \
     template __global__ void pdhg_persistent<double, MAXT, 2>(KernelParams);  \
-    template __global__ void pdhg_recentred<MAXT, true>(KernelParams);        \
-    template __global__ void pdhg_recentred<MAXT, false>(KernelParams);
+    template __global__ void pdhg_recentred<MAXT, true, false>(KernelParams); \
+    template __global__ void pdhg_recentred<MAXT, false, false>(KernelParams); \
+    template __global__ void pdhg_recentred<MAXT, true, true>(KernelParams);  \
+    template __global__ void pdhg_recentred<MAXT, false, true>(KernelParams);
 FBALP_INSTANTIATE(512)
 FBALP_INSTANTIATE(1024)
 // the re-centred kernel also at 768 threads (an 85-register budget: more
 // warps per scheduler to hide shared-memory latency)
-template __global__ void pdhg_recentred<768, true>(KernelParams);
-template __global__ void pdhg_recentred<768, false>(KernelParams);
+template __global__ void pdhg_recentred<768, true, false>(KernelParams);
+template __global__ void pdhg_recentred<768, false, false>(KernelParams);
+template __global__ void pdhg_recentred<768, true, true>(KernelParams);
+template __global__ void pdhg_recentred<768, false, true>(KernelParams);
 #undef FBALP_INSTANTIATE
 
 // Blocks of up to 512 threads use the variant with a 128-register budget,
@@ -1538,29 +1543,41 @@ cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem
     return cudaGetLastError();
 }
 
-const void* recentred_symbol(int threads, bool staged) {
-    if (threads <= 512)
-        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<512, true>)
-                      : reinterpret_cast<const void*>(&pdhg_recentred<512, false>);
-    if (threads <= 768)
-        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<768, true>)
-                      : reinterpret_cast<const void*>(&pdhg_recentred<768, false>);
-    return staged ? reinterpret_cast<const void*>(&pdhg_recentred<1024, true>)
-                  : reinterpret_cast<const void*>(&pdhg_recentred<1024, false>);
+// `patched`: the variant that applies per-instance patched entries (launched
+// only for batches that bind patch values; the other variant has none of
+// that code).
+template <int MAXT>
+static const void* recentred_for(bool staged, bool patched) {
+    if (patched)
+        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<MAXT, true, true>)
+                      : reinterpret_cast<const void*>(&pdhg_recentred<MAXT, false, true>);
+    return staged ? reinterpret_cast<const void*>(&pdhg_recentred<MAXT, true, false>)
+                  : reinterpret_cast<const void*>(&pdhg_recentred<MAXT, false, false>);
 }
 
-cudaError_t launch_recentred(bool staged, int grid, int threads, size_t smem, cudaStream_t stream,
-                             const KernelParams& p) {
-    if (threads <= 512) {
-        if (staged) pdhg_recentred<512, true><<<grid, threads, smem, stream>>>(p);
-        else pdhg_recentred<512, false><<<grid, threads, smem, stream>>>(p);
-    } else if (threads <= 768) {
-        if (staged) pdhg_recentred<768, true><<<grid, threads, smem, stream>>>(p);
-        else pdhg_recentred<768, false><<<grid, threads, smem, stream>>>(p);
+const void* recentred_symbol(int threads, bool staged, bool patched) {
+    if (threads <= 512) return recentred_for<512>(staged, patched);
+    if (threads <= 768) return recentred_for<768>(staged, patched);
+    return recentred_for<1024>(staged, patched);
+}
+
+template <int MAXT>
+static void launch_recentred_for(bool staged, bool patched, int grid, int threads, size_t smem,
+                                 cudaStream_t stream, const KernelParams& p) {
+    if (patched) {
+        if (staged) pdhg_recentred<MAXT, true, true><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<MAXT, false, true><<<grid, threads, smem, stream>>>(p);
     } else {
-        if (staged) pdhg_recentred<1024, true><<<grid, threads, smem, stream>>>(p);
-        else pdhg_recentred<1024, false><<<grid, threads, smem, stream>>>(p);
+        if (staged) pdhg_recentred<MAXT, true, false><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<MAXT, false, false><<<grid, threads, smem, stream>>>(p);
     }
+}
+
+cudaError_t launch_recentred(bool staged, bool patched, int grid, int threads, size_t smem, cudaStream_t stream,
+                             const KernelParams& p) {
+    if (threads <= 512) launch_recentred_for<512>(staged, patched, grid, threads, smem, stream, p);
+    else if (threads <= 768) launch_recentred_for<768>(staged, patched, grid, threads, smem, stream, p);
+    else launch_recentred_for<1024>(staged, patched, grid, threads, smem, stream, p);
     return cudaGetLastError();
 }
 
