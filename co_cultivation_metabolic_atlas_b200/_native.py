@@ -92,6 +92,10 @@ def load(path: os.PathLike | None = None):
         "fbalp_engine_set_iteration_hints": (ctypes.c_int, [vp, vp]),
         "fbalp_engine_set_patches": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, c_int32_p, c_int32_p]),
         "fbalp_engine_set_patch_values": (ctypes.c_int, [vp, vp, ctypes.c_int32]),
+        "fbalp_scaled_certificate": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                    vp, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp,
+                                                    vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int32, vp,
+                                                    vp, vp, vp, vp]),
         "fbalp_engine_solve": (ctypes.c_int, [vp, vp, vp, vp, ctypes.POINTER(SolveParams), vp, vp, vp, vp,
                                               vp, vp, vp]),
         "fbalp_engine_destroy": (ctypes.c_int, [vp]),

@@ -13,7 +13,7 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libfbalp.so"
 
-SOURCES = ["prepare.cpp", "engine.cu", "pdhg_kernel.cu", "mlp_kernels.cu", "noalloc.cu"]
+SOURCES = ["prepare.cpp", "engine.cu", "pdhg_kernel.cu", "mlp_kernels.cu", "noalloc.cu", "certify.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

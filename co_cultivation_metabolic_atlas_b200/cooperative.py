@@ -44,6 +44,7 @@ reference's gate.
 
 from __future__ import annotations
 
+import ctypes
 import warnings
 from dataclasses import dataclass, field
 
@@ -244,6 +245,37 @@ class _Template:
         self.prow = torch.as_tensor(patch[0], device=device)
         self.pcol = torch.as_tensor(patch[1], device=device)
         self.m, self.n = a.shape
+        # int32 CSR arrays for the fused certificate kernel
+        i32 = lambda v: torch.as_tensor(np.asarray(v, dtype=np.int32), device=device)  # noqa: E731
+        f64 = lambda v: torch.as_tensor(np.asarray(v, dtype=np.float64), device=device)  # noqa: E731
+        ca, ct = csr_matrix(a), csr_matrix(a).T.tocsr()
+        ca.sort_indices()
+        ct.sort_indices()
+        self.csr = (i32(ca.indptr), i32(ca.indices), f64(ca.data), i32(ct.indptr), i32(ct.indices), f64(ct.data))
+        self.prow32, self.pcol32 = i32(patch[0]), i32(patch[1])
+
+
+def fused_certificate(tpl: _Template, deltas, x, y, c, lower, upper, rhs, neq, row_group, col_group, table):
+    """``certificate`` in one launch of the native kernel
+    (``fbalp_scaled_certificate``): ``row_group`` / ``col_group`` int32
+    group indices into the per-environment scale ``table``."""
+    E = x.shape[0]
+    dev = x.device
+    out = torch.empty(3, E, dtype=torch.float64, device=dev)
+    lib = N.load()
+    p = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+    ap, ai, av, tp, ti, tv = tpl.csr
+    npatch = 0 if deltas is None else int(deltas.shape[1])
+    args = [x, y, c, lower, upper, rhs, table]
+    if any(not t.is_contiguous() for t in args) or (deltas is not None and not deltas.is_contiguous()):
+        raise ValueError("certificate inputs must be contiguous")
+    N.check(lib.fbalp_scaled_certificate(
+        E, tpl.m, tpl.n, int(neq), p(ap), p(ai), p(av), p(tp), p(ti), p(tv), npatch,
+        p(tpl.prow32) if npatch else None, p(tpl.pcol32) if npatch else None, p(deltas) if npatch else None,
+        p(x), p(y), p(c), p(lower), p(upper), p(rhs), p(row_group), p(col_group), int(table.shape[1]),
+        p(table), p(out[0]), p(out[1]), p(out[2]),
+        ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+    return out[0], out[1], out[2]
 
 
 def certificate(tpl: _Template, deltas, x, y, c, lower, upper, rhs, neq, row_scale, col_scale):
@@ -446,6 +478,11 @@ class CooperativeSolver:
             self.engine3 = LPEngine([(st.template3, st.neq)], options=self.options, device=self.device)
             self.engine3.set_patches(0, *st.patch3)
         self.asm = StageAssembly(st, self.device)
+        i32 = lambda v: torch.as_tensor(np.asarray(v, dtype=np.int32), device=self.device)  # noqa: E731
+        self._rg32 = {"max_min": i32(st.row_group1), "aggregate_objective": i32(st.row_group1),
+                      "parsimonious_exchange": i32(st.row_group3)}
+        self._cg32 = {"max_min": i32(st.col_group1), "aggregate_objective": i32(st.col_group1),
+                      "parsimonious_exchange": i32(st.col_group3)}
         self._tpl1 = _Template(st.template1, st.patch1, self.device)
         self._tpl3 = _Template(st.template3, st.patch3, self.device) if self.parsimonious else None
         self.warm_start = bool(warm_start)
@@ -493,8 +530,9 @@ class CooperativeSolver:
         n, m = cost.shape[1], rhs.shape[1]
         x = res.x[:E * n].view(E, n)
         y = res.y[:E * m].view(E, m)
-        primal, dual, gap = certificate(tpl, deltas, x, y, cost, lower, upper, rhs, self.structure.neq,
-                                        table[:, rg], table[:, cg])
+        primal, dual, gap = fused_certificate(tpl, deltas, x, y, cost.contiguous(), lower.contiguous(),
+                                              upper.contiguous(), rhs.contiguous(), self.structure.neq,
+                                              self._rg32[key], self._cg32[key], table.contiguous())
         ok = (res.status == N.STATUS_OPTIMAL) & (primal <= PRIMAL_GATE) & (dual <= DUAL_GATE) & (gap <= GAP_GATE)
         self._prev[key] = (x, y, res.omega, table, res.iterations)
         info = dict(status=res.status, iterations=res.iterations, primal=primal, dual=dual, gap=gap,

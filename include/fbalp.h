@@ -203,6 +203,31 @@ int fbalp_engine_set_patches(fbalp_engine* engine, int32_t species, int32_t coun
  * set_instances / set_patch_values. */
 int fbalp_engine_set_patch_values(fbalp_engine* engine, const double* values, int32_t stride);
 
+/* Certificate of the ORIGINAL LPs of a batch from solutions of their
+ * diagonally scaled copies, in one launch on `stream` (asynchronous).
+ * Instance i solved  A_i w (=,<=) b_i, l_i <= w <= u_i, min c_i.w  with
+ * A_i = A + sum_q deltas[i*npatch+q] e_{patch_rows[q]} e_{patch_cols[q]}^T
+ * (A: `rows` x `cols` DEVICE CSR a_ptr/a_idx/a_val with its transpose
+ * at_ptr/at_idx/at_val, rows [0, neq) equalities), and A_i = R A_orig D^-1,
+ * b_i = R b_orig, w = D v, c_i = D^-1 c_orig, where row r is scaled by
+ * scale_table[i*groups + row_group[r]] and column j by
+ * scale_table[i*groups + col_group[j]].  x, cost, lower, upper are DEVICE
+ * [count*cols], y and rhs [count*rows].  Writes per instance the original
+ * LP's primal residual, dual violation and relative KKT gap (the formulas of
+ * out_metrics, in the original units; NaN if any input is NaN) to DEVICE
+ * out_primal/out_dual/out_gap [count].  Indices must lie inside the matrix.
+ * Replaces certify_blocks_device (`src/gpu_block_lp.py:52-132`) applied to
+ * the cooperative stage LPs, whose coefficients the reference scales by the
+ * biomass (`src/community_solver.py:1084-1151, 116-204`). */
+int fbalp_scaled_certificate(int32_t count, int32_t rows, int32_t cols, int32_t neq, const int32_t* a_ptr,
+                             const int32_t* a_idx, const double* a_val, const int32_t* at_ptr,
+                             const int32_t* at_idx, const double* at_val, int32_t npatch,
+                             const int32_t* patch_rows, const int32_t* patch_cols, const double* deltas,
+                             const double* x, const double* y, const double* cost, const double* lower,
+                             const double* upper, const double* rhs, const int32_t* row_group,
+                             const int32_t* col_group, int32_t groups, const double* scale_table,
+                             double* out_primal, double* out_dual, double* out_gap, void* stream);
+
 /* Solve every bound instance.  Warm starts (`warm_x`, `warm_y`: flat DEVICE,
  * original units; `warm_omega`: per instance) may be NULL (cold start).
  * Outputs are DEVICE arrays: status[count], objective[count],

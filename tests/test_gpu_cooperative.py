@@ -148,3 +148,40 @@ def test_cooperative_rollout_full_size_community():
     assert torch.isfinite(com.biomass).all() and (com.biomass > 0).all()
     assert st.template1.shape[1] == st.n_fluxes + 1
     com.close()
+
+
+def test_fused_certificate_equals_the_tensor_certificate():
+    """The native batched certificate (``fbalp_scaled_certificate``, one
+    launch) equals the tensor-op restatement on random scaled LPs of the
+    stage-3 template (patched entries, free and infinite bounds, inequality
+    rows); a NaN makes its instance's three values NaN."""
+    models = syn.community_models(SMALL_SIZES, seed=0, n_medium=12, per_species=6)
+    st = co.CommunityStructure(co.synthetic_members(models), optimize_live_objectives=True)
+    dev = torch.device("cuda")
+    tpl = co._Template(st.template3, st.patch3, dev)
+    rng = np.random.default_rng(7)
+    E, n, m = 5, st.n3, st.m3
+    T = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev).contiguous()  # noqa: E731
+    x = T(rng.normal(0, 3, (E, n)))
+    y = T(rng.normal(0, 1, (E, m)))
+    y[:, st.neq:] = -y[:, st.neq:].abs()
+    y[:, st.neq + 3] = 0.5                      # a wrong-signed inequality dual
+    c = T(rng.normal(0, 1, (E, n)))
+    lo = T(rng.uniform(-5, 0, (E, n)))
+    up = T(rng.uniform(0, 5, (E, n)))
+    up[:, -st.n_aux:] = float("inf")
+    lo[:, :7] = -float("inf")
+    rhs = T(rng.normal(0, 1, (E, m)))
+    deltas = T(rng.normal(0, 0.3, (E, len(st.patch3[0]))))
+    table = T(rng.uniform(0.05, 2.0, (E, st.n_species + 3)))
+    rg = torch.as_tensor(st.row_group3, device=dev)
+    cg = torch.as_tensor(st.col_group3, device=dev)
+    want = co.certificate(tpl, deltas, x, y, c, lo, up, rhs, st.neq, table[:, rg], table[:, cg])
+    got = co.fused_certificate(tpl, deltas, x, y, c, lo, up, rhs, st.neq, rg.int(), cg.int(), table)
+    for w, g in zip(want, got):
+        np.testing.assert_allclose(g.cpu().numpy(), w.cpu().numpy(), rtol=1e-11, atol=1e-300)
+    x[2, 11] = float("nan")
+    got = co.fused_certificate(tpl, deltas, x, y, c, lo, up, rhs, st.neq, rg.int(), cg.int(), table)
+    for g in got:
+        v = g.cpu().numpy()
+        assert np.isnan(v[2]) and np.isfinite(v[[0, 1, 3, 4]]).all()
