@@ -354,6 +354,7 @@ class StageAssembly:
         self.var_stoich = t(st.var_stoich, torch.float64)
         self.growth_cols = t(st.growth_cols)
         self.objectives = [t(o, torch.float64) for o in st.objectives]
+        self._c1 = None
 
     def scales(self, biomass) -> Scales:
         X = biomass.clamp_min(BIOMASS_FLOOR)
@@ -368,6 +369,8 @@ class StageAssembly:
         """Cross-feeding relaxation of the exchange lower bounds
         (``_bounds`` ``:1010-1017``, Python scalar max: a NaN limit keeps the
         original bound)."""
+        if not len(self.st.relax_cols):
+            return lower
         lo = lower.clone()
         if len(self.st.relax_cols):
             limit = -abs(float(max_crossfeed_uptake))
@@ -388,19 +391,28 @@ class StageAssembly:
         rhs1 = torch.cat([torch.zeros(E, st.neq + st.n_species, **f64), supply / sc.xbar[:, None]], dim=1)
         l1 = torch.cat([lw, torch.zeros(E, 1, **f64)], dim=1)
         u1 = torch.cat([uw, torch.full((E, 1), float(growth_upper), **f64)], dim=1)
-        c1 = torch.zeros(E, st.n1, **f64)
-        c1[:, st.nu] = -1.0
+        c1 = self._stage1_cost(E, sc.xbar.device)
         d1 = (sc.rho - 1.0).contiguous()
         return lw, uw, l1, u1, c1, rhs1, d1
 
-    def stage2(self, sc: Scales, lw, uw, floor, nu_hi):
+    def _stage1_cost(self, E, device):
+        """The stage-1 cost (-1 on nu), the same for every call: built once
+        per batch size and shared (read-only)."""
+        c1 = self._c1
+        if c1 is None or c1.shape[0] != E or c1.device != torch.device(device):
+            c1 = torch.zeros(E, self.st.n1, dtype=torch.float64, device=device)
+            c1[:, self.st.nu] = -1.0
+            self._c1 = c1
+        return c1
+
+    def stage2(self, sc: Scales, lw, uw, floor, nu_hi, cost=True):
         """Bounds with ``nu`` in ``[floor, nu_hi]`` and the live-objective
-        cost (minimisation form, scaled)."""
+        cost (minimisation form, scaled; None unless ``cost``)."""
         E = sc.xbar.shape[0]
         f64 = dict(dtype=torch.float64, device=sc.xbar.device)
         l2 = torch.cat([lw, floor[:, None]], dim=1)
         u2 = torch.cat([uw, nu_hi[:, None]], dim=1)
-        c2 = torch.cat([-self.g[None, :] / sc.rho_col, torch.zeros(E, 1, **f64)], dim=1)
+        c2 = torch.cat([-self.g[None, :] / sc.rho_col, torch.zeros(E, 1, **f64)], dim=1) if cost else None
         return l2, u2, c2
 
     def aggregate(self, sc: Scales, x):
@@ -513,9 +525,8 @@ class CooperativeSolver:
         if prev is None or not self.warm_start:
             return None, None, None
         x, y, omega, old, _ = prev
-        cs_new, cs_old = table[:, cg], old[:, cg]
-        rs_new, rs_old = table[:, rg], old[:, rg]
-        return (x * (cs_new / cs_old)).reshape(-1), (y * (rs_old / rs_new)).reshape(-1), omega
+        ratio = table / old                       # per scale group, then one gather per vector
+        return (x * ratio[:, cg]).reshape(-1), (y / ratio[:, rg]).reshape(-1), omega
 
     def _run(self, engine, key, table, rg, cg, lower, upper, cost, rhs, deltas, tpl, warm=None):
         E = self.E
@@ -560,7 +571,8 @@ class CooperativeSolver:
         if lower.shape != (E, st.n_fluxes) or upper.shape != (E, st.n_fluxes):
             raise ValueError("flux bounds do not match the community")
         lo = asm.relaxed_lower(lower, max_crossfeed_uptake)
-        if bool(torch.isnan(lo).any()) or bool(torch.isnan(upper).any()) or bool((lo > upper).any()):
+        # one pass: false for lo > upper and for a NaN on either side
+        if not bool((lo <= upper).all()):
             raise ValueError("invalid flux bounds")
         if E != self.E:
             self._bind(E)
@@ -575,7 +587,7 @@ class CooperativeSolver:
         stage = torch.where(ok1, STAGE_MAX_MIN, STAGE_FAILED)
         chosen_x, chosen_y, chosen_r = x1, y1, r1
         nu_hi = coexistence if self.optimize_live_objectives else floor
-        l2, u2, c2 = asm.stage2(sc, lw, uw, floor, nu_hi)
+        l2, u2, c2 = asm.stage2(sc, lw, uw, floor, nu_hi, cost=self.optimize_live_objectives)
         if self.optimize_live_objectives:
             x2, y2, r2, ok2, stages["aggregate_objective"] = self._run(
                 self.engine1, "aggregate_objective", sc.table, asm.row_group1, asm.col_group1, l2, u2, c2, rhs1, d1,
@@ -667,10 +679,14 @@ class CooperativeCommunity:
         self.growth_cols = torch.as_tensor(st.growth_cols, device=dev)
         self.step_index = 0
         self.result: CooperativeResult | None = None
+        self._lower = None
 
     def live_bounds(self):
-        """Flux lower bounds after the Michaelis-Menten uptake update."""
-        lower = self.base_lower[None, :].repeat(self.E, 1)
+        """Flux lower bounds after the Michaelis-Menten uptake update (one
+        buffer: only the medium exchange columns change between steps)."""
+        if self._lower is None:
+            self._lower = self.base_lower[None, :].repeat(self.E, 1)
+        lower = self._lower
         total = self.biomass.clamp_min(1e-6).sum(dim=1, keepdim=True)
         for mm in self.mm:
             lower[:, mm["cols"]] = uptake_lower(self.medium[:, mm["ids"]], total, self.dt, mm)
