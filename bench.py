@@ -502,7 +502,7 @@ def coop_config(args, st, stages):
                         f"({', '.join(f'{m}x{n}' for m, n in syn.COMMUNITY_SIZES)}) + {st.n_medium_rows} shared "
                         f"medium rows: stage 1 {st.m1}x{st.n1}, stage 3 {st.m3}x{st.n3}; {stages} stage LPs/env-step, "
                         f"dt=0.05 h",
-            "envs_per_gpu": args.envs, "seed": args.seed,
+            "envs_per_gpu": args.envs, "seed": args.seed, "community_seed": syn.COOPERATIVE_SEED,
             "l2": "inputs larger than L2 (per-stage bounds of one step > 400 MB), no flush"}
 
 
@@ -546,7 +546,7 @@ def run_cooperative(args):
 
     ranks = Ranks("nccl")
     world, rank, local, dev = ranks.world, ranks.rank, ranks.local_rank, ranks.device
-    models = syn.community_models(seed=args.seed)
+    models = syn.community_models(seed=syn.COOPERATIVE_SEED)
     medium, biomass = syn.initial_environments(args.envs, seed=ranks.environment_seed(args.seed))
     cap = args.coop_growth_cap if args.coop_growth_cap > 0 else None
     stages = 2
@@ -583,7 +583,7 @@ def run_cooperative(args):
         com, ms_max, ok_envs, it, first_its = trajectory(True)
     st = com.solver.structure
     value = ranks.sum(ok_envs * stages) / (ms_max / 1e3)
-    state = (com.biomass.cpu().numpy(), com.medium[:, com.met_ids].cpu().numpy(),
+    state = (com.biomass.cpu().numpy(), com.shared_medium().cpu().numpy(),
              com.live_bounds().cpu().numpy(), com.upper.cpu().numpy())
     res = com.step()
     torch.cuda.synchronize()
@@ -633,7 +633,7 @@ def run_cooperative(args):
     K = args.e2e_steps if args.e2e_steps > 0 else min(args.steps, 3)
     rec = []
     for _ in range(K + 1):
-        rec.append(tuple(t.cpu().pin_memory() for t in (com.biomass, com.medium[:, com.met_ids].contiguous(),
+        rec.append(tuple(t.cpu().pin_memory() for t in (com.biomass, com.shared_medium(),
                                                         com.live_bounds())))
         com.step()
     up_h = com.upper.cpu().pin_memory()
@@ -688,14 +688,17 @@ def run_reference_cooperative(args):
     from co_cultivation_metabolic_atlas_b200 import cooperative as coop
     from co_cultivation_metabolic_atlas_b200 import synthetic as syn
     from oracle import dfba
-    models = syn.community_models(seed=args.seed)
+    models = syn.community_models(seed=syn.COOPERATIVE_SEED)
     members = coop.synthetic_members(models)
     st = coop.CommunityStructure(members)
     medium, biomass = syn.initial_environments(args.envs, seed=args.seed)
     lower = np.concatenate([dfba.uptake_lower_bounds(m, medium, biomass, 0.05) for m in models], axis=1)
     upper = np.repeat(np.concatenate([m.upper for m in models])[None], args.envs, 0)
-    ids = [int(name[1:3]) for name in st.metabolites]
-    state = (biomass, medium[:, ids], lower, upper)
+    shared = np.zeros((args.envs, len(st.metabolites)))
+    for k, name in enumerate(st.metabolites):
+        if int(name[1:4]) < coop.SECONDARY_OFFSET:
+            shared[:, k] = medium[:, int(name[1:4])]
+    state = (biomass, shared, lower, upper)
     cap = args.coop_growth_cap if args.coop_growth_cap > 0 else None
     rates, cores = [], None
     for k in range(args.warmup + args.steps):

@@ -478,7 +478,9 @@ class CooperativeSolver:
         if len(st.patch3[0] if self.parsimonious else st.patch1[0]) > N.MAX_PATCHES:
             raise ValueError(f"the cooperative LP needs more than {N.MAX_PATCHES} per-environment coefficients "
                              "(members + live-objective nonzeros)")
-        self.config = config or SolveConfig()
+        # stage LPs of coupled communities take up to a few 10^4 iterations
+        # cold (the parsimonious stage with binding shared pools)
+        self.config = config or SolveConfig(max_iterations=100_000, fp32_max_iterations=100_000)
         if self.config.precision != "mixed" or not self.config.recentre:
             raise ValueError("environment-dependent coefficients need the re-centred mixed schedule")
         self.device = torch.device(device) if device is not None else torch.device("cuda")
@@ -621,21 +623,35 @@ class CooperativeSolver:
                 e.close()
 
 
-def synthetic_members(models):
-    """Members of the synthetic community: each species' medium exchange
-    columns (stoichiometry -1, metabolite ``m{id:02d}_e``) are its
-    extracellular exchange terms, with their default lower bounds as the
-    original bounds; the growth reaction is the biomass column (coefficient
-    1) and the live objective maximises it.  The other exchange columns are
-    species-private boundary fluxes (no shared pool)."""
+SECONDARY_POOL = 60       # shared extracellular metabolites outside the medium
+SECONDARY_OFFSET = 100    # their ids: m100_e ... (medium ids stay below)
+
+
+def synthetic_members(models, *, secondary=SECONDARY_POOL, seed=0):
+    """Members of the synthetic community.  As in the reference, where every
+    exchange reaction of an extracellular metabolite joins that
+    metabolite's shared pool (``src/community_solver.py:775-790``), every
+    exchange column is an exchange term (stoichiometry -1): a medium column
+    exchanges its medium metabolite ``m{id:03d}_e``, every other exchange
+    column one of ``secondary`` shared metabolites ``m{100+k:03d}_e`` drawn
+    with a seeded generator.  The secondary metabolites are absent from the
+    medium (supply 0), so a member can take one up only as far as others
+    secrete it in the same step.  Original lower bounds are the default
+    ones; the growth reaction is the biomass column (coefficient 1) and the
+    live objective maximises it."""
+    rng = np.random.default_rng(seed + 4242)
     out = []
     for m in models:
-        cols = [int(c) for c in m.medium_columns]
+        medium = {int(c): int(i) for c, i in zip(m.medium_columns, m.medium_ids)}
+        others = [c for c in range(m.n_exchange) if c not in medium]
+        draw = rng.integers(0, secondary, len(others)) if secondary > 0 else np.empty(0, np.int64)
+        ids = dict(medium)
+        ids.update({c: SECONDARY_OFFSET + int(k) for c, k in zip(others, draw)})
+        cols = range(m.n_exchange) if secondary > 0 else sorted(medium)
         out.append(Member(
             name=m.name, S=m.S, growth=int(m.biomass), objective=-np.asarray(m.cost, dtype=np.float64),
-            direction="max",
-            exchanges=tuple((f"m{int(i):02d}_e", c, -1.0) for c, i in zip(cols, m.medium_ids)),
-            original_lower={c: float(m.lower[c]) for c in cols}))
+            direction="max", exchanges=tuple((f"m{ids[c]:03d}_e", int(c), -1.0) for c in cols),
+            original_lower={int(c): float(m.lower[c]) for c in cols}))
     return out
 
 
@@ -667,7 +683,11 @@ class CooperativeCommunity:
         self.base_lower = torch.as_tensor(np.concatenate([m.lower for m in models]), device=dev)
         self.upper = torch.as_tensor(np.concatenate([m.upper for m in models]), device=dev)[None, :].expand(
             self.E, -1).contiguous()
-        self.met_ids = torch.as_tensor([int(name[1:3]) for name in st.metabolites], device=dev)
+        # medium column of every shared metabolite (-1: not in the medium,
+        # supply 0)
+        ids = [int(name[1:4]) for name in st.metabolites]
+        self.met_ids = torch.as_tensor([i if i < SECONDARY_OFFSET else -1 for i in ids], device=dev)
+        self._in_medium = self.met_ids >= 0
         self.mm = []
         for s, m in enumerate(models):
             cols = st.col_start[s] + np.asarray(m.medium_columns, dtype=np.int64)
@@ -681,6 +701,13 @@ class CooperativeCommunity:
         self.result: CooperativeResult | None = None
         self._lower = None
 
+    def shared_medium(self):
+        """Concentrations of the shared metabolites (``structure.metabolites``
+        order); secondary metabolites are not in the medium."""
+        out = torch.zeros(self.E, len(self.solver.structure.metabolites), dtype=torch.float64, device=self.device)
+        out[:, self._in_medium] = self.medium[:, self.met_ids[self._in_medium]]
+        return out
+
     def live_bounds(self):
         """Flux lower bounds after the Michaelis-Menten uptake update (one
         buffer: only the medium exchange columns change between steps)."""
@@ -693,7 +720,7 @@ class CooperativeCommunity:
         return lower
 
     def step(self) -> CooperativeResult:
-        res = self.solver.solve(self.biomass, self.medium[:, self.met_ids], self.dt, self.live_bounds(), self.upper,
+        res = self.solver.solve(self.biomass, self.shared_medium(), self.dt, self.live_bounds(), self.upper,
                                 max_crossfeed_uptake=self.max_uptake_rate)
         self.integrate(res)
         self.result = res

@@ -525,18 +525,22 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     const bool patched = recentred && p.patch_values != nullptr;
     const void* k = recentred ? fbalp::recentred_symbol(threads, recentred == 1, patched)
                               : fbalp::kernel_symbol(fp64, threads, all_fast);
-    auto attr = std::find_if(e->smem_attr.begin(), e->smem_attr.end(),
-                             [&](const std::pair<const void*, int>& a) { return a.first == k; });
-    if (attr == e->smem_attr.end() || attr->second < dyn) {
+    // the dynamic shared-memory limit is a property of the kernel in this
+    // process (shared by every engine): raise it when this launch needs
+    // more, never lower it
+    cudaFuncAttributes fa{};
+    check(cudaFuncGetAttributes(&fa, k), "cudaFuncGetAttributes");
+    if (fa.maxDynamicSharedSizeBytes < dyn)
         check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
               "cudaFuncSetAttribute");
-        if (attr == e->smem_attr.end()) e->smem_attr.emplace_back(k, static_cast<int>(dyn));
-        else attr->second = static_cast<int>(dyn);
-    }
     int per_sm = 0;
     check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, dyn), "occupancy");
     if (e->opt.blocks_per_sm > 0) per_sm = std::min(per_sm, e->opt.blocks_per_sm);
-    if (per_sm < 1) throw CudaError("kernel does not fit on an SM with this configuration");
+    if (per_sm < 1)
+        throw CudaError("kernel does not fit on an SM with this configuration (threads " + std::to_string(threads) +
+                        ", dynamic shared memory " + std::to_string(dyn) + " B, static " +
+                        std::to_string(fa.sharedSizeBytes) + " B, registers " + std::to_string(fa.numRegs) +
+                        ", opt-in limit " + std::to_string(e->smem_optin) + " B)");
     const int grid = static_cast<int>(std::min<int64_t>(e->count, static_cast<int64_t>(per_sm) * e->sm_count));
     p.layouts = static_cast<const fbalp::Layout*>(dl.ptr);
     if (slab > 0) {

@@ -106,7 +106,6 @@ struct fbalp_engine {
     // copy, so it can be captured in a CUDA graph
     Buffer layout_dev[4];
     std::vector<fbalp::Layout> layout_host[4];
-    std::vector<std::pair<const void*, int>> smem_attr;  // kernel -> dynamic smem set
     std::vector<fbalp::Layout> layouts32, layouts64;
     int last_grid[2] = {0, 0};
     int64_t last_smem[2] = {0, 0};

@@ -141,8 +141,13 @@ extern "C" int fbalp_engine_solve_noalloc(fbalp_engine* e, int64_t count, const 
 
     try {
         const void* k = fbalp::kernel_symbol(true, threads, staged);
-        check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
-              "cudaFuncSetAttribute");
+        // the kernel's dynamic shared-memory limit is shared with every
+        // engine in the process: raise it if needed, never lower it
+        cudaFuncAttributes fa{};
+        check(cudaFuncGetAttributes(&fa, k), "cudaFuncGetAttributes");
+        if (fa.maxDynamicSharedSizeBytes < dyn)
+            check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)),
+                  "cudaFuncSetAttribute");
         int per_sm = 0;
         check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, dyn), "occupancy");
         if (e->opt.blocks_per_sm > 0) per_sm = std::min(per_sm, e->opt.blocks_per_sm);

@@ -31,6 +31,7 @@ def main():
     models = syn.community_models()
     if args.cooperative:
         from .cooperative import CooperativeCommunity
+        models = syn.community_models(seed=syn.COOPERATIVE_SEED)
         medium, biomass = syn.initial_environments(args.envs)
         com = CooperativeCommunity(models, medium, biomass)
         for k in range(args.steps):

@@ -117,6 +117,11 @@ def single_species_workload(count: int = 256, *, m: int = 1200, n: int = 2600, s
 
 
 COMMUNITY_SIZES = ((950, 1800), (1400, 2700), (1100, 2200))
+# Seed of the full-size community used for the cooperative (max-min growth)
+# LP: the lowest seed whose three members can all grow at default bounds
+# (seed 0's first member cannot, which pins the max-min growth at 0 and
+# makes every cooperative LP's optimum the zero flux).
+COOPERATIVE_SEED = 11
 LARGE_SIZES = ((3000, 6000), (2500, 5200), (3400, 6800))
 MEDIUM_SIZE = 40
 MEDIUM_PER_SPECIES = 25

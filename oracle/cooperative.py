@@ -254,3 +254,33 @@ def stage_problems(blocks, growth_terms, exchange_terms, objective, lower, upper
                                     np.concatenate([lo2, np.zeros(n_aux)]),
                                     np.concatenate([up2, np.full(n_aux, np.inf)]), c3, neq)
     return out
+
+
+def synthetic_terms(models, secondary=60, seed=0):
+    """The cooperative LP data of the synthetic community, restated: every
+    exchange column is an exchange term (stoichiometry -1) -- a medium column
+    of its medium metabolite ``m{id:03d}_e``, every other exchange column of
+    one of ``secondary`` shared metabolites ``m{100+k:03d}_e`` (seeded
+    draws, generator ``default_rng(seed + 4242)``, in species then column
+    order), absent from the medium; original bounds = the default lower
+    bounds; the growth reaction is the biomass column (coefficient 1); the
+    objective maximises biomass.  Returns ``(blocks, growth_terms,
+    exchange_terms, objective, original_lower, col_start)``."""
+    rng = np.random.default_rng(seed + 4242)
+    col_start = np.concatenate([[0], np.cumsum([m.S.shape[1] for m in models])]).astype(int)
+    growth, exchange, orig, obj = [], {}, {}, []
+    for s, m in enumerate(models):
+        growth.append((s, int(col_start[s] + m.biomass), 1.0))
+        medium = {int(c): int(i) for c, i in zip(m.medium_columns, m.medium_ids)}
+        others = [c for c in range(m.n_exchange) if c not in medium]
+        draw = rng.integers(0, secondary, len(others))
+        ids = dict(medium)
+        for c, k in zip(others, draw):
+            ids[c] = 100 + int(k)
+        for c in range(m.n_exchange):
+            gcol = int(col_start[s] + c)
+            exchange.setdefault(f"m{ids[c]:03d}_e", []).append((s, gcol, -1.0))
+            if m.lower[c] < 0:
+                orig[gcol] = float(m.lower[c])
+        obj.append(-np.asarray(m.cost, dtype=float))
+    return [m.S for m in models], growth, exchange, np.concatenate(obj), orig, col_start

@@ -15,6 +15,11 @@ from tests.test_cooperative import SMALL_SIZES, crossfeeding_members, oracle_arg
 
 pytestmark = pytest.mark.gpu
 
+# the small community seed whose three members can all grow (uptake-limited
+# optima 5.3, 19.4, 3.9 at default bounds), so that the max-min growth and
+# the exchanges are not trivially zero
+GROWING_SMALL_SEED = 17
+
 
 def reference_solution(solver, key, i, optimize, aggregate):
     """Environment i's last solution of stage ``key`` in the reference's
@@ -99,7 +104,7 @@ def test_crossfeeding_community_on_gpu():
 
 @pytest.mark.parametrize("optimize", [False, True])
 def test_synthetic_community_stages_match_oracle(optimize):
-    models = syn.community_models(SMALL_SIZES, seed=0, n_medium=12, per_species=6)
+    models = syn.community_models(SMALL_SIZES, seed=GROWING_SMALL_SEED, n_medium=12, per_species=6)
     members = co.synthetic_members(models)
     gmax = None if optimize else 0.005
     solver = co.CooperativeSolver(members, optimize_live_objectives=optimize, maximum_coexistence_growth=gmax)
@@ -128,14 +133,14 @@ def test_synthetic_community_stages_match_oracle(optimize):
 def test_cooperative_rollout_full_size_community():
     """Three steps of the cooperative dFBA on the full-size synthetic
     community (one 6,701-column joint LP per environment and stage)."""
-    models = syn.community_models()
+    models = syn.community_models(seed=syn.COOPERATIVE_SEED)
     medium, biomass = syn.initial_environments(16)
     com = co.CooperativeCommunity(models, medium, biomass, dt=0.05)
     st = com.solver.structure
     members = com.solver.structure.members
     for step in range(3):
         X = com.biomass.cpu().numpy()
-        C = com.medium[:, com.met_ids].cpu().numpy()
+        C = com.shared_medium().cpu().numpy()
         lower = com.live_bounds()
         lo = lower.cpu().numpy()
         up = com.upper.cpu().numpy()
@@ -185,3 +190,47 @@ def test_fused_certificate_equals_the_tensor_certificate():
     for g in got:
         v = g.cpu().numpy()
         assert np.isnan(v[2]) and np.isfinite(v[[0, 1, 3, 4]]).all()
+
+
+@pytest.mark.parametrize("cap", [0.005, None])
+def test_cooperative_rollout_lockstep_with_oracle(cap):
+    """Twenty cooperative dFBA steps of the small community (4 environments):
+    at every step the oracle solves each environment from the GPU's current
+    state with HiGHS (the reference's exact-CPU stage sequence); the
+    stage-1 optimum, the stage-3 optimum of the GPU fluxes and the biomass
+    Euler update must agree."""
+    from oracle import dfba as odfba
+    models = syn.community_models(SMALL_SIZES, seed=GROWING_SMALL_SEED, n_medium=12, per_species=6)
+    medium, biomass = syn.initial_environments(4, n_medium=12)
+    com = co.CooperativeCommunity(models, medium, biomass, maximum_coexistence_growth=cap)
+    st = com.solver.structure
+    blocks, growth, exchange, obj, orig, col_start = oc.synthetic_terms(models)
+    assert sorted(exchange) == st.metabolites
+    upper = np.concatenate([m.upper for m in models])
+    for step in range(20):
+        X = com.biomass.cpu().numpy()
+        C = com.medium.cpu().numpy()
+        res = com.step()
+        torch.cuda.synchronize()
+        assert bool(res.ok.all()), step
+        flux = res.fluxes.cpu().numpy()
+        mu_gpu = flux[:, st.growth_cols]
+        lower = np.concatenate([odfba.uptake_lower_bounds(m, C, X, com.dt) for m in models], axis=1)
+        for e in range(4):
+            med = {f"m{i:03d}_e": C[e, i] for i in range(C.shape[1])}
+            sol = oc.solve(blocks, growth, exchange, obj, lower[e], upper, dict(enumerate(X[e])), med, com.dt,
+                           original_lower=orig, maximum_coexistence_growth=cap)
+            assert sol.status == "optimal"
+            nu = float(res.coexistence[e])
+            assert nu == pytest.approx(sol.coexistence, rel=1e-6, abs=1e-9), (step, e)
+            # the GPU fluxes are optimal for the oracle's stage-3 LP
+            probs = oc.stage_problems(blocks, growth, exchange, obj, lower[e], upper, dict(enumerate(X[e])), med,
+                                      com.dt, coexistence=nu, original_lower=orig, maximum_coexistence_growth=cap)
+            a3, b3, l3, u3, c3, neq = probs["parsimonious_exchange"]
+            n = st.n_fluxes
+            t = np.abs(a3[neq + st.n_species + len(st.metabolites)::2, :n] @ flux[e])
+            mine = float(t.sum())
+            assert mine == pytest.approx(sol.stages["parsimonious_exchange"].fun, rel=1e-6, abs=1e-7), (step, e)
+        want = odfba.update_biomass(X, mu_gpu, com.dt)
+        np.testing.assert_allclose(com.biomass.cpu().numpy(), want, rtol=1e-12)
+    com.close()
