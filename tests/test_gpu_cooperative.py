@@ -234,3 +234,57 @@ def test_cooperative_rollout_lockstep_with_oracle(cap):
         want = odfba.update_biomass(X, mu_gpu, com.dt)
         np.testing.assert_allclose(com.biomass.cpu().numpy(), want, rtol=1e-12)
     com.close()
+
+
+def test_reference_style_callers_through_the_bridge():
+    """The reference's exact-backend cooperative stage sequence, written as
+    per-environment code calling ``backend.solve(objective, **linprog
+    kwargs)`` with the reference's own assembly (oracle restatement), for
+    four states of the reference's cross-feeding pair, run through
+    ``BatchingBridge`` onto ``B200LPBackend``: one batched GPU solve per
+    stage round, optima equal to HiGHS."""
+    from scipy.sparse import block_diag, csr_matrix, hstack
+
+    from co_cultivation_metabolic_atlas_b200 import B200LPBackend
+    from co_cultivation_metabolic_atlas_b200.bridge import BatchingBridge
+    members, lower, upper = crossfeeding_members()
+    st, blocks, growth, exchange, orig = oracle_args(members)
+    obj = st.global_objective
+    biomass = np.array([[1.0, 1.0], [1.0, 0.7], [0.23, 1.9], [0.5, 0.05]])
+    media = [{"carbon_e": 10.0, "factor_e": 0.0}, {"carbon_e": 10.0, "factor_e": 0.0},
+             {"carbon_e": 2.0, "factor_e": 0.4}, {"carbon_e": 5.0, "factor_e": 1.0}]
+    a_flux = block_diag([csr_matrix(b) for b in blocks], format="csr")
+    n = a_flux.shape[1]
+    a_eq = hstack([a_flux, csr_matrix((a_flux.shape[0], 1))], format="csr")
+    ex_cols = [i for terms in exchange.values() for _, i, _ in terms]
+
+    def environment(e):
+        def run(backend):
+            bio = dict(enumerate(biomass[e]))
+            lo, up = oc.relaxed_bounds(lower, upper, ex_cols, orig, 20.0)
+            a_ub, b_ub = oc.community_inequalities(n, growth, exchange, bio, media[e], 0.2)
+            bounds = [(float(a), float(b)) for a, b in zip(lo, up)] + [(0.0, 10.0)]
+            c1 = np.zeros(n + 1)
+            c1[-1] = -1.0
+            s1 = backend.solve(c1, A_ub=a_ub, b_ub=b_ub, A_eq=a_eq, b_eq=np.zeros(a_eq.shape[0]), bounds=bounds,
+                               method="highs")
+            assert s1.success, s1.message
+            nu = max(0.0, float(s1.x[-1]))
+            bounds[-1] = (nu * 0.99, nu * 0.99)
+            c3, a3, b3, e3 = oc.parsimonious_lp(a_ub, b_ub, a_eq, n, exchange, bio, obj, 0.0, False, 0.99)
+            s3 = backend.solve(c3, A_ub=a3, b_ub=b3, A_eq=e3, b_eq=np.zeros(e3.shape[0]),
+                               bounds=bounds + [(0.0, None)] * (len(c3) - n - 1), method="highs")
+            assert s3.success, s3.message
+            return nu, float(s3.fun)
+        return run
+
+    parent = B200LPBackend(mode="cold", iterations=100_000, fp32_iterations=100_000)
+    bridge = BatchingBridge(parent)
+    res = bridge.run({e: environment(e) for e in range(4)})
+    parent.close()
+    assert bridge.rounds == [4, 4]
+    for e, (nu, fun3) in res.items():
+        sol = oc.solve(blocks, growth, exchange, obj, lower, upper, dict(enumerate(biomass[e])), media[e], 0.2,
+                       original_lower=orig)
+        assert nu == pytest.approx(sol.coexistence, rel=1e-6, abs=1e-9)
+        assert fun3 == pytest.approx(sol.stages["parsimonious_exchange"].fun, rel=1e-5, abs=1e-7)
