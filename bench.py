@@ -236,12 +236,14 @@ def run_product(args):
         data = tw.build_dataset(models, envs=args.envs, steps=args.learn_steps,
                                 seeds=ranks.training_seeds(args.seed, args.learn_seeds),
                                 config=cfg, device=dev, log=lambda *_: None)
-        ws, losses = tw.fit(models, data, epochs=args.learn_epochs, device=dev, log=lambda *_: None)
+        # data-parallel over the ranks' own rollouts (one network for the job)
+        ws, losses = tw.fit(models, data, epochs=args.learn_epochs, device=dev, log=lambda *_: None, ranks=ranks)
         torch.cuda.synchronize()
         learned_info = {"training_pairs": int(data.F.shape[0]), "final_train_mse_standardised": losses[-1],
                         "train_seconds": time.perf_counter() - t0,
                         "model": "MLP 44 -> 4 x 512 GELU -> x,y of 3 species, BF16 tcgen05 kernels; seeds an "
-                                 "environment's first solve, the temporal base seeds the later ones"}
+                                 "environment's first solve, the temporal base seeds the later ones",
+                        "training": f"data-parallel over {world} rank(s)"}
         del data
 
     def trajectory(warm, learned=None):

@@ -49,15 +49,20 @@ def build_dataset(models, *, envs, steps, seeds, config=None, device=None, log=p
 
 
 def fit(models, data: Rollouts, *, epochs=20, batch=4096, lr=1e-3, lr_final=5e-5, seed=0, device=None,
-        log=print):
+        log=print, ranks=None):
     """Train the network (state -> solution) on standardised targets;
-    returns the warm start and the per-epoch losses."""
+    returns the warm start and the per-epoch losses.  With ``ranks`` of a
+    multi-GPU job the training is data-parallel over every rank's rollouts
+    (global standardisation, gradients averaged each step; the same
+    network on every rank)."""
+    from .distributed import min_int
     omega = data.omega.median(dim=0).values
-    codec = Codec.fit(data.F, data.T, omega)
+    codec = Codec.fit(data.F, data.T, omega, ranks=ranks)
     width = data.T.shape[1]
     net = MLP([N_FEATURES, *HIDDEN, width], device=device, seed=seed)
     losses = train(net, codec.features(data.F), codec.targets(data.T), epochs=epochs,
-                   batch=min(batch, data.F.shape[0]), lr=lr, lr_final=lr_final, seed=seed, log=log)
+                   batch=min_int(min(batch, data.F.shape[0]), ranks), lr=lr, lr_final=lr_final, seed=seed,
+                   log=log, ranks=ranks)
     return LearnedWarmStart(net, codec, models), losses
 
 

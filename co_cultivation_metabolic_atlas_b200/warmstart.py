@@ -237,12 +237,16 @@ class Codec:
     omega: torch.Tensor      # per species median primal weight
 
     @staticmethod
-    def fit(F, T, omegas):
-        f_mean = F.mean(0)
-        f_std = F.std(0).clamp_min(1e-3)
-        t_mean = T.mean(0)
-        t_std = T.std(0).clamp_min(1e-6)
-        return Codec(f_mean, f_std, t_mean, t_std, omegas)
+    def fit(F, T, omegas, ranks=None):
+        """Standardisation of the rows of ``F`` / ``T``; with ``ranks`` (a
+        data-parallel job) over every rank's rows, and the primal weights
+        averaged over the ranks."""
+        from .distributed import allreduce_mean_, global_moments
+        f_mean, f_std = global_moments(F, ranks)
+        t_mean, t_std = global_moments(T, ranks)
+        omegas = omegas.clone()
+        allreduce_mean_([omegas], ranks)
+        return Codec(f_mean, f_std.clamp_min(1e-3), t_mean, t_std.clamp_min(1e-6), omegas)
 
     def features(self, F):
         return (F - self.f_mean) / self.f_std
@@ -362,21 +366,25 @@ class LearnedWarmStart:
         return bx, by, com.prev.omega
 
 
-def train(mlp: MLP, F, T, *, epochs=20, batch=4096, lr=1e-3, lr_final=1e-4, seed=0, log=None):
-    """Full-batch-shuffled Adam on the MSE of standardised targets."""
+def train(mlp: MLP, F, T, *, epochs=20, batch=4096, lr=1e-3, lr_final=1e-4, seed=0, log=None, ranks=None):
+    """Full-batch-shuffled Adam on the MSE of standardised targets.  With
+    ``ranks`` (data-parallel): every rank takes the same number of steps on
+    its own rows and applies the gradient averaged over the ranks."""
+    from .distributed import allreduce_mean_, min_int
     ops = mlp.ops
     n = F.shape[0]
     width = T.shape[1]
     gen = torch.Generator(device="cpu").manual_seed(seed)
     losses = []
-    steps_total = epochs * max(1, n // batch)
+    per_epoch = min_int(max(1, n // batch), ranks)
+    steps_total = epochs * per_epoch
     step = 0
     loss_acc = torch.zeros(1, dtype=torch.float64, device=mlp.device)
     for ep in range(epochs):
         perm = torch.randperm(n, generator=gen).to(mlp.device)
         loss_acc.zero_()
         count = 0
-        for i in range(0, n - batch + 1, batch):
+        for i in range(0, per_epoch * batch, batch):
             idx = perm[i:i + batch]
             X = F[idx]
             Y = mlp.forward(X, keep=True)
@@ -386,12 +394,16 @@ def train(mlp: MLP, F, T, *, epochs=20, batch=4096, lr=1e-3, lr_final=1e-4, seed
             dY16 = torch.empty(Y.shape, dtype=BF16, device=mlp.device)
             ops.mse_grad(Y, Tp, 2.0 / (batch * width), dY32=dY, dY16=dY16, loss=loss_acc)
             gW, gb = mlp.backward(dY, dY16)
+            allreduce_mean_(gW + gb, ranks)
             frac = step / max(1, steps_total - 1)
             cur = lr * (lr_final / lr) ** frac
             mlp.adam_step(gW, gb, cur)
             step += 1
             count += batch * width
-        losses.append(float(loss_acc.item()) / max(1, count))
+        if ranks is not None and ranks.world > 1:
+            losses.append(ranks.sum(float(loss_acc.item())) / ranks.sum(float(count)))
+        else:
+            losses.append(float(loss_acc.item()) / max(1, count))
         if log:
             log(f"epoch {ep}: mse {losses[-1]:.4e}")
     if ops.error_flag():
