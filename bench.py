@@ -555,8 +555,7 @@ def run_cooperative(args):
 
     def trajectory(warm):
         com = coop.CooperativeCommunity(models, medium, biomass, dt=0.05, device=dev,
-                                        maximum_coexistence_growth=cap)
-        com.solver.warm_start = warm
+                                        maximum_coexistence_growth=cap, warm_start="extrapolate" if warm else False)
         warm_its = []
         for _ in range(args.warmup):
             r = com.step()
@@ -675,7 +674,8 @@ def run_cooperative(args):
                 "first_step_mean_iterations": (None if first_its is None else
                                                {"max_min": float(first_its[0].mean()),
                                                 "parsimonious_exchange": float(first_its[1].mean())}),
-                "warm_start": "previous step's stage solutions rescaled to the new biomass",
+                "warm_start": "first-order extrapolation of the last two steps' stage solutions (reference "
+                              "units), rescaled to the new biomass",
                 "cold": cold, "warm_vs_cold": value / cold["value"] if cold["value"] else None,
                 "roofline": roofline, "cpu_baseline": cpu, "highs_check": check, "e2e": e2e,
                 "gpu_launches": stages * args.steps, "clocks": clocks.summary()}

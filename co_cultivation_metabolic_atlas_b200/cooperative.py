@@ -459,13 +459,16 @@ class CooperativeSolver:
     stage's solution must meet the engine's tolerances and pass the
     reference's certificate on the unscaled LP, otherwise the environment
     reports no solution (the exact-backend rule of ``:1747-1749, 1794-1796``,
-    no CPU fallback).  Solutions of the previous call warm-start the next
-    one (rescaled to the new biomass)."""
+    no CPU fallback).  Calls warm-start from the previous ones: ``warm_start
+    = "extrapolate"`` (default) from the first-order extrapolation of the
+    last two solutions, ``"previous"`` from the last one, both in the
+    reference's units and rescaled to the new biomass; ``False`` solves
+    cold."""
 
     def __init__(self, members, *, coexistence_fraction=0.99, objective_fraction=0.99,
                  maximum_coexistence_growth=None, optimize_live_objectives=False, parsimonious_exchange=True,
                  config: SolveConfig | None = None, options: EngineOptions | None = None, device=None,
-                 warm_start=True):
+                 warm_start="extrapolate"):
         if not torch.cuda.is_available():
             raise RuntimeError("a CUDA device is required (no CPU fallback)")
         self.structure = st = CommunityStructure(members, optimize_live_objectives=optimize_live_objectives)
@@ -499,7 +502,12 @@ class CooperativeSolver:
                       "parsimonious_exchange": i32(st.col_group3)}
         self._tpl1 = _Template(st.template1, st.patch1, self.device)
         self._tpl3 = _Template(st.template3, st.patch3, self.device) if self.parsimonious else None
-        self.warm_start = bool(warm_start)
+        if warm_start is True:
+            warm_start = "previous"
+        if warm_start not in (False, None, "previous", "extrapolate"):
+            raise ValueError("warm_start must be False, 'previous' or 'extrapolate'")
+        self.warm_start = warm_start or False
+        self._prev2 = {}
         self.E = 0
         self._prev = {}
 
@@ -515,10 +523,12 @@ class CooperativeSolver:
             z3 = torch.zeros(E * st.n3, **f64)
             self.engine3.set_instances(sid, z3, z3, z3, torch.zeros(E * st.m3, **f64))
         self._prev = {}
+        self._prev2 = {}
 
     def reset(self):
         """Forget the warm-start history."""
         self._prev = {}
+        self._prev2 = {}
 
     def _warm(self, key, table, rg, cg):
         """The previous call's solution of stage ``key`` rescaled to the
@@ -527,8 +537,17 @@ class CooperativeSolver:
         if prev is None or not self.warm_start:
             return None, None, None
         x, y, omega, old, _ = prev
-        ratio = table / old                       # per scale group, then one gather per vector
-        return (x * ratio[:, cg]).reshape(-1), (y / ratio[:, rg]).reshape(-1), omega
+        prev2 = self._prev2.get(key) if self.warm_start == "extrapolate" else None
+        if prev2 is None:
+            ratio = table / old                   # per scale group, then one gather per vector
+            return (x * ratio[:, cg]).reshape(-1), (y / ratio[:, rg]).reshape(-1), omega
+        # first-order extrapolation of the last two solutions in the
+        # reference's units (v = w / D, y_v = R y_w), mapped to the current
+        # scaling; the kernel projects onto the bounds and y_ub <= 0
+        x2, y2, _, old2, _ = prev2
+        xv = 2.0 * x / old[:, cg] - x2 / old2[:, cg]
+        yv = 2.0 * y * old[:, rg] - y2 * old2[:, rg]
+        return (xv * table[:, cg]).reshape(-1), (yv / table[:, rg]).reshape(-1), omega
 
     def _run(self, engine, key, table, rg, cg, lower, upper, cost, rhs, deltas, tpl, warm=None):
         E = self.E
@@ -547,6 +566,8 @@ class CooperativeSolver:
                                               upper.contiguous(), rhs.contiguous(), self.structure.neq,
                                               self._rg32[key], self._cg32[key], table.contiguous())
         ok = (res.status == N.STATUS_OPTIMAL) & (primal <= PRIMAL_GATE) & (dual <= DUAL_GATE) & (gap <= GAP_GATE)
+        if key in self._prev:
+            self._prev2[key] = self._prev[key]
         self._prev[key] = (x, y, res.omega, table, res.iterations)
         info = dict(status=res.status, iterations=res.iterations, primal=primal, dual=dual, gap=gap,
                     certified=ok)
@@ -666,7 +687,8 @@ class CooperativeCommunity:
 
     def __init__(self, models, medium, biomass, *, dt=0.05, capacity=CARRYING_CAPACITY, max_uptake_rate=20.0,
                  maximum_coexistence_growth=0.005, optimize_live_objectives=False, parsimonious_exchange=True,
-                 config: SolveConfig | None = None, options: EngineOptions | None = None, device=None):
+                 config: SolveConfig | None = None, options: EngineOptions | None = None, device=None,
+                 warm_start="extrapolate"):
         self.device = dev = torch.device(device) if device is not None else torch.device("cuda")
         self.models = models
         self.dt = float(dt)
@@ -675,7 +697,7 @@ class CooperativeCommunity:
         self.solver = CooperativeSolver(
             synthetic_members(models), maximum_coexistence_growth=maximum_coexistence_growth,
             optimize_live_objectives=optimize_live_objectives, parsimonious_exchange=parsimonious_exchange,
-            config=config, options=options, device=dev)
+            config=config, options=options, device=dev, warm_start=warm_start)
         st = self.solver.structure
         self.medium = torch.as_tensor(medium, dtype=torch.float64, device=dev).clone()
         self.biomass = torch.as_tensor(biomass, dtype=torch.float64, device=dev).clone()
