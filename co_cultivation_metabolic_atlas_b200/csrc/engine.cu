@@ -374,15 +374,21 @@ int fbalp_engine_set_patches(fbalp_engine* e, int32_t species, int32_t count, co
     std::vector<int32_t> row_new(sh.m), col_new(sh.n);
     for (int32_t i = 0; i < sh.m; ++i) row_new[sh.row_perm[i]] = i;
     for (int32_t j = 0; j < sh.n; ++j) col_new[sh.col_perm[j]] = j;
-    for (int32_t q = 0; q < count; ++q)
+    for (int32_t q = 0; q < count; ++q) {
         if (rows[q] < 0 || rows[q] >= sh.m || cols[q] < 0 || cols[q] >= sh.n)
             return fail(FBALP_ERR_INVALID, "patched entry outside the species matrix");
+        for (int32_t p = 0; p < q; ++p)
+            if (rows[p] == rows[q] && cols[p] == cols[q])
+                return fail(FBALP_ERR_INVALID, "a patched entry is declared twice");
+    }
     fbalp::DevSpecies& d = e->dev_species_host[species];
     d.npatch = count;
     for (int q = 0; q < fbalp::kMaxPatches; ++q) {
         d.patch_row[q] = d.patch_col[q] = 0;
         d.patch_scale[q] = 0.0;
+        d.patch_base[q] = 0.0;
     }
+    d.patch_col_f2 = 0.0;
     for (auto& v : sh.alist) v.w = 0;
     for (auto& v : sh.atlist) v.w = 0;
     for (int32_t q = 0; q < count; ++q) {
@@ -394,6 +400,30 @@ int fbalp_engine_set_patches(fbalp_engine* e, int32_t species, int32_t count, co
             if (v.x == r / 32) v.w = 1;
         for (auto& v : sh.atlist)
             if (v.x == c / 32) v.w = 1;
+    }
+    // scaled template values of the patched columns (row c of A~^T in the
+    // SELL slices): each patched entry's base value, and the sum of squares
+    // of the columns' other entries, for the per-instance step bound
+    // ||A_i~||^2 <= ||A~||^2 + ||A_i~[:, patched columns]||_F^2
+    std::vector<int32_t> cols_done;
+    for (int32_t q = 0; q < count; ++q) {
+        const int32_t c = d.patch_col[q];
+        const bool first = std::find(cols_done.begin(), cols_done.end(), c) == cols_done.end();
+        if (first) cols_done.push_back(c);
+        const int32_t sl = c / 32, lane = c % 32;
+        for (int32_t k = 0; k < sh.AT.length[sl]; ++k) {
+            const int32_t e2 = sh.AT.off[sl] + k * 32 + lane;
+            const int32_t r = sh.AT.idx[e2];
+            const double v = sh.AT.val[e2];
+            if (r >= sh.m || v == 0.0) continue;  // padding
+            bool patched = false;
+            for (int32_t p = 0; p < count; ++p)
+                if (d.patch_col[p] == c && d.patch_row[p] == r) {
+                    patched = true;
+                    if (p == q) d.patch_base[q] = v;
+                }
+            if (first && !patched) d.patch_col_f2 += v * v;
+        }
     }
     try {
         check(cudaMemcpy(sh.d_alist, sh.alist.data(), sh.alist.size() * sizeof(int4), cudaMemcpyHostToDevice),

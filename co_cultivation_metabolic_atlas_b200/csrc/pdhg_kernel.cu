@@ -1303,12 +1303,18 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         }
 
         // step size: the shared matrix's, shrunk so that it stays below
-        // 1/||A~ + patches|| (||A~|| + ||deltas||_F bounds the latter)
+        // 1/||A~ + patches||, bounded by the smaller of ||A~|| + ||deltas||_F
+        // and sqrt(||A~||^2 + ||patched columns of this instance||_F^2)
         double eta = sp->eta;
         if (PATCHED && npatch) {
-            double f2 = 0.0;
-            for (int q = 0; q < npatch; ++q) f2 += s_pv64[q] * s_pv64[q];
-            eta *= sp->sigma_max / (sp->sigma_max + sqrt(f2));
+            double f2 = 0.0, c2 = sp->patch_col_f2;
+            for (int q = 0; q < npatch; ++q) {
+                f2 += s_pv64[q] * s_pv64[q];
+                const double v = sp->patch_base[q] + s_pv64[q];
+                c2 += v * v;
+            }
+            const double s = sp->sigma_max;
+            eta *= s / fmin(s + sqrt(f2), sqrt(s * s + c2));
         }
         int status = -1;
         int cur = 0;   // buffer holding the base

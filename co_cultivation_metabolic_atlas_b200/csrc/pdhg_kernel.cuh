@@ -83,6 +83,8 @@ struct DevSpecies {
     int32_t patch_row[kMaxPatches];
     int32_t patch_col[kMaxPatches];
     double patch_scale[kMaxPatches];
+    double patch_base[kMaxPatches];  // scaled template value at each patched entry
+    double patch_col_f2;             // sum of squares of the patched columns' other entries (scaled)
     double sigma_max;             // ||A~||_2 estimate of the shared matrix
 };
 
