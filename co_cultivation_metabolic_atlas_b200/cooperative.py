@@ -468,7 +468,7 @@ class CooperativeSolver:
     def __init__(self, members, *, coexistence_fraction=0.99, objective_fraction=0.99,
                  maximum_coexistence_growth=None, optimize_live_objectives=False, parsimonious_exchange=True,
                  config: SolveConfig | None = None, options: EngineOptions | None = None, device=None,
-                 warm_start="extrapolate"):
+                 warm_start="extrapolate", retry_iterations=400_000):
         if not torch.cuda.is_available():
             raise RuntimeError("a CUDA device is required (no CPU fallback)")
         self.structure = st = CommunityStructure(members, optimize_live_objectives=optimize_live_objectives)
@@ -508,6 +508,12 @@ class CooperativeSolver:
             raise ValueError("warm_start must be False, 'previous' or 'extrapolate'")
         self.warm_start = warm_start or False
         self._prev2 = {}
+        # environments stopped by the iteration cap get one more pass of
+        # this many iterations, alone (0: no second pass)
+        self.retry_iterations = int(retry_iterations)
+        self._retry_engines = {}
+        self.retries: dict = {}        # stage -> environments retried so far
+        self.last_retried: dict = {}   # stage -> environments retried by the last call
         self.E = 0
         self._prev = {}
 
@@ -566,12 +572,53 @@ class CooperativeSolver:
                                               upper.contiguous(), rhs.contiguous(), self.structure.neq,
                                               self._rg32[key], self._cg32[key], table.contiguous())
         ok = (res.status == N.STATUS_OPTIMAL) & (primal <= PRIMAL_GATE) & (dual <= DUAL_GATE) & (gap <= GAP_GATE)
+        if self.retry_iterations > 0:
+            self._retry_laggards(key, res, x, y, ok, primal, dual, gap, table, lower, upper, cost, rhs, deltas, tpl)
         if key in self._prev:
             self._prev2[key] = self._prev[key]
         self._prev[key] = (x, y, res.omega, table, res.iterations)
         info = dict(status=res.status, iterations=res.iterations, primal=primal, dual=dual, gap=gap,
                     certified=ok)
         return x, y, res, ok, info
+
+    def _retry_laggards(self, key, res, x, y, ok, primal, dual, gap, table, lower, upper, cost, rhs, deltas, tpl):
+        """Environments whose stage stopped at the iteration cap continue,
+        alone, from their own iterates with ``retry_iterations`` more; their
+        results (and certificate) replace the first pass's in place."""
+        lag = (~ok) & (res.status == N.STATUS_ITERATION_LIMIT)
+        idx = lag.nonzero().flatten()
+        if idx.numel() == 0:
+            return
+        st = self.structure
+        eng = self._retry_engines.get(key)
+        if eng is None:
+            stage3 = key == "parsimonious_exchange"
+            eng = LPEngine([(st.template3 if stage3 else st.template1, st.neq)], options=self.options,
+                           device=self.device)
+            eng.set_patches(0, *(st.patch3 if stage3 else st.patch1))
+            self._retry_engines[key] = eng
+        k = int(idx.numel())
+        sub = lambda t: t[idx].contiguous()  # noqa: E731
+        lo, up, c, b, d, tb = (sub(t) for t in (lower, upper, cost, rhs, deltas, table))
+        eng.set_instances(np.zeros(k, np.int32), lo.reshape(-1), up.reshape(-1), c.reshape(-1), b.reshape(-1))
+        eng.set_patch_values(d)
+        cfg = SolveConfig(**{**self.config.__dict__, "max_iterations": self.retry_iterations,
+                             "fp32_max_iterations": self.retry_iterations})
+        r2 = eng.solve(warm_x=sub(x).reshape(-1), warm_y=sub(y).reshape(-1), warm_omega=res.omega[idx].contiguous(),
+                       config=cfg)
+        n, m = x.shape[1], y.shape[1]
+        x2, y2 = r2.x[:k * n].view(k, n), r2.y[:k * m].view(k, m)
+        p2, d2, g2 = fused_certificate(tpl, d, x2, y2, c, lo, up, b, st.neq, self._rg32[key], self._cg32[key], tb)
+        ok2 = (r2.status == N.STATUS_OPTIMAL) & (p2 <= PRIMAL_GATE) & (d2 <= DUAL_GATE) & (g2 <= GAP_GATE)
+        x[idx], y[idx] = x2, y2
+        res.status[idx] = r2.status
+        res.iterations[idx] = res.iterations[idx] + r2.iterations
+        res.omega[idx] = r2.omega
+        res.metrics[idx] = r2.metrics
+        primal[idx], dual[idx], gap[idx] = p2, d2, g2
+        ok[idx] = ok2
+        self.retries[key] = self.retries.get(key, 0) + k
+        self.last_retried[key] = idx.tolist()
 
     # -- solve -----------------------------------------------------------------
     def solve(self, biomass, medium, dt, lower, upper, *, max_crossfeed_uptake=20.0) -> CooperativeResult:
@@ -582,6 +629,7 @@ class CooperativeSolver:
         n_fluxes) live flux bounds of all members (member order);
         ``max_crossfeed_uptake`` as the reference's ``solve``."""
         st, dev, asm = self.structure, self.device, self.asm
+        self.last_retried = {}
         if dt <= 0:
             raise ValueError("dt must be positive")
         biomass = torch.as_tensor(biomass, dtype=torch.float64, device=dev)
@@ -639,7 +687,7 @@ class CooperativeSolver:
                                  aggregate=aggregate, objective_values=asm.objective_values(fluxes), stages=stages)
 
     def close(self):
-        for e in (self.engine1, self.engine3):
+        for e in (self.engine1, self.engine3, *self._retry_engines.values()):
             if e is not None:
                 e.close()
 

@@ -288,3 +288,36 @@ def test_reference_style_callers_through_the_bridge():
                        original_lower=orig)
         assert nu == pytest.approx(sol.coexistence, rel=1e-6, abs=1e-9)
         assert fun3 == pytest.approx(sol.stages["parsimonious_exchange"].fun, rel=1e-5, abs=1e-7)
+
+
+def test_stalled_environments_finish_in_a_second_pass():
+    """In the binding regime (small community, growth cap lifted) a few of
+    1,024 stage-3 LPs stop at the first pass's iteration cap; they continue
+    alone from their iterates and certify, with the optima of HiGHS."""
+    from oracle import dfba as odfba
+    models = syn.community_models(SMALL_SIZES, seed=GROWING_SMALL_SEED, n_medium=12, per_species=6)
+    medium, biomass = syn.initial_environments(1024, n_medium=12)
+    com = co.CooperativeCommunity(models, medium, biomass, maximum_coexistence_growth=None)
+    X = com.biomass.cpu().numpy()
+    res = com.step()
+    torch.cuda.synchronize()
+    retried = com.solver.last_retried.get("parsimonious_exchange", [])
+    assert bool(res.ok.all()), (int(res.ok.sum()), retried)
+    assert retried, "no environment needed the second pass in this sample"
+    st = com.solver.structure
+    blocks, growth, exchange, obj, orig, _ = oc.synthetic_terms(models)
+    upper = np.concatenate([m.upper for m in models])
+    Cm = medium                          # the state the step started from
+    lower = np.concatenate([odfba.uptake_lower_bounds(m, Cm, X, com.dt) for m in models], axis=1)
+    flux = res.fluxes.cpu().numpy()
+    for e in retried[:3]:
+        med = {f"m{i:03d}_e": Cm[e, i] for i in range(Cm.shape[1])}
+        sol = oc.solve(blocks, growth, exchange, obj, lower[e], upper, dict(enumerate(X[e])), med, com.dt,
+                       original_lower=orig)
+        assert sol.status == "optimal"
+        probs = oc.stage_problems(blocks, growth, exchange, obj, lower[e], upper, dict(enumerate(X[e])), med, com.dt,
+                                  coexistence=float(res.coexistence[e]), original_lower=orig)
+        a3, _, _, _, _, neq = probs["parsimonious_exchange"]
+        t = np.abs(a3[neq + st.n_species + len(st.metabolites)::2, :st.n_fluxes] @ flux[e])
+        assert float(t.sum()) == pytest.approx(sol.stages["parsimonious_exchange"].fun, rel=1e-5, abs=1e-7)
+    com.close()
