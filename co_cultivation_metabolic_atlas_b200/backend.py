@@ -30,6 +30,11 @@ equality block), the reduced LPs are solved on the GPU, and the primal is
 expanded and the duals lifted back; the row is accepted only when the
 original-LP certificate passes on the lifted pair.
 
+Requests stopped by the iteration cap get one more GPU pass, alone, from
+their own iterates, of up to ``retry_iterations`` (default 400,000; 0
+disables) iterations; cold genome-scale LPs need 10^5 iterations, far above
+the first pass's budget.  A row is still accepted only on its certificate.
+
 With ``split_rows=L`` (off by default) rows longer than ``L`` (the hub
 metabolites of genome-scale models hold up to ~1,200 reactions) are split
 exactly into segments with auxiliary variables (``rowsplit.py``) before the
@@ -68,7 +73,7 @@ class B200LPBackend:
     def __init__(self, *, mode='previous', precision='mixed', iterations=20000,
                  fp32_iterations=20000, check_interval=64, stage=None,
                  options: EngineOptions | None = None, warm_start_model=None, device=None,
-                 equality_reduction=False, split_rows=None):
+                 equality_reduction=False, split_rows=None, retry_iterations=400_000):
         if mode not in ('cold', 'previous', 'mlp'):
             raise ValueError('Unknown warm-start mode')
         if mode == 'mlp' and warm_start_model is None:
@@ -98,6 +103,10 @@ class B200LPBackend:
             raise ValueError('split_rows must be None or an integer >= 2')
         self.split_rows = None if split_rows is None else int(split_rows)
         self._split_plans: dict = {}
+        if isinstance(retry_iterations, (bool, np.bool_)) or not isinstance(retry_iterations, (int, np.integer)) \
+                or retry_iterations < 0:
+            raise ValueError('retry_iterations must be a non-negative integer')
+        self.retry_iterations = int(retry_iterations)
         self._plans: dict = {}
         self._keys: list[str] = []
         self._matrices = []
@@ -189,6 +198,7 @@ class B200LPBackend:
         metrics = res.metrics.cpu().numpy()
         x = res.x.cpu().numpy()
         y = res.y.cpu().numpy()
+        retried = self._retry(eng, res, species, co, ro, lower, upper, cost, rhs, tr, status, iters, metrics, x, y, t)
         solved = time.perf_counter()
         rows = []
         certified = {}
@@ -240,12 +250,37 @@ class B200LPBackend:
             self.model.commit(ids)
         self.history.append(dict(stage=self.stage, mode=self.mode, batch=len(ids), environment_ids=ids,
                                  accepted=sum(r.success for r in rows), cpu_lp_calls=0,
-                                 engine_rebuilt=rebuilt, iterations=iters.tolist(),
+                                 engine_rebuilt=rebuilt, iterations=iters.tolist(), retried=retried,
                                  host_preparation_seconds=prep - started,
                                  solve_seconds=solved - prep,
                                  total_seconds=time.perf_counter() - started,
                                  rows=[r.diagnostics for r in rows]))
         return rows
+
+    def _retry(self, eng, res, species, co, ro, lower, upper, cost, rhs, tr, status, iters, metrics, x, y, t):
+        """Requests stopped by the iteration cap continue on the GPU, alone,
+        from their own iterates for up to ``retry_iterations`` more; their
+        results replace the first pass's (host arrays, in place).  Returns
+        the retried request indices."""
+        lag = np.flatnonzero(status == N.STATUS_ITERATION_LIMIT)
+        if self.retry_iterations == 0 or lag.size == 0:
+            return []
+        cols = [np.arange(co[i], co[i] + eng.shapes[species[i]][1]) for i in lag]
+        rows = [np.arange(ro[i], ro[i] + eng.shapes[species[i]][0]) for i in lag]
+        ci, ri = np.concatenate(cols), np.concatenate(rows) if tr else np.empty(0, np.int64)
+        eng.set_instances(species[lag], t(lower[ci]), t(upper[ci]), t(cost[ci]), t(rhs[ri]) if tr else None)
+        cfg = SolveConfig(**{**self.config.__dict__, 'max_iterations': self.retry_iterations,
+                             'fp32_max_iterations': self.retry_iterations})
+        r2 = eng.solve(warm_x=res.x[torch.as_tensor(ci, device=res.x.device)],
+                       warm_y=res.y[torch.as_tensor(ri, device=res.y.device)] if tr else None,
+                       warm_omega=res.omega[torch.as_tensor(lag, device=res.omega.device)], config=cfg)
+        status[lag] = r2.status.cpu().numpy()
+        iters[lag] += r2.iterations.cpu().numpy()
+        metrics[lag] = r2.metrics.cpu().numpy()
+        x[ci] = r2.x.cpu().numpy()[:ci.size]
+        if tr:
+            y[ri] = r2.y.cpu().numpy()[:ri.size]
+        return lag.tolist()
 
     def _splits(self, problems):
         """The long-row split plan of every request's matrix (built once per

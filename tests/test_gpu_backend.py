@@ -73,11 +73,17 @@ def test_invalid_requests_fail_before_any_state_change():
 def test_unsolved_rows_fail_closed():
     from co_cultivation_metabolic_atlas_b200 import B200LPBackend
     model, lower, upper = syn.single_species_workload(2, m=120, n=260)
-    be = B200LPBackend(mode="cold", precision="fp64", iterations=64, fp32_iterations=0)
+    be = B200LPBackend(mode="cold", precision="fp64", iterations=64, fp32_iterations=0, retry_iterations=0)
     rows = be.solve_batch(requests_for(model, lower, upper))
     assert not any(r.success for r in rows)
     assert all(r.x is None and r.fun is None for r in rows)
     assert "no CPU fallback" in rows[0].message
+    be.close()
+    # by default the rows stopped by the cap continue in a second GPU pass
+    be = B200LPBackend(mode="cold", precision="fp64", iterations=64, fp32_iterations=0)
+    rows = be.solve_batch(requests_for(model, lower, upper))
+    assert all(r.success for r in rows)
+    assert be.history[-1]["retried"] == [0, 1] and be.history[-1]["cpu_lp_calls"] == 0
     be.close()
 
 
