@@ -572,8 +572,9 @@ class CooperativeSolver:
                                               upper.contiguous(), rhs.contiguous(), self.structure.neq,
                                               self._rg32[key], self._cg32[key], table.contiguous())
         ok = (res.status == N.STATUS_OPTIMAL) & (primal <= PRIMAL_GATE) & (dual <= DUAL_GATE) & (gap <= GAP_GATE)
-        if self.retry_iterations > 0:
-            self._retry_laggards(key, res, x, y, ok, primal, dual, gap, table, lower, upper, cost, rhs, deltas, tpl)
+        # what a second pass for this stage's laggards needs (run by solve()
+        # for the last stage, after the only host synchronisation of a call)
+        self._last_run = (key, res, x, y, ok, primal, dual, gap, table, lower, upper, cost, rhs, deltas, tpl)
         if key in self._prev:
             self._prev2[key] = self._prev[key]
         self._prev[key] = (x, y, res.omega, table, res.iterations)
@@ -681,6 +682,25 @@ class CooperativeSolver:
             ok = ok & ok3
             stage = torch.where(ok, STAGE_PARSIMONIOUS, STAGE_FAILED)
             final_x = x3
+        if self.retry_iterations > 0:
+            # the last stage's laggards continue in a second pass, which
+            # updates that stage's solution and flags in place; this is the
+            # only host synchronisation of a call (laggards of an earlier
+            # stage, not observed, fail closed)
+            self._retry_laggards(*self._last_run)
+            self._last_run = None
+            ok = ok1
+            if self.optimize_live_objectives:
+                ok = ok & ok2
+            if self.parsimonious:
+                ok = ok & ok3
+                stage = torch.where(ok, STAGE_PARSIMONIOUS, STAGE_FAILED)
+            elif self.optimize_live_objectives:
+                stage = torch.where(ok, STAGE_AGGREGATE, STAGE_FAILED)
+                aggregate = asm.aggregate(sc, chosen_x)
+            else:
+                stage = torch.where(ok, STAGE_MAX_MIN, STAGE_FAILED)
+                coexistence = torch.where(ok1, x1[:, st.nu].clamp_min(0.0), torch.zeros_like(sc.xbar))
         fluxes = asm.fluxes(sc, final_x)
         fluxes = torch.where(ok[:, None], fluxes, torch.full_like(fluxes, float("nan")))
         return CooperativeResult(ok=ok, stage=stage, fluxes=fluxes, nu=final_x[:, st.nu], coexistence=coexistence,
