@@ -100,3 +100,93 @@ def test_sbml_fixtures_load_and_certify():
         problem, x, y = lp_trace.load_trace_lp(SBML_DIR, e)
         key, variant = e["filename"][:-4].rsplit("_", 1)
         assert float(problem[4] @ x) == pytest.approx(meta[key]["highs_objective"][variant], rel=1e-12)
+
+
+FBC2 = """<?xml version="1.0" encoding="UTF-8"?>
+<sbml xmlns="http://www.sbml.org/sbml/level3/version1/core"
+      xmlns:fbc="http://www.sbml.org/sbml/level3/version1/fbc/version2" level="3" version="1" fbc:required="false">
+  <model id="toy" name="toy model" fbc:strict="true">
+    <listOfCompartments>
+      <compartment id="C_c" name="cytosol" constant="true"/>
+      <compartment id="C_x" name="extracellular space" constant="true"/>
+    </listOfCompartments>
+    <listOfSpecies>
+      <species id="M_a_c" compartment="C_c" boundaryCondition="false" hasOnlySubstanceUnits="false" constant="false"/>
+      <species id="M_a_x" compartment="C_x" boundaryCondition="false" hasOnlySubstanceUnits="false" constant="false"/>
+      <species id="M_b_c" compartment="C_c" boundaryCondition="false" hasOnlySubstanceUnits="false" constant="false"/>
+      <species id="M_src" compartment="C_x" boundaryCondition="true" hasOnlySubstanceUnits="false" constant="false"/>
+    </listOfSpecies>
+    <listOfParameters>
+      <parameter id="lo" value="-INF" constant="true"/>
+      <parameter id="up" value="INF" constant="true"/>
+      <parameter id="zero" value="0" constant="true"/>
+      <parameter id="ten" value="10" constant="true"/>
+    </listOfParameters>
+    <listOfReactions>
+      <reaction id="R_EX_a" reversible="true" fbc:lowerFluxBound="lo" fbc:upperFluxBound="ten">
+        <listOfReactants><speciesReference species="M_a_x" stoichiometry="1" constant="true"/></listOfReactants>
+      </reaction>
+      <reaction id="R_T_a" reversible="false" fbc:lowerFluxBound="zero" fbc:upperFluxBound="up">
+        <listOfReactants><speciesReference species="M_a_x" stoichiometry="1" constant="true"/></listOfReactants>
+        <listOfProducts><speciesReference species="M_a_c" stoichiometry="1" constant="true"/></listOfProducts>
+      </reaction>
+      <reaction id="R_CONV" reversible="true">
+        <listOfReactants><speciesReference species="M_a_c" stoichiometry="2" constant="true"/>
+                         <speciesReference species="M_src" stoichiometry="1" constant="true"/></listOfReactants>
+        <listOfProducts><speciesReference species="M_b_c" stoichiometry="1" constant="true"/>
+                        <speciesReference species="M_a_c" stoichiometry="0.5" constant="true"/></listOfProducts>
+      </reaction>
+      <reaction id="R_SINK_b" reversible="false">
+        <listOfReactants><speciesReference species="M_b_c" stoichiometry="1" constant="true"/></listOfReactants>
+      </reaction>
+    </listOfReactions>
+    <fbc:listOfObjectives fbc:activeObjective="o2">
+      <fbc:objective fbc:id="o1" fbc:type="maximize">
+        <fbc:listOfFluxObjectives><fbc:fluxObjective fbc:reaction="R_SINK_b" fbc:coefficient="1"/></fbc:listOfFluxObjectives>
+      </fbc:objective>
+      <fbc:objective fbc:id="o2" fbc:type="minimize">
+        <fbc:listOfFluxObjectives><fbc:fluxObjective fbc:reaction="R_T_a" fbc:coefficient="2"/></fbc:listOfFluxObjectives>
+      </fbc:objective>
+    </fbc:listOfObjectives>
+  </model>
+</sbml>
+"""
+
+
+def test_reader_format_rules(tmp_path):
+    """COBRA's id rules (one R_ / M_ prefix removed, compartments kept),
+    boundary species without rows, accumulated stoichiometry of a species on
+    both sides, INF bounds, default bounds by reversibility, the active
+    (minimised) objective, and the external compartment found by name."""
+    path = tmp_path / "toy.xml"
+    path.write_text(FBC2)
+    m = sbml.read_sbml(path)
+    assert m.id == "toy" and m.reactions == ["EX_a", "T_a", "CONV", "SINK_b"]
+    assert m.metabolites == ["a_c", "a_x", "b_c"] and m.compartments == ["C_c", "C_x", "C_c"]
+    A = m.S.toarray()
+    np.testing.assert_array_equal(A[:, 2], [-1.5, 0.0, 1.0])       # a_c: -2 + 0.5; M_src dropped
+    np.testing.assert_array_equal(A[:, 0], [0.0, -1.0, 0.0])
+    assert m.lower.tolist() == [-np.inf, 0.0, -1000.0, 0.0]
+    assert m.upper.tolist() == [10.0, np.inf, 1000.0, 1000.0]
+    assert m.direction == "min" and m.objective.tolist() == [0.0, 2.0, 0.0, 0.0]
+    np.testing.assert_array_equal(m.fba_cost(), m.objective)
+    assert m.external_compartment == "C_x" and m.exchanges.tolist() == [0]
+    assert m.exchange_metabolite(0) == "a_x"
+
+
+def test_reader_fbc_version_1_bounds(tmp_path):
+    """FBC version 1 keeps flux bounds in a listOfFluxBounds."""
+    text = FBC2.replace("fbc/version2", "fbc/version1")
+    for name in ("lo", "up", "zero", "ten"):
+        text = text.replace(f' fbc:lowerFluxBound="{name}"', "").replace(f' fbc:upperFluxBound="{name}"', "")
+    text = text.replace("    <fbc:listOfObjectives", """    <fbc:listOfFluxBounds>
+      <fbc:fluxBound fbc:reaction="R_EX_a" fbc:operation="greaterEqual" fbc:value="-5"/>
+      <fbc:fluxBound fbc:reaction="R_EX_a" fbc:operation="lessEqual" fbc:value="7"/>
+      <fbc:fluxBound fbc:reaction="R_CONV" fbc:operation="equal" fbc:value="2"/>
+    </fbc:listOfFluxBounds>
+    <fbc:listOfObjectives""")
+    path = tmp_path / "toy1.xml"
+    path.write_text(text)
+    m = sbml.read_sbml(path)
+    assert m.lower.tolist() == [-5.0, 0.0, 2.0, 0.0]
+    assert m.upper.tolist() == [7.0, 1000.0, 2.0, 1000.0]
