@@ -106,3 +106,23 @@ def test_engine_entry_points_reject_null_handles(native_built):
     assert lib.fbalp_engine_create(0, None, None, None, None, None, None, None, None,
                                    ctypes.byref(out)) == N.FBALP_ERR_INVALID
     assert out.value is None
+
+
+def test_scaled_certificate_rejects_invalid_arguments(native_built):
+    """Argument checks of the batched certificate run on the host before any
+    device call (a zero-instance call with valid arguments is a no-op)."""
+    from co_cultivation_metabolic_atlas_b200 import _native as N
+    lib = N.load()
+    fake = ctypes.c_void_p(16)        # never dereferenced: every call below returns on the host
+
+    def call(count=0, rows=2, cols=3, neq=1, npatch=0, groups=1, prow=fake, pcol=fake, x=fake):
+        return lib.fbalp_scaled_certificate(count, rows, cols, neq, fake, fake, fake, fake, fake, fake,
+                                            npatch, prow, pcol, None, x, fake, fake, fake, fake, fake,
+                                            fake, fake, groups, fake, fake, fake, fake, None)
+
+    assert call() == N.FBALP_OK
+    for kwargs, match in [({"neq": 3}, "dimensions"), ({"cols": 0}, "dimensions"), ({"groups": 0}, "dimensions"),
+                          ({"count": -1}, "dimensions"), ({"npatch": N.MAX_PATCHES + 1}, "npatch"),
+                          ({"npatch": 1, "prow": None}, "npatch"), ({"x": None}, "NULL")]:
+        assert call(**kwargs) == N.FBALP_ERR_INVALID, kwargs
+        assert match in lib.fbalp_last_error().decode(), kwargs
