@@ -42,6 +42,61 @@ def test_gemm_matches_fp32_reference(M, N, K, tA, tB):
     torch.testing.assert_close(C, ref, rtol=1e-4, atol=1e-4 * K ** 0.5)
 
 
+@pytest.mark.parametrize("M,N,K,tA,tB", [
+    (264, 136, 72, False, False),     # TMA-fed kernel: ragged tiles, every operand storage
+    (264, 136, 72, True, False),
+    (264, 136, 72, False, True),
+    (264, 136, 72, True, True),
+    (520, 264, 4096, True, True),     # weight-gradient shape: 64 k-tiles through the stage ring
+    (4096, 1024, 512, False, False),  # many tiles, two CTAs per SM
+])
+def test_tma_gemm_matches_fp32_reference(M, N, K, tA, tB):
+    """Operands on 16-byte boundaries with row strides of multiples of 8
+    elements take the TMA-fed kernel (K-major or MN-major tiles)."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(M + 3 * N + K)
+    A = (torch.randn(K, M, generator=g) if tA else torch.randn(M, K, generator=g)).cuda().bfloat16()
+    B = (torch.randn(K, N, generator=g) if tB else torch.randn(N, K, generator=g)).cuda().bfloat16()
+    C = torch.empty(M, N, device="cuda")
+    o = ops()
+    o.gemm(A, B, M, N, K, transA=tA, transB=tB, out32=C)
+    torch.cuda.synchronize()
+    assert o.error_flag() == 0
+    torch.testing.assert_close(C, ref_gemm(A, B, tA, tB), rtol=1e-4, atol=1e-4 * K ** 0.5)
+
+
+@pytest.mark.parametrize("pad", [0, 3])
+def test_both_gemm_kernels_agree_and_accumulate(pad):
+    """The same product through the TMA-fed kernel (aligned operands) and
+    the register-staged one (operands shifted off the 16-byte boundary),
+    accumulated into an FP32 output with an aligned or odd row stride."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(11 + pad)
+    M, N, K = 200, 144, 136
+    A = torch.randn(M, K, generator=g).cuda().bfloat16()
+    B = torch.randn(N, K, generator=g).cuda().bfloat16()
+    shifted = []
+    for X in (A, B):
+        buf = torch.zeros(X.numel() + 8, dtype=torch.bfloat16, device="cuda")
+        buf[1:1 + X.numel()] = X.reshape(-1)
+        shifted.append(buf[1:1 + X.numel()].view(X.shape))
+    assert shifted[0].data_ptr() % 16 != 0
+    o = ops()
+    base = torch.randn(M, N + pad, generator=g).cuda()
+    outs = []
+    for a, b in ((A, B), tuple(shifted)):
+        C = base.clone()
+        o.gemm(a, b, M, N, K, out32=C, accumulate=True)
+        outs.append(C)
+    torch.cuda.synchronize()
+    assert o.error_flag() == 0
+    ref = base.clone()
+    ref[:, :N] += ref_gemm(A, B, False, False)
+    for C in outs:
+        torch.testing.assert_close(C, ref, rtol=1e-4, atol=1e-4 * K ** 0.5)
+    torch.testing.assert_close(outs[0], outs[1], rtol=1e-5, atol=1e-5)
+
+
 def test_gemm_bias_gelu_epilogue_and_bf16_output():
     import torch
     from co_cultivation_metabolic_atlas_b200.warmstart import EPI_BIAS_GELU
