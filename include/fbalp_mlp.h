@@ -33,7 +33,9 @@ extern "C" {
  * (transB = 0) or B[k*ldb + n] (transB = 1).  A, B are BF16; the FP32
  * accumulator lives in tensor memory (tcgen05.mma kind::f16).  Results go to
  * C32 (FP32; added to its contents when accumulate_c = 1) and/or C16 (BF16),
- * row stride ldc.  Replaces torch.nn.Linear forward/backward in
+ * row stride ldc.  Operands that start on a 16-byte boundary with a row
+ * stride (lda, ldb) of a multiple of 8 elements are read by TMA; any other
+ * operand is staged by ordinary loads (same results, slower).  Replaces torch.nn.Linear forward/backward in
  * `src/temporal_lp_model.py:58-142`. */
 int fbalp_gemm_bf16(int M, int N, int K, const void* A, int lda, int transA, const void* B, int ldb,
                     int transB, const float* bias, int epilogue, float alpha, float* C32, void* C16,
