@@ -574,6 +574,16 @@ bool encode_operand(CUtensorMap* map, const void* X, int ld, int trans, int R, i
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The dynamic shared-memory limit of a kernel is an attribute of the
+// current device's context: query it on every call (a host-side read) and
+// raise it when this launch needs more, never lower it.
+bool allow_dynamic_smem(const void* kernel, int bytes) {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return false;
+    if (fa.maxDynamicSharedSizeBytes >= bytes) return true;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+}
+
 }  // namespace
 
 extern "C" int fbalp_gemm_bf16(int M, int N, int K, const void* A, int lda, int transA, const void* B,
@@ -587,25 +597,14 @@ extern "C" int fbalp_gemm_bf16(int M, int N, int K, const void* A, int lda, int 
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
     CUtensorMap mapA, mapB;
     if (encode_operand(&mapA, A, lda, transA, M, K) && encode_operand(&mapB, B, ldb, transB, N, K)) {
-        static bool attr_tma = false;
-        if (!attr_tma) {
-            if (cudaFuncSetAttribute(gemm_tcgen05_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmem) !=
-                cudaSuccess)
-                return FBALP_MLP_ERR_CUDA;
-            attr_tma = true;
-        }
+        if (!allow_dynamic_smem(reinterpret_cast<const void*>(gemm_tcgen05_tma), kTmaSmem)) return FBALP_MLP_ERR_CUDA;
         gemm_tcgen05_tma<<<grid, kThreads, kTmaSmem, static_cast<cudaStream_t>(stream)>>>(
             mapA, mapB, M, N, K, transA, transB, bias, epilogue, alpha, C32, static_cast<__nv_bfloat16*>(C16), ldc,
             Z, ldz > 0 ? ldz : ldc, accumulate_c);
         return cudaGetLastError() == cudaSuccess ? FBALP_MLP_OK : FBALP_MLP_ERR_CUDA;
     }
     const int smem = kStages * kStageBytes + 1024;
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(gemm_tcgen05, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-            return FBALP_MLP_ERR_CUDA;
-        attr = true;
-    }
+    if (!allow_dynamic_smem(reinterpret_cast<const void*>(gemm_tcgen05), smem)) return FBALP_MLP_ERR_CUDA;
     gemm_tcgen05<<<grid, kThreads, smem, static_cast<cudaStream_t>(stream)>>>(
         M, N, K, static_cast<const __nv_bfloat16*>(A), lda, transA, static_cast<const __nv_bfloat16*>(B), ldb,
         transB, bias, epilogue, alpha, C32, static_cast<__nv_bfloat16*>(C16), ldc, Z, ldz > 0 ? ldz : ldc,
