@@ -4,7 +4,13 @@ launch per precision phase, then the Euler update), warm start vs cold.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
 
-Prints one JSON line (rank 0).  See DESIGN.md for the roofline model.
+Prints one JSON line (rank 0).  Roofline model of the dominant kernel
+(the re-centred PDHG phase), a design that streams everything from HBM:
+w (3 n + 3 m + 2 n_medium) bytes per instance-iteration (w = 4 bytes per
+FP32 value) plus, per species and iteration of its longest instance, the
+matrix and its transpose, 2 (nnz (w + 4) + 4 (m + 1)) bytes; their sum over
+the phase's launch divided by its CUDA-event time, against the measured
+copy bandwidth.
 """
 
 from __future__ import annotations
