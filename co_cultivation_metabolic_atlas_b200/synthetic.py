@@ -2,7 +2,7 @@
 
 The reference project solves FBA LPs built from curated genome-scale models
 (``src/dfba_simulator.py:1061-1102`` builds ``max c.v s.t. S v = 0,
-l <= v <= u`` from a COBRA model).  Those models are not part of this build;
+l <= v <= u`` from a COBRA model).  Those models do not ship with this package;
 the workloads below are seeded synthetic stand-ins with the shapes and value
 distributions of the batched-LP benchmark:
 

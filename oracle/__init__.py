@@ -2,7 +2,7 @@
 
 Nothing in the product package imports this directory.  Only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference legs
-use it, and only as the checker (or as the timed CPU reference), never as a
+use it, and only to check results (or as the timed CPU reference), never as a
 solver behind the product API.
 
 Contents

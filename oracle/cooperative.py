@@ -1,5 +1,5 @@
 """Cooperative (shared-medium) community LP restated on the CPU -- TEST
-INFRASTRUCTURE ONLY (the checker for the batched GPU solver in
+INFRASTRUCTURE ONLY (it checks the results of the batched GPU solver in
 ``co_cultivation_metabolic_atlas_b200.cooperative``).
 
 Restates, in flux space ``v`` exactly as the reference assembles it,

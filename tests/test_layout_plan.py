@@ -8,7 +8,7 @@ import pytest
 from tests.conftest import ROOT
 
 
-@pytest.mark.skipif(shutil.which("nvcc") is None, reason="nvcc needed to compile the host checker")
+@pytest.mark.skipif(shutil.which("nvcc") is None, reason="nvcc needed to compile the host-side layout check")
 def test_layouts_are_aligned_and_disjoint(tmp_path):
     exe = tmp_path / "layout_check"
     src = ROOT / "tests" / "layout_check.cpp"
