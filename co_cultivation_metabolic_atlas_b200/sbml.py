@@ -14,7 +14,9 @@ path needs:
 * flux bounds from ``fbc:lowerFluxBound`` / ``fbc:upperFluxBound`` parameter
   references (FBC v2) or ``fbc:listOfFluxBounds`` (FBC v1); ``INF`` values
   become infinities; a reaction without a bound gets ``[-1000, 1000]``
-  (``[0, 1000]`` if irreversible), COBRA's defaults;
+  (``[0, 1000]`` if irreversible), COBRA's defaults; a reference to an
+  undefined parameter, or a lower bound above the upper one, is an error
+  (COBRA refuses both);
 * the active objective (``fbc:listOfObjectives``): coefficients and
   direction.
 
@@ -177,10 +179,17 @@ def read_sbml(path) -> GenomeScaleModel:
                 cols.append(j)
                 vals.append(v)
         lo_ref, up_ref = _attr(rx, "lowerFluxBound"), _attr(rx, "upperFluxBound")
-        lo = params[lo_ref] if lo_ref in params else v1_bounds.get(rid, {}).get("lower")
-        up = params[up_ref] if up_ref in params else v1_bounds.get(rid, {}).get("upper")
-        lower.append((-DEFAULT_BOUND if reversible else 0.0) if lo is None else lo)
-        upper.append(DEFAULT_BOUND if up is None else up)
+        for ref in (lo_ref, up_ref):
+            if ref and ref not in params:
+                raise ValueError(f"{path}: reaction {rid} references undefined bound parameter {ref}")
+        lo = params[lo_ref] if lo_ref else v1_bounds.get(rid, {}).get("lower")
+        up = params[up_ref] if up_ref else v1_bounds.get(rid, {}).get("upper")
+        lo = (-DEFAULT_BOUND if reversible else 0.0) if lo is None else lo
+        up = DEFAULT_BOUND if up is None else up
+        if not lo <= up:
+            raise ValueError(f"{path}: reaction {rid} has lower bound {lo} above upper bound {up}")
+        lower.append(lo)
+        upper.append(up)
     m, n = len(metabolites), len(reactions)
     S = csr_matrix((vals, (rows, cols)), shape=(m, n), dtype=np.float64)
     S.sum_duplicates()

@@ -190,3 +190,15 @@ def test_reader_fbc_version_1_bounds(tmp_path):
     m = sbml.read_sbml(path)
     assert m.lower.tolist() == [-5.0, 0.0, 2.0, 0.0]
     assert m.upper.tolist() == [7.0, 1000.0, 2.0, 1000.0]
+
+
+@pytest.mark.parametrize("edit,match", [
+    (('fbc:upperFluxBound="ten"', 'fbc:upperFluxBound="eleven"'), "undefined bound parameter eleven"),
+    (('fbc:lowerFluxBound="zero" fbc:upperFluxBound="up"', 'fbc:lowerFluxBound="ten" fbc:upperFluxBound="zero"'),
+     "above upper bound"),
+])
+def test_reader_rejects_inconsistent_bounds(tmp_path, edit, match):
+    path = tmp_path / "bad.xml"
+    path.write_text(FBC2.replace(*edit))
+    with pytest.raises(ValueError, match=match):
+        sbml.read_sbml(path)
