@@ -1,7 +1,6 @@
 """Without a CUDA device or without the native library the product path
 raises; it never falls back to a CPU solver.  (Runs where no GPU is
 visible; on a GPU host these cases cannot be staged and are skipped.)"""
-import numpy as np
 import pytest
 
 from tests.conftest import cuda_available
