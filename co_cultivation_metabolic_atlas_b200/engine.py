@@ -12,7 +12,7 @@ species matrix is stored once and shared by all of its instances.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 import torch

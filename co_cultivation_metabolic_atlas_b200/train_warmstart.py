@@ -22,7 +22,7 @@ import torch
 
 from . import synthetic as syn
 from .engine import SolveConfig
-from .warmstart import MLP, Codec, LearnedWarmStart, Rollouts, collect, solution_layout, train
+from .warmstart import MLP, Codec, LearnedWarmStart, Rollouts, collect, train
 
 HIDDEN = (512, 512, 512, 512)
 N_FEATURES = 44

@@ -35,7 +35,6 @@ import ctypes
 import math
 from dataclasses import dataclass
 
-import numpy as np
 import torch
 
 from . import _native as N

@@ -44,7 +44,7 @@ from __future__ import annotations
 from dataclasses import dataclass
 
 import numpy as np
-from scipy.sparse import csr_matrix, diags
+from scipy.sparse import csr_matrix
 
 BETA_SUFFICIENT = 0.2
 BETA_NECESSARY = 0.8
