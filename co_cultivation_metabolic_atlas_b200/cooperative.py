@@ -701,6 +701,8 @@ class CooperativeSolver:
             else:
                 stage = torch.where(ok, STAGE_MAX_MIN, STAGE_FAILED)
                 coexistence = torch.where(ok1, x1[:, st.nu].clamp_min(0.0), torch.zeros_like(sc.xbar))
+                # the retried stage-1 solution is the chosen one
+                aggregate = asm.aggregate(sc, chosen_x)
         fluxes = asm.fluxes(sc, final_x)
         fluxes = torch.where(ok[:, None], fluxes, torch.full_like(fluxes, float("nan")))
         return CooperativeResult(ok=ok, stage=stage, fluxes=fluxes, nu=final_x[:, st.nu], coexistence=coexistence,

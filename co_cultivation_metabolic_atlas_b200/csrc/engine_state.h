@@ -72,6 +72,24 @@ struct Buffer {
     }
 };
 
+// Checks of the solve parameters shared by every solve entry point.
+inline bool valid_params(const fbalp_solve_params& q, std::string* err) {
+    if (q.precision < 0 || q.precision > 2) return *err = "precision must be FP64, MIXED or FP32", false;
+    if (q.max_iterations < 0 || q.fp32_max_iterations < 0) return *err = "iteration budgets must be non-negative", false;
+    if (q.check_every < 1) return *err = "check_every must be positive", false;
+    for (double t : {q.tol_primal, q.tol_dual, q.tol_gap, q.fp32_tol_primal, q.fp32_tol_dual, q.fp32_tol_gap})
+        if (!(t >= 0.0) || !std::isfinite(t)) return *err = "tolerances must be finite and non-negative", false;
+    if (!(q.reflection >= 0.0 && q.reflection <= 1.0)) return *err = "reflection must be in [0,1]", false;
+    if (q.restarts != 0 && q.restarts != 1) return *err = "restarts must be 0 or 1", false;
+    if (q.fp32_stall_checks < 0 || q.fp64_stall_checks < 0) return *err = "stall checks must be non-negative", false;
+    if (!(q.floor_tol >= 0.0) || !std::isfinite(q.floor_tol)) return *err = "floor_tol must be finite and non-negative", false;
+    if (q.fallback_iterations < 0) return *err = "fallback_iterations must be non-negative", false;
+    if (q.fp32_recentre != 0 && q.fp32_recentre != 1) return *err = "fp32_recentre must be 0 or 1", false;
+    if (!(q.fp32_passthrough_tol >= 0.0) || !std::isfinite(q.fp32_passthrough_tol))
+        return *err = "fp32_passthrough_tol must be finite and non-negative", false;
+    return true;
+}
+
 }  // namespace fbalp_detail
 
 using namespace fbalp_detail;

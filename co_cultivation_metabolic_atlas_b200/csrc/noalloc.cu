@@ -1,22 +1,26 @@
 // Allocation-free solve entry point (fbalp_engine_solve_noalloc).
 //
-// Some callers cannot allocate device memory at solve time: code that runs
-// inside a CUDA stream capture (cudaMalloc is not a capturable operation),
-// real-time control loops that forbid allocator calls after start-up, and
-// hosts that run under a fixed device-memory budget set by another
-// allocator.  They create the engine (which allocates its species data) at
-// start-up and then call this entry point, which uses only the caller's
-// inputs/outputs and the scratch array below: the work-queue counter, the
-// per-instance metadata of a single-species batch, the layout record and the
-// per-CTA spill slabs of the FP64 PDHG kernel.
+// Some callers cannot allocate device memory at solve time: real-time
+// control loops that forbid allocator calls once they have started, and
+// hosts whose device memory is owned and budgeted by another allocator (a
+// framework's caching pool, a fixed-size arena) so that a cudaMalloc behind
+// its back either fails or breaks its accounting.  They create the engine
+// (which allocates its species data) at start-up and then call this entry
+// point, which uses only the caller's inputs/outputs and the scratch array
+// below: the work-queue counter, the per-instance metadata of a
+// single-species batch, the layout record and the per-CTA spill slabs of the
+// FP64 PDHG kernel.
 //
 // The scratch is a file-scope __device__ array of kNoallocScratchBytes
 // (32 MiB); every GPU that loads the library holds it until the process
 // exits.  Host code must not use the array's name as a device address: on
-// the first call on each device (with that device current) the entry point
-// obtains the real address with cudaGetSymbolAddress and remembers it.
-// Every call shares the array, so calls whose kernels overlap on the GPU
-// race; the queue counter is cleared at the start of every call.
+// the first call on each device (with that device current, which must be
+// the engine's device) the entry point obtains the real address with
+// cudaGetSymbolAddress and remembers it; that first call should come before
+// any stream capture.  Every call shares the array and it keeps the last
+// call's contents, so calls whose kernels overlap on the GPU race; the
+// queue counter is cleared at the start of every call and the metadata is
+// rewritten by every call.
 #include <cstdint>
 #include <mutex>
 
@@ -49,11 +53,13 @@ __global__ void fill_uniform_batch(int count, int n, int m, int32_t* order, int3
 }
 
 // Device address of the scratch array on the current device (set-up on the
-// first call per device).
-int scratch_address(unsigned char** out) {
+// first call per device).  The current device must be `want`, the engine's:
+// its species data, stream and kernels live there.
+int scratch_address(int want, unsigned char** out) {
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return fail(FBALP_ERR_CUDA, cudaGetErrorString(err));
+    if (dev != want) return fail(FBALP_ERR_INVALID, "current device is not the engine's device");
     if (dev < 0 || dev >= kMaxDevices) return fail(FBALP_ERR_INVALID, "device index out of range");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_addr[dev]) {
@@ -87,16 +93,16 @@ extern "C" int fbalp_engine_solve_noalloc(fbalp_engine* e, int64_t count, const 
     fbalp_solve_params q;
     fbalp_default_solve_params(&q);
     if (params) q = *params;
+    std::string err;
+    if (!valid_params(q, &err)) return fail(FBALP_ERR_INVALID, err);
     if (q.precision != FBALP_PRECISION_FP64)
         return fail(FBALP_ERR_INVALID, "the no-allocation solve runs the FP64 kernel only (precision FP64)");
-    if (q.max_iterations < 0 || q.check_every < 1 || q.fp64_stall_checks < 0 ||
-        !(q.reflection >= 0.0 && q.reflection <= 1.0) || (q.restarts != 0 && q.restarts != 1))
-        return fail(FBALP_ERR_INVALID, "invalid solve parameters");
-    for (double t : {q.tol_primal, q.tol_dual, q.tol_gap, q.floor_tol})
-        if (!(t >= 0.0) || !std::isfinite(t)) return fail(FBALP_ERR_INVALID, "tolerances must be finite and non-negative");
 
     unsigned char* scratch = nullptr;
-    if (int rc = scratch_address(&scratch)) return rc;
+    if (int rc = scratch_address(e->device, &scratch)) return rc;
+    // the per-phase queries (times, iterations) cover fbalp_engine_solve
+    // only: this call leaves them reporting no phase
+    e->ran[0] = e->ran[1] = false;
 
     const SpeciesHost& sh = e->species[0];
     const int threads = e->opt.warps_per_block * 32;

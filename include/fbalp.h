@@ -243,23 +243,25 @@ int fbalp_engine_solve(fbalp_engine* engine, const double* warm_x, const double*
                        int32_t* out_iterations, double* out_metrics, double* out_omega);
 
 /* Allocation-free solve.  No counterpart in the reference: it exists for
- * callers that cannot allocate device memory at solve time -- code running
- * inside a CUDA stream capture (cudaMalloc cannot be captured), real-time
- * loops that forbid allocator calls after start-up, hosts whose device
- * memory is budgeted by another allocator.  They create the engine (which
- * allocates its species data) up front; this call then allocates nothing:
- * besides the caller's inputs and outputs it uses one library-wide scratch
- * array of 32 MiB in device memory (held by every GPU that loads the library
- * until the process exits).
+ * callers that cannot allocate device memory at solve time -- real-time
+ * loops that forbid allocator calls once running, and hosts whose device
+ * memory is owned and budgeted by another allocator (a caching pool or a
+ * fixed arena), where a cudaMalloc behind its back fails or breaks its
+ * accounting.  They create the engine (which allocates its species data) up
+ * front; this call then allocates nothing: besides the caller's inputs and
+ * outputs it uses one library-wide scratch array of 32 MiB in device memory
+ * (held by every GPU that loads the library until the process exits).
  * Limits: one-species engine, FP64 precision only (params->precision must be
  * FBALP_PRECISION_FP64), instances laid out uniformly (instance i at columns
  * [i*n, (i+1)*n) and rows [i*m, (i+1)*m)), and a batch whose metadata and
  * per-CTA spill slabs fit in the scratch; larger requests fail with
- * FBALP_ERR_INVALID before any work is queued.  The first call on each
- * device (with that device current) looks up the scratch address with
- * cudaGetSymbolAddress, so make it before any stream capture.  All calls
- * share the scratch: calls whose kernels overlap on the GPU race.  Outputs
- * and their meaning are those of fbalp_engine_solve. */
+ * FBALP_ERR_INVALID before any work is queued.  The current device must be
+ * the engine's device (FBALP_ERR_INVALID otherwise).  The first call on each
+ * device looks up the scratch address with cudaGetSymbolAddress, so make it
+ * before any stream capture.  All calls share the scratch, which keeps the
+ * last call's contents: calls whose kernels overlap on the GPU race.
+ * Outputs and their meaning are those of fbalp_engine_solve; the phase
+ * queries (fbalp_engine_phase_times / _iterations) do not cover this call. */
 int fbalp_engine_solve_noalloc(fbalp_engine* engine, int64_t count, const double* lower,
                                const double* upper, const double* cost, const double* rhs,
                                const double* warm_x, const double* warm_y, const double* warm_omega,

@@ -1,9 +1,10 @@
 """The allocation-free entry point (fbalp_engine_solve_noalloc).
 
-It serves callers that cannot allocate device memory when they solve (code
-inside a CUDA stream capture, real-time loops, hosts with a budgeted device
-allocator): after an engine is created up front, this call uses only the
-caller's buffers and a fixed library-wide scratch array.  The test calls it
+It serves callers that cannot allocate device memory when they solve
+(real-time loops that forbid allocator calls once running, hosts whose device
+memory another allocator owns and budgets): after an engine is created up
+front, this call uses only the caller's buffers and a fixed library-wide
+scratch array.  The test calls it
 through the C ABI twice in a row and checks both results against the regular
 entry point.  The file name makes pytest collect it last.
 """
@@ -51,6 +52,8 @@ def test_noalloc_solve_matches_regular_solve_on_two_calls():
         rc = _noalloc(eng, lo, up, c, params, out)
         assert rc == N.FBALP_OK, eng.lib.fbalp_last_error()
     torch.cuda.synchronize()
+    # the phase queries cover the regular entry point only
+    assert eng.phase_times() == (0.0, 0.0)
     st = ref.status.cpu().numpy()
     assert (st == 0).all()
     for out in outs:
