@@ -3,6 +3,14 @@ dFBA workload (one step = 12,288 LPs of uneven size, solved in one persistent
 launch per precision phase, then the Euler update), warm start vs cold.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
+    python bench.py --profile fba|cooperative|mlp [--envs E] [--steps K]
+
+``--profile`` runs a short, untimed driver of one workload for an external
+profiler (ncu) instead of the benchmark: warm-started dFBA steps of the FBA
+community (per-step phase instance-iterations and times printed), steps of
+the cooperative community (the last one inside the NVTX range
+``coop_step``), or inference and training passes of the warm-start network
+(random weights; TFLOP/s of the GEMMs printed).
 
 Prints one JSON line (rank 0).  Roofline model of the dominant kernel
 (the re-centred PDHG phase), a design that streams everything from HBM:
@@ -44,7 +52,13 @@ def parse():
     ap.add_argument("--envs", type=int, default=4096, help="environments per GPU")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", default="mixed", choices=("mixed", "fp64", "fp32"))
-    ap.add_argument("--cpu-sample", type=int, default=48, help="LPs per species in the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=48,
+                    help="reference arm: LPs per step in its bounded CPU HiGHS sample (a third per species)")
+    ap.add_argument("--highs-check", type=int, default=1536,
+                    help="product arm: LPs of one step checked against HiGHS (a third per species); their CPU "
+                         "time is the cpu_baseline")
+    ap.add_argument("--drop-in", type=int, default=1,
+                    help="1: also time one step's LPs through B200LPBackend.solve_batch (host preparation included)")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = the same number of steps as the timed region")
     ap.add_argument("--no-cold", action="store_true")
     ap.add_argument("--warm", default="extrapolate", choices=("previous", "extrapolate"),
@@ -61,6 +75,9 @@ def parse():
                     help="fba: the per-species FBA step (headline); cooperative: the three-stage shared-medium "
                          "community LP per environment")
     ap.add_argument("--coop-sample", type=int, default=6, help="environments in the cooperative CPU sample")
+    ap.add_argument("--profile", default=None, choices=("fba", "cooperative", "mlp"),
+                    help="run a short profiling driver of one workload instead of the benchmark")
+    ap.add_argument("--warps", type=int, default=16, help="--profile fba: warps per CTA")
     ap.add_argument("--coop-growth-cap", type=float, default=0.005,
                     help="coexistence growth upper bound (the reference simulator's 0.005 /h; <= 0: the solver "
                          "default 10)")
@@ -188,18 +205,23 @@ def run_reference(args):
     medium, biomass = syn.initial_environments(args.envs, seed=args.seed)
     lowers = [dfba.uptake_lower_bounds(m, medium, biomass, 0.05) for m in models]
     per = max(4, args.cpu_sample // 3)
-    rates = []
+    rates, walls = [], []
     cores = None
     for k in range(args.warmup + args.steps):
         rate, cores, wall, _ = cpu_highs_sample(models, lowers, per, args.seed + k)
         if k >= args.warmup:
             rates.append(rate)
+            walls.append(wall)
     value = statistics.mean(rates)
     lps = args.envs * len(models)
+    # one step of this arm is the bounded sample (3 * per LPs); the time a
+    # whole 12,288-LP step would take at this rate is reported beside it
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * lps / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+            "projected_full_step_ms": 1e3 * lps / value,
+            "step": f"a bounded sample of {3 * per} of the step's {lps} LPs",
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(args, lps),
+            "data": "synthetic (seeded generator; no public dataset)", "config": workload_config(args, lps),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{3 * per} LPs per step (seeded, {per} per species) of the step's "
                                        f"{lps} LPs; scipy.optimize.linprog(method='highs-ds'), one HiGHS "
@@ -210,6 +232,124 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------------------- product arm
+def timed_trajectory(com, args, barrier, pdhg_launches):
+    """Warm-up, (graph capture,) then ``args.steps`` timed dFBA steps.  The
+    whole region is timed with CUDA events on the stream; each step's PDHG
+    launches are bracketed by the engine's timing slots (external event
+    nodes inside the captured graphs), read two steps behind so the host
+    never drains the queue.  Returns (ms, certified, iterations, launches,
+    per-step PDHG kernel ms)."""
+    import torch
+    for _ in range(args.warmup):
+        com.step()
+    graphs = bool(args.graphs and args.warmup >= 2)
+    if graphs:
+        com.capture()  # the timed steps replay CUDA graphs of whole dFBA steps
+    else:
+        com.engine.timing_slots(3)
+    torch.cuda.synchronize()
+    barrier()
+    stream = torch.cuda.current_stream()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    certified, iters, kernel_ms, slots = [], [], [], []
+    launches = 0
+
+    def harvest(slot):
+        t32, t64 = com.engine.slot_times(slot)
+        kernel_ms.append(t32 + t64)
+
+    start.record(stream)
+    for j in range(args.steps):
+        if not graphs:
+            com.engine.use_timing_slot(j % 3)
+        st = com.step()
+        slots.append(com.last_replay_slot() if graphs else j % 3)
+        certified.append(st.certified.clone())
+        iters.append(st.iterations.clone())
+        launches += pdhg_launches
+        if j >= 2:
+            harvest(slots[j - 2])
+    stop.record(stream)
+    torch.cuda.synchronize()
+    for j in range(max(0, args.steps - 2), args.steps):
+        harvest(slots[j])
+    if not graphs:
+        com.engine.use_timing_slot(-1)
+    barrier()
+    ms = start.elapsed_time(stop)
+    cert = int(sum(int(c.item()) for c in certified))
+    it = torch.stack(iters).cpu().numpy()  # (steps, lps)
+    return ms, cert, it, launches, kernel_ms
+
+
+def streaming_bytes(models, species_id, it, w=4):
+    """Algorithmic bytes of one launch of the PDHG phase in the streaming
+    model: per instance-iteration w (3 n + 3 m + 2 n_medium), plus per
+    species and iteration of its longest instance the matrix and its
+    transpose, 2 (nnz (w + 4) + 4 (m + 1))."""
+    per_inst = np.array([w * (3 * m.S.shape[1] + 3 * m.S.shape[0] + 2 * len(m.medium_columns))
+                         for m in models], dtype=np.float64)
+    total = float(np.sum(it.astype(np.float64) * per_inst[species_id]))
+    for s, m in enumerate(models):
+        its = it[species_id == s]
+        total += float(its.max() if its.size else 0) * 2 * (m.S.nnz * (w + 4) + 4 * (m.S.shape[0] + 1))
+    return total
+
+
+def profiled_onchip():
+    """Shared-memory wavefronts per instance-iteration of the re-centred
+    phase from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "pdhg_recentred_community_small.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("shared_wavefronts_per_instance_iteration:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def certificate_summary(res, lps):
+    """Distribution of the kernel's FP64 certificate fields over every LP of
+    a step (primal residual, dual violation, relative KKT gap)."""
+    mt = res.metrics.cpu().numpy()
+    st = res.status.cpu().numpy()
+    out = {"lps": int(lps), "optimal": int(np.sum(st == 0))}
+    for k, name in enumerate(("primal", "dual", "kkt_gap")):
+        v = mt[:, k]
+        out[name] = {"max": float(np.max(v)), "p99": float(np.percentile(v, 99)), "median": float(np.median(v))}
+    out["gate_passed"] = int(np.sum((st == 0) & (mt[:, 0] <= 1e-5) & (mt[:, 1] <= 1e-7) & (mt[:, 2] <= 1e-7)))
+    return out
+
+
+def drop_in_measure(models, lower_host, envs, device):
+    """The reference-facing drop-in (``B200LPBackend.solve_batch``) on one
+    step's LPs as ``linprog``-kwargs requests: a first call builds the engine,
+    a second call (warm-started from the first) is reported with its host
+    preparation, GPU solve and total seconds."""
+    from co_cultivation_metabolic_atlas_b200.backend import B200LPBackend
+    reqs, ids = [], []
+    for s, m in enumerate(models):
+        zeros = np.zeros(m.S.shape[0])
+        for e in range(envs):
+            reqs.append((m.cost, dict(A_eq=m.S, b_eq=zeros, bounds=np.column_stack([lower_host[s][e], m.upper]),
+                                      method="highs-ds")))
+            ids.append((s, e))
+    be = B200LPBackend(mode="previous", device=device)
+    be.solve_batch(reqs, environment_ids=ids)
+    rows = be.solve_batch(reqs, environment_ids=ids)
+    h = be.history[-1]
+    be.close()
+    return {"requests": len(reqs), "accepted": int(sum(r.success for r in rows)),
+            "host_preparation_seconds": h["host_preparation_seconds"], "solve_seconds": h["solve_seconds"],
+            "total_seconds": h["total_seconds"], "lps_per_s": len(reqs) / h["total_seconds"],
+            "api": "B200LPBackend.solve_batch(requests) with scipy-linprog kwargs, warm-started from the previous "
+                   "call (mode='previous')"}
+
+
 def run_product(args):
     import torch
 
@@ -254,84 +394,78 @@ def run_product(args):
 
     def trajectory(warm, learned=None):
         com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, learned=learned, device=dev)
-        for _ in range(args.warmup):
+        first = None
+        if args.warmup:
+            # the first (history-free) step: the network's seed or a cold start
             com.step()
-        if args.graphs and args.warmup >= 2:
-            com.capture()  # the timed steps replay CUDA graphs of whole dFBA steps
-        torch.cuda.synchronize()
-        barrier()
-        stream = torch.cuda.current_stream()
-        start = torch.cuda.Event(enable_timing=True)
-        stop = torch.cuda.Event(enable_timing=True)
-        certified = []
-        iters = []
-        launches = 0
-        start.record(stream)
-        for _ in range(args.steps):
-            st = com.step()
-            certified.append(st.certified.clone())
-            iters.append(st.iterations.clone())
-            launches += pdhg_launches
-        stop.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        ms = start.elapsed_time(stop)
-        cert = int(sum(int(c.item()) for c in certified))
-        it = torch.cat(iters).cpu().numpy()
-        return com, ms, cert, it, launches
+            first = com.prev.iterations.float().mean().item()
+            args_w = argparse.Namespace(**{**vars(args), "warmup": args.warmup - 1})
+        else:
+            args_w = args
+        ms, cert, it, launches, kms = timed_trajectory(com, args_w, barrier, pdhg_launches)
+        return com, ms, cert, it, launches, kms, first
 
     headline = "learned" if ws is not None else args.warm
     with ClockSampler(local) as clocks:
-        com, ms, cert, it, launches = trajectory(headline, learned=ws)
+        com, ms, cert, it, launches, kernel_ms, first_its = trajectory(headline, learned=ws)
     clock_summary = clocks.summary()
     ms_max = max_over_ranks(ms)
     cert_all = sum_over_ranks(cert)
     value = cert_all / (ms_max / 1e3)
 
-    # --- roofline of the dominant kernel (the re-centred FP32 phase of one
-    # more step of the same trajectory) ---
+    # --- roofline of the dominant kernel over the timed steps themselves:
+    # streaming-model bytes of every timed step's PDHG launches over their
+    # CUDA-event durations (graph event nodes) ---
     peak, peak_kind = hbm_peak()
-    com.uptake_bounds()
-    res = com.solve()
-    torch.cuda.synchronize()
-    t32, t64 = com.engine.phase_times()
-    dom_ms = t32 if args.precision != "fp64" else t64
     w = 4 if args.precision != "fp64" else 8
-    if args.precision == "mixed":
-        it32 = com.engine.phase_iterations().cpu().numpy().astype(np.int64)
-    else:
-        it32 = res.iterations.cpu().numpy().astype(np.int64)
     sid = com.species_id
-    per_inst = np.array([w * (3 * m.S.shape[1] + 3 * m.S.shape[0] + 2 * len(m.medium_columns))
-                         for m in models], dtype=np.float64)
-    inst_bytes = float(np.sum(it32 * per_inst[sid]))
-    mat_bytes = 0.0
-    for s, m in enumerate(models):
-        its = it32[sid == s]
-        mat_bytes += float(its.max() if its.size else 0) * 2 * (m.S.nnz * (w + 4) + 4 * (m.S.shape[0] + 1))
-    alg_bytes = inst_bytes + mat_bytes
-    achieved = alg_bytes / (dom_ms / 1e3) / 1e9
+    step_bytes = [streaming_bytes(models, sid, it[j], w) for j in range(it.shape[0])]
+    kernel_total_ms = float(sum(kernel_ms))
+    achieved = sum(step_bytes) / (kernel_total_ms / 1e3) / 1e9
+    inst_its = int(it.sum())
     tpi = profiled_traffic()
-    traffic = None if tpi is None else tpi * float(it32.sum())
+    traffic = None if tpi is None else tpi * inst_its / it.shape[0]
     kname = {"mixed": "pdhg_recentred", "fp32": "pdhg_persistent<float>", "fp64": "pdhg_persistent<double>"}
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} copy bandwidth",
-                "kernel": kname[args.precision], "algorithmic_bytes": alg_bytes, "kernel_ms": dom_ms,
-                "instance_iterations": int(it32.sum())}
+                "kernel": kname[args.precision], "algorithmic_bytes": sum(step_bytes) / len(step_bytes),
+                "kernel_ms": kernel_total_ms / len(kernel_ms), "kernel_share_of_step": kernel_total_ms / ms,
+                "instance_iterations_per_launch": inst_its / it.shape[0],
+                "measured_on": f"the {args.steps} timed steps (CUDA events around each step's PDHG launches)"}
+    wf = profiled_onchip()
+    sm_mhz = clock_summary.get("sm_mhz") or 1965.0
+    if wf is not None:
+        sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+        onchip_peak = sm_count * 128.0 * sm_mhz * 1e6 / 1e9
+        onchip = wf * 128.0 * inst_its / (kernel_total_ms / 1e3) / 1e9
+        roofline["shared_memory"] = {"achieved": onchip, "peak": onchip_peak, "unit": "GB/s", "frac": onchip / onchip_peak,
+                                     "wavefronts_per_instance_iteration": wf,
+                                     "model": "ncu shared-memory wavefronts per instance-iteration x 128 B, over "
+                                              "SMs x 128 B/clk at the sampled SM clock"}
 
-    # --- CPU baseline on a sample of this step's LPs + HiGHS objective check ---
+    # --- the last timed step's certificate distribution over all its LPs,
+    # and HiGHS on a sample of its LPs (objective check + CPU baseline) ---
+    res = com.prev
+    cert_dist = certificate_summary(res, lps)
     cpu = None
     highs_check = None
+    lower_host = None
     if rank == 0:
+        # the bounds the last step was solved with are the state's uptake
+        # bounds before its Euler update: recompute them from the previous
+        # state is not possible, so solve one more eager step and check it
+        com.uptake_bounds()
+        res = com.solve()
+        torch.cuda.synchronize()
         lower = com.lower.cpu().numpy()
         co = com.col_offsets.cpu().numpy()
-        lowers = []
+        lower_host = []
         for s, m in enumerate(models):
             n = m.S.shape[1]
             base = int(co[s * args.envs])
-            lowers.append(lower[base:base + args.envs * n].reshape(args.envs, n))
-        per = max(4, args.cpu_sample // 3)
-        rate, cores, wall, funs = cpu_highs_sample(models, lowers, per, args.seed)
+            lower_host.append(lower[base:base + args.envs * n].reshape(args.envs, n))
+        per = max(4, args.highs_check // 3)
+        rate, cores, wall, funs = cpu_highs_sample(models, lower_host, per, args.seed)
         obj = res.objective.cpu().numpy()
         status = res.status.cpu().numpy()
         errs = []
@@ -348,26 +482,32 @@ def run_product(args):
                          f"scipy.optimize.linprog(method='highs-ds'), one HiGHS thread per LP, thread "
                          f"pool over all cores (ParallelCpuLP pattern); {wall:.1f} s wall"}
         highs_check = {"sampled": len(funs), "within_1e-6": int(agree),
-                       "max_rel_obj_err": max(errs) if errs else None}
+                       "max_rel_obj_err": max(errs) if errs else None,
+                       "step_certificates": certificate_summary(res, lps)}
     com.close()
     com = None
 
     # --- the same trajectory without the network (temporal base only) and cold ---
     extrap = None
     if ws is not None:
-        com_e, ms_e, cert_e, it_e, _ = trajectory(args.warm)
+        com_e, ms_e, cert_e, it_e, _, _, first_e = trajectory(args.warm)
         com_e.close()
         extrap = {"value": sum_over_ranks(cert_e) / (max_over_ranks(ms_e) / 1e3),
-                  "mean_iterations": float(np.mean(it_e)), "warm_start": args.warm}
+                  "mean_iterations": float(np.mean(it_e)), "warm_start": args.warm,
+                  "first_step_mean_iterations": first_e}
     cold = None
     cold_iters = None
+    cold_first = None
     if not args.no_cold:
-        com_c, ms_c, cert_c, it_c, _ = trajectory("cold")
+        com_c, ms_c, cert_c, it_c, _, _, cold_first = trajectory("cold")
         cold = sum_over_ranks(cert_c) / (max_over_ranks(ms_c) / 1e3)
         cold_iters = float(np.mean(it_c))
         com_c.close()
     # --- e2e through the public engine API with host buffers ---
     e2e = run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, sum_over_ranks, ws)
+    drop_in = None
+    if rank == 0 and args.drop_in and lower_host is not None:
+        drop_in = drop_in_measure(models, lower_host, args.envs, dev)
 
     if rank == 0:
         warm_desc = {"previous": "previous-step solution",
@@ -376,24 +516,27 @@ def run_product(args):
             warm_desc = ("learned: MLP prediction from the medium state at an environment's first step, then the "
                          "temporal base (" + warm_desc + ")")
         if learned_info is not None:
-            learned_info.update(value=value, mean_iterations=float(np.mean(it)))
+            learned_info.update(value=value, mean_iterations=float(np.mean(it)),
+                                first_step_mean_iterations=first_its,
+                                first_step_iterations_vs_cold=(first_its / cold_first) if cold_first else None)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "cuda_graphs": bool(args.graphs and args.warmup >= 2),
+                "cuda_graphs": bool(args.graphs and args.warmup >= 3),
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "fp32+fp64" if args.precision == "mixed" else args.precision,
                 "data": "synthetic (seeded generator; no public dataset)",
-                "config": dict(workload_config(args, lps), warm_start=warm_desc,
-                               parallelism=f"env-sharded x{world}"),
+                "config": workload_config(args, lps),
+                "warm_start": warm_desc, "parallelism": f"env-sharded x{world}",
                 "certified_fraction": cert / (lps * args.steps),
                 "env_steps_per_s": world * args.envs * args.steps / (ms_max / 1e3),
                 "iterations": {"mean": float(np.mean(it)), "p50": float(np.median(it)),
                                "p99": float(np.percentile(it, 99)), "max": int(np.max(it))},
                 "cold_value": cold, "warm_vs_cold": (value / cold) if cold else None,
-                "cold_mean_iterations": cold_iters,
+                "cold_mean_iterations": cold_iters, "cold_first_step_mean_iterations": cold_first,
                 "without_network": extrap, "network_gain": (value / extrap["value"]) if extrap else None,
                 "learned": learned_info, "learned_vs_cold": (value / cold) if (ws is not None and cold) else None,
-                "roofline": roofline, "cpu_baseline": cpu, "highs_check": highs_check, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "highs_check": highs_check,
+                "timed_step_certificates": cert_dist, "e2e": e2e, "drop_in": drop_in,
                 "gpu_launches": launches, "clocks": clock_summary}
         print(json.dumps(line), flush=True)
     ranks.close()
@@ -728,9 +871,101 @@ def run_reference_cooperative(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- profiling driver
+def run_profile(args):
+    """Short untimed runs of one workload for an external profiler."""
+    import torch
+
+    from co_cultivation_metabolic_atlas_b200 import synthetic as syn
+    from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
+    from co_cultivation_metabolic_atlas_b200.engine import EngineOptions, SolveConfig
+
+    models = syn.community_models()
+    if args.profile == "mlp":
+        from co_cultivation_metabolic_atlas_b200.train_warmstart import HIDDEN, N_FEATURES
+        from co_cultivation_metabolic_atlas_b200.warmstart import BF16, MLP, solution_layout
+        _, width = solution_layout(models)
+        net = MLP([N_FEATURES, *HIDDEN, width], seed=0)
+        g = torch.Generator(device="cuda").manual_seed(0)
+        X = torch.randn(args.envs, N_FEATURES, device="cuda", generator=g)
+        T = torch.randn(args.envs, net.pdims[-1], device="cuda", generator=g)
+        # 2 B sum(in * out) per forward pass (padded widths: the FLOPs the
+        # kernels issue); backward: dW for every layer, dH for all but the first
+        mac = [net.pdims[l] * net.pdims[l + 1] for l in range(net.layers)]
+        fwd = 2.0 * args.envs * sum(mac)
+        train = fwd + 2.0 * args.envs * (sum(mac) + sum(mac[1:]))
+        dY32 = torch.empty_like(T)
+        dY16 = torch.empty(T.shape, dtype=BF16, device="cuda")
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        for k in range(args.steps):
+            ev[0].record()
+            net.forward(X)
+            ev[1].record()
+            Y = net.forward(X, keep=True)
+            net.ops.mse_grad(Y, T, 2.0 / Y.numel(), dY32, dY16, loss)
+            gW, gb = net.backward(dY32, dY16)
+            net.adam_step(gW, gb, 1e-4)
+            ev[2].record()
+            torch.cuda.synchronize()
+            if net.ops.error_flag():
+                raise RuntimeError("tensor-core kernel reported a timeout")
+            t_inf, t_train = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+            print(f"step {k}: inference {t_inf:.3f} ms ({fwd / t_inf / 1e9:.1f} TFLOP/s), "
+                  f"training step {t_train:.3f} ms ({train / t_train / 1e9:.1f} TFLOP/s)")
+        return
+    if args.profile == "cooperative":
+        from co_cultivation_metabolic_atlas_b200.cooperative import CooperativeCommunity
+        models = syn.community_models(seed=syn.COOPERATIVE_SEED)
+        medium, biomass = syn.initial_environments(args.envs)
+        com = CooperativeCommunity(models, medium, biomass)
+        for k in range(args.steps):
+            last = k == args.steps - 1
+            if last:
+                torch.cuda.nvtx.range_push("coop_step")
+            res = com.step()
+            torch.cuda.synchronize()
+            if last:
+                torch.cuda.nvtx.range_pop()
+            its = {name: float(v["iterations"].float().mean()) for name, v in res.stages.items()}
+            print(f"step {k}: certified {int(res.ok.sum())}/{args.envs}, mean iterations {its}")
+        com.close()
+        return
+    medium, biomass = syn.initial_environments(args.envs)
+    com = DeviceCommunity(models, medium, biomass, config=SolveConfig(precision=args.precision),
+                          options=EngineOptions(warps_per_block=args.warps), warm_start=args.warm)
+    for k in range(args.steps):
+        st = com.step()
+        if args.precision == "mixed":
+            phase = com.engine.phase_iterations()
+            t32, t64 = com.engine.phase_times()
+            print(f"step {k}: first-phase instance-iterations {int(phase.sum().item())}, "
+                  f"first phase {t32:.3f} ms, FP64 phase {t64:.3f} ms")
+    torch.cuda.synchronize()
+    print("certified", int(st.certified.item()), "of", st.lps)
+    com.close()
+
+
+def spawn_ranks(n):
+    """``--gpus N`` without a ``torchrun`` environment: run this command as
+    N ranks under ``torch.distributed.run`` on this node and return its
+    exit code (rank 0 prints the line)."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
-    if args.workload == "cooperative":
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and not args.profile:
+        sys.exit(spawn_ranks(args.gpus))
+    if args.profile:
+        run_profile(args)
+    elif args.workload == "cooperative":
         (run_reference_cooperative if args.impl == "reference" else run_cooperative)(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -109,6 +109,10 @@ def load(path: os.PathLike | None = None):
         "fbalp_engine_phase_times": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_float),
                                                     ctypes.POINTER(ctypes.c_float)]),
         "fbalp_engine_phase_iterations": (ctypes.c_int, [vp, vp]),
+        "fbalp_engine_timing_slots": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "fbalp_engine_use_timing_slot": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "fbalp_engine_slot_times": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_float),
+                                                   ctypes.POINTER(ctypes.c_float)]),
         "fbalp_last_error": (ctypes.c_char_p, []),
         # BF16 tensor-core kernels of the learned warm start (include/fbalp_mlp.h)
         "fbalp_gemm_bf16": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int,

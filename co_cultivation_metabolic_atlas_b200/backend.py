@@ -57,7 +57,7 @@ import torch
 from . import _native as N
 from .engine import EngineOptions, LPEngine, SolveConfig
 from .lp_trace import certificate as original_certificate
-from .problem import matrix_key, normalize
+from .problem import matrix_key, normalize_batch
 from .reduction import EqualityReduction
 from .rowsplit import RowSplit
 
@@ -125,8 +125,22 @@ class B200LPBackend:
             for env in ids:
                 self.last_certified.pop(env, None)
 
+    @staticmethod
+    def _matrix_keys(problems):
+        """Content key of every request's matrix, hashed once per distinct
+        canonical matrix object (``normalize_batch`` shares one object among
+        requests that passed the same matrices)."""
+        memo = {}
+        out = []
+        for p in problems:
+            k = memo.get((id(p[0]), p[5]))
+            if k is None:
+                k = memo[(id(p[0]), p[5])] = matrix_key(p[0], p[5])
+            out.append(k)
+        return out
+
     def _engine_for(self, problems):
-        keys = [matrix_key(p[0], p[5]) for p in problems]
+        keys = self._matrix_keys(problems)
         new = [(k, p) for k, p in zip(keys, problems) if k not in self._keys]
         rebuilt = False
         if new:
@@ -149,7 +163,7 @@ class B200LPBackend:
         ids = list(range(len(requests))) if environment_ids is None else list(environment_ids)
         if not requests or len(ids) != len(requests) or len(set(ids)) != len(ids):
             raise ValueError('Nonempty requests and unique environment IDs required')
-        originals = [normalize(c, kw) for c, kw in requests]
+        originals = normalize_batch(requests)
         if self.stage is not None and any(kw.get('_stage', self.stage) != self.stage for _, kw in requests):
             raise ValueError('Use a separate backend and history for each LP stage')
         reduced = self._reduce(originals) if self.equality_reduction else None
@@ -289,8 +303,7 @@ class B200LPBackend:
             # the learned warm start proposes points of the unsplit LPs
             return [None] * len(problems)
         out = []
-        for p in problems:
-            key = matrix_key(p[0], p[5])
+        for p, key in zip(problems, self._matrix_keys(problems)):
             if key not in self._split_plans:
                 plan = RowSplit(p[0], p[5], max_length=self.split_rows)
                 self._split_plans[key] = plan if plan.active else None
@@ -302,8 +315,7 @@ class B200LPBackend:
         once per block); a request whose bounds are infeasible under the
         eliminated equalities maps to None (a failed row)."""
         out = []
-        for p in originals:
-            key = matrix_key(p[0], p[5])
+        for p, key in zip(originals, self._matrix_keys(originals)):
             plan = self._plans.get(key)
             if plan is None:
                 plan = self._plans[key] = EqualityReduction(p)

@@ -589,11 +589,20 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     // phase timing events only outside a capture (a graph replay has no
     // per-phase timing)
     if (!capturing) check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
+    // a selected timing slot records around the launch in either case (an
+    // external event node under capture)
+    cudaEvent_t* sev = e->slot >= 0 ? &e->slot_ev[4 * static_cast<size_t>(e->slot)] : nullptr;
+    const unsigned rec_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (sev) check(cudaEventRecordWithFlags(sev[2 * ph], e->stream, rec_flags), "timing slot record");
     if (recentred)
         check(fbalp::launch_recentred(recentred == 1, patched, grid, threads, dyn, e->stream, p),
               "re-centred pdhg kernel launch");
     else
         check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
+    if (sev) {
+        check(cudaEventRecordWithFlags(sev[2 * ph + 1], e->stream, rec_flags), "timing slot record");
+        e->slot_ran[2 * static_cast<size_t>(e->slot) + ph] = 1;
+    }
     if (!capturing) check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
     e->ran[ph] = !capturing;
     e->last_grid[fp64 ? 1 : 0] = grid;
@@ -803,6 +812,46 @@ extern "C" int fbalp_engine_phase_times(fbalp_engine* e, float* ms_fp32, float* 
         if (!e->ran[ph]) continue;
         cudaError_t err = cudaEventSynchronize(e->ev[2 * ph + 1]);
         if (err == cudaSuccess) err = cudaEventElapsedTime(outs[ph], e->ev[2 * ph], e->ev[2 * ph + 1]);
+        if (err != cudaSuccess) return fail(FBALP_ERR_CUDA, cudaGetErrorString(err));
+    }
+    return FBALP_OK;
+}
+
+extern "C" int fbalp_engine_timing_slots(fbalp_engine* e, int32_t slots) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (slots < 0 || slots > 64) return fail(FBALP_ERR_INVALID, "slots must be in [0, 64]");
+    for (cudaEvent_t& v : e->slot_ev)
+        if (v) cudaEventDestroy(v);
+    e->slot_ev.assign(4 * static_cast<size_t>(slots), nullptr);
+    e->slot_ran.assign(2 * static_cast<size_t>(slots), 0);
+    e->slot = -1;
+    for (cudaEvent_t& v : e->slot_ev) {
+        cudaError_t err = cudaEventCreate(&v);
+        if (err != cudaSuccess) return fail(FBALP_ERR_CUDA, cudaGetErrorString(err));
+    }
+    return FBALP_OK;
+}
+
+extern "C" int fbalp_engine_use_timing_slot(fbalp_engine* e, int32_t slot) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (slot < -1 || slot >= static_cast<int32_t>(e->slot_ran.size() / 2))
+        return fail(FBALP_ERR_INVALID, "timing slot out of range");
+    e->slot = slot;
+    return FBALP_OK;
+}
+
+extern "C" int fbalp_engine_slot_times(fbalp_engine* e, int32_t slot, float* ms_fp32, float* ms_fp64) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (slot < 0 || slot >= static_cast<int32_t>(e->slot_ran.size() / 2))
+        return fail(FBALP_ERR_INVALID, "timing slot out of range");
+    float* outs[2] = {ms_fp32, ms_fp64};
+    for (int ph = 0; ph < 2; ++ph) {
+        if (!outs[ph]) continue;
+        *outs[ph] = 0.0f;
+        if (!e->slot_ran[2 * static_cast<size_t>(slot) + ph]) continue;
+        const cudaEvent_t* sev = &e->slot_ev[4 * static_cast<size_t>(slot)];
+        cudaError_t err = cudaEventSynchronize(sev[2 * ph + 1]);
+        if (err == cudaSuccess) err = cudaEventElapsedTime(outs[ph], sev[2 * ph], sev[2 * ph + 1]);
         if (err != cudaSuccess) return fail(FBALP_ERR_CUDA, cudaGetErrorString(err));
     }
     return FBALP_OK;

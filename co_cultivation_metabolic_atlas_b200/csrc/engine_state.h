@@ -129,8 +129,17 @@ struct fbalp_engine {
     int64_t last_smem[2] = {0, 0};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase start/stop: fp32, fp64
     bool ran[2] = {false, false};
+    // timing slots: per slot the same four events, recorded around the
+    // phase launches while the slot is selected -- as external event nodes
+    // when the launches are captured into a CUDA graph, so that every replay
+    // of that graph re-records them
+    std::vector<cudaEvent_t> slot_ev;
+    std::vector<char> slot_ran;  // per slot and phase: events recorded (or captured)
+    int slot = -1;               // selected slot (-1: none)
     ~fbalp_engine() {
         for (cudaEvent_t& v : ev)
+            if (v) cudaEventDestroy(v);
+        for (cudaEvent_t& v : slot_ev)
             if (v) cudaEventDestroy(v);
         for (void* p : owned) cudaFree(p);
         for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,

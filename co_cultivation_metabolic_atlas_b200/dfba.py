@@ -214,19 +214,28 @@ class DeviceCommunity:
         old_stream = self.engine.stream
         self._graphs, self._graph_stats = [], []
         torch.cuda.synchronize(self.device)
+        # graph k brackets its PDHG launches by the engine's timing slot k
+        self.engine.timing_slots(3)
         try:
-            for _ in range(3):
+            for k in range(3):
                 g = torch.cuda.CUDAGraph()
+                self.engine.use_timing_slot(k)
                 with torch.cuda.graph(g):
                     self.engine.set_stream(torch.cuda.current_stream(self.device))
                     st = self._eager_step()
                 self._graphs.append(g)
                 self._graph_stats.append(st)
         finally:
+            self.engine.use_timing_slot(-1)
             self.engine.set_stream(old_stream)
             # capture ran nothing: the state is where it was
             self.step_index, self.prev, self.prev2, self.result, self._which = saved
         self._replay = 0
+
+    def last_replay_slot(self, back: int = 0):
+        """Timing slot (the graph index) of the step replayed ``back`` steps
+        before the last one."""
+        return (self._replay - 1 - back) % 3
 
     def release_graphs(self):
         self._graphs, self._graph_stats = [], []

@@ -305,6 +305,23 @@ class LPEngine:
         N.check(self.lib.fbalp_engine_phase_times(self.handle, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def timing_slots(self, slots: int):
+        """Create ``slots`` timing slots (benchmark instrumentation)."""
+        N.check(self.lib.fbalp_engine_timing_slots(self.handle, int(slots)))
+
+    def use_timing_slot(self, slot: int):
+        """Bracket the following solves' phase launches by the events of
+        ``slot`` (-1: none); captured launches keep their slot in the graph."""
+        N.check(self.lib.fbalp_engine_use_timing_slot(self.handle, int(slot)))
+
+    def slot_times(self, slot: int):
+        """Device milliseconds of the (FP32, FP64) phase launches last
+        recorded in ``slot``; waits for them."""
+        a = ctypes.c_float()
+        b = ctypes.c_float()
+        N.check(self.lib.fbalp_engine_slot_times(self.handle, int(slot), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def phase_iterations(self):
         """FP32-phase iteration counts of the last mixed solve (device int32)."""
         out = torch.empty(self.count, dtype=torch.int32, device=self.device)

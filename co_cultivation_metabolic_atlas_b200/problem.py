@@ -38,8 +38,14 @@ def split_bounds(bounds, variables):
     return lower, upper
 
 
-def normalize(objective, kwargs):
-    """Validate one ``(c, linprog kwargs)`` request; see module docstring."""
+def normalize(objective, kwargs, _cache=None):
+    """Validate one ``(c, linprog kwargs)`` request; see module docstring.
+
+    ``_cache`` (a dict owned by one ``normalize_batch`` call) maps the
+    identities of the request's ``A_eq`` / ``A_ub`` objects to their
+    canonical stacked matrix, so requests that pass the same matrix objects
+    (every environment of a species in a dFBA rollout) canonicalise it once.
+    """
     c = np.asarray(objective, dtype=np.float64)
     if c.ndim != 1 or not len(c) or not np.isfinite(c).all():
         raise ValueError('A finite one-dimensional objective is required')
@@ -49,29 +55,52 @@ def normalize(objective, kwargs):
         raise ValueError('The batched engine supports continuous LPs only')
     if kwargs.get('method', 'highs-ds') not in ('highs', 'highs-ds'):
         raise ValueError('The request method must name HiGHS (highs or highs-ds)')
+    supplied = (kwargs.get('A_eq'), kwargs.get('A_ub'))
+    key = (id(supplied[0]), id(supplied[1]), n)
+    hit = None if _cache is None else _cache.get(key)
+    if hit is not None and not (hit[0][0] is supplied[0] and hit[0][1] is supplied[1]):
+        hit = None
     blocks, rhs = [], []
-    for matrix_name, rhs_name in (('A_eq', 'b_eq'), ('A_ub', 'b_ub')):
-        supplied = kwargs.get(matrix_name)
-        matrix = (csr_matrix((0, n), dtype=float) if supplied is None
-                  else csr_matrix(supplied, dtype=float))
-        if matrix.shape[1] != n or not np.isfinite(matrix.data).all():
-            raise ValueError('Invalid LP matrix')
+    for k, rhs_name in enumerate(('b_eq', 'b_ub')):
+        if hit is None:
+            matrix = (csr_matrix((0, n), dtype=float) if supplied[k] is None
+                      else csr_matrix(supplied[k], dtype=float))
+            if matrix.shape[1] != n or not np.isfinite(matrix.data).all():
+                raise ValueError('Invalid LP matrix')
+            blocks.append(matrix)
+            rows = matrix.shape[0]
+        else:
+            rows = hit[2][k]
         values = kwargs.get(rhs_name)
-        values = (np.empty(0) if values is None and not matrix.shape[0]
+        values = (np.empty(0) if values is None and not rows
                   else np.asarray(values, dtype=float))
-        if values.shape != (matrix.shape[0],) or not np.isfinite(values).all():
+        if values.shape != (rows,) or not np.isfinite(values).all():
             raise ValueError('Each matrix row requires a finite RHS')
-        blocks.append(matrix)
         rhs.append(values)
-    a = vstack(blocks, format='csr')
-    a.sum_duplicates()
-    a.eliminate_zeros()
-    a.sort_indices()
-    neq = blocks[0].shape[0]
+    if hit is None:
+        a = vstack(blocks, format='csr')
+        a.sum_duplicates()
+        a.eliminate_zeros()
+        a.sort_indices()
+        shapes = (blocks[0].shape[0], blocks[1].shape[0])
+        if _cache is not None:
+            # the entry keeps the objects alive, so their ids stay theirs
+            _cache[key] = (supplied, a, shapes)
+    else:
+        a, shapes = hit[1], hit[2]
+    neq = shapes[0]
     lower, upper = split_bounds(kwargs.get('bounds'), n)
     if np.isnan(lower).any() or np.isnan(upper).any() or (lower > upper).any():
         raise ValueError('Invalid variable bounds')
     return a, np.concatenate(rhs), lower, upper, c.copy(), neq
+
+
+def normalize_batch(requests):
+    """``normalize`` of every request of one batch, canonicalising each
+    distinct matrix object once.  The returned problems of requests that
+    share matrix objects share one canonical matrix (treat it as read-only)."""
+    cache = {}
+    return [normalize(c, kw, cache) for c, kw in requests]
 
 
 def request(problem, *, stage=None):

@@ -17,6 +17,17 @@ distributions of the batched-LP benchmark:
   as ``src/dfba_simulator.py:1080`` passes ``-c``).
 
 Column order is ``[exchange | internal | biomass]``.
+
+With the generator as specified the internal reactions do not conserve
+anything (random signs), so internal cycles can supply every biomass
+precursor and the biomass optimum is set by the internal bounds, not by
+uptake: every instance of a species has the same optimal value.
+``conserved=True`` draws positive metabolite weights ``w ~ U[0.5, 2]`` and
+rescales one entry of every internal column so that ``w . column = 0``:
+internal reactions then only move weight between metabolites, biomass
+(which consumes weight) must be paid for by uptake, and the per-instance
+uptake caps set the optimal value (``binding_species_workload``, a parity
+family whose objectives differ per instance).
 """
 
 from __future__ import annotations
@@ -52,8 +63,9 @@ class SpeciesModel:
 
 
 def species_matrix(m: int, n: int, *, n_exchange: int = 200, biomass_nnz: int = 60,
-                   seed: int = 0, name: str = "species"):
-    """Build one synthetic species (see module docstring)."""
+                   seed: int = 0, name: str = "species", conserved: bool = False):
+    """Build one synthetic species (see module docstring; ``conserved``:
+    internal reactions balanced against positive metabolite weights)."""
     if n < n_exchange + 2 or m < 6 or biomass_nnz > m:
         raise ValueError("species dimensions too small")
     rng = np.random.default_rng(seed)
@@ -71,6 +83,27 @@ def species_matrix(m: int, n: int, *, n_exchange: int = 200, biomass_nnz: int = 
     u = rng.random(total)
     mag = np.where(u < 0.85, 1.0, np.where(u < 0.95, 2.0, 0.5))
     sgn = np.where(rng.random(total) < 0.5, -1.0, 1.0)
+    if conserved:
+        # per column, the entry of the heaviest metabolite balances the rest;
+        # a balancing value below 0.05 in magnitude (a near-cancelling draw)
+        # flips the sign of another entry first
+        weight = conservation_weights(m, seed)
+        v = mag * sgn
+        pos = 0
+        for k in counts:
+            k = int(k)
+            wr = weight[r_int[pos:pos + k]]
+            vs = v[pos:pos + k]
+            j = int(np.argmax(wr))
+            q = (j + 1) % k
+            for _ in range(2):
+                vj = -(float(np.dot(wr, vs)) - wr[j] * vs[j]) / wr[j]
+                if abs(vj) >= 0.05:
+                    break
+                vs[q] = -vs[q]
+            vs[j] = vj
+            pos += k
+        mag, sgn = np.abs(v), np.sign(v)
     rows.append(r_int)
     cols.append(np.repeat(np.arange(n_exchange, n_exchange + n_int), counts))
     vals.append(mag * sgn)
@@ -95,6 +128,13 @@ def species_matrix(m: int, n: int, *, n_exchange: int = 200, biomass_nnz: int = 
                         n_exchange=n_exchange, biomass=n - 1), rng
 
 
+def conservation_weights(m: int, seed: int = 0) -> np.ndarray:
+    """The positive metabolite weights ``w`` of ``species_matrix(...,
+    conserved=True)`` with the same ``m`` and ``seed``: ``w . S[:, j] = 0``
+    for every internal column ``j``."""
+    return np.random.default_rng(seed + 15485863).uniform(0.5, 2.0, m)
+
+
 def exchange_batch(model: SpeciesModel, count: int, *, seed: int = 1):
     """Per-instance bounds for the single-species batch: exchange lower
     bounds ``-u_i`` with ``u_i ~ U[0, 20]`` drawn independently per instance.
@@ -116,12 +156,23 @@ def single_species_workload(count: int = 256, *, m: int = 1200, n: int = 2600, s
     return model, lower, upper
 
 
+def binding_species_workload(count: int = 256, *, m: int = 1200, n: int = 2600, seed: int = 0):
+    """The single-species batch on a weight-conserving species: uptake caps
+    ``u_i ~ U[0, 20]`` bind, so the optimal value differs per instance."""
+    model, _ = species_matrix(m, n, seed=seed, name="binding", conserved=True)
+    lower, upper = exchange_batch(model, count, seed=seed + 1)
+    return model, lower, upper
+
+
 COMMUNITY_SIZES = ((950, 1800), (1400, 2700), (1100, 2200))
 # Seed of the full-size community used for the cooperative (max-min growth)
 # LP: the lowest seed whose three members can all grow at default bounds
 # (seed 0's first member cannot, which pins the max-min growth at 0 and
 # makes every cooperative LP's optimum the zero flux).
 COOPERATIVE_SEED = 11
+# Seed of the weight-conserving (uptake-binding) community: the lowest seed
+# whose three conserved members all grow at the initial media.
+BINDING_SEED = 2
 LARGE_SIZES = ((3000, 6000), (2500, 5200), (3400, 6800))
 MEDIUM_SIZE = 40
 MEDIUM_PER_SPECIES = 25
@@ -129,7 +180,7 @@ MEDIUM_PER_SPECIES = 25
 
 def community_models(sizes=COMMUNITY_SIZES, *, seed: int = 0, n_medium: int = MEDIUM_SIZE,
                      per_species: int = MEDIUM_PER_SPECIES, fixed_fraction: float = 0.0,
-                     duplicate_fraction: float = 0.0):
+                     duplicate_fraction: float = 0.0, conserved: bool = False):
     """Three species sharing an ``n_medium``-metabolite medium.
 
     Each species maps ``per_species`` of its exchange columns onto a random
@@ -139,6 +190,8 @@ def community_models(sizes=COMMUNITY_SIZES, *, seed: int = 0, n_medium: int = ME
     the non-medium exchange bounds are fixed (``l = u``) and
     ``duplicate_fraction`` of the reversible internal reactions receive a
     parallel duplicate column (the scale/degeneracy stress workload).
+    ``conserved`` builds weight-conserving species (module docstring), whose
+    growth is limited by the Michaelis-Menten uptake of the medium.
 
     Fixed exchange values drawn independently (``U[0, 2]``) make most draws
     infeasible (measured: with secretions fixed two of the three large
@@ -158,7 +211,7 @@ def community_models(sizes=COMMUNITY_SIZES, *, seed: int = 0, n_medium: int = ME
             # Reserve columns for duplicates so that the total column count
             # stays at n: build a narrower matrix, then append duplicates.
             dup = int(round(duplicate_fraction * 0.3 * (n - 201)))
-        model, _ = species_matrix(m, n - dup, seed=seed * 101 + k, name=f"species{k}")
+        model, _ = species_matrix(m, n - dup, seed=seed * 101 + k, name=f"species{k}", conserved=conserved)
         if dup:
             reversible = np.flatnonzero(model.lower[model.n_exchange:model.biomass] < 0) + model.n_exchange
             pick = rng.choice(reversible, dup, replace=False)

@@ -296,6 +296,19 @@ int fbalp_prepare_matrix(int32_t rows, int32_t cols, const int64_t* indptr,
  * its `timing` dicts (`src/gpu_pdhg_corrector.py:392-405`). */
 int fbalp_engine_phase_times(fbalp_engine* engine, float* ms_fp32, float* ms_fp64);
 
+/* Timing slots (benchmark instrumentation): create `slots` (0..64) pairs of
+ * CUDA events per precision phase (previous slots are destroyed).  While a
+ * slot is selected with fbalp_engine_use_timing_slot (-1 selects none), every
+ * phase launch of fbalp_engine_solve is bracketed by that slot's events;
+ * under stream capture they become external event nodes of the graph, so
+ * each replay of the graph re-records them.  fbalp_engine_slot_times waits
+ * for the slot's last recorded launch and returns its device times (0 for a
+ * phase the slot never bracketed).  Lets a benchmark time the PDHG launches
+ * of graph-replayed solves without leaving the graph. */
+int fbalp_engine_timing_slots(fbalp_engine* engine, int32_t slots);
+int fbalp_engine_use_timing_slot(fbalp_engine* engine, int32_t slot);
+int fbalp_engine_slot_times(fbalp_engine* engine, int32_t slot, float* ms_fp32, float* ms_fp64);
+
 /* After a MIXED solve: copy the per-instance FP32-phase iteration counts into
  * the DEVICE array `out_fp32_iterations[count]` (asynchronous). */
 int fbalp_engine_phase_iterations(fbalp_engine* engine, int32_t* out_fp32_iterations);

@@ -59,3 +59,37 @@ def dual_objective(a, rhs, lower, upper, c, neq, y):
     term = np.where(r > 0, np.where(np.isfinite(lower), r * lower, 0.0),
                     np.where(r < 0, np.where(np.isfinite(upper), r * upper, 0.0), 0.0))
     return float(rhs @ y + term.sum())
+
+
+def certificate_rows(a, rhs, lower, upper, c, neq, X, Y):
+    """``certificate`` of many instances that share the matrix ``a``: row
+    ``i`` of ``X`` / ``Y`` (and of ``rhs``, ``lower``, ``upper``, ``c`` when
+    they are 2-D; 1-D ones are shared) is one instance.  Returns arrays of the
+    primal residual, dual violation and relative KKT gap per instance, with
+    the formulas (and operation order per instance) of ``certificate``."""
+    X = np.asarray(X, dtype=float)
+    Y = np.asarray(Y, dtype=float)
+    E = X.shape[0]
+    lower = np.broadcast_to(lower, X.shape)
+    upper = np.broadcast_to(upper, X.shape)
+    c = np.broadcast_to(c, X.shape)
+    rhs = np.broadcast_to(rhs, Y.shape)
+    activity = np.asarray((a @ X.T).T)
+    reduced = c - np.asarray((a.T @ Y.T).T)
+    row_error = activity - rhs
+    zero = np.zeros(E)
+    primal = np.maximum.reduce([zero,
+                                np.abs(row_error[:, :neq]).max(axis=1, initial=0.0),
+                                row_error[:, neq:].max(axis=1, initial=0.0),
+                                (lower - X).max(axis=1, initial=0.0),
+                                (X - upper).max(axis=1, initial=0.0)])
+    dual = np.maximum.reduce([zero,
+                              Y[:, neq:].max(axis=1, initial=0.0),
+                              np.where(~np.isfinite(lower), reduced, 0.0).max(axis=1, initial=0.0),
+                              np.where(~np.isfinite(upper), -reduced, 0.0).max(axis=1, initial=0.0)])
+    target = np.where(reduced >= 0.0, lower, upper)
+    bound_gap = np.abs(reduced * (X - np.where(np.isfinite(target), target, X))).sum(axis=1)
+    row_gap = np.abs(Y[:, neq:] * (rhs - activity)[:, neq:]).sum(axis=1)
+    objective = (c * X).sum(axis=1)
+    gap = (bound_gap + row_gap) / np.maximum(1.0, np.abs(objective))
+    return primal, dual, gap

@@ -25,6 +25,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
+from tests.golden._reference import reference_root  # noqa: E402
 from co_cultivation_metabolic_atlas_b200 import synthetic as syn  # noqa: E402
 
 
@@ -53,7 +54,7 @@ def cases():
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = Path(sys.argv[1] if len(sys.argv) > 1 else reference_root())
     sys.path.insert(0, str(ref))
     from src.lp_equality_reduction import HomogeneousEqualityReduction
     blob = {}

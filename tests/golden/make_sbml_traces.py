@@ -33,6 +33,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
+from tests.golden._reference import reference_root  # noqa: E402
 from co_cultivation_metabolic_atlas_b200 import lp_trace, sbml  # noqa: E402
 
 MODELS = {
@@ -90,4 +91,4 @@ def main(reference):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else reference_root())

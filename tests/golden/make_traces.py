@@ -28,6 +28,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
+from tests.golden._reference import reference_root  # noqa: E402
 from co_cultivation_metabolic_atlas_b200 import synthetic as syn  # noqa: E402
 from oracle import highs  # noqa: E402
 
@@ -49,7 +50,7 @@ def problems():
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = Path(sys.argv[1] if len(sys.argv) > 1 else reference_root())
     sys.path.insert(0, str(ref))
     from src.cpu_repeated_lp import _problem
     from src.lp_trace import load_trace_lp, problem_hash, problem_request, write_trace_lp

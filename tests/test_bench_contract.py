@@ -33,10 +33,26 @@ def test_reference_arm_line(workload, extra):
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
-    assert d["data"] == "synthetic" and "workload" in d["config"]
+    assert d["data"].startswith("synthetic") and "workload" in d["config"]
     assert d["ms_per_step"] > 0 and d["vs_baseline"] is None
 
 
 def test_reference_arm_other_ranks_print_nothing():
     assert run_bench("--impl", "reference", "--steps", "1", "--warmup", "0", "--envs", "16",
                      env={"RANK": "1"}) == []
+
+
+def test_reference_arm_step_is_the_bounded_sample():
+    """The reference arm's step is its bounded HiGHS sample: ms_per_step is
+    that sample's wall time, and the full step's time is a projection."""
+    d = run_bench("--impl", "reference", "--steps", "1", "--warmup", "0", "--envs", "32", "--cpu-sample", "6")[0]
+    assert d["ms_per_step"] < d["projected_full_step_ms"]
+    assert d["config"]["lps_per_step"] == 96 and "sample" in d["step"]
+
+
+def test_gpus_flag_launches_that_many_ranks():
+    """``--gpus 2`` outside torchrun re-launches the command as two ranks on
+    this node; rank 0 alone prints the one line."""
+    lines = run_bench("--gpus", "2", "--impl", "reference", "--steps", "1", "--warmup", "0", "--envs", "16",
+                      "--cpu-sample", "6")
+    assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"

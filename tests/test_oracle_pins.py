@@ -241,3 +241,25 @@ def test_medium_exchange_fluxes_are_not_determined_by_the_lps():
     vmin = linprog(e, **kw).fun
     vmax = -linprog(-e, **kw).fun
     assert vmin == pytest.approx(lo[col], abs=1e-6) and vmax == pytest.approx(mdl.upper[col], rel=1e-6)
+
+
+def test_certificate_rows_equal_the_per_instance_certificate():
+    """The batched certificate restates ``certificate`` row by row (equality
+    and inequality rows, finite and infinite bounds)."""
+    from scipy.sparse import random as sprandom
+    rng = np.random.default_rng(5)
+    a = sprandom(30, 50, density=0.1, random_state=6, format="csr")
+    neq = 20
+    E = 7
+    X = rng.normal(size=(E, 50))
+    Y = rng.normal(size=(E, 30))
+    lower = np.where(rng.random(50) < 0.2, -np.inf, -1.0)
+    upper = np.where(rng.random(50) < 0.2, np.inf, 1.0)
+    c = rng.normal(size=(E, 50))
+    rhs = rng.normal(size=(E, 30))
+    p, d, g = certificate.certificate_rows(a, rhs, lower, upper, c, neq, X, Y)
+    for i in range(E):
+        ref = certificate.certificate(a, rhs[i], lower, upper, c[i], neq, X[i], Y[i])
+        assert p[i] == pytest.approx(ref["primal_residual"], rel=1e-13)
+        assert d[i] == pytest.approx(ref["dual_violation"], rel=1e-13)
+        assert g[i] == pytest.approx(ref["relative_kkt_gap"], rel=1e-12)

@@ -1,8 +1,10 @@
 """SBML reader: known answers from the reference's own tests on its
-consortium models (read when the reference checkout is present), and the
-committed real-model LP fixtures (always)."""
+consortium models (read when the reference checkout is named by the
+``FBALP_REFERENCE`` environment variable), and the committed real-model LP
+fixtures (always)."""
 
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -11,10 +13,10 @@ from scipy.optimize import linprog
 
 from co_cultivation_metabolic_atlas_b200 import lp_trace, sbml
 
-REFERENCE = Path("/root/reference")
+REFERENCE = Path(os.environ.get("FBALP_REFERENCE", "")) if os.environ.get("FBALP_REFERENCE") else None
 SBML_DIR = Path(__file__).resolve().parent / "golden" / "sbml"
-needs_reference = pytest.mark.skipif(not (REFERENCE / "models" / "sbml").is_dir(),
-                                     reason="reference models not present")
+needs_reference = pytest.mark.skipif(REFERENCE is None or not (REFERENCE / "models" / "sbml").is_dir(),
+                                     reason="reference models not present (set FBALP_REFERENCE)")
 
 
 def _open_growth(m):

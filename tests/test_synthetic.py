@@ -44,3 +44,33 @@ def test_large_species_with_fixed_and_duplicate_columns():
     for mdl in models:
         fixed = mdl.lower[:mdl.n_exchange] == mdl.upper[:mdl.n_exchange]
         assert abs(fixed.sum() - round(0.2 * (mdl.n_exchange - 25))) <= 1
+
+
+def test_conserved_species_balances_every_internal_reaction():
+    """``conserved=True``: every internal column is balanced against the
+    positive metabolite weights, so biomass can only be paid for by uptake."""
+    model, lower, upper = syn.binding_species_workload(4, m=300, n=650, seed=3)
+    w = syn.conservation_weights(300, 3)
+    S = model.S.tocsc()
+    internal = S[:, model.n_exchange:model.biomass]
+    np.testing.assert_allclose(w @ internal.toarray(), 0.0, atol=1e-12)
+    counts = np.diff(S.indptr)
+    assert counts[:model.n_exchange].tolist() == [1] * model.n_exchange
+    assert counts[model.n_exchange:model.biomass].min() >= 2 and counts[model.biomass] == 60
+    assert np.abs(internal.data).min() > 0.04
+    # the biomass column consumes weight
+    assert float(w @ S[:, model.biomass].toarray().ravel()) < 0
+
+
+def test_uptake_binds_in_the_conserved_family():
+    """The binding family's HiGHS optima differ per instance (uptake caps
+    set them), unlike the specification's generator, where every instance
+    of a species has the same optimum."""
+    from oracle import highs
+    model, lower, upper = syn.binding_species_workload(6, m=300, n=900, seed=3)
+    res, _ = highs.solve_batch([model.S] * 6, list(lower), list(upper), [model.cost] * 6, workers=2)
+    funs = np.array([r[1] for r in res])
+    assert all(r[0] == 0 for r in res) and np.ptp(funs) > 1e-2 * np.abs(funs).max()
+    spec, lo2, up2 = syn.single_species_workload(3, m=300, n=900, seed=3)
+    res2, _ = highs.solve_batch([spec.S] * 3, list(lo2), list(up2), [spec.cost] * 3, workers=2)
+    assert np.ptp([r[1] for r in res2]) < 1e-9
