@@ -425,10 +425,10 @@ def run_product(args):
     inst_its = int(it.sum())
     tpi = profiled_traffic()
     traffic = None if tpi is None else tpi * inst_its / it.shape[0]
-    kname = {"mixed": "pdhg_recentred", "fp32": "pdhg_persistent<float>", "fp64": "pdhg_persistent<double>"}
+    first_kernel, fp64_kernel = com.engine.phase_kernels()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} copy bandwidth",
-                "kernel": kname[args.precision], "algorithmic_bytes": sum(step_bytes) / len(step_bytes),
+                "kernel": first_kernel, "fp64_phase_kernel": fp64_kernel, "algorithmic_bytes": sum(step_bytes) / len(step_bytes),
                 "kernel_ms": kernel_total_ms / len(kernel_ms), "kernel_share_of_step": kernel_total_ms / ms,
                 "instance_iterations_per_launch": inst_its / it.shape[0],
                 "measured_on": f"the {args.steps} timed steps (CUDA events around each step's PDHG launches)"}

@@ -46,7 +46,8 @@ class Options(ctypes.Structure):
     _fields_ = [("ruiz_iterations", ctypes.c_int32), ("power_iterations", ctypes.c_int32),
                 ("step_safety", ctypes.c_double), ("warps_per_block", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("max_dynamic_smem", ctypes.c_int32),
-                ("stage_matrix", ctypes.c_int32), ("fp64_max_dynamic_smem", ctypes.c_int32)]
+                ("stage_matrix", ctypes.c_int32), ("fp64_max_dynamic_smem", ctypes.c_int32),
+                ("pair_instances", ctypes.c_int32)]
 
 
 class SolveParams(ctypes.Structure):
@@ -59,6 +60,10 @@ class SolveParams(ctypes.Structure):
                 ("fp32_stall_checks", ctypes.c_int32), ("fp64_stall_checks", ctypes.c_int32),
                 ("floor_tol", ctypes.c_double), ("fp32_passthrough_tol", ctypes.c_double),
                 ("fallback_iterations", ctypes.c_int32), ("fp32_recentre", ctypes.c_int32)]
+
+
+KERNEL_NAMES = {-1: None, 0: "pdhg_persistent<float>", 1: "pdhg_persistent<double>", 2: "pdhg_recentred<staged>",
+                3: "pdhg_recentred<streamed>", 4: "pdhg_recentred_pair"}
 
 
 class NativeError(RuntimeError):
@@ -109,6 +114,7 @@ def load(path: os.PathLike | None = None):
         "fbalp_engine_phase_times": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_float),
                                                     ctypes.POINTER(ctypes.c_float)]),
         "fbalp_engine_phase_iterations": (ctypes.c_int, [vp, vp]),
+        "fbalp_engine_phase_kernels": (ctypes.c_int, [vp, c_int32_p, c_int32_p]),
         "fbalp_engine_timing_slots": (ctypes.c_int, [vp, ctypes.c_int32]),
         "fbalp_engine_use_timing_slot": (ctypes.c_int, [vp, ctypes.c_int32]),
         "fbalp_engine_slot_times": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_float),

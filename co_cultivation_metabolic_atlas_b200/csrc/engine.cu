@@ -85,6 +85,7 @@ void fbalp_default_options(fbalp_options* o) {
     o->max_dynamic_smem = 0;
     o->stage_matrix = 1;
     o->fp64_max_dynamic_smem = 0;
+    o->pair_instances = 1;
 }
 
 void fbalp_default_solve_params(fbalp_solve_params* p) {
@@ -121,6 +122,7 @@ static bool valid_options(const fbalp_options& o, std::string* err) {
     if (o.max_dynamic_smem < 0) return *err = "max_dynamic_smem must be non-negative", false;
     if (o.stage_matrix != 0 && o.stage_matrix != 1) return *err = "stage_matrix must be 0 or 1", false;
     if (o.fp64_max_dynamic_smem < 0) return *err = "fp64_max_dynamic_smem must be non-negative", false;
+    if (o.pair_instances != 0 && o.pair_instances != 1) return *err = "pair_instances must be 0 or 1", false;
     return true;
 }
 
@@ -308,9 +310,12 @@ int fbalp_engine_set_instances(fbalp_engine* e, int64_t count, const int32_t* sp
     // longest instances first: better balance for the persistent queue
     std::vector<int32_t> ord(count);
     std::iota(ord.begin(), ord.end(), 0);
+    // (species of equal size stay grouped: the paired kernel restages when
+    // the species changes)
     std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) {
         const SpeciesHost &a = e->species[hs[x]], &b = e->species[hs[y]];
-        return (a.A.off.back() + a.AT.off.back()) > (b.A.off.back() + b.AT.off.back());
+        const int64_t sa = a.A.off.back() + a.AT.off.back(), sb = b.A.off.back() + b.AT.off.back();
+        return sa != sb ? sa > sb : hs[x] < hs[y];
     });
     try {
         e->inst_species.ensure(count * sizeof(int32_t));
@@ -491,8 +496,34 @@ int recentred_mode(fbalp_engine* e) {
     return staged ? 1 : (streamed ? 2 : 0);
 }
 
+// The paired re-centred kernel (mode 3) instead of the staged one: enabled,
+// reflection 1, no patched entries, every species of the batch fits the
+// paired layout, and at least two instances per CTA of a full grid (below
+// that, one instance per CTA keeps more SMs busy).
+bool pair_mode(fbalp_engine* e, double reflection, bool patched) {
+    if (!e->opt.pair_instances || reflection != 1.0 || patched) return false;
+    if (e->count < 2 * static_cast<int64_t>(e->sm_count)) return false;
+    const int threads = e->opt.warps_per_block * 32;
+    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
+                      ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
+    if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
+    std::vector<char> used(e->species.size(), 0);
+    for (int32_t s : e->h_species) used[s] = 1;
+    for (size_t s = 0; s < e->species.size(); ++s) {
+        if (!used[s]) continue;
+        const SpeciesHost& sh = e->species[s];
+        if (!sh.A.nslices && !sh.AT.nslices) return false;
+        if (!fbalp::plan_layout_pair(sh.n, sh.m, sh.neq, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                     sh.A.off.back(), sh.AT.off.back(), cap).layout.recentred)
+            return false;
+    }
+    return true;
+}
+
 // Launch one precision phase over the bound batch (`recentred`: the
-// re-centred FP32 kernel in mode 1 (staged matrix) or 2 (streamed)).
+// re-centred FP32 kernel in mode 1 (staged matrix), 2 (streamed) or 3
+// (staged, two instances per CTA)).
 void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred = 0) {
     const int esz = fp64 ? static_cast<int>(sizeof(double)) : static_cast<int>(sizeof(float));
     const int threads = e->opt.warps_per_block * 32;
@@ -521,7 +552,10 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     for (size_t s = 0; s < e->species.size(); ++s) {
         if (!used[s]) continue;
         const SpeciesHost& sh = e->species[s];
-        fbalp::LayoutPlan P = recentred
+        fbalp::LayoutPlan P = recentred == 3
+            ? fbalp::plan_layout_pair(sh.n, sh.m, sh.neq, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
+                                      sh.A.off.back(), sh.AT.off.back(), cap)
+            : recentred
             ? fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
                                            sh.A.off.back(), sh.AT.off.back(), cap, recentred == 1)
             : unscaled
@@ -553,8 +587,10 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
         cached = layouts;
     }
     const bool patched = recentred && p.patch_values != nullptr;
-    const void* k = recentred ? fbalp::recentred_symbol(threads, recentred == 1, patched)
-                              : fbalp::kernel_symbol(fp64, threads, all_fast);
+    const bool pair = recentred == 3;
+    const void* k = pair ? fbalp::pair_symbol(threads)
+                         : recentred ? fbalp::recentred_symbol(threads, recentred == 1, patched)
+                                     : fbalp::kernel_symbol(fp64, threads, all_fast);
     // the dynamic shared-memory limit is a property of the kernel in this
     // process (shared by every engine): raise it when this launch needs
     // more, never lower it
@@ -571,12 +607,16 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
                         ", dynamic shared memory " + std::to_string(dyn) + " B, static " +
                         std::to_string(fa.sharedSizeBytes) + " B, registers " + std::to_string(fa.numRegs) +
                         ", opt-in limit " + std::to_string(e->smem_optin) + " B)");
-    const int grid = static_cast<int>(std::min<int64_t>(e->count, static_cast<int64_t>(per_sm) * e->sm_count));
+    // the paired kernel holds two instances (and two slabs) per CTA
+    const int64_t per_cta = pair ? 2 : 1;
+    const int grid = static_cast<int>(std::min<int64_t>((e->count + per_cta - 1) / per_cta,
+                                                        static_cast<int64_t>(per_sm) * e->sm_count));
     p.layouts = static_cast<const fbalp::Layout*>(dl.ptr);
     if (slab > 0) {
-        if (capturing && e->spill.bytes < static_cast<size_t>(slab) * grid)
+        const size_t want = static_cast<size_t>(slab) * per_cta * grid;
+        if (capturing && e->spill.bytes < want)
             throw CudaError("workspace would grow during stream capture; solve once before capturing");
-        e->spill.ensure(static_cast<size_t>(slab) * grid);
+        e->spill.ensure(want);
         p.spill = static_cast<unsigned char*>(e->spill.ptr);
         p.spill_stride = slab;
     } else {
@@ -594,7 +634,9 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     cudaEvent_t* sev = e->slot >= 0 ? &e->slot_ev[4 * static_cast<size_t>(e->slot)] : nullptr;
     const unsigned rec_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     if (sev) check(cudaEventRecordWithFlags(sev[2 * ph], e->stream, rec_flags), "timing slot record");
-    if (recentred)
+    if (pair)
+        check(fbalp::launch_pair(grid, threads, dyn, e->stream, p), "paired re-centred pdhg kernel launch");
+    else if (recentred)
         check(fbalp::launch_recentred(recentred == 1, patched, grid, threads, dyn, e->stream, p),
               "re-centred pdhg kernel launch");
     else
@@ -606,6 +648,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     if (!capturing) check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
     e->ran[ph] = !capturing;
     e->last_grid[fp64 ? 1 : 0] = grid;
+    e->last_kind[fp64 ? 1 : 0] = kind;
     e->last_smem[fp64 ? 1 : 0] = dyn;
 }
 
@@ -628,6 +671,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
     if (!valid_params(q, &err)) return fail(FBALP_ERR_INVALID, err);
     try {
         e->ran[0] = e->ran[1] = false;
+        e->last_kind[0] = e->last_kind[1] = -1;
         fbalp::KernelParams p{};
         p.species = e->dev_species;
         p.count = static_cast<int32_t>(e->count);
@@ -714,7 +758,8 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             pr.patch_values = patched ? e->patch_values : nullptr;
             pr.patch_stride = e->patch_stride;
             if (patched) pr.handoff_on_stall = 0;  // the FP64 phase has no patched entries
-            run_phase(e, false, pr, recentred_mode(e));
+            const int mode = recentred_mode(e);
+            run_phase(e, false, pr, mode == 1 && pair_mode(e, q.reflection, patched) ? 3 : mode);
             fbalp::KernelParams p64 = p;
             p64.order = static_cast<const int32_t*>(e->hand_list.ptr);
             p64.count_dev = static_cast<const int32_t*>(e->hand_count.ptr);
@@ -814,6 +859,13 @@ extern "C" int fbalp_engine_phase_times(fbalp_engine* e, float* ms_fp32, float* 
         if (err == cudaSuccess) err = cudaEventElapsedTime(outs[ph], e->ev[2 * ph], e->ev[2 * ph + 1]);
         if (err != cudaSuccess) return fail(FBALP_ERR_CUDA, cudaGetErrorString(err));
     }
+    return FBALP_OK;
+}
+
+extern "C" int fbalp_engine_phase_kernels(fbalp_engine* e, int32_t* fp32_kind, int32_t* fp64_kind) {
+    if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
+    if (fp32_kind) *fp32_kind = e->last_kind[0];
+    if (fp64_kind) *fp64_kind = e->last_kind[1];
     return FBALP_OK;
 }
 

@@ -119,13 +119,15 @@ struct fbalp_engine {
     Buffer hand_list, hand_count;  // re-centred phase -> FP64 phase work list
     Buffer layout32_buf, layout64_buf;
     // device copies of the launch layouts, one per kernel kind (plain FP32,
-    // FP64, re-centred staged, re-centred streamed), uploaded only when their
+    // FP64, re-centred staged, re-centred streamed, paired re-centred),
+    // uploaded only when their
     // content changes: a solve that reuses them issues no host-to-device
     // copy, so it can be captured in a CUDA graph
-    Buffer layout_dev[4];
-    std::vector<fbalp::Layout> layout_host[4];
+    Buffer layout_dev[5];
+    std::vector<fbalp::Layout> layout_host[5];
     std::vector<fbalp::Layout> layouts32, layouts64;
     int last_grid[2] = {0, 0};
+    int last_kind[2] = {-1, -1};  // kernel kind of the last solve's phases (the layout_dev index)
     int64_t last_smem[2] = {0, 0};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase start/stop: fp32, fp64
     bool ran[2] = {false, false};
@@ -145,7 +147,7 @@ struct fbalp_engine {
         for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
                           &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill, &layout32_buf,
                           &layout64_buf, &hand_list, &hand_count, &layout_dev[0], &layout_dev[1],
-                          &layout_dev[2], &layout_dev[3]})
+                          &layout_dev[2], &layout_dev[3], &layout_dev[4]})
             b->release();
     }
 };

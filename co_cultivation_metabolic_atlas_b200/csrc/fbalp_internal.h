@@ -236,6 +236,80 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, 
     return P;
 }
 
+// Paired re-centred FP32 layout: two instances of one species share one CTA
+// and one staged copy of the species' packed matrix words.  Their vectors
+// are interleaved as float2 (component s = instance slot s): the gather
+// targets dxbar (n+1) and dy (m+1), then the packed words (16-bit index =
+// float2 element offset of the gather target from the start of shared
+// memory | BF16 value), then d, l - x^, u - x^ (n each), r (m) and the
+// inequality bound -y^ of the rows at and beyond neq (m - neq).  The
+// Halpern iterate x is not stored: with reflection 1 it equals w xbar, with
+// w the previous iteration's Halpern weight.  The slab holds ONE instance's
+// FP64 data (the re-centred slab); a CTA uses two consecutive slabs.
+// Returns recentred = 0 when the shared part does not fit.
+inline LayoutPlan plan_layout_pair(int n, int m, int neq, int warps, int a_nslices, int at_nslices,
+                                   int64_t a_elems, int64_t at_elems, int64_t smem_cap) {
+    LayoutPlan P{};
+    Layout& L = P.layout;
+    int64_t off = 0;
+    L.sched_a_off = off;
+    off += 4 * (warps + 1);
+    L.sched_at_off = off;
+    off += 4 * (warps + 1);
+    off = align_up(off, 16);
+    L.list_a = off;
+    off += static_cast<int64_t>(sizeof(int4)) * a_nslices;
+    L.list_at = off;
+    off += static_cast<int64_t>(sizeof(int4)) * at_nslices;
+    off = align_up(off, 16);
+    if (n + 1 >= 65536 || m + 1 >= 65536 || neq < 0 || neq > m) return P;
+    L.smem_mask = 0;
+    auto put = [&](int a, int64_t elems) {
+        L.arr[a] = off;
+        L.smem_mask |= 1 << a;
+        off += align_up(elems * 8, 16);
+    };
+    put(kXbar, int64_t(n) + 1);
+    put(kY, int64_t(m) + 1);
+    // every staged 16-bit index is a float2 element offset of a gather
+    // target from the start of shared memory
+    if (off / 8 > (int64_t(1) << 16) - 1) return P;
+    L.mat_a_idx = off;
+    off += align_up(4 * a_elems, 16);
+    L.mat_at_idx = off;
+    off += align_up(4 * at_elems, 16);
+    L.mat_a_val = L.mat_a_idx;
+    L.mat_at_val = L.mat_at_idx;
+    put(kC, n);
+    put(kL, n);
+    put(kU, n);
+    put(kB, m);
+    put(kYa, int64_t(m) - neq);
+    if (off > smem_cap) return P;
+    L.mat_smem = 1;
+    L.recentred = 2;
+    int64_t slab = 0;
+    for (int b = 0; b < 2; ++b) {
+        L.pt_x[b] = slab;
+        slab += align_up((int64_t(n) + 1) * 8, 16);
+        L.pt_y[b] = slab;
+        slab += align_up((int64_t(m) + 1) * 8, 16);
+    }
+    L.dcand = slab;
+    slab += align_up(int64_t(n) * 4, 16);
+    L.rcand = slab;
+    slab += align_up(int64_t(m) * 4, 16);
+    for (int64_t* o : {&L.sc_c, &L.sc_l, &L.sc_u}) {
+        *o = slab;
+        slab += align_up(int64_t(n) * 8, 16);
+    }
+    L.sc_b = slab;
+    slab += align_up(int64_t(m) * 8, 16);
+    P.smem_bytes = off;
+    P.slab_bytes = slab;
+    return P;
+}
+
 // Every region must start on a 16-byte boundary (int4 lists, FP64 arrays).
 inline bool layout_aligned(const Layout& L) {
     const int64_t offs[] = {L.sched_a_off, L.sched_at_off, L.list_a, L.list_at, L.mat_a_idx,
@@ -251,6 +325,8 @@ const void* kernel_symbol(bool fp64, int threads, bool fast);
 const void* recentred_symbol(int threads, bool staged, bool patched);
 cudaError_t launch_recentred(bool staged, bool patched, int grid, int threads, size_t smem, cudaStream_t stream,
                              const KernelParams& p);
+const void* pair_symbol(int threads);
+cudaError_t launch_pair(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p);
 cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,
                         const KernelParams& p);
 

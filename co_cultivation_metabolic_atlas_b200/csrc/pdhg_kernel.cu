@@ -957,11 +957,13 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fmaf(pt.v32[q], S[o.y + pt.row[q]], g);
         if (own) {
-            const float xn = clampT(xo - tau * (dj - g), lj, uj);
-            const float xb = xn + xn - xo;
+            // explicit roundings (no contraction choice left to the compiler):
+            // the paired kernel repeats them bit for bit
+            const float xn = clampT(__fmaf_rn(-tau, __fsub_rn(dj, g), xo), lj, uj);
+            const float xb = __fsub_rn(__fadd_rn(xn, xn), xo);
             S[o.xbar + j] = xb;
             const float xh = (rho == 1.0f) ? xb : (1.0f + rho) * xn - rho * xo;
-            S[o.x + j] = w * xh;  // the anchor is the base: dx_anchor = 0
+            S[o.x + j] = __fmul_rn(w, xh);  // the anchor is the base: dx_anchor = 0
             if (check) {
                 cx[j] = bx[j] + static_cast<double>(xn);
                 const double d = static_cast<double>(xn) - static_cast<double>(xo);
@@ -992,10 +994,10 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fmaf(pt.v32[q], S[o.xbar + pt.col[q]], h);
         if (own) {
-            float yn = yo + sigma * (ri - h);
+            float yn = __fmaf_rn(sigma, __fsub_rn(ri, h), yo);
             if (i >= neq && yn > yl) yn = yl;  // y^ + dy <= 0
-            const float yh = (rho == 1.0f) ? yn + yn - yo : (1.0f + rho) * yn - rho * yo;
-            S[o.y + i] = w * yh;
+            const float yh = (rho == 1.0f) ? __fsub_rn(__fadd_rn(yn, yn), yo) : (1.0f + rho) * yn - rho * yo;
+            S[o.y + i] = __fmul_rn(w, yh);
             if (check) {
                 cy[i] = by[i] + static_cast<double>(yn);
                 const double d = static_cast<double>(yn) - static_cast<double>(yo);
@@ -1494,6 +1496,670 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Paired re-centred FP32 PDHG: two instances of one species per CTA.
+//
+// The arithmetic of pdhg_recentred (reflection 1, staged matrix, no patched
+// entries) applied to two instances at once.  Their FP32 vectors are
+// interleaved as float2 in shared memory (component s belongs to instance
+// slot s), so every packed matrix word read from shared memory serves both
+// instances and one 64-bit shared load gathers both instances' operands:
+// the species' matrix multiplies a block of two vectors (a sparse matrix
+// times a dense n x 2 block) instead of one.  Each slot runs its own solve
+// -- iteration count, Halpern weight, step sizes, restarts, convergence
+// tests, FP64 slab and work-queue instance -- with the operations of
+// pdhg_recentred in the same order, so a slot's iterates equal the
+// single-instance kernel's bit for bit.  The Halpern iterate x is not
+// stored: with reflection 1 it is w xbar (w the previous iteration's
+// Halpern weight), which is how pdhg_recentred computes it.  A slot whose
+// instance finishes takes the next queued instance of the staged species;
+// an instance of another species waits until both slots are free, then the
+// CTA restages.  A free slot's vectors are zero (step sizes and weights
+// zero), so it computes zeros beside the busy one.
+// ---------------------------------------------------------------------------
+
+struct PairOffsets {
+    int xbar, y, c, l, u, b, ya;  // float2 element offsets from the start of shared memory
+};
+
+__device__ __forceinline__ PairOffsets pair_offsets(const Layout& L) {
+    PairOffsets o;
+    o.xbar = static_cast<int>(L.arr[kXbar] / 8);
+    o.y = static_cast<int>(L.arr[kY] / 8);
+    o.c = static_cast<int>(L.arr[kC] / 8);
+    o.l = static_cast<int>(L.arr[kL] / 8);
+    o.u = static_cast<int>(L.arr[kU] / 8);
+    o.b = static_cast<int>(L.arr[kB] / 8);
+    o.ya = static_cast<int>(L.arr[kYa] / 8);
+    return o;
+}
+
+// Stage a species for the paired kernel: schedule lists, packed words with
+// the indices pre-offset to the float2 gather targets, and every vector
+// region zeroed (both slots free).
+__device__ void stage_species_pair(const DevSpecies* sp, const Layout& L, unsigned char* sm, int warps) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int32_t* soa = reinterpret_cast<int32_t*>(sm + L.sched_a_off);
+    int32_t* sot = reinterpret_cast<int32_t*>(sm + L.sched_at_off);
+    for (int w = tid; w <= warps; w += nt) {
+        soa[w] = sp->a_sched_off[w];
+        sot[w] = sp->at_sched_off[w];
+    }
+    int4* la = reinterpret_cast<int4*>(sm + L.list_a);
+    int4* lt = reinterpret_cast<int4*>(sm + L.list_at);
+    for (int t = tid; t < sp->a_nslices; t += nt) la[t] = sp->a_list[t];
+    for (int t = tid; t < sp->at_nslices; t += nt) lt[t] = sp->at_list[t];
+    uint32_t* pa = reinterpret_cast<uint32_t*>(sm + L.mat_a_idx);
+    uint32_t* pt = reinterpret_cast<uint32_t*>(sm + L.mat_at_idx);
+    const uint32_t a_add = static_cast<uint32_t>(L.arr[kXbar] / 8), t_add = static_cast<uint32_t>(L.arr[kY] / 8);
+    for (int64_t e = tid; e < sp->a_elems; e += nt) {
+        const uint32_t w = sp->a_pk[e];
+        pa[e] = (w & 0xffff0000u) | ((w & 0xffffu) + a_add);
+    }
+    for (int64_t e = tid; e < sp->at_elems; e += nt) {
+        const uint32_t w = sp->at_pk[e];
+        pt[e] = (w & 0xffff0000u) | ((w & 0xffffu) + t_add);
+    }
+    float2* const S2 = reinterpret_cast<float2*>(sm);
+    const PairOffsets o = pair_offsets(L);
+    const int n = sp->n, m = sp->m, mi = sp->m - sp->neq;
+    const float2 z = make_float2(0.0f, 0.0f);
+    for (int j = tid; j <= n; j += nt) S2[o.xbar + j] = z;  // [n]: the padding target
+    for (int i = tid; i <= m; i += nt) S2[o.y + i] = z;     // [m]: the padding target
+    for (int j = tid; j < n; j += nt) {
+        S2[o.c + j] = z;
+        S2[o.l + j] = z;
+        S2[o.u + j] = z;
+    }
+    for (int i = tid; i < m; i += nt) S2[o.b + i] = z;
+    for (int i = tid; i < mi; i += nt) S2[o.ya + i] = z;
+}
+
+// Slice product of the packed words against both slots' gather targets:
+// per slot the accumulation of slice_dot_pk (even k into a0, odd k into a1,
+// then a0 + a1).
+__device__ __forceinline__ float2 slice_dot_pk2(const uint32_t* wp, const float2* g, int len) {
+    float a0x = 0.0f, a0y = 0.0f, a1x = 0.0f, a1y = 0.0f;
+    int k = 0;
+    for (; k + 4 <= len; k += 4, wp += 128) {
+        const uint32_t w0 = wp[0], w1 = wp[32], w2 = wp[64], w3 = wp[96];
+        const float2 g0 = g[w0 & 0xffffu], g1 = g[w1 & 0xffffu], g2 = g[w2 & 0xffffu], g3 = g[w3 & 0xffffu];
+        const float v0 = __uint_as_float(w0 & 0xffff0000u), v1 = __uint_as_float(w1 & 0xffff0000u);
+        const float v2 = __uint_as_float(w2 & 0xffff0000u), v3 = __uint_as_float(w3 & 0xffff0000u);
+        a0x = fmaf(v0, g0.x, a0x);
+        a0y = fmaf(v0, g0.y, a0y);
+        a1x = fmaf(v1, g1.x, a1x);
+        a1y = fmaf(v1, g1.y, a1y);
+        a0x = fmaf(v2, g2.x, a0x);
+        a0y = fmaf(v2, g2.y, a0y);
+        a1x = fmaf(v3, g3.x, a1x);
+        a1y = fmaf(v3, g3.y, a1y);
+    }
+    if (k + 2 <= len) {
+        const uint32_t w0 = wp[0], w1 = wp[32];
+        const float2 g0 = g[w0 & 0xffffu], g1 = g[w1 & 0xffffu];
+        const float v0 = __uint_as_float(w0 & 0xffff0000u), v1 = __uint_as_float(w1 & 0xffff0000u);
+        a0x = fmaf(v0, g0.x, a0x);
+        a0y = fmaf(v0, g0.y, a0y);
+        a1x = fmaf(v1, g1.x, a1x);
+        a1y = fmaf(v1, g1.y, a1y);
+        k += 2;
+        wp += 64;
+    }
+    if (k < len) {
+        const uint32_t w0 = wp[0];
+        const float2 g0 = g[w0 & 0xffffu];
+        const float v0 = __uint_as_float(w0 & 0xffff0000u);
+        a0x = fmaf(v0, g0.x, a0x);
+        a0y = fmaf(v0, g0.y, a0y);
+    }
+    return make_float2(a0x + a1x, a0y + a1y);
+}
+
+// One slot's FP64 slab: the re-centred slab of pdhg_recentred.
+struct PairSlab {
+    double *px0, *px1, *py0, *py1;
+    float *dcand, *rcand;
+    double *cs, *ls, *us, *bs;
+    __device__ double* X(int b) const { return b ? px1 : px0; }
+    __device__ double* Y(int b) const { return b ? py1 : py0; }
+};
+
+__device__ __forceinline__ PairSlab pair_slab(const KernelParams& p, const Layout& L, int slot) {
+    unsigned char* const base = p.spill + (2 * static_cast<int64_t>(blockIdx.x) + slot) * p.spill_stride;
+    PairSlab b;
+    b.px0 = reinterpret_cast<double*>(base + L.pt_x[0]);
+    b.px1 = reinterpret_cast<double*>(base + L.pt_x[1]);
+    b.py0 = reinterpret_cast<double*>(base + L.pt_y[0]);
+    b.py1 = reinterpret_cast<double*>(base + L.pt_y[1]);
+    b.dcand = reinterpret_cast<float*>(base + L.dcand);
+    b.rcand = reinterpret_cast<float*>(base + L.rcand);
+    b.cs = reinterpret_cast<double*>(base + L.sc_c);
+    b.ls = reinterpret_cast<double*>(base + L.sc_l);
+    b.us = reinterpret_cast<double*>(base + L.sc_u);
+    b.bs = reinterpret_cast<double*>(base + L.sc_b);
+    return b;
+}
+
+// Per-slot solve state (block-uniform: every thread holds the same values).
+struct PairSlot {
+    int inst;  // -1: free
+    int cur, ev, k, it, stall;
+    bool fell_back, early;
+    int64_t coff, roff;
+    double omega, eta, cinf, r_restart, r_prev, best_err;
+};
+
+__device__ __forceinline__ float& comp(float2* a, int slot) { return reinterpret_cast<float*>(a)[slot]; }
+
+__device__ __forceinline__ int lane_id() { return static_cast<int>(threadIdx.x & 31); }
+
+// Move slot `slot`'s base to (bx, by) (the candidate last evaluated): its
+// components of d, l - x^, u - x^, r, -y^ and zero differences.
+__device__ __forceinline__ void recentre_pair(const DevSpecies* sp, const PairOffsets& o, int slot, const double* bx,
+                                              const double* by, const float* dcand, const float* rcand,
+                                              const double* ls, const double* us) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
+    const int n = sp->n, m = sp->m, neq = sp->neq;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double xb = bx[j];
+        comp(S2 + o.c + j, slot) = dcand[j];
+        comp(S2 + o.l + j, slot) = static_cast<float>(ls[j] - xb);
+        comp(S2 + o.u + j, slot) = static_cast<float>(us[j] - xb);
+        comp(S2 + o.xbar + j, slot) = 0.0f;
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        comp(S2 + o.b + i, slot) = rcand[i];
+        if (i >= neq) comp(S2 + o.ya + (i - neq), slot) = static_cast<float>(-by[i]);
+        comp(S2 + o.y + i, slot) = 0.0f;
+    }
+}
+
+// Free slot `slot`: zero its vector components (it then computes zeros).
+__device__ __forceinline__ void clear_slot(const DevSpecies* sp, const PairOffsets& o, int slot) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
+    const int n = sp->n, m = sp->m, neq = sp->neq;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        comp(S2 + o.c + j, slot) = 0.0f;
+        comp(S2 + o.l + j, slot) = 0.0f;
+        comp(S2 + o.u + j, slot) = 0.0f;
+        comp(S2 + o.xbar + j, slot) = 0.0f;
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        comp(S2 + o.b + i, slot) = 0.0f;
+        if (i >= neq) comp(S2 + o.ya + (i - neq), slot) = 0.0f;
+        comp(S2 + o.y + i, slot) = 0.0f;
+    }
+}
+
+// Primal pass of both slots.  CHECK: some slot tests this iteration (c0 /
+// c1 say which); it then writes its candidate and accumulates pd[4 s + 0..1]
+// (|xn - x|^2 and |xn|^2).  xo = wp xbar (reflection 1).
+template <bool CHECK>
+__device__ __forceinline__ void primal_pass_pair(const PairOffsets& o, int pt_off, int lt_off, int t0, int t1, int n,
+                                                 float2 tau, float2 wp, bool c0, bool c1, const double* bx0,
+                                                 double* cx0, const double* bx1, double* cx1, double* pd) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
+    const uint32_t* const PT = reinterpret_cast<const uint32_t*>(dyn_smem + pt_off);
+    const int4* const atlist = reinterpret_cast<const int4*>(dyn_smem + lt_off);
+    const int lane = threadIdx.x & 31;
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = atlist[t];
+        const int j = (sl.x << 5) + lane;
+        const bool own = j < n;
+        const int jj = own ? j : 0;
+        const float2 xbo = S2[o.xbar + jj], dj = S2[o.c + jj], lj = S2[o.l + jj], uj = S2[o.u + jj];
+        const float2 g = slice_dot_pk2(PT + sl.y + lane, S2, sl.z);
+        if (own) {
+            const float xo0 = __fmul_rn(wp.x, xbo.x), xo1 = __fmul_rn(wp.y, xbo.y);
+            const float xn0 = clampT(__fmaf_rn(-tau.x, __fsub_rn(dj.x, g.x), xo0), lj.x, uj.x);
+            const float xn1 = clampT(__fmaf_rn(-tau.y, __fsub_rn(dj.y, g.y), xo1), lj.y, uj.y);
+            S2[o.xbar + j] = make_float2(__fsub_rn(__fadd_rn(xn0, xn0), xo0), __fsub_rn(__fadd_rn(xn1, xn1), xo1));
+            if (CHECK) {
+                if (c0) {
+                    cx0[j] = bx0[j] + static_cast<double>(xn0);
+                    const double d = static_cast<double>(xn0) - static_cast<double>(xo0);
+                    pd[0] += d * d;
+                    pd[1] += static_cast<double>(xn0) * static_cast<double>(xn0);
+                }
+                if (c1) {
+                    cx1[j] = bx1[j] + static_cast<double>(xn1);
+                    const double d = static_cast<double>(xn1) - static_cast<double>(xo1);
+                    pd[4] += d * d;
+                    pd[5] += static_cast<double>(xn1) * static_cast<double>(xn1);
+                }
+            }
+        }
+    }
+}
+
+// Dual pass of both slots (pd[4 s + 2..3] on check iterations).
+template <bool CHECK>
+__device__ __forceinline__ void dual_pass_pair(const PairOffsets& o, int pa_off, int la_off, int t0, int t1, int m,
+                                               int neq, float2 sigma, float2 w, bool c0, bool c1, const double* by0,
+                                               double* cy0, const double* by1, double* cy1, double* pd) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
+    const uint32_t* const PA = reinterpret_cast<const uint32_t*>(dyn_smem + pa_off);
+    const int4* const alist = reinterpret_cast<const int4*>(dyn_smem + la_off);
+    const int lane = threadIdx.x & 31;
+    for (int t = t0; t < t1; ++t) {
+        const int4 sl = alist[t];
+        const int i = (sl.x << 5) + lane;
+        const bool own = i < m;
+        const int ii = own ? i : 0;
+        const float2 yo = S2[o.y + ii], ri = S2[o.b + ii];
+        const float2 yl = (own && i >= neq) ? S2[o.ya + (i - neq)] : make_float2(0.0f, 0.0f);
+        const float2 h = slice_dot_pk2(PA + sl.y + lane, S2, sl.z);
+        if (own) {
+            float yn0 = __fmaf_rn(sigma.x, __fsub_rn(ri.x, h.x), yo.x);
+            float yn1 = __fmaf_rn(sigma.y, __fsub_rn(ri.y, h.y), yo.y);
+            if (i >= neq) {  // y^ + dy <= 0
+                if (yn0 > yl.x) yn0 = yl.x;
+                if (yn1 > yl.y) yn1 = yl.y;
+            }
+            S2[o.y + i] = make_float2(__fmul_rn(w.x, __fsub_rn(__fadd_rn(yn0, yn0), yo.x)),
+                                      __fmul_rn(w.y, __fsub_rn(__fadd_rn(yn1, yn1), yo.y)));
+            if (CHECK) {
+                if (c0) {
+                    cy0[i] = by0[i] + static_cast<double>(yn0);
+                    const double d = static_cast<double>(yn0) - static_cast<double>(yo.x);
+                    pd[2] += d * d;
+                    pd[3] += static_cast<double>(yn0) * static_cast<double>(yn0);
+                }
+                if (c1) {
+                    cy1[i] = by1[i] + static_cast<double>(yn1);
+                    const double d = static_cast<double>(yn1) - static_cast<double>(yo.y);
+                    pd[6] += d * d;
+                    pd[7] += static_cast<double>(yn1) * static_cast<double>(yn1);
+                }
+            }
+        }
+    }
+}
+
+// Everything a slot's solve needs besides its state (block-uniform).
+struct PairCtx {
+    const DevSpecies* sp;
+    const Layout* L;
+    PairOffsets o;
+    int pa_off, pt_off, la_off, lt_off;  // byte offsets into shared memory
+    int aw0, aw1, tw0, tw1, a_sub, t_sub;
+    __device__ const uint32_t* PA() const { return smem_at<uint32_t>(pa_off); }
+    __device__ const uint32_t* PT() const { return smem_at<uint32_t>(pt_off); }
+    __device__ const int4* alist() const { return smem_at<int4>(la_off); }
+    __device__ const int4* atlist() const { return smem_at<int4>(lt_off); }
+    template <typename T> __device__ static const T* smem_at(int off) {
+        extern __shared__ __align__(16) unsigned char dyn_smem[];
+        return reinterpret_cast<const T*>(dyn_smem + off);
+    }
+};
+
+// The slot's results (original units and order) from its last evaluated
+// point, then the slot is freed.  All threads call it.
+__device__ __noinline__ void finish_pair_slot(const KernelParams& p, const PairCtx& c, PairSlot& st, int slot, int status,
+                                 const Metrics& M) {
+    const DevSpecies* sp = c.sp;
+    const int n = sp->n, m = sp->m, tid = threadIdx.x, nthreads = blockDim.x;
+    const PairSlab b = pair_slab(p, *c.L, slot);
+    const bool hand = p.handoff_list != nullptr && status == kStatusHandoff;
+    const double* fx = b.X(st.ev);
+    const double* fy = b.Y(st.ev);
+    double* ox = hand ? p.hand_x : p.out_x;
+    double* oy = hand ? p.hand_y : p.out_y;
+    const int inst = st.inst;
+    const double* lo_i = p.lower + st.coff;
+    const double* up_i = p.upper + st.coff;
+    for (int j = tid; j < n; j += nthreads) {
+        const int jo = sp->col_perm[j];
+        double xv = fx[j] * sp->dc[j];
+        if (p.clip_output && !hand) {
+            const double lv = lo_i[jo], uv = up_i[jo];
+            xv = xv < lv ? lv : (xv > uv ? uv : xv);
+        }
+        ox[st.coff + jo] = xv;
+    }
+    for (int i = tid; i < m; i += nthreads) oy[st.roff + sp->row_perm[i]] = fy[i] * sp->dr[i];
+    if (tid == 0) {
+        if (p.hand_iters) p.hand_iters[inst] = st.it;
+        if (hand) {
+            p.hand_omega[inst] = st.omega;
+            p.handoff_list[atomicAdd(p.handoff_count, 1)] = inst;
+        } else {
+            double* mo = p.out_metrics + static_cast<int64_t>(inst) * kMetrics;
+            mo[0] = M.primal;
+            mo[1] = M.dual;
+            mo[2] = M.kgap;
+            mo[3] = M.pobj;
+            mo[4] = M.dobj;
+            mo[5] = M.rgap;
+            mo[6] = M.xinf;
+            mo[7] = st.omega;
+            p.out_obj[inst] = M.pobj;
+            p.out_status[inst] = status;
+            p.out_iters[inst] = st.it;
+            if (p.out_omega) p.out_omega[inst] = st.omega;
+        }
+    }
+    clear_slot(sp, c.o, slot);
+    st.inst = -1;
+    __syncthreads();  // the slab and the slot's components are reused
+}
+
+// Load instance `inst` into slot `slot`: scaled data, start point and its
+// test; a start point that already passes finishes the slot at once.  All
+// threads call it.
+__device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairCtx& c, PairSlot& st, int slot, int inst,
+                                double (*s_red)[kRed], double* s_tot) {
+    const DevSpecies* sp = c.sp;
+    const int n = sp->n, m = sp->m, neq = sp->neq, tid = threadIdx.x, nthreads = blockDim.x;
+    const PairSlab b = pair_slab(p, *c.L, slot);
+    const Patches nopatch{0, nullptr, nullptr, nullptr, nullptr};
+    st.inst = inst;
+    st.coff = p.col_off[inst];
+    st.roff = p.row_off[inst];
+    const double* lo_i = p.lower + st.coff;
+    const double* up_i = p.upper + st.coff;
+    const double* c_i = p.cost + st.coff;
+    const double* b_i = p.rhs ? p.rhs + st.roff : nullptr;
+    int bad = 0;
+    for (int j = tid; j < n; j += nthreads) {
+        const int jo = sp->col_perm[j];
+        const double dcj = sp->dc[j];
+        const double lv = lo_i[jo], uv = up_i[jo], cv = c_i[jo];
+        if (isnan(lv) || isnan(uv) || lv > uv || !isfinite(cv) || lv == INFINITY || uv == -INFINITY) bad = 1;
+        const double lsj = lv / dcj, usj = uv / dcj;
+        b.cs[j] = cv * dcj;
+        b.ls[j] = lsj;
+        b.us[j] = usj;
+        double x0 = p.warm_x ? p.warm_x[st.coff + jo] / dcj : 0.0;
+        if (!isfinite(x0)) x0 = 0.0;
+        b.px0[j] = x0 < lsj ? lsj : (x0 > usj ? usj : x0);
+    }
+    for (int i = tid; i < m; i += nthreads) {
+        const int io = sp->row_perm[i];
+        const double dri = sp->dr[i];
+        const double bv = b_i ? b_i[io] : 0.0;
+        if (!isfinite(bv)) bad = 1;
+        b.bs[i] = bv * dri;
+        double y0 = p.warm_y ? p.warm_y[st.roff + io] / dri : 0.0;
+        if (!isfinite(y0)) y0 = 0.0;
+        if (i >= neq && y0 > 0.0) y0 = 0.0;
+        b.py0[i] = y0;
+    }
+    if (tid == 0) {
+        b.px0[n] = 0.0;
+        b.px1[n] = 0.0;
+        b.py0[m] = 0.0;
+        b.py1[m] = 0.0;
+    }
+    bad = __syncthreads_or(bad);
+    st.omega = 1.0;
+    if (p.warm_omega) {
+        const double w0 = p.warm_omega[inst];
+        if (isfinite(w0) && w0 > 0.0) st.omega = w0;
+    }
+    if (bad) {
+        for (int j = tid; j < n; j += nthreads) p.out_x[st.coff + sp->col_perm[j]] = NAN;
+        for (int i = tid; i < m; i += nthreads) p.out_y[st.roff + sp->row_perm[i]] = NAN;
+        if (tid == 0) {
+            p.out_status[inst] = kStatusInvalid;
+            p.out_iters[inst] = 0;
+            if (p.hand_iters) p.hand_iters[inst] = 0;
+            p.out_obj[inst] = NAN;
+            for (int k = 0; k < kMetrics; ++k) p.out_metrics[static_cast<int64_t>(inst) * kMetrics + k] = NAN;
+            if (p.out_omega) p.out_omega[inst] = st.omega;
+        }
+        st.inst = -1;
+        __syncthreads();
+        return;
+    }
+    st.eta = sp->eta;
+    st.cur = 0;
+    st.ev = 0;
+    double v[kRed];
+#pragma unroll
+    for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
+    kkt_partials_recentred<true, false>(sp, c.PA(), c.PT(), c.alist(), c.atlist(), c.aw0, c.aw1, c.tw0, c.tw1, c.a_sub,
+                                        c.t_sub, b.px0, b.py0, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, true, lane_id(),
+                                        v, nopatch);
+    block_reduce(v, s_red, s_tot);
+    st.cinf = s_tot[14];
+    const Metrics M = evaluate(s_tot, st.omega, p.tol_p, p.tol_d, p.tol_g);
+    int status = -1;
+    if (M.conv) status = p.final_status;
+    else if (p.max_iters <= 0) status = M.nan ? kStatusNumerical : kStatusIterationLimit;
+    if (status >= 0) {
+        st.it = 0;
+        finish_pair_slot(p, c, st, slot, status, M);
+        return;
+    }
+    recentre_pair(sp, c.o, slot, b.px0, b.py0, b.dcand, b.rcand, b.ls, b.us);
+    st.k = 0;
+    st.it = 0;
+    st.stall = 0;
+    st.fell_back = false;
+    st.early = p.hint_iters == nullptr || p.hint_iters[inst] < p.check_every;
+    st.r_restart = INFINITY;
+    st.r_prev = INFINITY;
+    st.best_err = INFINITY;
+    __syncthreads();
+}
+
+// The convergence test of slot `slot` after a check iteration (its
+// candidate is in the buffer cur ^ 1): termination, stall, hand-off, cold
+// fallback and restart rules of pdhg_recentred.  All threads call it.
+__device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairCtx& c, PairSlot& st, int slot, bool full,
+                                const double* pd, double (*s_red)[kRed], double* s_tot) {
+    const DevSpecies* sp = c.sp;
+    const int n = sp->n, m = sp->m, tid = threadIdx.x, nthreads = blockDim.x;
+    const PairSlab b = pair_slab(p, *c.L, slot);
+    const Patches nopatch{0, nullptr, nullptr, nullptr, nullptr};
+    double v[kRed];
+#pragma unroll
+    for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
+    v[5] = pd[0];
+    v[6] = pd[2];
+    v[7] = pd[1];
+    v[8] = pd[3];
+    kkt_partials_recentred<true, false>(sp, c.PA(), c.PT(), c.alist(), c.atlist(), c.aw0, c.aw1, c.tw0, c.tw1, c.a_sub,
+                                        c.t_sub, b.X(st.cur ^ 1), b.Y(st.cur ^ 1), b.cs, b.ls, b.us, b.bs, b.dcand,
+                                        b.rcand, false, lane_id(), v, nopatch);
+    block_reduce(v, s_red, s_tot);
+    if (tid == 0) s_tot[14] = st.cinf;
+    __syncthreads();
+    const Metrics M = evaluate(s_tot, st.omega, p.tol_p, p.tol_d, p.tol_g);
+    const double nx = sqrt(s_tot[7]), ny = sqrt(s_tot[8]);
+    __syncthreads();  // s_tot is rewritten by the other slot's test
+    st.ev = st.cur ^ 1;
+    int status = -1;
+    if (M.nan || !isfinite(M.r)) status = kStatusNumerical;
+    else if (M.conv) status = p.final_status;
+    else if (st.it >= p.max_iters) status = kStatusIterationLimit;
+    if (status < 0 && full) {
+        const double e = fmax(fmax(M.primal / (1.0 + M.xinf), M.dual / (1.0 + M.cinf)), fmax(M.rgap, M.kgap));
+        if (e < 0.5 * st.best_err) {
+            st.best_err = e;
+            st.stall = 0;
+        } else {
+            ++st.stall;
+        }
+        if (p.stall_checks > 0 && st.stall >= p.stall_checks && e <= p.floor_tol &&
+            M.primal <= p.floor_tol * (1.0 + M.xinf) && M.dual <= p.floor_tol * (1.0 + M.cinf))
+            status = p.final_status;
+        else if (p.handoff_on_stall > 0 && st.stall >= p.handoff_on_stall)
+            status = kStatusHandoff;
+    }
+    if (status >= 0) {
+        finish_pair_slot(p, c, st, slot, status, M);
+        return;
+    }
+    if (!full) return;
+    if (p.fallback_iters > 0 && !st.fell_back && st.it >= p.fallback_iters &&
+        (p.warm_x != nullptr || p.warm_y != nullptr)) {
+        // cold fallback: evaluate the cold point in the candidate buffer
+        // and re-centre there
+        st.fell_back = true;
+        st.omega = 1.0;
+        double* cx = b.X(st.cur ^ 1);
+        double* cyv = b.Y(st.cur ^ 1);
+        for (int j = tid; j < n; j += nthreads) cx[j] = 0.0 < b.ls[j] ? b.ls[j] : (0.0 > b.us[j] ? b.us[j] : 0.0);
+        for (int i = tid; i < m; i += nthreads) cyv[i] = 0.0;
+        __syncthreads();
+        double vv[kRed];
+#pragma unroll
+        for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
+        kkt_partials_recentred<true, false>(sp, c.PA(), c.PT(), c.alist(), c.atlist(), c.aw0, c.aw1, c.tw0, c.tw1, c.a_sub,
+                                            c.t_sub, cx, cyv, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, false,
+                                            lane_id(), vv, nopatch);
+        block_reduce(vv, s_red, s_tot);
+        st.cur ^= 1;
+        st.ev = st.cur;
+        recentre_pair(sp, c.o, slot, b.X(st.cur), b.Y(st.cur), b.dcand, b.rcand, b.ls, b.us);
+        st.k = 0;
+        st.r_restart = INFINITY;
+        st.r_prev = INFINITY;
+        st.best_err = INFINITY;
+        st.stall = 0;
+        __syncthreads();
+        return;
+    }
+    if (p.restarts && (M.r <= kBetaSufficient * st.r_restart ||
+                       (M.r <= kBetaNecessary * st.r_restart && M.r > st.r_prev) || st.k >= kBetaArtificial * st.it)) {
+        if (nx > 1e-10 && ny > 1e-10)
+            st.omega = exp(kOmegaSmoothing * log(ny / nx) + (1.0 - kOmegaSmoothing) * log(st.omega));
+        st.cur ^= 1;  // the candidate becomes the base
+        recentre_pair(sp, c.o, slot, b.X(st.cur), b.Y(st.cur), b.dcand, b.rcand, b.ls, b.us);
+        st.k = 0;
+        st.r_restart = M.r;
+        st.r_prev = INFINITY;
+        __syncthreads();
+    } else {
+        st.r_prev = M.r;
+    }
+}
+
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    __shared__ double s_red[MAXT / 32][kRed];
+    __shared__ double s_tot[kRed];
+    __shared__ int s_q;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int warps = blockDim.x >> 5;
+    const int count = p.count_dev ? *p.count_dev : p.count;
+    PairSlot st[2];
+    st[0].inst = -1;
+    st[1].inst = -1;
+    int staged = -1, pending = -1;
+    bool drained = false;
+    PairCtx c{};
+
+    for (;;) {
+        // ---- fill the free slots from the work queue ----
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            while (st[s].inst < 0 && !drained) {
+                int q = pending;
+                if (q < 0) {
+                    if (tid == 0) s_q = atomicAdd(p.queue, 1);
+                    __syncthreads();
+                    q = s_q;
+                    __syncthreads();  // s_q is rewritten by the next fetch
+                }
+                if (q >= count) {
+                    drained = true;
+                    break;
+                }
+                const int inst = p.order[q];
+                const int species = p.inst_species[inst];
+                if (species != staged) {
+                    if (st[s ^ 1].inst >= 0) {  // the other slot still runs the staged species
+                        pending = q;
+                        break;
+                    }
+                    const Layout& L = p.layouts[species];
+                    stage_species_pair(p.species + species, L, dyn_smem, warps);
+                    __syncthreads();
+                    staged = species;
+                    c.sp = p.species + species;
+                    c.L = &p.layouts[species];
+                    c.o = pair_offsets(L);
+                    c.pa_off = static_cast<int>(L.mat_a_idx);
+                    c.pt_off = static_cast<int>(L.mat_at_idx);
+                    c.la_off = static_cast<int>(L.list_a);
+                    c.lt_off = static_cast<int>(L.list_at);
+                    const int32_t* soa = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_a_off);
+                    const int32_t* sot = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_at_off);
+                    c.aw0 = soa[warp];
+                    c.aw1 = soa[warp + 1];
+                    c.tw0 = sot[warp];
+                    c.tw1 = sot[warp + 1];
+                    c.a_sub = c.o.xbar;
+                    c.t_sub = c.o.y;
+                }
+                pending = -1;
+                start_pair_slot(p, c, st[s], s, inst, s_red, s_tot);
+            }
+        }
+        const bool a0 = st[0].inst >= 0, a1 = st[1].inst >= 0;
+        if (!a0 && !a1) {
+            if (pending >= 0) continue;
+            break;
+        }
+
+        // ---- one iteration of every busy slot ----
+        bool chk[2], full[2];
+        float tau[2], sig[2], w[2], wp[2];
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            PairSlot& t = st[s];
+            if (t.inst >= 0) {
+                ++t.it;
+                full[s] = (t.it % p.check_every == 0) || (t.it >= p.max_iters);
+                chk[s] = full[s] || (t.early && t.it >= 8 && t.it < p.check_every && (t.it & (t.it - 1)) == 0);
+                tau[s] = static_cast<float>(t.eta / t.omega);
+                sig[s] = static_cast<float>(t.eta * t.omega);
+                w[s] = static_cast<float>((t.k + 1.0) / (t.k + 2.0));
+                wp[s] = static_cast<float>(t.k / (t.k + 1.0));
+            } else {
+                full[s] = chk[s] = false;
+                tau[s] = sig[s] = w[s] = wp[s] = 0.0f;
+            }
+        }
+        const float2 tau2 = make_float2(tau[0], tau[1]), sig2 = make_float2(sig[0], sig[1]);
+        const float2 w2 = make_float2(w[0], w[1]), wp2 = make_float2(wp[0], wp[1]);
+        const int n = c.sp->n, m = c.sp->m, neq = c.sp->neq;
+        double pd[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) pd[q] = 0.0;
+        if (chk[0] || chk[1]) {
+            const PairSlab b0 = pair_slab(p, *c.L, 0), b1 = pair_slab(p, *c.L, 1);
+            primal_pass_pair<true>(c.o, c.pt_off, c.lt_off, c.tw0, c.tw1, n, tau2, wp2, chk[0], chk[1],
+                                   b0.X(st[0].cur), b0.X(st[0].cur ^ 1), b1.X(st[1].cur), b1.X(st[1].cur ^ 1), pd);
+            __syncthreads();
+            dual_pass_pair<true>(c.o, c.pa_off, c.la_off, c.aw0, c.aw1, m, neq, sig2, w2, chk[0], chk[1],
+                                 b0.Y(st[0].cur), b0.Y(st[0].cur ^ 1), b1.Y(st[1].cur), b1.Y(st[1].cur ^ 1), pd);
+        } else {
+            primal_pass_pair<false>(c.o, c.pt_off, c.lt_off, c.tw0, c.tw1, n, tau2, wp2, false, false, nullptr,
+                                    nullptr, nullptr, nullptr, pd);
+            __syncthreads();
+            dual_pass_pair<false>(c.o, c.pa_off, c.la_off, c.aw0, c.aw1, m, neq, sig2, w2, false, false, nullptr,
+                                  nullptr, nullptr, nullptr, pd);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+            if (st[s].inst >= 0) ++st[s].k;
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+            if (chk[s]) check_pair_slot(p, c, st[s], s, full[s], pd + 4 * s, s_red, s_tot);
+    }
+}
+
 #define FBALP_INSTANTIATE(MAXT)                                               \
     template __global__ void pdhg_persistent<float, MAXT, 0>(KernelParams);   \
     template __global__ void pdhg_persistent<float, MAXT, 1>(KernelParams);   \
@@ -1512,6 +2178,8 @@ template __global__ void pdhg_recentred<768, true, false>(KernelParams);
 template __global__ void pdhg_recentred<768, false, false>(KernelParams);
 template __global__ void pdhg_recentred<768, true, true>(KernelParams);
 template __global__ void pdhg_recentred<768, false, true>(KernelParams);
+template __global__ void pdhg_recentred_pair<512>(KernelParams);
+template __global__ void pdhg_recentred_pair<1024>(KernelParams);
 #undef FBALP_INSTANTIATE
 
 // Blocks of up to 512 threads use the variant with a 128-register budget,
@@ -1584,6 +2252,17 @@ cudaError_t launch_recentred(bool staged, bool patched, int grid, int threads, s
     if (threads <= 512) launch_recentred_for<512>(staged, patched, grid, threads, smem, stream, p);
     else if (threads <= 768) launch_recentred_for<768>(staged, patched, grid, threads, smem, stream, p);
     else launch_recentred_for<1024>(staged, patched, grid, threads, smem, stream, p);
+    return cudaGetLastError();
+}
+
+const void* pair_symbol(int threads) {
+    return threads <= 512 ? reinterpret_cast<const void*>(&pdhg_recentred_pair<512>)
+                          : reinterpret_cast<const void*>(&pdhg_recentred_pair<1024>);
+}
+
+cudaError_t launch_pair(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p) {
+    if (threads <= 512) pdhg_recentred_pair<512><<<grid, threads, smem, stream>>>(p);
+    else pdhg_recentred_pair<1024><<<grid, threads, smem, stream>>>(p);
     return cudaGetLastError();
 }
 

@@ -87,6 +87,7 @@ class EngineOptions:
     max_dynamic_smem: int = 0
     stage_matrix: bool = True
     fp64_max_dynamic_smem: int = 0
+    pair_instances: bool = True        # two instances per CTA in the re-centred phase where possible
 
     def native(self) -> N.Options:
         o = N.default_options()
@@ -98,6 +99,7 @@ class EngineOptions:
         o.max_dynamic_smem = int(self.max_dynamic_smem)
         o.stage_matrix = 1 if self.stage_matrix else 0
         o.fp64_max_dynamic_smem = int(self.fp64_max_dynamic_smem)
+        o.pair_instances = 1 if self.pair_instances else 0
         return o
 
 
@@ -304,6 +306,14 @@ class LPEngine:
         b = ctypes.c_float()
         N.check(self.lib.fbalp_engine_phase_times(self.handle, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def phase_kernels(self):
+        """Names of the kernels the last solve launched for its (first,
+        FP64) phases (None for a phase that did not run)."""
+        a = ctypes.c_int32()
+        b = ctypes.c_int32()
+        N.check(self.lib.fbalp_engine_phase_kernels(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return N.KERNEL_NAMES[a.value], N.KERNEL_NAMES[b.value]
 
     def timing_slots(self, slots: int):
         """Create ``slots`` timing slots (benchmark instrumentation)."""

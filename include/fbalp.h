@@ -94,6 +94,13 @@ typedef struct fbalp_options {
     int32_t fp64_max_dynamic_smem; /* cap for the FP64 phase (0 = same as
                                   max_dynamic_smem); a smaller cap spills the
                                   cold arrays and fits more CTAs per SM     */
+    int32_t pair_instances;    /* 1 (default): the re-centred phase runs two
+                                  instances of a species per CTA (one staged
+                                  matrix, interleaved vectors) when every
+                                  species fits that layout, the reflection is
+                                  1, no entries are patched and the batch has
+                                  at least two instances per CTA; 0: one
+                                  instance per CTA.  Same results.          */
 } fbalp_options;
 
 /* Solve parameters.  Replaces `iterations` / `check_interval` of
@@ -295,6 +302,16 @@ int fbalp_prepare_matrix(int32_t rows, int32_t cols, const int64_t* indptr,
  * instrumentation for benchmarks; the reference reports per-phase seconds in
  * its `timing` dicts (`src/gpu_pdhg_corrector.py:392-405`). */
 int fbalp_engine_phase_times(fbalp_engine* engine, float* ms_fp32, float* ms_fp64);
+
+/* Kernel kinds the last fbalp_engine_solve launched for its first (FP32 /
+ * re-centred) and FP64 phases: FBALP_KERNEL_* or -1 for a phase that did not
+ * run.  Instrumentation for tests and benchmarks. */
+#define FBALP_KERNEL_FP32 0
+#define FBALP_KERNEL_FP64 1
+#define FBALP_KERNEL_RECENTRED_STAGED 2
+#define FBALP_KERNEL_RECENTRED_STREAMED 3
+#define FBALP_KERNEL_RECENTRED_PAIRED 4
+int fbalp_engine_phase_kernels(fbalp_engine* engine, int32_t* fp32_kind, int32_t* fp64_kind);
 
 /* Timing slots (benchmark instrumentation): create `slots` (0..64) pairs of
  * CUDA events per precision phase (previous slots are destroyed).  While a
