@@ -1,10 +1,11 @@
 """Autotuner for the batched LP engine.
 
-The engine's launch shape and test period are tunable: warps per block (the
-SELL-32 slice schedule is rebalanced per warp count), the shared-memory cap
-(a smaller cap spills cold arrays and can fit more CTAs per SM for small
-species), and ``check_every``, the period of the FP64 convergence tests at
-which restarts are decided.  ``autotune`` times a seeded sample of the batch
+The engine's launch shape and test period are tunable: instances per CTA in
+the re-centred phase (1, or 2 sharing one staged matrix: the width of the
+sparse-matrix times dense-block tile), warps per block (the SELL-32 slice
+schedule, one lane per row, is rebalanced per warp count, which sets the
+rows each warp walks per pass), and ``check_every``, the period of the FP64
+convergence tests at which restarts are decided.  ``autotune`` times a seeded sample of the batch
 (every species represented, solved to the production tolerances) for every
 candidate and keeps the fastest per certified LP; results are cached in a
 JSON file keyed by the species matrices' shapes and nonzero counts and the
@@ -27,6 +28,7 @@ from .engine import EngineOptions, LPEngine, SolveConfig
 
 WARPS = (8, 16, 32)
 CHECK_EVERY = (32, 64, 128)
+PAIR = (True, False)
 
 
 def workload_key(matrices, device=None) -> str:
@@ -51,8 +53,8 @@ def _sample(species_id, count):
 
 
 def autotune(matrices, species_id, lower, upper, cost, col_offsets, *, config: SolveConfig | None = None,
-             sample=296, warps=WARPS, check_every=CHECK_EVERY, cache: str | Path | None = None, device=None,
-             log=None):
+             sample=592, warps=WARPS, check_every=CHECK_EVERY, pair=PAIR, cache: str | Path | None = None,
+             device=None, log=None):
     """Pick ``(EngineOptions, SolveConfig)`` for a batch.
 
     ``matrices``: the engine's ``(A, neq)`` list; ``species_id``: per
@@ -66,7 +68,8 @@ def autotune(matrices, species_id, lower, upper, cost, col_offsets, *, config: S
         table = json.loads(Path(cache).read_text())
         if key in table:
             best = table[key]
-            return (replace(EngineOptions(), warps_per_block=best["warps_per_block"]),
+            return (replace(EngineOptions(), warps_per_block=best["warps_per_block"],
+                            pair_instances=best.get("pair_instances", True)),
                     replace(config, check_every=best["check_every"]), best["timings"])
     pick = _sample(species_id, sample)
     sid = np.asarray(species_id)[pick].astype(np.int32)
@@ -76,11 +79,12 @@ def autotune(matrices, species_id, lower, upper, cost, col_offsets, *, config: S
     cols = torch.cat(cols)
     lo, up, c = lower[cols].contiguous(), upper[cols].contiguous(), cost[cols].contiguous()
     timings = []
-    for w, ce in itertools.product(warps, check_every):
+    for w, ce, pr in itertools.product(warps, check_every, pair):
         try:
-            eng = LPEngine(matrices, options=replace(EngineOptions(), warps_per_block=w), device=device)
+            eng = LPEngine(matrices, options=replace(EngineOptions(), warps_per_block=w, pair_instances=pr),
+                           device=device)
         except Exception as exc:  # a launch shape this device cannot run
-            timings.append({"warps_per_block": w, "check_every": ce, "error": str(exc)})
+            timings.append({"warps_per_block": w, "check_every": ce, "pair_instances": pr, "error": str(exc)})
             continue
         eng.set_instances(sid, lo, up, c)
         cfg = replace(config, check_every=ce)
@@ -91,9 +95,10 @@ def autotune(matrices, species_id, lower, upper, cost, col_offsets, *, config: S
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         ok = int((res.status == 0).sum().item())
+        kernel = eng.phase_kernels()[0]
         eng.close()
-        row = {"warps_per_block": w, "check_every": ce, "seconds": dt, "certified": ok,
-               "seconds_per_certified_lp": dt / max(ok, 1)}
+        row = {"warps_per_block": w, "check_every": ce, "pair_instances": pr, "kernel": kernel, "seconds": dt,
+               "certified": ok, "seconds_per_certified_lp": dt / max(ok, 1)}
         timings.append(row)
         if log:
             log(row)
@@ -106,5 +111,5 @@ def autotune(matrices, species_id, lower, upper, cost, col_offsets, *, config: S
         tmp = Path(str(cache) + ".tmp")
         tmp.write_text(json.dumps(table, indent=1))
         tmp.replace(cache)
-    return (replace(EngineOptions(), warps_per_block=best["warps_per_block"]),
+    return (replace(EngineOptions(), warps_per_block=best["warps_per_block"], pair_instances=best["pair_instances"]),
             replace(config, check_every=best["check_every"]), timings)

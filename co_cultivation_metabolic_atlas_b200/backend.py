@@ -124,6 +124,8 @@ class B200LPBackend:
         else:
             for env in ids:
                 self.last_certified.pop(env, None)
+        if self.mode == 'mlp':
+            self.model.reset(ids)
 
     @staticmethod
     def _matrix_keys(problems):
@@ -156,7 +158,7 @@ class B200LPBackend:
             self._engine = LPEngine(self._matrices, options=self.options, device=self.device)
             rebuilt = True
         index = {k: i for i, k in enumerate(self._keys)}
-        return np.array([index[k] for k in keys], dtype=np.int32), rebuilt
+        return np.array([index[k] for k in keys], dtype=np.int32), rebuilt, keys
 
     def solve_batch(self, requests, *, environment_ids=None):
         started = time.perf_counter()
@@ -172,7 +174,7 @@ class B200LPBackend:
         splits = self._splits(problems)
         problems = [sp.split_problem(p) if sp is not None else p for sp, p in zip(splits, problems)]
         prep = time.perf_counter()
-        species, rebuilt = self._engine_for(problems)
+        species, rebuilt, keys = self._engine_for(problems)
         eng = self._engine
         lower = np.concatenate([p[2] for p in problems])
         upper = np.concatenate([p[3] for p in problems])
@@ -200,7 +202,7 @@ class B200LPBackend:
                     wo[i] = prev[3]
             warm_x, warm_y, warm_o = wx, wy, wo
         elif self.mode == 'mlp':
-            warm_x, warm_y, warm_o = self.model.propose(ids, problems, species, eng)
+            warm_x, warm_y, warm_o = self.model.propose(ids, problems, species, eng, keys=keys)
         dev = self.device
         t = lambda a: torch.as_tensor(a, dtype=torch.float64).pin_memory().to(dev, non_blocking=True)
         eng.set_instances(species, t(lower), t(upper), t(cost), t(rhs) if tr else None)
@@ -260,8 +262,8 @@ class B200LPBackend:
                 self.last_certified[env] = certified[env]
             else:
                 self.last_certified.pop(env, None)
-        if self.mode == 'mlp' and hasattr(self.model, 'commit'):
-            self.model.commit(ids)
+        if self.mode == 'mlp':
+            self.model.commit(ids, {env: (v[1], v[2], v[3]) for env, v in certified.items()}, keys)
         self.history.append(dict(stage=self.stage, mode=self.mode, batch=len(ids), environment_ids=ids,
                                  accepted=sum(r.success for r in rows), cpu_lp_calls=0,
                                  engine_rebuilt=rebuilt, iterations=iters.tolist(), retried=retried,

@@ -12,6 +12,11 @@ One ``DeviceCommunity.step`` is the reference simulator's step
 4. medium Euler step with the beginning-of-step biomass
    (``_update_environment`` ``:1326-1435``, ``integration_biomass`` ``:1680``).
 
+With ``parsimonious=True`` every (environment, species) LP gets the
+parsimonious second stage of ``parsimonious.py`` (weighted exchange fluxes
+minimised at the stage-1 growth, a unique optimum) on a second engine, and
+the Euler steps use its fluxes.
+
 Everything stays on the GPU; the LP batch is laid out species-major
 (all environments of species 0, then species 1, then species 2).
 """
@@ -66,7 +71,8 @@ class DeviceCommunity:
 
     def __init__(self, models, medium, biomass, *, dt=0.05, capacity=CARRYING_CAPACITY,
                  options: EngineOptions | None = None, config: SolveConfig | None = None,
-                 warm_start: str = "previous", learned=None, horizon_steps: int = 960, device=None):
+                 warm_start: str = "previous", learned=None, horizon_steps: int = 960, device=None,
+                 parsimonious: bool = False):
         if warm_start not in ("cold", "previous", "extrapolate", "learned"):
             raise ValueError("warm_start must be 'cold', 'previous', 'extrapolate' or 'learned'")
         if warm_start == "learned" and learned is None:
@@ -122,6 +128,98 @@ class DeviceCommunity:
         self._bufs = [self.engine.allocate_result() for _ in range(3)]
         self._which = 0
         self._wx = self._wy = None
+        self.parsimonious = bool(parsimonious)
+        self.engine2 = None
+        if self.parsimonious:
+            self._init_stage2(options)
+
+    # -- parsimonious second stage ----------------------------------------
+    def _init_stage2(self, options):
+        """Second engine with the stage-2 matrices ``[S 0; E -I; -E -I]``
+        and the index maps between the two stages' flat layouts."""
+        from .parsimonious import stage_cost, stage_matrix
+        dev = self.device
+        E, sid = self.E, self.species_id
+        self.engine2 = LPEngine([(stage_matrix(m), m.S.shape[0]) for m in self.models], options=options, device=dev)
+        co2, ro2, tc2, tr2 = self.engine2.layout(sid)
+        co1 = self.col_offsets.cpu().numpy()
+        _, ro1, _, _ = self.engine.layout(sid)
+        vmap, tmap, ex1, ymap = [], [], [], []
+        cost2, up_t = [], []
+        bio1, bio2 = [], []
+        for s, m in enumerate(self.models):
+            r, n = m.S.shape
+            k = m.n_exchange
+            for e in range(E):
+                i = s * E + e
+                vmap.append(co2[i] + np.arange(n))
+                tmap.append(co2[i] + n + np.arange(k))
+                ex1.append(co1[i] + np.arange(k))
+                ymap.append(ro2[i] + np.arange(r))
+                bio1.append(co1[i] + m.biomass)
+                bio2.append(co2[i] + m.biomass)
+            cost2.append(np.tile(stage_cost(m, s), E))
+        t = lambda a: torch.as_tensor(np.concatenate(a) if isinstance(a, list) else a, device=dev)  # noqa: E731
+        self._vmap, self._tmap, self._ex1, self._ymap = (t(vmap).long(), t(tmap).long(), t(ex1).long(),
+                                                         t(ymap).long())
+        self._bio1, self._bio2 = t(np.asarray(bio1)).long(), t(np.asarray(bio2)).long()
+        self.lower2 = torch.zeros(tc2, dtype=torch.float64, device=dev)
+        self.upper2 = torch.zeros(tc2, dtype=torch.float64, device=dev)
+        self.cost2 = t(cost2).double()
+        self.total_cols2, self.total_rows2 = tc2, tr2
+        self._stage2_bounds()
+        self.upper2.index_put_((self._vmap,), self.upper)
+        self.engine2.set_instances(sid, self.lower2, self.upper2, self.cost2)
+        self._bufs2 = [self.engine2.allocate_result() for _ in range(3)]
+        self.prev_p = self.prev2_p = None
+        self._wx2 = torch.zeros(tc2, dtype=torch.float64, device=dev)
+        self._wy2 = torch.zeros(max(1, tr2), dtype=torch.float64, device=dev)
+
+    def _stage2_bounds(self, growth=None):
+        """Stage-2 bounds from the current stage-1 bounds (and the stage-1
+        growth fluxes, ``(E S,)`` in the batch order): ``parsimonious.
+        stage_bounds`` on the device."""
+        from .parsimonious import GROWTH_FLOOR_ABS, GROWTH_RELAXATION
+        self.lower2.index_put_((self._vmap,), self.lower)
+        lo_ex = self.lower[self._ex1]
+        self.upper2.index_put_((self._tmap,), torch.maximum(lo_ex.abs(), self.upper[self._ex1].abs()))
+        if growth is not None:
+            floor = torch.maximum(self.lower[self._bio1], growth * (1.0 - GROWTH_RELAXATION) - GROWTH_FLOOR_ABS)
+            self.lower2.index_put_((self._bio2,), torch.minimum(floor, self.upper[self._bio1]))
+
+    def solve_stage2(self, res: SolveResult) -> SolveResult:
+        """The parsimonious second stage of every LP of the step, warm
+        started from the last two stage-2 solutions (extrapolated) or, at
+        the first step, from stage 1's solution with ``t = |v_exchange|``."""
+        self._stage2_bounds(res.x[self._bio1])
+        # the buffer index of this step's stage-1 result (``solve`` has
+        # advanced the rotation already)
+        out = self._bufs2[(self._which + 2) % 3]
+        nc, nr = self.total_cols2, self.total_rows2
+        self.engine2.set_iteration_hints(None if self.prev_p is None else self.prev_p.iterations)
+        if self.prev_p is not None:
+            if self.prev2_p is not None:
+                torch.sub(self.prev_p.x[:nc] * 2.0, self.prev2_p.x[:nc], out=self._wx2)
+                torch.sub(self.prev_p.y[:nr] * 2.0, self.prev2_p.y[:nr], out=self._wy2[:nr])
+            else:
+                self._wx2.copy_(self.prev_p.x[:nc])
+                self._wy2[:nr].copy_(self.prev_p.y[:nr])
+            omega = self.prev_p.omega
+        else:
+            self._wx2.zero_()
+            self._wx2.index_put_((self._vmap,), res.x[:self.total_cols])
+            self._wx2.index_put_((self._tmap,), res.x[self._ex1].abs())
+            self._wy2.zero_()
+            self._wy2.index_put_((self._ymap,), res.y[:self.total_rows])
+            omega = res.omega
+        res2 = self.engine2.solve(warm_x=self._wx2, warm_y=self._wy2[:nr], warm_omega=omega, config=self.config,
+                                  out=out)
+        self.prev2_p, self.prev_p = self.prev_p, res2
+        return res2
+
+    def stage2_fluxes(self, res2: SolveResult):
+        """Stage-2 fluxes in stage 1's flat layout."""
+        return res2.x.index_select(0, self._vmap)
 
     # -- pieces of one step --------------------------------------------------
     def uptake_bounds(self):
@@ -162,9 +260,10 @@ class DeviceCommunity:
         self.result = res
         return res
 
-    def integrate(self, res: SolveResult):
-        """Euler biomass and medium updates from the solved fluxes."""
-        x = res.x
+    def integrate(self, res: SolveResult, x=None):
+        """Euler biomass and medium updates from the solved fluxes (``x``
+        in stage 1's flat layout; default ``res.x``)."""
+        x = res.x if x is None else x
         E = self.E
         mu = torch.stack([x[idx] for idx in self.bio_index], dim=1)            # (E, S)
         X0 = self.biomass.clone()
@@ -179,13 +278,16 @@ class DeviceCommunity:
         self.medium.copy_(torch.clamp(self.medium + delta, min=0.0))
         self.step_index += 1
 
+    @staticmethod
+    def certified_mask(res: SolveResult):
+        mt = res.metrics
+        return (res.status == 0) & (mt[:, 0] <= 1e-5) & (mt[:, 1] <= 1e-7) & (mt[:, 2] <= 1e-7)
+
     def certified(self, res: SolveResult):
         """Count of LPs that meet the engine's FP64 tolerances AND the
         reference's certificate gate (primal <= 1e-5, dual <= 1e-7, relative
         KKT gap <= 1e-7, ``src/gpu_block_lp.py:84``) -- on the device."""
-        mt = res.metrics
-        ok = (res.status == 0) & (mt[:, 0] <= 1e-5) & (mt[:, 1] <= 1e-7) & (mt[:, 2] <= 1e-7)
-        return ok.sum()
+        return self.certified_mask(res).sum()
 
     def step(self) -> StepStats:
         """One dFBA step: a captured graph's replay after ``capture``,
@@ -210,7 +312,8 @@ class DeviceCommunity:
             raise RuntimeError("the network's first-step seed is not captured")
         if self.warm_start == "extrapolate" and self._wx is None:
             raise RuntimeError("run a warm-started step before capturing")
-        saved = (self.step_index, self.prev, self.prev2, self.result, self._which)
+        saved = (self.step_index, self.prev, self.prev2, self.result, self._which,
+                 getattr(self, "prev_p", None), getattr(self, "prev2_p", None))
         old_stream = self.engine.stream
         self._graphs, self._graph_stats = [], []
         torch.cuda.synchronize(self.device)
@@ -222,14 +325,19 @@ class DeviceCommunity:
                 self.engine.use_timing_slot(k)
                 with torch.cuda.graph(g):
                     self.engine.set_stream(torch.cuda.current_stream(self.device))
+                    if self.engine2 is not None:
+                        self.engine2.set_stream(torch.cuda.current_stream(self.device))
                     st = self._eager_step()
                 self._graphs.append(g)
                 self._graph_stats.append(st)
         finally:
             self.engine.use_timing_slot(-1)
             self.engine.set_stream(old_stream)
+            if self.engine2 is not None:
+                self.engine2.set_stream(old_stream)
             # capture ran nothing: the state is where it was
-            self.step_index, self.prev, self.prev2, self.result, self._which = saved
+            (self.step_index, self.prev, self.prev2, self.result, self._which, self.prev_p,
+             self.prev2_p) = saved
         self._replay = 0
 
     def last_replay_slot(self, back: int = 0):
@@ -243,14 +351,23 @@ class DeviceCommunity:
     def _eager_step(self) -> StepStats:
         self.uptake_bounds()
         res = self.solve()
-        self.integrate(res)
-        return StepStats(lps=self.E * self.S, certified=self.certified(res),
-                         iterations=res.iterations, status=res.status)
+        if not self.parsimonious:
+            self.integrate(res)
+            return StepStats(lps=self.E * self.S, certified=self.certified(res),
+                             iterations=res.iterations, status=res.status)
+        res2 = self.solve_stage2(res)
+        self.integrate(res, self.stage2_fluxes(res2))
+        cert = self.certified_mask(res).sum() + self.certified_mask(res2).sum()
+        return StepStats(lps=2 * self.E * self.S, certified=cert,
+                         iterations=torch.cat([res.iterations, res2.iterations]),
+                         status=torch.cat([res.status, res2.status]))
 
     def _graph_step(self) -> StepStats:
         k = self._replay
         self._graphs[k].replay()
         res = self._bufs[self._which]
+        if self.parsimonious:
+            self.prev2_p, self.prev_p = self.prev_p, self._bufs2[self._which]
         self._which = (self._which + 1) % 3
         self.prev2, self.prev, self.result = self.prev, res, res
         self.step_index += 1
@@ -260,3 +377,5 @@ class DeviceCommunity:
     def close(self):
         self.release_graphs()
         self.engine.close()
+        if self.engine2 is not None:
+            self.engine2.close()

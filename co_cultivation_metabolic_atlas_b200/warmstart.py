@@ -35,6 +35,7 @@ import ctypes
 import math
 from dataclasses import dataclass
 
+import numpy as np
 import torch
 
 from . import _native as N
@@ -408,3 +409,226 @@ def train(mlp: MLP, F, T, *, epochs=20, batch=4096, lr=1e-3, lr_final=1e-4, seed
     if ops.error_flag():
         raise RuntimeError("a tensor-core GEMM wait timed out during training")
     return losses
+
+
+# ------------------------------------------------------------ drop-in backend
+def signed_log(values):
+    """``sign(v) log(1 + |v|)`` with infinities clipped to +-1e13 (the
+    reference's feature transform, ``src/temporal_lp_data.py:15-17``)."""
+    v = np.nan_to_num(np.asarray(values, dtype=np.float64), nan=0.0, posinf=1e13, neginf=-1e13)
+    return np.sign(v) * np.log1p(np.abs(v))
+
+
+MAX_REQUEST_FEATURES = 128
+
+
+@dataclass
+class RequestMember:
+    """The network of one species matrix: request features -> [x; y]."""
+    mlp: MLP
+    index: np.ndarray        # int64 positions in [lower, upper, c, rhs] used as features
+    f_mean: torch.Tensor
+    f_std: torch.Tensor
+    t_mean: torch.Tensor
+    t_std: torch.Tensor
+    n: int
+    m: int
+    omega: float             # median primal weight of the training solutions
+
+    def features(self, lower, upper, cost, rhs):
+        """Feature rows of a batch ((k, n), (k, n), (k, n), (k, m) arrays)."""
+        full = np.concatenate([lower, upper, cost, rhs], axis=1)
+        return signed_log(full[:, self.index])
+
+    def predict(self, feats):
+        X = torch.as_tensor(feats, dtype=F32, device=self.mlp.device)
+        Y = self.mlp.forward((X - self.f_mean) / self.f_std)[:, :self.n + self.m]
+        return (Y * self.t_std + self.t_mean).double()
+
+
+def select_request_features(full, limit=MAX_REQUEST_FEATURES):
+    """Feature positions of signed-log request rows ``full`` (k, d): the
+    columns that vary over the rows, one representative of identical
+    columns, at most ``limit`` (the largest spreads), ascending; a batch with
+    no varying entry keeps position 0."""
+    spread = full.std(axis=0)
+    cand = np.flatnonzero(spread > 1e-12)
+    _, first = np.unique(full[:, cand].T, axis=0, return_index=True)
+    cand = cand[np.sort(first)]
+    if cand.size > limit:
+        cand = np.sort(cand[np.argsort(-spread[cand], kind="stable")[:limit]])
+    if cand.size == 0:
+        cand = np.array([0], dtype=np.int64)
+    return cand.astype(np.int64)
+
+
+def fit_request_member(lower, upper, cost, rhs, X, Y, omega, *, hidden=(512, 512), epochs=20, batch=1024,
+                       seed=0, device=None, log=None):
+    """Train the network of one species matrix on (request -> certified
+    solution) pairs: rows of ``lower``/``upper``/``cost`` (k, n), ``rhs``
+    (k, m), solutions ``X`` (k, n), ``Y`` (k, m), primal weights ``omega``.
+    Features are the signed-log entries of ``[lower, upper, c, rhs]`` that
+    vary over the training rows, duplicates removed, at most 128 (the
+    largest spreads), as the reference's codec selects them
+    (``src/temporal_lp_data.py:62-175``); targets are standardised."""
+    full = signed_log(np.concatenate([lower, upper, cost, rhs], axis=1))
+    cand = select_request_features(full)
+    dev = torch.device(device) if device is not None else torch.device("cuda")
+    F = torch.as_tensor(full[:, cand], dtype=F32, device=dev)
+    T = torch.as_tensor(np.concatenate([X, Y], axis=1), dtype=F32, device=dev)
+    f_mean, f_std = F.mean(0), F.std(0).clamp_min(1e-3)
+    t_mean, t_std = T.mean(0), T.std(0).clamp_min(1e-6)
+    n, m = X.shape[1], Y.shape[1]
+    net = MLP([int(cand.size), *hidden, n + m], device=dev, seed=seed)
+    losses = train(net, (F - f_mean) / f_std, (T - t_mean) / t_std, epochs=epochs,
+                   batch=min(batch, F.shape[0]), seed=seed, log=log)
+    member = RequestMember(net, cand.astype(np.int64), f_mean, f_std, t_mean, t_std, n, m,
+                           float(np.median(np.asarray(omega, dtype=np.float64))))
+    return member, losses
+
+
+class RequestWarmStart:
+    """Learned warm start of the drop-in backend (``B200LPBackend(mode=
+    'mlp', warm_start_model=...)``), the counterpart of the reference's
+    ``TemporalLPModel`` / ``TemporalLPSession`` behind
+    ``TemporalGpuLPBackend(mode='mlp')`` (``src/temporal_gpu_lp.py:136-168``,
+    ``src/temporal_lp_model.py:221-285``).
+
+    ``members`` maps a species matrix's content key (``problem.matrix_key``)
+    to its trained network.  For every request of a batch, ``propose``
+    returns the temporal base of the environment's last certified solutions
+    of the same matrix (the previous one extrapolated linearly from the last
+    two, as the dFBA loop's warm start) when it has any, else the network's
+    prediction from the request's features, else the cold start.  Proposals
+    are pending until ``commit``: the backend commits after every row of a
+    call is built, with the call's certified solutions, so a call that
+    raises leaves every environment's history as it was (the reference's
+    propose/commit transaction).  A failed row clears its environment's
+    history."""
+
+    def __init__(self, members: dict):
+        self.members = dict(members)
+        self._history: dict = {}   # env -> [(key, x, y, omega)] oldest first, at most two
+        self.last_sources: list = []
+
+    def reset(self, environment_ids=None):
+        if environment_ids is None:
+            self._history.clear()
+        else:
+            for env in environment_ids:
+                self._history.pop(env, None)
+
+    def propose(self, ids, problems, species, eng, keys=None):
+        """Flat warm-start arrays (x, y, omega) in the engine's batch layout
+        (host numpy, FP64)."""
+        from .problem import matrix_key
+        if keys is None:
+            keys = [matrix_key(p[0], p[5]) for p in problems]
+        co, ro, tc, tr = eng.layout(species)
+        wx = np.zeros(tc)
+        wy = np.zeros(tr)
+        wo = np.ones(len(ids))
+        sources = ["cold"] * len(ids)
+        by_key: dict = {}
+        for i, (env, key) in enumerate(zip(ids, keys)):
+            hist = [h for h in self._history.get(env, []) if h[0] == key]
+            n, m = problems[i][4].shape[0], problems[i][1].shape[0]
+            if hist:
+                x1, y1, o1 = hist[-1][1:]
+                if len(hist) > 1:
+                    x0, y0, _ = hist[-2][1:]
+                    x1, y1 = temporal_base(x1, x0), temporal_base(y1, y0)
+                wx[co[i]:co[i] + n] = x1
+                wy[ro[i]:ro[i] + m] = y1
+                wo[i] = o1
+                sources[i] = "temporal"
+            elif key in self.members:
+                by_key.setdefault(key, []).append(i)
+        for key, rows in by_key.items():
+            mem = self.members[key]
+            lo = np.stack([problems[i][2] for i in rows])
+            up = np.stack([problems[i][3] for i in rows])
+            c = np.stack([problems[i][4] for i in rows])
+            b = np.stack([problems[i][1] for i in rows])
+            pred = mem.predict(mem.features(lo, up, c, b)).cpu().numpy()
+            for r, i in enumerate(rows):
+                wx[co[i]:co[i] + mem.n] = pred[r, :mem.n]
+                wy[ro[i]:ro[i] + mem.m] = pred[r, mem.n:]
+                wo[i] = mem.omega
+                sources[i] = "network"
+        self.last_sources = sources
+        return wx, wy, wo
+
+    def commit(self, ids, certified, keys):
+        """Advance the history of every environment of a finished call:
+        ``certified`` maps an environment to its (x, y, omega), ``keys``
+        gives each environment's matrix key."""
+        for env, key in zip(ids, keys):
+            if env in certified:
+                x, y, om = certified[env]
+                hist = [h for h in self._history.get(env, []) if h[0] == key][-1:]
+                hist.append((key, x, y, om))
+                self._history[env] = hist
+            else:
+                self._history.pop(env, None)
+
+
+def species_key(model):
+    """The drop-in's content key of a species' FBA matrix (the key
+    ``B200LPBackend`` computes for its requests)."""
+    from .problem import matrix_key, normalize
+    zeros = np.zeros(model.S.shape[0])
+    p = normalize(model.cost, dict(A_eq=model.S, b_eq=zeros, bounds=np.column_stack([model.lower, model.upper])))
+    return matrix_key(p[0], p[5])
+
+
+def collect_request_pairs(models, *, envs, steps, seed, config=None, device=None):
+    """Per species, (lower bounds, certified x, y, omega) rows of every
+    certified (environment, step) of a rollout with extrapolated warm
+    starts: the drop-in's training pairs (its requests differ only in their
+    lower bounds)."""
+    from . import synthetic as syn
+    from .dfba import DeviceCommunity
+    medium, biomass = syn.initial_environments(envs, seed=seed)
+    com = DeviceCommunity(models, medium, biomass, config=config, warm_start="extrapolate", device=device)
+    co = com.col_offsets.cpu().numpy()
+    _, ro, _, _ = com.engine.layout(com.species_id)
+    out = [dict(lower=[], x=[], y=[], omega=[]) for _ in models]
+    for _ in range(steps):
+        com.uptake_bounds()
+        lower = com.lower.cpu().numpy()
+        res = com.solve()
+        x, y = res.x.cpu().numpy(), res.y.cpu().numpy()
+        ok = (res.status == 0).cpu().numpy()
+        om = res.omega.cpu().numpy()
+        for s, mdl in enumerate(models):
+            m, n = mdl.S.shape
+            c0, r0 = int(co[s * envs]), int(ro[s * envs])
+            sel = ok[s * envs:(s + 1) * envs]
+            out[s]["lower"].append(lower[c0:c0 + envs * n].reshape(envs, n)[sel])
+            out[s]["x"].append(x[c0:c0 + envs * n].reshape(envs, n)[sel])
+            out[s]["y"].append(y[r0:r0 + envs * m].reshape(envs, m)[sel])
+            out[s]["omega"].append(om[s * envs:(s + 1) * envs][sel])
+        com.integrate(res)
+    com.close()
+    return [{k: np.concatenate(v) for k, v in d.items()} for d in out]
+
+
+def fit_request_warm_start(models, *, envs, steps, seeds, epochs=20, hidden=(512, 512), config=None, device=None,
+                           log=None):
+    """Train one network per species on the engine's own rollouts (seeds
+    disjoint from the evaluated environments) and return the drop-in's
+    ``RequestWarmStart`` and the per-species losses."""
+    parts = [collect_request_pairs(models, envs=envs, steps=steps, seed=sd, config=config, device=device)
+             for sd in seeds]
+    members, losses = {}, []
+    for s, mdl in enumerate(models):
+        d = {k: np.concatenate([p[s][k] for p in parts]) for k in ("lower", "x", "y", "omega")}
+        k = d["lower"].shape[0]
+        member, ls = fit_request_member(d["lower"], np.broadcast_to(mdl.upper, (k, mdl.S.shape[1])),
+                                        np.broadcast_to(mdl.cost, (k, mdl.S.shape[1])),
+                                        np.zeros((k, mdl.S.shape[0])), d["x"], d["y"], d["omega"],
+                                        hidden=hidden, epochs=epochs, device=device, log=log)
+        members[species_key(mdl)] = member
+        losses.append(ls)
+    return RequestWarmStart(members), losses

@@ -84,3 +84,34 @@ def step(models, medium, biomass, dt, solve):
     biomass = update_biomass(biomass, mu, dt)
     medium = update_medium(medium, models, fluxes, biomass0, dt)
     return medium, biomass, fluxes
+
+
+def parsimonious_fluxes(model, species_index, lower, upper, growth):
+    """The parsimonious second stage of one species' FBA LP restated with
+    HiGHS (the reference's exact solver): minimise the weighted sum of
+    absolute exchange fluxes (weights of ``parsimonious.exchange_weights``)
+    with growth held at ``growth`` (1 - 1e-6) - 1e-9, through the split
+    ``t_j >= v_j, t_j >= -v_j`` (the pattern of
+    ``_assemble_parsimonious_exchange_lp``, ``src/community_solver.py:
+    116-204``).  Returns ``(status, fluxes v)``."""
+    from scipy.optimize import linprog
+    from scipy.sparse import csr_matrix, hstack, identity, vstack
+
+    from co_cultivation_metabolic_atlas_b200.parsimonious import (GROWTH_FLOOR_ABS, GROWTH_RELAXATION,
+                                                                  exchange_weights)
+    S = csr_matrix(model.S)
+    m, n = S.shape
+    k = model.n_exchange
+    w = exchange_weights(model, species_index)
+    pick = csr_matrix((np.ones(k), (np.arange(k), np.arange(k))), shape=(k, n))
+    a_eq = hstack([S, csr_matrix((m, k))]).tocsr()
+    a_ub = vstack([hstack([pick, -identity(k)]), hstack([-pick, -identity(k)])]).tocsr()
+    lo = np.concatenate([lower, np.zeros(k)])
+    up = np.concatenate([upper, np.maximum(np.abs(lower[:k]), np.abs(upper[:k]))])
+    b = model.biomass
+    lo[b] = min(max(lower[b], growth * (1.0 - GROWTH_RELAXATION) - GROWTH_FLOOR_ABS), up[b])
+    res = linprog(np.concatenate([np.zeros(n), w]), A_eq=a_eq, b_eq=np.zeros(m), A_ub=a_ub,
+                  b_ub=np.zeros(2 * k), bounds=np.column_stack([lo, up]), method="highs-ds")
+    if res.status != 0:
+        return res.status, None
+    return 0, np.asarray(res.x[:n])
