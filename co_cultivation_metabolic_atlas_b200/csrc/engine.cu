@@ -71,6 +71,39 @@ static std::vector<uint32_t> pack_bf16(const std::vector<int32_t>& idx, const st
     return out;
 }
 
+// Device copy of one re-centred operand (slices without the long lines in
+// warp-schedule order, the long lines, masks, packed words, FP64 values);
+// the uploaded slice list is kept on the host for the patched-slice flags.
+fbalp::DevLines upload_lines(const fbalp::Sell& S, const std::vector<int32_t>& sched_off,
+                             const std::vector<int32_t>& sched, const std::vector<int32_t>& lsched_off,
+                             const std::vector<int32_t>& lsched, bool packable, std::vector<int4>* host_list,
+                             int4** dev_list, std::vector<void*>& owned) {
+    fbalp::DevLines d{};
+    d.nslices = S.nslices;
+    d.nlong = static_cast<int32_t>(S.long_line.size());
+    d.elems = S.off.back();
+    d.long_elems = S.long_off.back();
+    host_list->clear();
+    for (int32_t sl : sched) host_list->push_back(make_int4(sl, S.off[sl], S.length[sl], 0));
+    std::vector<int4> llist;
+    for (int32_t q : lsched) llist.push_back(make_int4(S.long_line[q], S.long_off[q], S.long_off[q + 1] - S.long_off[q], 0));
+    d.list = *dev_list = dev_upload(*host_list, owned);
+    d.sched_off = dev_upload(sched_off, owned);
+    d.lmask = dev_upload(S.lmask, owned);
+    d.long_list = dev_upload(llist, owned);
+    d.long_sched_off = dev_upload(lsched_off, owned);
+    const std::vector<float> v32(S.val.begin(), S.val.end()), l32(S.long_val.begin(), S.long_val.end());
+    if (packable) {
+        d.pk = dev_upload(pack_bf16(S.idx, v32), owned);
+        d.long_pk = dev_upload(pack_bf16(S.long_idx, l32), owned);
+    }
+    d.idx = dev_upload(S.idx, owned);
+    d.v64 = dev_upload(S.val, owned);
+    d.long_idx = dev_upload(S.long_idx, owned);
+    d.long_v64 = dev_upload(S.long_val, owned);
+    return d;
+}
+
 }  // namespace
 
 extern "C" {
@@ -202,6 +235,12 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             sh.ATraw = fbalp::build_sell(at, sh.col_perm, row_new, ones_n, ones_m, sh.m);
             fbalp::warp_schedule(sh.A, o.warps_per_block, &sh.a_sched_off, &sh.a_sched);
             fbalp::warp_schedule(sh.AT, o.warps_per_block, &sh.at_sched_off, &sh.at_sched);
+            sh.Ar = fbalp::build_sell(a, sh.row_perm, col_new, sh.scaling.dr, sh.scaling.dc, sh.n, fbalp::kLongCut);
+            sh.ATr = fbalp::build_sell(at, sh.col_perm, row_new, sh.scaling.dc, sh.scaling.dr, sh.m, fbalp::kLongCut);
+            fbalp::warp_schedule_split(sh.Ar, o.warps_per_block, &sh.ra_sched_off, &sh.ra_sched, &sh.ra_lsched_off,
+                                       &sh.ra_lsched);
+            fbalp::warp_schedule_split(sh.ATr, o.warps_per_block, &sh.rat_sched_off, &sh.rat_sched,
+                                       &sh.rat_lsched_off, &sh.rat_lsched);
             E->species.push_back(std::move(sh));
         }
         // --- device ---
@@ -230,10 +269,11 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             d.a_idx = dev_upload(sh.A.idx, E->owned);
             d.a_v32 = dev_upload(a32, E->owned);
             d.a_v64 = dev_upload(sh.A.val, E->owned);
-            if (sh.n + 1 < 65536 && sh.m + 1 < 65536) {
-                d.a_pk = dev_upload(pack_bf16(sh.A.idx, a32), E->owned);
-                d.at_pk = dev_upload(pack_bf16(sh.AT.idx, at32), E->owned);
-            }
+            const bool packable = sh.n + 1 < 65536 && sh.m + 1 < 65536;
+            d.ra = upload_lines(sh.Ar, sh.ra_sched_off, sh.ra_sched, sh.ra_lsched_off, sh.ra_lsched, packable,
+                                &sh.ralist, &sh.d_ralist, E->owned);
+            d.rat = upload_lines(sh.ATr, sh.rat_sched_off, sh.rat_sched, sh.rat_lsched_off, sh.rat_lsched, packable,
+                                 &sh.ratlist, &sh.d_ratlist, E->owned);
             d.at_idx = dev_upload(sh.AT.idx, E->owned);
             d.at_v32 = dev_upload(at32, E->owned);
             d.at_v64 = dev_upload(sh.AT.val, E->owned);
@@ -394,17 +434,19 @@ int fbalp_engine_set_patches(fbalp_engine* e, int32_t species, int32_t count, co
         d.patch_base[q] = 0.0;
     }
     d.patch_col_f2 = 0.0;
-    for (auto& v : sh.alist) v.w = 0;
-    for (auto& v : sh.atlist) v.w = 0;
+    for (auto* l : {&sh.alist, &sh.atlist, &sh.ralist, &sh.ratlist})
+        for (auto& v : *l) v.w = 0;
     for (int32_t q = 0; q < count; ++q) {
         const int32_t r = row_new[rows[q]], c = col_new[cols[q]];
         d.patch_row[q] = r;
         d.patch_col[q] = c;
         d.patch_scale[q] = sh.scaling.dr[rows[q]] * sh.scaling.dc[cols[q]];
-        for (auto& v : sh.alist)
-            if (v.x == r / 32) v.w = 1;
-        for (auto& v : sh.atlist)
-            if (v.x == c / 32) v.w = 1;
+        for (auto* l : {&sh.alist, &sh.ralist})
+            for (auto& v : *l)
+                if (v.x == r / 32) v.w = 1;
+        for (auto* l : {&sh.atlist, &sh.ratlist})
+            for (auto& v : *l)
+                if (v.x == c / 32) v.w = 1;
     }
     // scaled template values of the patched columns (row c of A~^T in the
     // SELL slices): each patched entry's base value, and the sum of squares
@@ -435,6 +477,13 @@ int fbalp_engine_set_patches(fbalp_engine* e, int32_t species, int32_t count, co
               "copy schedule");
         check(cudaMemcpy(sh.d_atlist, sh.atlist.data(), sh.atlist.size() * sizeof(int4), cudaMemcpyHostToDevice),
               "copy schedule");
+        if (!sh.ralist.empty())
+            check(cudaMemcpy(sh.d_ralist, sh.ralist.data(), sh.ralist.size() * sizeof(int4), cudaMemcpyHostToDevice),
+                  "copy schedule");
+        if (!sh.ratlist.empty())
+            check(cudaMemcpy(sh.d_ratlist, sh.ratlist.data(), sh.ratlist.size() * sizeof(int4),
+                             cudaMemcpyHostToDevice),
+                  "copy schedule");
         check(cudaMemcpy(e->dev_species + species, &d, sizeof(d), cudaMemcpyHostToDevice), "copy species");
     } catch (const CudaError& ex) {
         return fail(FBALP_ERR_CUDA, ex.what());
@@ -487,8 +536,8 @@ int recentred_mode(fbalp_engine* e) {
         const SpeciesHost& sh = e->species[s];
         for (int st = 0; st < 2; ++st) {
             bool& ok = st ? staged : streamed;
-            if (ok && !fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
-                                                    sh.A.off.back(), sh.AT.off.back(), cap, st != 0)
+            if (ok && !fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.shape_a(), sh.shape_at(),
+                                                    cap, st != 0)
                            .layout.recentred)
                 ok = false;
         }
@@ -513,9 +562,8 @@ bool pair_mode(fbalp_engine* e, double reflection, bool patched) {
     for (size_t s = 0; s < e->species.size(); ++s) {
         if (!used[s]) continue;
         const SpeciesHost& sh = e->species[s];
-        if (!sh.A.nslices && !sh.AT.nslices) return false;
-        if (!fbalp::plan_layout_pair(sh.n, sh.m, sh.neq, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
-                                     sh.A.off.back(), sh.AT.off.back(), cap).layout.recentred)
+        if (!fbalp::plan_layout_pair(sh.n, sh.m, sh.neq, e->opt.warps_per_block, sh.shape_a(), sh.shape_at(), cap)
+                 .layout.recentred)
             return false;
     }
     return true;
@@ -553,11 +601,10 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
         if (!used[s]) continue;
         const SpeciesHost& sh = e->species[s];
         fbalp::LayoutPlan P = recentred == 3
-            ? fbalp::plan_layout_pair(sh.n, sh.m, sh.neq, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
-                                      sh.A.off.back(), sh.AT.off.back(), cap)
+            ? fbalp::plan_layout_pair(sh.n, sh.m, sh.neq, e->opt.warps_per_block, sh.shape_a(), sh.shape_at(), cap)
             : recentred
-            ? fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
-                                           sh.A.off.back(), sh.AT.off.back(), cap, recentred == 1)
+            ? fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.shape_a(), sh.shape_at(), cap,
+                                           recentred == 1)
             : unscaled
             ? fbalp::plan_layout_unscaled(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
                                           sh.A.off.back(), sh.AT.off.back(), cap)

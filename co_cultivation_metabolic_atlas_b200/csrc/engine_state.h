@@ -52,6 +52,20 @@ struct SpeciesHost {
     std::vector<int4> alist, atlist;  // schedule entries as uploaded (w: patched slice)
     int4* d_alist = nullptr;           // their device copies
     int4* d_atlist = nullptr;
+    // the re-centred kernels' operands: slices without the long lines, the
+    // long lines, their schedules and uploaded lists
+    fbalp::Sell Ar, ATr;
+    std::vector<int32_t> ra_sched_off, ra_sched, ra_lsched_off, ra_lsched;
+    std::vector<int32_t> rat_sched_off, rat_sched, rat_lsched_off, rat_lsched;
+    std::vector<int4> ralist, ratlist;
+    int4* d_ralist = nullptr;
+    int4* d_ratlist = nullptr;
+    fbalp::LinesShape shape_a() const {
+        return {Ar.nslices, static_cast<int32_t>(Ar.long_line.size()), Ar.off.back(), Ar.long_off.back()};
+    }
+    fbalp::LinesShape shape_at() const {
+        return {ATr.nslices, static_cast<int32_t>(ATr.long_line.size()), ATr.off.back(), ATr.long_off.back()};
+    }
 };
 
 struct Buffer {

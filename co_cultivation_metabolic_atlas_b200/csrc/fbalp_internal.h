@@ -164,31 +164,56 @@ inline LayoutPlan plan_layout_unscaled(int n, int m, int warps, int a_nslices, i
     return P;
 }
 
-// Re-centred FP32 layout: everything the iteration touches in shared memory
-// (schedule lists; the FP32 gather targets dxbar (n+1) and dy (m+1); the
-// matrix slices as packed words (16-bit index, BF16 value); dx, d, l - x^,
-// u - x^ (n each);
-// r and the inequality bound -y^ (m each)), and in the CTA's global slab the
-// two FP64 point buffers of x and y, the FP32 reduced cost / residual of
-// the last evaluated candidate, and the instance's scaled FP64 objective,
-// bounds and right-hand side.  Returns recentred = 0 when the shared part
-// does not fit.  With `stage` false the matrix is not staged (it is streamed
-// from L2 every iteration) and only the vectors need to fit.
-inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, int at_nslices,
-                                        int64_t a_elems, int64_t at_elems, int64_t smem_cap, bool stage = true) {
-    LayoutPlan P{};
-    Layout& L = P.layout;
+// Sizes of one re-centred operand (DevLines) for the layout planners.
+struct LinesShape {
+    int32_t nslices = 0, nlong = 0;
+    int64_t elems = 0, long_elems = 0;
+};
+
+// The part of a re-centred layout that describes the operands: slice and
+// long-line schedule offsets, slice lists, long-line lists and per-slice
+// long-lane masks of A and A^T.  Returns the next free offset (16-aligned).
+inline int64_t place_recentred_lists(Layout& L, int warps, const LinesShape& a, const LinesShape& at) {
     int64_t off = 0;
     L.sched_a_off = off;
     off += 4 * (warps + 1);
     L.sched_at_off = off;
     off += 4 * (warps + 1);
+    L.lsched_a_off = off;
+    off += 4 * (warps + 1);
+    L.lsched_at_off = off;
+    off += 4 * (warps + 1);
     off = align_up(off, 16);
     L.list_a = off;
-    off += static_cast<int64_t>(sizeof(int4)) * a_nslices;
+    off += static_cast<int64_t>(sizeof(int4)) * a.nslices;
     L.list_at = off;
-    off += static_cast<int64_t>(sizeof(int4)) * at_nslices;
-    off = align_up(off, 16);
+    off += static_cast<int64_t>(sizeof(int4)) * at.nslices;
+    L.llist_a = off;
+    off += static_cast<int64_t>(sizeof(int4)) * a.nlong;
+    L.llist_at = off;
+    off += static_cast<int64_t>(sizeof(int4)) * at.nlong;
+    L.lmask_a = off;
+    off += 4 * static_cast<int64_t>(a.nslices);
+    L.lmask_at = off;
+    off += 4 * static_cast<int64_t>(at.nslices);
+    return align_up(off, 16);
+}
+
+// Re-centred FP32 layout: everything the iteration touches in shared memory
+// (the operand lists; the FP32 gather targets dxbar (n+1) and dy (m+1); the
+// matrix as packed words (16-bit index, BF16 value) -- slices, then long
+// lines; dx, d, l - x^, u - x^ (n each); r and the inequality bound -y^ (m
+// each)), and in the CTA's global slab the two FP64 point buffers of x and
+// y, the FP32 reduced cost / residual of the last evaluated candidate, and
+// the instance's scaled FP64 objective, bounds and right-hand side.  Returns
+// recentred = 0 when the shared part does not fit.  With `stage` false the
+// matrix is not staged (it is streamed from L2 every iteration) and only the
+// lists and vectors need to fit.
+inline LayoutPlan plan_layout_recentred(int n, int m, int warps, const LinesShape& sa, const LinesShape& sat,
+                                        int64_t smem_cap, bool stage = true) {
+    LayoutPlan P{};
+    Layout& L = P.layout;
+    int64_t off = place_recentred_lists(L, warps, sa, sat);
     if (n + 1 >= 65536 || m + 1 >= 65536) return P;
     const int64_t e[kArrayCount] = {n + 1, m + 1, n, 0, m, n, n, n, m, 0, 0, 0};
     L.smem_mask = 0;
@@ -201,9 +226,13 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, 
     put(kY);
     if (stage) {  // packed 32-bit words (16-bit index | BF16 value)
         L.mat_a_idx = off;
-        off += align_up(4 * a_elems, 16);
+        off += align_up(4 * sa.elems, 16);
         L.mat_at_idx = off;
-        off += align_up(4 * at_elems, 16);
+        off += align_up(4 * sat.elems, 16);
+        L.mat_a_long = off;
+        off += align_up(4 * sa.long_elems, 16);
+        L.mat_at_long = off;
+        off += align_up(4 * sat.long_elems, 16);
         L.mat_a_val = L.mat_a_idx;
         L.mat_at_val = L.mat_at_idx;
     }
@@ -241,27 +270,18 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, int a_nslices, 
 // are interleaved as float2 (component s = instance slot s): the gather
 // targets dxbar (n+1) and dy (m+1), then the packed words (16-bit index =
 // float2 element offset of the gather target from the start of shared
-// memory | BF16 value), then d, l - x^, u - x^ (n each), r (m) and the
-// inequality bound -y^ of the rows at and beyond neq (m - neq).  The
-// Halpern iterate x is not stored: with reflection 1 it equals w xbar, with
-// w the previous iteration's Halpern weight.  The slab holds ONE instance's
-// FP64 data (the re-centred slab); a CTA uses two consecutive slabs.
-// Returns recentred = 0 when the shared part does not fit.
-inline LayoutPlan plan_layout_pair(int n, int m, int neq, int warps, int a_nslices, int at_nslices,
-                                   int64_t a_elems, int64_t at_elems, int64_t smem_cap) {
+// memory | BF16 value; slices, then long lines), then d, l - x^, u - x^ (n
+// each), r (m) and the inequality bound -y^ of the rows at and beyond neq
+// (m - neq).  The Halpern iterate x is not stored: with reflection 1 it
+// equals w xbar, with w the previous iteration's Halpern weight.  The slab
+// holds ONE instance's FP64 data (the re-centred slab); a CTA uses two
+// consecutive slabs.  Returns recentred = 0 when the shared part does not
+// fit.
+inline LayoutPlan plan_layout_pair(int n, int m, int neq, int warps, const LinesShape& sa, const LinesShape& sat,
+                                   int64_t smem_cap) {
     LayoutPlan P{};
     Layout& L = P.layout;
-    int64_t off = 0;
-    L.sched_a_off = off;
-    off += 4 * (warps + 1);
-    L.sched_at_off = off;
-    off += 4 * (warps + 1);
-    off = align_up(off, 16);
-    L.list_a = off;
-    off += static_cast<int64_t>(sizeof(int4)) * a_nslices;
-    L.list_at = off;
-    off += static_cast<int64_t>(sizeof(int4)) * at_nslices;
-    off = align_up(off, 16);
+    int64_t off = place_recentred_lists(L, warps, sa, sat);
     if (n + 1 >= 65536 || m + 1 >= 65536 || neq < 0 || neq > m) return P;
     L.smem_mask = 0;
     auto put = [&](int a, int64_t elems) {
@@ -275,9 +295,13 @@ inline LayoutPlan plan_layout_pair(int n, int m, int neq, int warps, int a_nslic
     // target from the start of shared memory
     if (off / 8 > (int64_t(1) << 16) - 1) return P;
     L.mat_a_idx = off;
-    off += align_up(4 * a_elems, 16);
+    off += align_up(4 * sa.elems, 16);
     L.mat_at_idx = off;
-    off += align_up(4 * at_elems, 16);
+    off += align_up(4 * sat.elems, 16);
+    L.mat_a_long = off;
+    off += align_up(4 * sa.long_elems, 16);
+    L.mat_at_long = off;
+    off += align_up(4 * sat.long_elems, 16);
     L.mat_a_val = L.mat_a_idx;
     L.mat_at_val = L.mat_at_idx;
     put(kC, n);
@@ -312,13 +336,15 @@ inline LayoutPlan plan_layout_pair(int n, int m, int neq, int warps, int a_nslic
 
 // Every region must start on a 16-byte boundary (int4 lists, FP64 arrays).
 inline bool layout_aligned(const Layout& L) {
-    const int64_t offs[] = {L.sched_a_off, L.sched_at_off, L.list_a, L.list_at, L.mat_a_idx,
-                            L.mat_at_idx, L.mat_a_val, L.mat_at_val};
+    const int64_t offs[] = {L.list_a, L.list_at, L.mat_a_idx, L.mat_at_idx, L.mat_a_val, L.mat_at_val,
+                            L.llist_a, L.llist_at, L.mat_a_long, L.mat_at_long};
     for (int64_t o : offs)
-        if (o % 16 != 0 && o != L.sched_at_off) return false;
+        if (o % 16 != 0) return false;
     for (int a = 0; a < kArrayCount; ++a)
         if (L.arr[a] % 16 != 0) return false;
-    return L.sched_a_off % 4 == 0 && L.sched_at_off % 4 == 0;
+    for (int64_t o : {L.sched_a_off, L.sched_at_off, L.lsched_a_off, L.lsched_at_off, L.lmask_a, L.lmask_at})
+        if (o % 4 != 0) return false;
+    return true;
 }
 
 const void* kernel_symbol(bool fp64, int threads, bool fast);

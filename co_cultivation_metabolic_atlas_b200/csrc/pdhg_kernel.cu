@@ -212,8 +212,64 @@ __device__ __forceinline__ bool layout_is_fast(const Layout& L) {
 // For fast layouts the staged 16-bit indices are ELEMENT offsets from the
 // start of dynamic shared memory (the gather target's base already added),
 // so a gather is one shared load of S[idx].
+// Stage the re-centred kernels' operands (A and A^T with their long lines
+// split off): slice and long-line schedules, lists and per-slice long-lane
+// masks, and -- when the layout stages the matrix -- the packed words with
+// their indices pre-offset to the gather targets (dxbar for A, dy for A^T)
+// in units of `unit` bytes from the start of shared memory (4: FP32
+// targets, 8: the paired kernel's float2 targets).
+__device__ void stage_recentred_ops(const DevSpecies* sp, const Layout& L, unsigned char* sm, int warps, int unit) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const DevLines& a = sp->ra;
+    const DevLines& t = sp->rat;
+    int32_t* soa = reinterpret_cast<int32_t*>(sm + L.sched_a_off);
+    int32_t* sot = reinterpret_cast<int32_t*>(sm + L.sched_at_off);
+    int32_t* loa = reinterpret_cast<int32_t*>(sm + L.lsched_a_off);
+    int32_t* lot = reinterpret_cast<int32_t*>(sm + L.lsched_at_off);
+    for (int w = tid; w <= warps; w += nt) {
+        soa[w] = a.sched_off[w];
+        sot[w] = t.sched_off[w];
+        loa[w] = a.long_sched_off[w];
+        lot[w] = t.long_sched_off[w];
+    }
+    int4* la = reinterpret_cast<int4*>(sm + L.list_a);
+    int4* lt = reinterpret_cast<int4*>(sm + L.list_at);
+    int4* lla = reinterpret_cast<int4*>(sm + L.llist_a);
+    int4* llt = reinterpret_cast<int4*>(sm + L.llist_at);
+    uint32_t* ma = reinterpret_cast<uint32_t*>(sm + L.lmask_a);
+    uint32_t* mt = reinterpret_cast<uint32_t*>(sm + L.lmask_at);
+    for (int q = tid; q < a.nslices; q += nt) {
+        la[q] = a.list[q];
+        ma[q] = a.lmask[q];
+    }
+    for (int q = tid; q < t.nslices; q += nt) {
+        lt[q] = t.list[q];
+        mt[q] = t.lmask[q];
+    }
+    for (int q = tid; q < a.nlong; q += nt) lla[q] = a.long_list[q];
+    for (int q = tid; q < t.nlong; q += nt) llt[q] = t.long_list[q];
+    if (!L.mat_smem) return;
+    const uint32_t a_add = static_cast<uint32_t>(L.arr[kXbar] / unit), t_add = static_cast<uint32_t>(L.arr[kY] / unit);
+    auto put = [&](uint32_t* dst, const uint32_t* src, int64_t count, uint32_t add) {
+        for (int64_t e = tid; e < count; e += nt) {
+            const uint32_t w = src[e];
+            dst[e] = (w & 0xffff0000u) | ((w & 0xffffu) + add);
+        }
+    };
+    put(reinterpret_cast<uint32_t*>(sm + L.mat_a_idx), a.pk, a.elems, a_add);
+    put(reinterpret_cast<uint32_t*>(sm + L.mat_at_idx), t.pk, t.elems, t_add);
+    put(reinterpret_cast<uint32_t*>(sm + L.mat_a_long), a.long_pk, a.long_elems, a_add);
+    put(reinterpret_cast<uint32_t*>(sm + L.mat_at_long), t.long_pk, t.long_elems, t_add);
+}
+
+// Stage one species' warp schedule (and, when the layout says so, its matrix
+// slices with 16-bit indices) into shared memory.
 template <typename T>
 __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned char* sm, int warps) {
+    if (L.recentred) {
+        stage_recentred_ops(sp, L, sm, warps, 4);
+        return;
+    }
     const int tid = threadIdx.x, nt = blockDim.x;
     int32_t* soa = reinterpret_cast<int32_t*>(sm + L.sched_a_off);
     int32_t* sot = reinterpret_cast<int32_t*>(sm + L.sched_at_off);
@@ -225,23 +281,7 @@ __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned ch
     int4* lt = reinterpret_cast<int4*>(sm + L.list_at);
     for (int t = tid; t < sp->a_nslices; t += nt) la[t] = sp->a_list[t];
     for (int t = tid; t < sp->at_nslices; t += nt) lt[t] = sp->at_list[t];
-    if (L.recentred) {
-        // packed words (16-bit index | BF16 value) with the index pre-offset
-        // to the FP32 gather targets dxbar (A slices) and dy (A^T slices)
-        if (L.mat_smem) {
-            uint32_t* pa = reinterpret_cast<uint32_t*>(sm + L.mat_a_idx);
-            uint32_t* pt = reinterpret_cast<uint32_t*>(sm + L.mat_at_idx);
-            const uint32_t a_add = static_cast<uint32_t>(L.arr[kXbar] / 4), t_add = static_cast<uint32_t>(L.arr[kY] / 4);
-            for (int64_t e = tid; e < sp->a_elems; e += nt) {
-                const uint32_t w = sp->a_pk[e];
-                pa[e] = (w & 0xffff0000u) | ((w & 0xffffu) + a_add);
-            }
-            for (int64_t e = tid; e < sp->at_elems; e += nt) {
-                const uint32_t w = sp->at_pk[e];
-                pt[e] = (w & 0xffff0000u) | ((w & 0xffffu) + t_add);
-            }
-        }
-    } else if (L.unscaled) {
+    if (L.unscaled) {
         // unscaled FP32 values; indices pre-offset to the FP64 gather targets
         // z (A pass) and w (A^T pass)
         uint16_t* ai = reinterpret_cast<uint16_t*>(sm + L.mat_a_idx);
@@ -264,7 +304,7 @@ __device__ void stage_species(const DevSpecies* sp, const Layout& L, unsigned ch
         T* tv = reinterpret_cast<T*>(sm + L.mat_at_val);
         const T* ga = Vals<T>::a(sp);
         const T* gt = Vals<T>::at(sp);
-        const bool fast = layout_is_fast<T>(L) || L.recentred;
+        const bool fast = layout_is_fast<T>(L);
         const int a_add = fast ? static_cast<int>(L.arr[kXbar] / sizeof(T)) : 0;
         const int t_add = fast ? static_cast<int>(L.arr[kY] / sizeof(T)) : 0;
         for (int64_t e = tid; e < sp->a_elems; e += nt) {
@@ -925,8 +965,6 @@ __device__ __forceinline__ float slice_dot_pk_global(const uint32_t* __restrict_
     return a0 + a1;
 }
 
-// STAGED: the species' packed matrix words are in shared memory (indices
-// pre-offset to the gather target); otherwise they are streamed from L2.
 // Per-instance patched entries held by the CTA for the current instance.
 struct Patches {
     int n;
@@ -936,75 +974,195 @@ struct Patches {
     const double* v64;
 };
 
-template <bool STAGED, bool PATCHED>
-__device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PT,
-                                                      const int4* atlist, int t0, int t1, int n, int lane, float tau,
-                                                      float w, float rho, bool check, const double* bx, double* cx,
-                                                      double& pdx2, double& pdxa2, const Patches& pt) {
+// One operand of the re-centred kernels as the calling warp sees it: its
+// slices and long lines, the per-slice long-lane masks and, when the matrix
+// is staged, the packed words in shared memory (indices pre-offset to the
+// gather target); otherwise the words are streamed from global memory.
+struct OpsView {
+    const int4* list;
+    int t0, t1;               // this warp's slices
+    const int4* llist;
+    int l0, l1;               // this warp's long lines
+    const uint32_t* lmask;    // per slice id
+    const uint32_t* words;    // staged slice words (or null)
+    const uint32_t* lwords;   // staged long-line words (or null)
+};
+
+// The calling warp's views of A (the dual pass) and A^T (the primal pass)
+// from a re-centred layout staged in shared memory.
+__device__ __forceinline__ void ops_views(const Layout& L, const unsigned char* sm, int warp, OpsView* A, OpsView* T) {
+    const int32_t* soa = reinterpret_cast<const int32_t*>(sm + L.sched_a_off);
+    const int32_t* sot = reinterpret_cast<const int32_t*>(sm + L.sched_at_off);
+    const int32_t* loa = reinterpret_cast<const int32_t*>(sm + L.lsched_a_off);
+    const int32_t* lot = reinterpret_cast<const int32_t*>(sm + L.lsched_at_off);
+    A->list = reinterpret_cast<const int4*>(sm + L.list_a);
+    T->list = reinterpret_cast<const int4*>(sm + L.list_at);
+    A->llist = reinterpret_cast<const int4*>(sm + L.llist_a);
+    T->llist = reinterpret_cast<const int4*>(sm + L.llist_at);
+    A->lmask = reinterpret_cast<const uint32_t*>(sm + L.lmask_a);
+    T->lmask = reinterpret_cast<const uint32_t*>(sm + L.lmask_at);
+    A->t0 = soa[warp];
+    A->t1 = soa[warp + 1];
+    T->t0 = sot[warp];
+    T->t1 = sot[warp + 1];
+    A->l0 = loa[warp];
+    A->l1 = loa[warp + 1];
+    T->l0 = lot[warp];
+    T->l1 = lot[warp + 1];
+    A->words = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_a_idx) : nullptr;
+    T->words = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_at_idx) : nullptr;
+    A->lwords = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_a_long) : nullptr;
+    T->lwords = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_at_long) : nullptr;
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Product of one long line's packed words with the gather target g, the
+// whole warp together: lane l takes entries l, l + 32, ... in order, then a
+// fixed xor-shuffle tree; every lane returns the sum.  GLOBAL: words from
+// global memory (raw indices relative to g).
+template <bool GLOBAL>
+__device__ __forceinline__ float long_dot_pk(const uint32_t* wp, const float* g, int len, int lane) {
+    float acc = 0.0f;
+    for (int k = lane; k < len; k += 32) {
+        const uint32_t w = GLOBAL ? __ldg(wp + k) : wp[k];
+        acc = fmaf(__uint_as_float(w & 0xffff0000u), g[w & 0xffffu], acc);
+    }
+    return warp_sum_f(acc);
+}
+
+// The FP64 product of one long line for the convergence test (the same
+// order): indices from the staged words (minus the gather-target offset
+// `sub`) or from global memory, FP64 values from global memory.
+template <bool STAGED>
+__device__ __forceinline__ double long_dot64(const uint32_t* wp, int sub, const int32_t* __restrict__ ip,
+                                             const double* __restrict__ vp, const double* g, int len, int lane) {
+    double acc = 0.0;
+    for (int k = lane; k < len; k += 32) {
+        const int i = STAGED ? static_cast<int>(wp[k] & 0xffffu) - sub : __ldg(ip + k);
+        acc = fma(__ldg(vp + k), g[i], acc);
+    }
+    return warp_sum_d(acc);
+}
+
+// The primal update of column j (shared by the slice lanes and the long
+// columns' lane 0).
+__device__ __forceinline__ void primal_update(const FastOffsets& o, int j, float xo, float dj, float lj, float uj,
+                                              float g, float tau, float w, float rho, bool check, const double* bx,
+                                              double* cx, double& pdx2, double& pdxa2) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
-    for (int t = t0; t < t1; ++t) {
-        const int4 sl = atlist[t];
+    // explicit roundings (no contraction choice left to the compiler): the
+    // paired kernel repeats them bit for bit
+    const float xn = clampT(__fmaf_rn(-tau, __fsub_rn(dj, g), xo), lj, uj);
+    const float xb = __fsub_rn(__fadd_rn(xn, xn), xo);
+    S[o.xbar + j] = xb;
+    const float xh = (rho == 1.0f) ? xb : (1.0f + rho) * xn - rho * xo;
+    S[o.x + j] = __fmul_rn(w, xh);  // the anchor is the base: dx_anchor = 0
+    if (check) {
+        cx[j] = bx[j] + static_cast<double>(xn);
+        const double d = static_cast<double>(xn) - static_cast<double>(xo);
+        pdx2 += d * d;
+        pdxa2 += static_cast<double>(xn) * static_cast<double>(xn);
+    }
+}
+
+__device__ __forceinline__ void dual_update(const FastOffsets& o, int i, int neq, float yo, float ri, float yl,
+                                            float h, float sigma, float w, float rho, bool check, const double* by,
+                                            double* cy, double& pdy2, double& pdya2) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float* const S = reinterpret_cast<float*>(dyn_smem);
+    float yn = __fmaf_rn(sigma, __fsub_rn(ri, h), yo);
+    if (i >= neq && yn > yl) yn = yl;  // y^ + dy <= 0
+    const float yh = (rho == 1.0f) ? __fsub_rn(__fadd_rn(yn, yn), yo) : (1.0f + rho) * yn - rho * yo;
+    S[o.y + i] = __fmul_rn(w, yh);
+    if (check) {
+        cy[i] = by[i] + static_cast<double>(yn);
+        const double d = static_cast<double>(yn) - static_cast<double>(yo);
+        pdy2 += d * d;
+        pdya2 += static_cast<double>(yn) * static_cast<double>(yn);
+    }
+}
+
+// STAGED: the species' packed matrix words are in shared memory (indices
+// pre-offset to the gather target); otherwise they are streamed from L2.
+template <bool STAGED, bool PATCHED>
+__device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const OpsView& T,
+                                                      int n, int lane, float tau, float w, float rho, bool check,
+                                                      const double* bx, double* cx, double& pdx2, double& pdxa2,
+                                                      const Patches& pt) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float* const S = reinterpret_cast<float*>(dyn_smem);
+    for (int t = T.t0; t < T.t1; ++t) {
+        const int4 sl = T.list[t];
         const int j = (sl.x << 5) + lane;
-        const bool own = j < n;
-        const int jj = own ? j : 0;
+        const bool own = j < n && !((T.lmask[sl.x] >> lane) & 1u);
+        const int jj = j < n ? j : 0;
         // the column's operands first: their latency overlaps the product
         const float xo = S[o.x + jj], dj = S[o.c + jj], lj = S[o.l + jj], uj = S[o.u + jj];
         float g = STAGED
-            ? slice_dot_pk(PT + sl.y + lane, S, sl.z)
-            : slice_dot_pk_global(sp->at_pk + sl.y + lane, S + o.y, sl.z);
+            ? slice_dot_pk(T.words + sl.y + lane, S, sl.z)
+            : slice_dot_pk_global(sp->rat.pk + sl.y + lane, S + o.y, sl.z);
         if (PATCHED && sl.w && pt.n)  // a slice holding a patched column
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fmaf(pt.v32[q], S[o.y + pt.row[q]], g);
-        if (own) {
-            // explicit roundings (no contraction choice left to the compiler):
-            // the paired kernel repeats them bit for bit
-            const float xn = clampT(__fmaf_rn(-tau, __fsub_rn(dj, g), xo), lj, uj);
-            const float xb = __fsub_rn(__fadd_rn(xn, xn), xo);
-            S[o.xbar + j] = xb;
-            const float xh = (rho == 1.0f) ? xb : (1.0f + rho) * xn - rho * xo;
-            S[o.x + j] = __fmul_rn(w, xh);  // the anchor is the base: dx_anchor = 0
-            if (check) {
-                cx[j] = bx[j] + static_cast<double>(xn);
-                const double d = static_cast<double>(xn) - static_cast<double>(xo);
-                pdx2 += d * d;
-                pdxa2 += static_cast<double>(xn) * static_cast<double>(xn);
-            }
-        }
+        if (own) primal_update(o, j, xo, dj, lj, uj, g, tau, w, rho, check, bx, cx, pdx2, pdxa2);
+    }
+    for (int t = T.l0; t < T.l1; ++t) {  // long columns: the warp together, lane 0 updates
+        const int4 ll = T.llist[t];
+        const int j = ll.x;
+        float g = STAGED ? long_dot_pk<false>(T.lwords + ll.y, S, ll.z, lane)
+                         : long_dot_pk<true>(sp->rat.long_pk + ll.y, S + o.y, ll.z, lane);
+        if (PATCHED && pt.n)
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.col[q] == j) g = fmaf(pt.v32[q], S[o.y + pt.row[q]], g);
+        if (lane == 0)
+            primal_update(o, j, S[o.x + j], S[o.c + j], S[o.l + j], S[o.u + j], g, tau, w, rho, check, bx, cx, pdx2,
+                          pdxa2);
     }
 }
 
 template <bool STAGED, bool PATCHED>
-__device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const uint32_t* PA,
-                                                    const int4* alist, int t0, int t1, int m, int neq, int lane,
-                                                    float sigma, float w, float rho, bool check, const double* by,
-                                                    double* cy, double& pdy2, double& pdya2, const Patches& pt) {
+__device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const OpsView& A,
+                                                    int m, int neq, int lane, float sigma, float w, float rho,
+                                                    bool check, const double* by, double* cy, double& pdy2,
+                                                    double& pdya2, const Patches& pt) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
-    for (int t = t0; t < t1; ++t) {
-        const int4 sl = alist[t];
+    for (int t = A.t0; t < A.t1; ++t) {
+        const int4 sl = A.list[t];
         const int i = (sl.x << 5) + lane;
-        const bool own = i < m;
-        const int ii = own ? i : 0;
+        const bool own = i < m && !((A.lmask[sl.x] >> lane) & 1u);
+        const int ii = i < m ? i : 0;
         const float yo = S[o.y + ii], ri = S[o.b + ii], yl = S[o.ya + ii];
         float h = STAGED
-            ? slice_dot_pk(PA + sl.y + lane, S, sl.z)
-            : slice_dot_pk_global(sp->a_pk + sl.y + lane, S + o.xbar, sl.z);
+            ? slice_dot_pk(A.words + sl.y + lane, S, sl.z)
+            : slice_dot_pk_global(sp->ra.pk + sl.y + lane, S + o.xbar, sl.z);
         if (PATCHED && sl.w && pt.n)  // a slice holding a patched row
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fmaf(pt.v32[q], S[o.xbar + pt.col[q]], h);
-        if (own) {
-            float yn = __fmaf_rn(sigma, __fsub_rn(ri, h), yo);
-            if (i >= neq && yn > yl) yn = yl;  // y^ + dy <= 0
-            const float yh = (rho == 1.0f) ? __fsub_rn(__fadd_rn(yn, yn), yo) : (1.0f + rho) * yn - rho * yo;
-            S[o.y + i] = __fmul_rn(w, yh);
-            if (check) {
-                cy[i] = by[i] + static_cast<double>(yn);
-                const double d = static_cast<double>(yn) - static_cast<double>(yo);
-                pdy2 += d * d;
-                pdya2 += static_cast<double>(yn) * static_cast<double>(yn);
-            }
-        }
+        if (own) dual_update(o, i, neq, yo, ri, yl, h, sigma, w, rho, check, by, cy, pdy2, pdya2);
+    }
+    for (int t = A.l0; t < A.l1; ++t) {  // long rows
+        const int4 ll = A.llist[t];
+        const int i = ll.x;
+        float h = STAGED ? long_dot_pk<false>(A.lwords + ll.y, S, ll.z, lane)
+                         : long_dot_pk<true>(sp->ra.long_pk + ll.y, S + o.xbar, ll.z, lane);
+        if (PATCHED && pt.n)
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.row[q] == i) h = fmaf(pt.v32[q], S[o.xbar + pt.col[q]], h);
+        if (lane == 0)
+            dual_update(o, i, neq, S[o.y + i], S[o.b + i], S[o.ya + i], h, sigma, w, rho, check, by, cy, pdy2, pdya2);
     }
 }
 
@@ -1066,6 +1224,51 @@ __device__ __forceinline__ double slice_dot64_global2(const int32_t* __restrict_
     return acc0 + acc1;
 }
 
+// One column's contribution to the FP64 KKT partials (see
+// kkt_partials_recentred).
+__device__ __forceinline__ void kkt_column(const DevSpecies* sp, int j, double g, double* xc, const double* cs,
+                                           const double* ls, const double* us, float* dcand, bool cinf, double* v) {
+    const double cj = cs[j], lj = ls[j], uj = us[j], dcj = __ldg(sp->dc + j);
+    double xsc = xc[j];
+    if (xsc < lj || xsc > uj) {
+        xsc = xsc < lj ? lj : uj;
+        xc[j] = xsc;
+    }
+    const double rs = cj - g;
+    dcand[j] = static_cast<float>(rs);
+    v[0] += cj * xsc;
+    if (rs > 0.0) {
+        if (isfinite(lj)) v[2] += rs * lj;
+        else v[11] = fmax(v[11], rs * __ldg(sp->inv_dc + j));
+    } else if (rs < 0.0) {
+        if (isfinite(uj)) v[2] += rs * uj;
+        else v[11] = fmax(v[11], -rs * __ldg(sp->inv_dc + j));
+    }
+    const double tg = (rs >= 0.0) ? lj : uj;
+    if (isfinite(tg)) v[3] += fabs(rs * (xsc - tg));
+    v[12] = fmax(v[12], dcj * fmax(lj - xsc, xsc - uj));
+    v[13] = fmax(v[13], fabs(xsc * dcj));
+    if (cinf) v[14] = fmax(v[14], fabs(cj * __ldg(sp->inv_dc + j)));
+    if (isnan(g) || isnan(xsc)) v[15] = 1.0;
+}
+
+__device__ __forceinline__ void kkt_row(const DevSpecies* sp, int i, double h, const double* yc, const double* bs,
+                                        float* rcand, double* v) {
+    const double bi = bs[i], ysc = yc[i];
+    const double rr = bi - h;                        // scaled b - A x
+    const double ro = -rr * __ldg(sp->inv_dr + i);   // A x - b in original units
+    rcand[i] = static_cast<float>(rr);
+    if (i < sp->neq) {
+        v[10] = fmax(v[10], fabs(ro));
+    } else {
+        v[10] = fmax(v[10], ro);
+        v[4] += fabs(ysc * rr);
+        v[11] = fmax(v[11], ysc * __ldg(sp->dr + i));
+    }
+    v[1] += bi * ysc;
+    if (isnan(h) || isnan(ysc)) v[15] = 1.0;
+}
+
 // FP64 KKT partials at the candidate (xc, yc) (scaled, FP64) in the index
 // map of kkt_partials, computed in scaled space with the slab's scaled
 // objective cs, bounds ls/us and right-hand side bs (c.x = cs.xs,
@@ -1073,79 +1276,58 @@ __device__ __forceinline__ double slice_dot64_global2(const int32_t* __restrict_
 // The candidate x is projected onto the exact FP64 bounds (written back: the
 // FP32 bounds l - x^ are rounded), and rs and the scaled primal residual
 // bs - A~ xc are stored in FP32 for a re-centring at this candidate.
-// |c|_inf (v[14]) is accumulated only when `cinf` is set.  All threads call
-// it (it synchronises between the column and the row loops).
+// |c|_inf (v[14]) is accumulated only when `cinf` is set.  Long lines are
+// walked by the whole warp and counted by its lane 0.  All threads call it
+// (it synchronises between the column and the row loops).
 template <bool STAGED, bool PATCHED>
-__device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const uint32_t* PA, const uint32_t* PT,
-                                                    const int4* alist, const int4* atlist, int a0, int a1, int t0,
-                                                    int t1, int a_sub, int t_sub, double* xc, const double* yc,
-                                                    const double* cs, const double* ls, const double* us,
-                                                    const double* bs, float* dcand, float* rcand, bool cinf, int lane,
-                                                    double* v, const Patches& pt) {
-    const int n = sp->n, m = sp->m, neq = sp->neq;
-    for (int t = t0; t < t1; ++t) {
-        const int4 sl = atlist[t];
+__device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const OpsView& A, const OpsView& T, int a_sub,
+                                                    int t_sub, double* xc, const double* yc, const double* cs,
+                                                    const double* ls, const double* us, const double* bs,
+                                                    float* dcand, float* rcand, bool cinf, int lane, double* v,
+                                                    const Patches& pt) {
+    const int n = sp->n, m = sp->m;
+    for (int t = T.t0; t < T.t1; ++t) {
+        const int4 sl = T.list[t];
         const int j = (sl.x << 5) + lane;
-        const bool own = j < n;
-        const int jj = own ? j : 0;
-        const double cj = cs[jj], lj = ls[jj], uj = us[jj], dcj = __ldg(sp->dc + jj);
-        double xsc = xc[jj];
         double g = STAGED
-            ? slice_dot64_staged(PT + sl.y + lane, t_sub, sp->at_v64 + sl.y + lane, yc, sl.z)
-            : slice_dot64_global2(sp->at_idx + sl.y + lane, sp->at_v64 + sl.y + lane, yc, sl.z);
+            ? slice_dot64_staged(T.words + sl.y + lane, t_sub, sp->rat.v64 + sl.y + lane, yc, sl.z)
+            : slice_dot64_global2(sp->rat.idx + sl.y + lane, sp->rat.v64 + sl.y + lane, yc, sl.z);
         if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fma(pt.v64[q], yc[pt.row[q]], g);
-        if (own) {
-            if (xsc < lj || xsc > uj) {
-                xsc = xsc < lj ? lj : uj;
-                xc[j] = xsc;
-            }
-            const double rs = cj - g;
-            dcand[j] = static_cast<float>(rs);
-            v[0] += cj * xsc;
-            if (rs > 0.0) {
-                if (isfinite(lj)) v[2] += rs * lj;
-                else v[11] = fmax(v[11], rs * __ldg(sp->inv_dc + j));
-            } else if (rs < 0.0) {
-                if (isfinite(uj)) v[2] += rs * uj;
-                else v[11] = fmax(v[11], -rs * __ldg(sp->inv_dc + j));
-            }
-            const double tg = (rs >= 0.0) ? lj : uj;
-            if (isfinite(tg)) v[3] += fabs(rs * (xsc - tg));
-            v[12] = fmax(v[12], dcj * fmax(lj - xsc, xsc - uj));
-            v[13] = fmax(v[13], fabs(xsc * dcj));
-            if (cinf) v[14] = fmax(v[14], fabs(cj * __ldg(sp->inv_dc + j)));
-            if (isnan(g) || isnan(xsc)) v[15] = 1.0;
-        }
+        if (j < n && !((T.lmask[sl.x] >> lane) & 1u)) kkt_column(sp, j, g, xc, cs, ls, us, dcand, cinf, v);
+    }
+    for (int t = T.l0; t < T.l1; ++t) {
+        const int4 ll = T.llist[t];
+        const int j = ll.x;
+        double g = long_dot64<STAGED>(STAGED ? T.lwords + ll.y : nullptr, t_sub, sp->rat.long_idx + ll.y,
+                                      sp->rat.long_v64 + ll.y, yc, ll.z, lane);
+        if (PATCHED && pt.n)
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.col[q] == j) g = fma(pt.v64[q], yc[pt.row[q]], g);
+        if (lane == 0) kkt_column(sp, j, g, xc, cs, ls, us, dcand, cinf, v);
     }
     __syncthreads();  // the projected xc is the gather target below
-    for (int t = a0; t < a1; ++t) {
-        const int4 sl = alist[t];
+    for (int t = A.t0; t < A.t1; ++t) {
+        const int4 sl = A.list[t];
         const int i = (sl.x << 5) + lane;
-        const bool own = i < m;
-        const int ii = own ? i : 0;
-        const double bi = bs[ii], ysc = yc[ii];
         double h = STAGED
-            ? slice_dot64_staged(PA + sl.y + lane, a_sub, sp->a_v64 + sl.y + lane, xc, sl.z)
-            : slice_dot64_global2(sp->a_idx + sl.y + lane, sp->a_v64 + sl.y + lane, xc, sl.z);
+            ? slice_dot64_staged(A.words + sl.y + lane, a_sub, sp->ra.v64 + sl.y + lane, xc, sl.z)
+            : slice_dot64_global2(sp->ra.idx + sl.y + lane, sp->ra.v64 + sl.y + lane, xc, sl.z);
         if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fma(pt.v64[q], xc[pt.col[q]], h);
-        if (own) {
-            const double rr = bi - h;                  // scaled b - A x
-            const double ro = -rr * __ldg(sp->inv_dr + i);  // A x - b in original units
-            rcand[i] = static_cast<float>(rr);
-            if (i < neq) {
-                v[10] = fmax(v[10], fabs(ro));
-            } else {
-                v[10] = fmax(v[10], ro);
-                v[4] += fabs(ysc * rr);
-                v[11] = fmax(v[11], ysc * __ldg(sp->dr + i));
-            }
-            v[1] += bi * ysc;
-            if (isnan(h) || isnan(ysc)) v[15] = 1.0;
-        }
+        if (i < m && !((A.lmask[sl.x] >> lane) & 1u)) kkt_row(sp, i, h, yc, bs, rcand, v);
+    }
+    for (int t = A.l0; t < A.l1; ++t) {
+        const int4 ll = A.llist[t];
+        const int i = ll.x;
+        double h = long_dot64<STAGED>(STAGED ? A.lwords + ll.y : nullptr, a_sub, sp->ra.long_idx + ll.y,
+                                      sp->ra.long_v64 + ll.y, xc, ll.z, lane);
+        if (PATCHED && pt.n)
+            for (int q = 0; q < pt.n; ++q)
+                if (pt.row[q] == i) h = fma(pt.v64[q], xc[pt.col[q]], h);
+        if (lane == 0) kkt_row(sp, i, h, yc, bs, rcand, v);
     }
 }
 
@@ -1209,8 +1391,8 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         const FastOffsets o = fast_offsets<float>(L);
         // the staged packed words' indices carry the gather-target offsets
         const int a_sub = static_cast<int>(L.arr[kXbar] / 4), t_sub = static_cast<int>(L.arr[kY] / 4);
-        const uint32_t* const PA = reinterpret_cast<const uint32_t*>(dyn_smem + L.mat_a_idx);
-        const uint32_t* const PT = reinterpret_cast<const uint32_t*>(dyn_smem + L.mat_at_idx);
+        OpsView OA, OT;
+        ops_views(L, dyn_smem, warp, &OA, &OT);
         // the two point buffers; selected by value (no local-memory array)
         double* const px0 = reinterpret_cast<double*>(slab + L.pt_x[0]);
         double* const px1 = reinterpret_cast<double*>(slab + L.pt_x[1]);
@@ -1224,12 +1406,6 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         double* const ls = reinterpret_cast<double*>(slab + L.sc_l);
         double* const us = reinterpret_cast<double*>(slab + L.sc_u);
         double* const bs = reinterpret_cast<double*>(slab + L.sc_b);
-        const int4* alist = reinterpret_cast<const int4*>(dyn_smem + L.list_a);
-        const int4* atlist = reinterpret_cast<const int4*>(dyn_smem + L.list_at);
-        const int32_t* soa = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_a_off);
-        const int32_t* sot = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_at_off);
-        const int aw0 = soa[warp], aw1 = soa[warp + 1];
-        const int tw0 = sot[warp], tw1 = sot[warp + 1];
         const double* lo_i = p.lower + coff;
         const double* up_i = p.upper + coff;
         const double* c_i = p.cost + coff;
@@ -1327,7 +1503,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             double v[kRed];
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-            kkt_partials_recentred<STAGED, PATCHED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(0), PY(0), cs, ls,
+            kkt_partials_recentred<STAGED, PATCHED>(sp, OA, OT, a_sub, t_sub, PX(0), PY(0), cs, ls,
                                    us, bs, dcand, rcand, true, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             cinf = s_tot[14];
@@ -1352,10 +1528,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             const float tau = static_cast<float>(eta / omega), sigma = static_cast<float>(eta * omega);
             const float w = static_cast<float>((k + 1.0) / (k + 2.0));
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
-            primal_pass_recentred<STAGED, PATCHED>(sp, o, PT, atlist, tw0, tw1, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
+            primal_pass_recentred<STAGED, PATCHED>(sp, o, OT, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
                                           pdx2, pdxa2, pt);
             __syncthreads();
-            dual_pass_recentred<STAGED, PATCHED>(sp, o, PA, alist, aw0, aw1, m, neq, lane, sigma, w, rho, check, PY(cur),
+            dual_pass_recentred<STAGED, PATCHED>(sp, o, OA, m, neq, lane, sigma, w, rho, check, PY(cur),
                                         PY(cur ^ 1), pdy2, pdya2, pt);
             __syncthreads();
             ++k;
@@ -1368,7 +1544,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             v[6] = pdy2;
             v[7] = pdxa2;
             v[8] = pdya2;
-            kkt_partials_recentred<STAGED, PATCHED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
+            kkt_partials_recentred<STAGED, PATCHED>(sp, OA, OT, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
                                    cs, ls, us, bs, dcand, rcand, false, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             if (threadIdx.x == 0) s_tot[14] = cinf;
@@ -1423,7 +1599,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 double vv[kRed];
 #pragma unroll
                 for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-                kkt_partials_recentred<STAGED, PATCHED>(sp, PA, PT, alist, atlist, aw0, aw1, tw0, tw1, a_sub, t_sub, cx, cyv, cs, ls, us,
+                kkt_partials_recentred<STAGED, PATCHED>(sp, OA, OT, a_sub, t_sub, cx, cyv, cs, ls, us,
                                        bs, dcand, rcand, false, lane, vv, pt);
                 block_reduce(vv, s_red, s_tot);
                 cur ^= 1;
@@ -1539,27 +1715,7 @@ __device__ __forceinline__ PairOffsets pair_offsets(const Layout& L) {
 // region zeroed (both slots free).
 __device__ void stage_species_pair(const DevSpecies* sp, const Layout& L, unsigned char* sm, int warps) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    int32_t* soa = reinterpret_cast<int32_t*>(sm + L.sched_a_off);
-    int32_t* sot = reinterpret_cast<int32_t*>(sm + L.sched_at_off);
-    for (int w = tid; w <= warps; w += nt) {
-        soa[w] = sp->a_sched_off[w];
-        sot[w] = sp->at_sched_off[w];
-    }
-    int4* la = reinterpret_cast<int4*>(sm + L.list_a);
-    int4* lt = reinterpret_cast<int4*>(sm + L.list_at);
-    for (int t = tid; t < sp->a_nslices; t += nt) la[t] = sp->a_list[t];
-    for (int t = tid; t < sp->at_nslices; t += nt) lt[t] = sp->at_list[t];
-    uint32_t* pa = reinterpret_cast<uint32_t*>(sm + L.mat_a_idx);
-    uint32_t* pt = reinterpret_cast<uint32_t*>(sm + L.mat_at_idx);
-    const uint32_t a_add = static_cast<uint32_t>(L.arr[kXbar] / 8), t_add = static_cast<uint32_t>(L.arr[kY] / 8);
-    for (int64_t e = tid; e < sp->a_elems; e += nt) {
-        const uint32_t w = sp->a_pk[e];
-        pa[e] = (w & 0xffff0000u) | ((w & 0xffffu) + a_add);
-    }
-    for (int64_t e = tid; e < sp->at_elems; e += nt) {
-        const uint32_t w = sp->at_pk[e];
-        pt[e] = (w & 0xffff0000u) | ((w & 0xffffu) + t_add);
-    }
+    stage_recentred_ops(sp, L, sm, warps, 8);
     float2* const S2 = reinterpret_cast<float2*>(sm);
     const PairOffsets o = pair_offsets(L);
     const int n = sp->n, m = sp->m, mi = sp->m - sp->neq;
@@ -1614,6 +1770,20 @@ __device__ __forceinline__ float2 slice_dot_pk2(const uint32_t* wp, const float2
         a0y = fmaf(v0, g0.y, a0y);
     }
     return make_float2(a0x + a1x, a0y + a1y);
+}
+
+// One long line's product against both slots' gather targets, the whole
+// warp together (per slot the order of long_dot_pk).
+__device__ __forceinline__ float2 long_dot_pk2(const uint32_t* wp, const float2* g, int len, int lane) {
+    float ax = 0.0f, ay = 0.0f;
+    for (int k = lane; k < len; k += 32) {
+        const uint32_t w = wp[k];
+        const float2 gg = g[w & 0xffffu];
+        const float v = __uint_as_float(w & 0xffff0000u);
+        ax = fmaf(v, gg.x, ax);
+        ay = fmaf(v, gg.y, ay);
+    }
+    return make_float2(warp_sum_f(ax), warp_sum_f(ay));
 }
 
 // One slot's FP64 slab: the re-centred slab of pdhg_recentred.
@@ -1694,90 +1864,121 @@ __device__ __forceinline__ void clear_slot(const DevSpecies* sp, const PairOffse
     }
 }
 
-// Primal pass of both slots.  CHECK: some slot tests this iteration (c0 /
-// c1 say which); it then writes its candidate and accumulates pd[4 s + 0..1]
+// Primal update of column j in both slots (shared by the slice lanes and the
+// long columns' lane 0).  CHECK: some slot tests this iteration (c0 / c1
+// say which); it then writes its candidate and accumulates pd[4 s + 0..1]
 // (|xn - x|^2 and |xn|^2).  xo = wp xbar (reflection 1).
 template <bool CHECK>
-__device__ __forceinline__ void primal_pass_pair(const PairOffsets& o, int pt_off, int lt_off, int t0, int t1, int n,
-                                                 float2 tau, float2 wp, bool c0, bool c1, const double* bx0,
-                                                 double* cx0, const double* bx1, double* cx1, double* pd) {
+__device__ __forceinline__ void primal_update_pair(const PairOffsets& o, int j, float2 xbo, float2 dj, float2 lj,
+                                                   float2 uj, float2 g, float2 tau, float2 wp, bool c0, bool c1,
+                                                   const double* bx0, double* cx0, const double* bx1, double* cx1,
+                                                   double* pd) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
-    const uint32_t* const PT = reinterpret_cast<const uint32_t*>(dyn_smem + pt_off);
-    const int4* const atlist = reinterpret_cast<const int4*>(dyn_smem + lt_off);
-    const int lane = threadIdx.x & 31;
-    for (int t = t0; t < t1; ++t) {
-        const int4 sl = atlist[t];
-        const int j = (sl.x << 5) + lane;
-        const bool own = j < n;
-        const int jj = own ? j : 0;
-        const float2 xbo = S2[o.xbar + jj], dj = S2[o.c + jj], lj = S2[o.l + jj], uj = S2[o.u + jj];
-        const float2 g = slice_dot_pk2(PT + sl.y + lane, S2, sl.z);
-        if (own) {
-            const float xo0 = __fmul_rn(wp.x, xbo.x), xo1 = __fmul_rn(wp.y, xbo.y);
-            const float xn0 = clampT(__fmaf_rn(-tau.x, __fsub_rn(dj.x, g.x), xo0), lj.x, uj.x);
-            const float xn1 = clampT(__fmaf_rn(-tau.y, __fsub_rn(dj.y, g.y), xo1), lj.y, uj.y);
-            S2[o.xbar + j] = make_float2(__fsub_rn(__fadd_rn(xn0, xn0), xo0), __fsub_rn(__fadd_rn(xn1, xn1), xo1));
-            if (CHECK) {
-                if (c0) {
-                    cx0[j] = bx0[j] + static_cast<double>(xn0);
-                    const double d = static_cast<double>(xn0) - static_cast<double>(xo0);
-                    pd[0] += d * d;
-                    pd[1] += static_cast<double>(xn0) * static_cast<double>(xn0);
-                }
-                if (c1) {
-                    cx1[j] = bx1[j] + static_cast<double>(xn1);
-                    const double d = static_cast<double>(xn1) - static_cast<double>(xo1);
-                    pd[4] += d * d;
-                    pd[5] += static_cast<double>(xn1) * static_cast<double>(xn1);
-                }
-            }
+    const float xo0 = __fmul_rn(wp.x, xbo.x), xo1 = __fmul_rn(wp.y, xbo.y);
+    const float xn0 = clampT(__fmaf_rn(-tau.x, __fsub_rn(dj.x, g.x), xo0), lj.x, uj.x);
+    const float xn1 = clampT(__fmaf_rn(-tau.y, __fsub_rn(dj.y, g.y), xo1), lj.y, uj.y);
+    S2[o.xbar + j] = make_float2(__fsub_rn(__fadd_rn(xn0, xn0), xo0), __fsub_rn(__fadd_rn(xn1, xn1), xo1));
+    if (CHECK) {
+        if (c0) {
+            cx0[j] = bx0[j] + static_cast<double>(xn0);
+            const double d = static_cast<double>(xn0) - static_cast<double>(xo0);
+            pd[0] += d * d;
+            pd[1] += static_cast<double>(xn0) * static_cast<double>(xn0);
+        }
+        if (c1) {
+            cx1[j] = bx1[j] + static_cast<double>(xn1);
+            const double d = static_cast<double>(xn1) - static_cast<double>(xo1);
+            pd[4] += d * d;
+            pd[5] += static_cast<double>(xn1) * static_cast<double>(xn1);
         }
     }
 }
 
-// Dual pass of both slots (pd[4 s + 2..3] on check iterations).
 template <bool CHECK>
-__device__ __forceinline__ void dual_pass_pair(const PairOffsets& o, int pa_off, int la_off, int t0, int t1, int m,
-                                               int neq, float2 sigma, float2 w, bool c0, bool c1, const double* by0,
-                                               double* cy0, const double* by1, double* cy1, double* pd) {
+__device__ __forceinline__ void dual_update_pair(const PairOffsets& o, int i, int neq, float2 yo, float2 ri,
+                                                 float2 yl, float2 h, float2 sigma, float2 w, bool c0, bool c1,
+                                                 const double* by0, double* cy0, const double* by1, double* cy1,
+                                                 double* pd) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
-    const uint32_t* const PA = reinterpret_cast<const uint32_t*>(dyn_smem + pa_off);
-    const int4* const alist = reinterpret_cast<const int4*>(dyn_smem + la_off);
-    const int lane = threadIdx.x & 31;
-    for (int t = t0; t < t1; ++t) {
-        const int4 sl = alist[t];
-        const int i = (sl.x << 5) + lane;
-        const bool own = i < m;
-        const int ii = own ? i : 0;
-        const float2 yo = S2[o.y + ii], ri = S2[o.b + ii];
-        const float2 yl = (own && i >= neq) ? S2[o.ya + (i - neq)] : make_float2(0.0f, 0.0f);
-        const float2 h = slice_dot_pk2(PA + sl.y + lane, S2, sl.z);
-        if (own) {
-            float yn0 = __fmaf_rn(sigma.x, __fsub_rn(ri.x, h.x), yo.x);
-            float yn1 = __fmaf_rn(sigma.y, __fsub_rn(ri.y, h.y), yo.y);
-            if (i >= neq) {  // y^ + dy <= 0
-                if (yn0 > yl.x) yn0 = yl.x;
-                if (yn1 > yl.y) yn1 = yl.y;
-            }
-            S2[o.y + i] = make_float2(__fmul_rn(w.x, __fsub_rn(__fadd_rn(yn0, yn0), yo.x)),
-                                      __fmul_rn(w.y, __fsub_rn(__fadd_rn(yn1, yn1), yo.y)));
-            if (CHECK) {
-                if (c0) {
-                    cy0[i] = by0[i] + static_cast<double>(yn0);
-                    const double d = static_cast<double>(yn0) - static_cast<double>(yo.x);
-                    pd[2] += d * d;
-                    pd[3] += static_cast<double>(yn0) * static_cast<double>(yn0);
-                }
-                if (c1) {
-                    cy1[i] = by1[i] + static_cast<double>(yn1);
-                    const double d = static_cast<double>(yn1) - static_cast<double>(yo.y);
-                    pd[6] += d * d;
-                    pd[7] += static_cast<double>(yn1) * static_cast<double>(yn1);
-                }
-            }
+    float yn0 = __fmaf_rn(sigma.x, __fsub_rn(ri.x, h.x), yo.x);
+    float yn1 = __fmaf_rn(sigma.y, __fsub_rn(ri.y, h.y), yo.y);
+    if (i >= neq) {  // y^ + dy <= 0
+        if (yn0 > yl.x) yn0 = yl.x;
+        if (yn1 > yl.y) yn1 = yl.y;
+    }
+    S2[o.y + i] = make_float2(__fmul_rn(w.x, __fsub_rn(__fadd_rn(yn0, yn0), yo.x)),
+                              __fmul_rn(w.y, __fsub_rn(__fadd_rn(yn1, yn1), yo.y)));
+    if (CHECK) {
+        if (c0) {
+            cy0[i] = by0[i] + static_cast<double>(yn0);
+            const double d = static_cast<double>(yn0) - static_cast<double>(yo.x);
+            pd[2] += d * d;
+            pd[3] += static_cast<double>(yn0) * static_cast<double>(yn0);
         }
+        if (c1) {
+            cy1[i] = by1[i] + static_cast<double>(yn1);
+            const double d = static_cast<double>(yn1) - static_cast<double>(yo.y);
+            pd[6] += d * d;
+            pd[7] += static_cast<double>(yn1) * static_cast<double>(yn1);
+        }
+    }
+}
+
+// Primal pass of both slots over this warp's A^T slices and long columns.
+template <bool CHECK>
+__device__ __forceinline__ void primal_pass_pair(const PairOffsets& o, const OpsView& T, int n, float2 tau, float2 wp,
+                                                 bool c0, bool c1, const double* bx0, double* cx0, const double* bx1,
+                                                 double* cx1, double* pd) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
+    const int lane = threadIdx.x & 31;
+    for (int t = T.t0; t < T.t1; ++t) {
+        const int4 sl = T.list[t];
+        const int j = (sl.x << 5) + lane;
+        const bool own = j < n && !((T.lmask[sl.x] >> lane) & 1u);
+        const int jj = j < n ? j : 0;
+        const float2 xbo = S2[o.xbar + jj], dj = S2[o.c + jj], lj = S2[o.l + jj], uj = S2[o.u + jj];
+        const float2 g = slice_dot_pk2(T.words + sl.y + lane, S2, sl.z);
+        if (own) primal_update_pair<CHECK>(o, j, xbo, dj, lj, uj, g, tau, wp, c0, c1, bx0, cx0, bx1, cx1, pd);
+    }
+    for (int t = T.l0; t < T.l1; ++t) {
+        const int4 ll = T.llist[t];
+        const int j = ll.x;
+        const float2 g = long_dot_pk2(T.lwords + ll.y, S2, ll.z, lane);
+        if (lane == 0)
+            primal_update_pair<CHECK>(o, j, S2[o.xbar + j], S2[o.c + j], S2[o.l + j], S2[o.u + j], g, tau, wp, c0, c1,
+                                      bx0, cx0, bx1, cx1, pd);
+    }
+}
+
+// Dual pass of both slots over this warp's A slices and long rows.
+template <bool CHECK>
+__device__ __forceinline__ void dual_pass_pair(const PairOffsets& o, const OpsView& A, int m, int neq, float2 sigma,
+                                               float2 w, bool c0, bool c1, const double* by0, double* cy0,
+                                               const double* by1, double* cy1, double* pd) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
+    const int lane = threadIdx.x & 31;
+    const float2 z = make_float2(0.0f, 0.0f);
+    for (int t = A.t0; t < A.t1; ++t) {
+        const int4 sl = A.list[t];
+        const int i = (sl.x << 5) + lane;
+        const bool own = i < m && !((A.lmask[sl.x] >> lane) & 1u);
+        const int ii = i < m ? i : 0;
+        const float2 yo = S2[o.y + ii], ri = S2[o.b + ii];
+        const float2 yl = (i < m && i >= neq) ? S2[o.ya + (i - neq)] : z;
+        const float2 h = slice_dot_pk2(A.words + sl.y + lane, S2, sl.z);
+        if (own) dual_update_pair<CHECK>(o, i, neq, yo, ri, yl, h, sigma, w, c0, c1, by0, cy0, by1, cy1, pd);
+    }
+    for (int t = A.l0; t < A.l1; ++t) {
+        const int4 ll = A.llist[t];
+        const int i = ll.x;
+        const float2 h = long_dot_pk2(A.lwords + ll.y, S2, ll.z, lane);
+        if (lane == 0)
+            dual_update_pair<CHECK>(o, i, neq, S2[o.y + i], S2[o.b + i], i >= neq ? S2[o.ya + (i - neq)] : z, h,
+                                    sigma, w, c0, c1, by0, cy0, by1, cy1, pd);
     }
 }
 
@@ -1786,16 +1987,8 @@ struct PairCtx {
     const DevSpecies* sp;
     const Layout* L;
     PairOffsets o;
-    int pa_off, pt_off, la_off, lt_off;  // byte offsets into shared memory
-    int aw0, aw1, tw0, tw1, a_sub, t_sub;
-    __device__ const uint32_t* PA() const { return smem_at<uint32_t>(pa_off); }
-    __device__ const uint32_t* PT() const { return smem_at<uint32_t>(pt_off); }
-    __device__ const int4* alist() const { return smem_at<int4>(la_off); }
-    __device__ const int4* atlist() const { return smem_at<int4>(lt_off); }
-    template <typename T> __device__ static const T* smem_at(int off) {
-        extern __shared__ __align__(16) unsigned char dyn_smem[];
-        return reinterpret_cast<const T*>(dyn_smem + off);
-    }
+    OpsView A, T;            // this warp's views of the staged operands
+    int a_sub, t_sub;        // gather-target offsets of the staged indices (float2 units)
 };
 
 // The slot's results (original units and order) from its last evaluated
@@ -1923,8 +2116,7 @@ __device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairCt
     double v[kRed];
 #pragma unroll
     for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-    kkt_partials_recentred<true, false>(sp, c.PA(), c.PT(), c.alist(), c.atlist(), c.aw0, c.aw1, c.tw0, c.tw1, c.a_sub,
-                                        c.t_sub, b.px0, b.py0, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, true, lane_id(),
+    kkt_partials_recentred<true, false>(sp, c.A, c.T, c.a_sub, c.t_sub, b.px0, b.py0, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, true, lane_id(),
                                         v, nopatch);
     block_reduce(v, s_red, s_tot);
     st.cinf = s_tot[14];
@@ -1965,8 +2157,7 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairCt
     v[6] = pd[2];
     v[7] = pd[1];
     v[8] = pd[3];
-    kkt_partials_recentred<true, false>(sp, c.PA(), c.PT(), c.alist(), c.atlist(), c.aw0, c.aw1, c.tw0, c.tw1, c.a_sub,
-                                        c.t_sub, b.X(st.cur ^ 1), b.Y(st.cur ^ 1), b.cs, b.ls, b.us, b.bs, b.dcand,
+    kkt_partials_recentred<true, false>(sp, c.A, c.T, c.a_sub, c.t_sub, b.X(st.cur ^ 1), b.Y(st.cur ^ 1), b.cs, b.ls, b.us, b.bs, b.dcand,
                                         b.rcand, false, lane_id(), v, nopatch);
     block_reduce(v, s_red, s_tot);
     if (tid == 0) s_tot[14] = st.cinf;
@@ -2012,8 +2203,7 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairCt
         double vv[kRed];
 #pragma unroll
         for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-        kkt_partials_recentred<true, false>(sp, c.PA(), c.PT(), c.alist(), c.atlist(), c.aw0, c.aw1, c.tw0, c.tw1, c.a_sub,
-                                            c.t_sub, cx, cyv, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, false,
+        kkt_partials_recentred<true, false>(sp, c.A, c.T, c.a_sub, c.t_sub, cx, cyv, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, false,
                                             lane_id(), vv, nopatch);
         block_reduce(vv, s_red, s_tot);
         st.cur ^= 1;
@@ -2088,16 +2278,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
                     c.sp = p.species + species;
                     c.L = &p.layouts[species];
                     c.o = pair_offsets(L);
-                    c.pa_off = static_cast<int>(L.mat_a_idx);
-                    c.pt_off = static_cast<int>(L.mat_at_idx);
-                    c.la_off = static_cast<int>(L.list_a);
-                    c.lt_off = static_cast<int>(L.list_at);
-                    const int32_t* soa = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_a_off);
-                    const int32_t* sot = reinterpret_cast<const int32_t*>(dyn_smem + L.sched_at_off);
-                    c.aw0 = soa[warp];
-                    c.aw1 = soa[warp + 1];
-                    c.tw0 = sot[warp];
-                    c.tw1 = sot[warp + 1];
+                    ops_views(L, dyn_smem, warp, &c.A, &c.T);
                     c.a_sub = c.o.xbar;
                     c.t_sub = c.o.y;
                 }
@@ -2138,17 +2319,15 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
         for (int q = 0; q < 8; ++q) pd[q] = 0.0;
         if (chk[0] || chk[1]) {
             const PairSlab b0 = pair_slab(p, *c.L, 0), b1 = pair_slab(p, *c.L, 1);
-            primal_pass_pair<true>(c.o, c.pt_off, c.lt_off, c.tw0, c.tw1, n, tau2, wp2, chk[0], chk[1],
-                                   b0.X(st[0].cur), b0.X(st[0].cur ^ 1), b1.X(st[1].cur), b1.X(st[1].cur ^ 1), pd);
+            primal_pass_pair<true>(c.o, c.T, n, tau2, wp2, chk[0], chk[1], b0.X(st[0].cur), b0.X(st[0].cur ^ 1),
+                                   b1.X(st[1].cur), b1.X(st[1].cur ^ 1), pd);
             __syncthreads();
-            dual_pass_pair<true>(c.o, c.pa_off, c.la_off, c.aw0, c.aw1, m, neq, sig2, w2, chk[0], chk[1],
-                                 b0.Y(st[0].cur), b0.Y(st[0].cur ^ 1), b1.Y(st[1].cur), b1.Y(st[1].cur ^ 1), pd);
+            dual_pass_pair<true>(c.o, c.A, m, neq, sig2, w2, chk[0], chk[1], b0.Y(st[0].cur), b0.Y(st[0].cur ^ 1),
+                                 b1.Y(st[1].cur), b1.Y(st[1].cur ^ 1), pd);
         } else {
-            primal_pass_pair<false>(c.o, c.pt_off, c.lt_off, c.tw0, c.tw1, n, tau2, wp2, false, false, nullptr,
-                                    nullptr, nullptr, nullptr, pd);
+            primal_pass_pair<false>(c.o, c.T, n, tau2, wp2, false, false, nullptr, nullptr, nullptr, nullptr, pd);
             __syncthreads();
-            dual_pass_pair<false>(c.o, c.pa_off, c.la_off, c.aw0, c.aw1, m, neq, sig2, w2, false, false, nullptr,
-                                  nullptr, nullptr, nullptr, pd);
+            dual_pass_pair<false>(c.o, c.A, m, neq, sig2, w2, false, false, nullptr, nullptr, nullptr, nullptr, pd);
         }
         __syncthreads();
 #pragma unroll

@@ -37,6 +37,26 @@ constexpr int kMaxPatches = 8;  // per-instance matrix entries per species
 // w = dr * y is the gather target of the A^T pass.
 enum ArrayId { kXbar = 0, kY, kX, kXa, kYa, kC, kL, kU, kB, kXs, kYs, kW };
 
+// One operand of the re-centred kernels (A for the dual pass, A^T for the
+// primal pass): SELL-32 slices whose long lines (more than 32 entries) are
+// left out -- their lanes are empty and flagged in `lmask` -- and the long
+// lines stored unpadded, each walked by a whole warp.
+struct DevLines {
+    int32_t nslices, nlong;
+    int64_t elems, long_elems;
+    const int4* list;             // slices in warp-schedule order {slice, base, len, patched}
+    const int32_t* sched_off;     // [warps + 1] ranges of `list` per warp
+    const uint32_t* lmask;        // per slice: lanes whose line is long
+    const int4* long_list;        // long lines in warp order {line, base, len, 0}
+    const int32_t* long_sched_off;  // [warps + 1] ranges of `long_list` per warp
+    const uint32_t* pk;           // packed slice words (16-bit index | BF16 value)
+    const int32_t* idx;           // slice indices (pad -> n or m)
+    const double* v64;            // slice FP64 scaled values
+    const uint32_t* long_pk;      // long-line words
+    const int32_t* long_idx;
+    const double* long_v64;
+};
+
 struct DevSpecies {
     int32_t m, n, neq, pad_;
     int32_t a_nslices, at_nslices;
@@ -69,12 +89,11 @@ struct DevSpecies {
     const double* lo_at_val;
     const double* inv_dr;         // 1 / dr, new order
     const double* inv_dc;         // 1 / dc, new order
-    // the scaled matrix as packed 32-bit words in the SELL slices: the
-    // 16-bit index in the low half, the value rounded to BF16 in the high
-    // half (the re-centred phase's FP32 passes; null when n or m exceeds
-    // 16-bit indices)
-    const uint32_t* a_pk;
-    const uint32_t* at_pk;
+    // the re-centred phase's operands (long lines split off): the scaled
+    // matrix as packed 32-bit words, the 16-bit index in the low half, the
+    // value rounded to BF16 in the high half (pk null when n or m exceeds
+    // 16-bit indices), with FP64 values for its convergence tests
+    DevLines ra, rat;
     // per-instance matrix entries: instance i's matrix is A + sum_p
     // delta_ip e_{row p} e_{col p}^T (new numbering; the slices holding a
     // patched row / column carry w = 1 in their schedule entries); the scaled
@@ -96,6 +115,9 @@ struct Layout {
     int32_t unscaled, recentred;
     int64_t mat_a_idx, mat_at_idx, mat_a_val, mat_at_val;
     int64_t arr[kArrayCount];
+    // re-centred layouts only: the long lines' schedule offsets [warps + 1],
+    // lists (int4), per-slice lane masks (uint32) and packed words
+    int64_t lsched_a_off, lsched_at_off, llist_a, llist_at, lmask_a, lmask_at, mat_a_long, mat_at_long;
     // re-centred FP32 layout only (slab offsets): the two FP64 point buffers
     // of x (n+1) and y (m+1) -- base and candidate, roles swapped at every
     // re-centring -- and the FP32 reduced cost / primal residual of the last

@@ -164,19 +164,26 @@ Scaling scale_matrix(const Csr& a, int ruiz_iterations, int power_iterations, do
 
 Sell build_sell(const Csr& a, const std::vector<int32_t>& row_order,
                 const std::vector<int32_t>& col_rename, const std::vector<double>& row_scale,
-                const std::vector<double>& col_scale, int32_t pad_index) {
+                const std::vector<double>& col_scale, int32_t pad_index, int32_t long_cut) {
     Sell s;
     const int32_t rows = a.rows;
+    auto len = [&](int32_t r) { return static_cast<int32_t>(a.ptr[row_order[r] + 1] - a.ptr[row_order[r]]); };
+    auto is_long = [&](int32_t r) { return long_cut > 0 && len(r) > long_cut; };
     s.nslices = (rows + 31) / 32;
     s.off.assign(s.nslices + 1, 0);
     s.length.assign(s.nslices, 0);
+    s.lmask.assign(s.nslices, 0u);
+    s.long_off.assign(1, 0);
     for (int32_t sl = 0; sl < s.nslices; ++sl) {
         int32_t L = 0;
         for (int32_t lane = 0; lane < 32; ++lane) {
             int32_t r = sl * 32 + lane;
             if (r >= rows) break;
-            int32_t o = row_order[r];
-            L = std::max<int32_t>(L, static_cast<int32_t>(a.ptr[o + 1] - a.ptr[o]));
+            if (is_long(r)) {
+                s.lmask[sl] |= 1u << lane;
+                continue;
+            }
+            L = std::max<int32_t>(L, len(r));
         }
         s.length[sl] = L;
         s.off[sl + 1] = s.off[sl] + 32 * L;
@@ -188,6 +195,15 @@ Sell build_sell(const Csr& a, const std::vector<int32_t>& row_order,
             int32_t r = sl * 32 + lane;
             if (r >= rows) break;
             int32_t o = row_order[r];
+            if (is_long(r)) {
+                for (int64_t p = a.ptr[o]; p < a.ptr[o + 1]; ++p) {
+                    s.long_idx.push_back(col_rename[a.idx[p]]);
+                    s.long_val.push_back(a.val[p] * row_scale[o] * col_scale[a.idx[p]]);
+                }
+                s.long_line.push_back(r);
+                s.long_off.push_back(static_cast<int32_t>(s.long_idx.size()));
+                continue;
+            }
             int32_t k = 0;
             for (int64_t p = a.ptr[o]; p < a.ptr[o + 1]; ++p, ++k) {
                 int32_t e = s.off[sl] + k * 32 + lane;
@@ -217,6 +233,43 @@ void warp_schedule(const Sell& s, int warps, std::vector<int32_t>* sched_off,
         std::sort(lists[w].begin(), lists[w].end());
         for (int32_t sl : lists[w]) sched->push_back(sl);
         (*sched_off)[w + 1] = static_cast<int32_t>(sched->size());
+    }
+}
+
+void warp_schedule_split(const Sell& s, int warps, std::vector<int32_t>* sched_off, std::vector<int32_t>* sched,
+                         std::vector<int32_t>* long_sched_off, std::vector<int32_t>* long_sched) {
+    std::vector<int64_t> load(warps, 0);
+    std::vector<std::vector<int32_t>> lists(warps), llists(warps);
+    const int32_t nlong = static_cast<int32_t>(s.long_line.size());
+    std::vector<int32_t> lorder(nlong);
+    std::iota(lorder.begin(), lorder.end(), 0);
+    auto llen = [&](int32_t q) { return s.long_off[q + 1] - s.long_off[q]; };
+    std::stable_sort(lorder.begin(), lorder.end(), [&](int32_t x, int32_t y) { return llen(x) > llen(y); });
+    for (int32_t q : lorder) {
+        int w = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+        llists[w].push_back(q);
+        load[w] += (llen(q) + 31) / 32 + 8;
+    }
+    std::vector<int32_t> order(s.nslices);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return s.length[x] > s.length[y]; });
+    for (int32_t sl : order) {
+        int w = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+        lists[w].push_back(sl);
+        load[w] += s.length[sl] + 4;
+    }
+    sched_off->assign(warps + 1, 0);
+    long_sched_off->assign(warps + 1, 0);
+    sched->clear();
+    long_sched->clear();
+    for (int w = 0; w < warps; ++w) {
+        std::sort(lists[w].begin(), lists[w].end());
+        for (int32_t sl : lists[w]) sched->push_back(sl);
+        (*sched_off)[w + 1] = static_cast<int32_t>(sched->size());
+        std::sort(llists[w].begin(), llists[w].end());
+        for (int32_t q : llists[w]) long_sched->push_back(q);
+        (*long_sched_off)[w + 1] = static_cast<int32_t>(long_sched->size());
     }
 }
 

@@ -40,14 +40,32 @@ struct Sell {
     std::vector<int32_t> idx;
     std::vector<double> val;
     std::vector<int32_t> length; // slice lengths
+    // long lines (build_sell with a cut): rows longer than the cut are left
+    // out of the slices (their lanes are empty, flagged in lmask) and stored
+    // unpadded, one after another, for a warp to walk together
+    std::vector<uint32_t> lmask;    // per slice: bit `lane` set = a long line
+    std::vector<int32_t> long_line; // new index of each long line
+    std::vector<int32_t> long_off;  // long lines + 1, in elements
+    std::vector<int32_t> long_idx;
+    std::vector<double> long_val;
 };
 
 Sell build_sell(const Csr& a, const std::vector<int32_t>& row_order,
                 const std::vector<int32_t>& col_rename, const std::vector<double>& row_scale,
-                const std::vector<double>& col_scale, int32_t pad_index);
+                const std::vector<double>& col_scale, int32_t pad_index, int32_t long_cut = 0);
+
+// Rows longer than this many entries are long lines (walked by a whole warp
+// in the re-centred kernels): one warp step covers 32 of their entries.
+constexpr int32_t kLongCut = 32;
 
 // Greedy longest-first assignment of slices to `warps` warps.
 void warp_schedule(const Sell& s, int warps, std::vector<int32_t>* sched_off,
                    std::vector<int32_t>* sched);
+
+// The same with the long lines of a cut Sell: long lines first (cost
+// ceil(len / 32) + 8: strided loads, a shuffle reduction and one lane's
+// update), then the slices (cost len + 4).
+void warp_schedule_split(const Sell& s, int warps, std::vector<int32_t>* sched_off, std::vector<int32_t>* sched,
+                         std::vector<int32_t>* long_sched_off, std::vector<int32_t>* long_sched);
 
 }  // namespace fbalp
