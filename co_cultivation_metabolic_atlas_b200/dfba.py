@@ -72,7 +72,7 @@ class DeviceCommunity:
     def __init__(self, models, medium, biomass, *, dt=0.05, capacity=CARRYING_CAPACITY,
                  options: EngineOptions | None = None, config: SolveConfig | None = None,
                  warm_start: str = "previous", learned=None, horizon_steps: int = 960, device=None,
-                 parsimonious: bool = False):
+                 parsimonious: bool = False, stage2_config: SolveConfig | None = None):
         if warm_start not in ("cold", "previous", "extrapolate", "learned"):
             raise ValueError("warm_start must be 'cold', 'previous', 'extrapolate' or 'learned'")
         if warm_start == "learned" and learned is None:
@@ -129,6 +129,8 @@ class DeviceCommunity:
         self._which = 0
         self._wx = self._wy = None
         self.parsimonious = bool(parsimonious)
+        # the parsimonious LPs need 1e4 iterations where FBA needs 1e2-1e3
+        self.stage2_config = stage2_config or SolveConfig(max_iterations=100_000, fp32_max_iterations=100_000)
         self.engine2 = None
         if self.parsimonious:
             self._init_stage2(options)
@@ -212,8 +214,8 @@ class DeviceCommunity:
             self._wy2.zero_()
             self._wy2.index_put_((self._ymap,), res.y[:self.total_rows])
             omega = res.omega
-        res2 = self.engine2.solve(warm_x=self._wx2, warm_y=self._wy2[:nr], warm_omega=omega, config=self.config,
-                                  out=out)
+        res2 = self.engine2.solve(warm_x=self._wx2, warm_y=self._wy2[:nr], warm_omega=omega,
+                                  config=self.stage2_config, out=out)
         self.prev2_p, self.prev_p = self.prev_p, res2
         return res2
 

@@ -12,14 +12,21 @@ Here each species' FBA step gets that second stage:
     min  sum_j w_j t_j              over the exchange columns j
     s.t. S v = 0
          v_j - t_j <= 0,  -v_j - t_j <= 0
-         l <= v <= u,  v_growth >= mu* (1 - 1e-6)  (the stage-1 optimum)
+         l <= v <= u,  v_growth >= 0.99 mu*  (mu* the stage-1 optimum)
          0 <= t_j <= max(|l_j|, |u_j|)
 
-with seeded weights ``w_j = 1 + 0.1 U[0, 1]`` per species: distinct generic
+with seeded weights ``w_j = 10^U[0, 1]`` per species: distinct generic
 weights make the optimal exchange fluxes unique (equal weights leave ties
 between exchange routes of equal length), so every exact solver returns the
-same fluxes and the trajectories can be compared.  Column order
-``[v | t]``, rows ``[S; (E, -I); (-E, -I)]`` (equalities first).
+same fluxes and the trajectories can be compared.  Measured with the CPU
+restatement of the engine's re-centred PDHG on the weight-conserving
+community: growth held within 1e-6 of its optimum leaves a sliver of a
+feasible set on which first-order iterations stall (primal residual ~2e-5
+after 6e4 iterations), and weights within 10 % of each other leave nearly
+tied vertices (some LPs miss 6e4 iterations); a 1 % growth relaxation (the
+reference's stage-3 objective fraction plays this role) and weights spread
+over a decade certify every probed LP in 9-12 thousand iterations.  Column
+order ``[v | t]``, rows ``[S; (E, -I); (-E, -I)]`` (equalities first).
 """
 
 from __future__ import annotations
@@ -27,14 +34,14 @@ from __future__ import annotations
 import numpy as np
 from scipy.sparse import csr_matrix, hstack, identity, vstack
 
-GROWTH_RELAXATION = 1e-6   # relative slack of the stage-1 growth in stage 2
+GROWTH_RELAXATION = 1e-2   # relative slack of the stage-1 growth in stage 2
 GROWTH_FLOOR_ABS = 1e-9    # absolute slack (growth near zero)
 
 
 def exchange_weights(model, species_index: int) -> np.ndarray:
     """The seeded exchange weights of one species (``n_exchange``)."""
     rng = np.random.default_rng(7001 + int(species_index))
-    return 1.0 + 0.1 * rng.random(model.n_exchange)
+    return 10.0 ** rng.random(model.n_exchange)
 
 
 def stage_matrix(model):

@@ -90,7 +90,7 @@ def parsimonious_fluxes(model, species_index, lower, upper, growth):
     """The parsimonious second stage of one species' FBA LP restated with
     HiGHS (the reference's exact solver): minimise the weighted sum of
     absolute exchange fluxes (weights of ``parsimonious.exchange_weights``)
-    with growth held at ``growth`` (1 - 1e-6) - 1e-9, through the split
+    with growth held at ``growth (1 - GROWTH_RELAXATION) - 1e-9``, through the split
     ``t_j >= v_j, t_j >= -v_j`` (the pattern of
     ``_assemble_parsimonious_exchange_lp``, ``src/community_solver.py:
     116-204``).  Returns ``(status, fluxes v)``."""

@@ -10,7 +10,7 @@ to the stage-2 fluxes.
 
     python tests/golden/make_parsimonious_trajectory.py [--steps 960] [--workers 8]
 
-Takes about an hour on 8 cores (24 HiGHS solves per step).
+Takes about three hours on 8 cores (24 HiGHS solves per step).
 """
 
 from __future__ import annotations
