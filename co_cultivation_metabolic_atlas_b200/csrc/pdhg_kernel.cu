@@ -1811,7 +1811,8 @@ __device__ __forceinline__ PairSlab pair_slab(const KernelParams& p, const Layou
     return b;
 }
 
-// Per-slot solve state (block-uniform: every thread holds the same values).
+// Per-slot solve state (block-uniform: one copy in shared memory, written by
+// thread 0 between barriers).
 struct PairSlot {
     int inst;  // -1: free
     int cur, ev, k, it, stall;
@@ -1982,30 +1983,34 @@ __device__ __forceinline__ void dual_pass_pair(const PairOffsets& o, const OpsVi
     }
 }
 
-// Everything a slot's solve needs besides its state (block-uniform).
-struct PairCtx {
+// The staged species' context (in shared memory: one copy per CTA).
+struct PairStage {
+    Layout L;                 // the species' layout record
     const DevSpecies* sp;
-    const Layout* L;
-    PairOffsets o;
-    OpsView A, T;            // this warp's views of the staged operands
-    int a_sub, t_sub;        // gather-target offsets of the staged indices (float2 units)
 };
 
+// This warp's views of the staged operands, and the gather-target offsets of
+// the staged indices (float2 units).
+__device__ __forceinline__ void pair_views(const PairStage& g, OpsView* A, OpsView* T) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    ops_views(g.L, dyn_smem, threadIdx.x >> 5, A, T);
+}
+
 // The slot's results (original units and order) from its last evaluated
-// point, then the slot is freed.  All threads call it.
-__device__ __noinline__ void finish_pair_slot(const KernelParams& p, const PairCtx& c, PairSlot& st, int slot, int status,
-                                 const Metrics& M) {
-    const DevSpecies* sp = c.sp;
+// point; the slot's vector components are zeroed.  All threads call it.
+__device__ __noinline__ void finish_pair_slot(const KernelParams& p, const PairStage& g, int slot, int inst,
+                                              int64_t coff, int64_t roff, int ev, int it, double omega, int status,
+                                              const Metrics& M) {
+    const DevSpecies* sp = g.sp;
     const int n = sp->n, m = sp->m, tid = threadIdx.x, nthreads = blockDim.x;
-    const PairSlab b = pair_slab(p, *c.L, slot);
+    const PairSlab b = pair_slab(p, g.L, slot);
     const bool hand = p.handoff_list != nullptr && status == kStatusHandoff;
-    const double* fx = b.X(st.ev);
-    const double* fy = b.Y(st.ev);
+    const double* fx = b.X(ev);
+    const double* fy = b.Y(ev);
     double* ox = hand ? p.hand_x : p.out_x;
     double* oy = hand ? p.hand_y : p.out_y;
-    const int inst = st.inst;
-    const double* lo_i = p.lower + st.coff;
-    const double* up_i = p.upper + st.coff;
+    const double* lo_i = p.lower + coff;
+    const double* up_i = p.upper + coff;
     for (int j = tid; j < n; j += nthreads) {
         const int jo = sp->col_perm[j];
         double xv = fx[j] * sp->dc[j];
@@ -2013,13 +2018,13 @@ __device__ __noinline__ void finish_pair_slot(const KernelParams& p, const PairC
             const double lv = lo_i[jo], uv = up_i[jo];
             xv = xv < lv ? lv : (xv > uv ? uv : xv);
         }
-        ox[st.coff + jo] = xv;
+        ox[coff + jo] = xv;
     }
-    for (int i = tid; i < m; i += nthreads) oy[st.roff + sp->row_perm[i]] = fy[i] * sp->dr[i];
+    for (int i = tid; i < m; i += nthreads) oy[roff + sp->row_perm[i]] = fy[i] * sp->dr[i];
     if (tid == 0) {
-        if (p.hand_iters) p.hand_iters[inst] = st.it;
+        if (p.hand_iters) p.hand_iters[inst] = it;
         if (hand) {
-            p.hand_omega[inst] = st.omega;
+            p.hand_omega[inst] = omega;
             p.handoff_list[atomicAdd(p.handoff_count, 1)] = inst;
         } else {
             double* mo = p.out_metrics + static_cast<int64_t>(inst) * kMetrics;
@@ -2030,27 +2035,33 @@ __device__ __noinline__ void finish_pair_slot(const KernelParams& p, const PairC
             mo[4] = M.dobj;
             mo[5] = M.rgap;
             mo[6] = M.xinf;
-            mo[7] = st.omega;
+            mo[7] = omega;
             p.out_obj[inst] = M.pobj;
             p.out_status[inst] = status;
-            p.out_iters[inst] = st.it;
-            if (p.out_omega) p.out_omega[inst] = st.omega;
+            p.out_iters[inst] = it;
+            if (p.out_omega) p.out_omega[inst] = omega;
         }
     }
-    clear_slot(sp, c.o, slot);
-    st.inst = -1;
-    __syncthreads();  // the slab and the slot's components are reused
+    clear_slot(sp, pair_offsets(g.L), slot);
+}
+
+// Publish a slot's state computed (identically) by every thread.
+__device__ __forceinline__ void store_slot(PairSlot* s_st, int slot, const PairSlot& st) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_st[slot] = st;
+    __syncthreads();
 }
 
 // Load instance `inst` into slot `slot`: scaled data, start point and its
 // test; a start point that already passes finishes the slot at once.  All
 // threads call it.
-__device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairCtx& c, PairSlot& st, int slot, int inst,
-                                double (*s_red)[kRed], double* s_tot) {
-    const DevSpecies* sp = c.sp;
+__device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairStage& g, PairSlot* s_st, int slot,
+                                             int inst, double (*s_red)[kRed], double* s_tot) {
+    const DevSpecies* sp = g.sp;
     const int n = sp->n, m = sp->m, neq = sp->neq, tid = threadIdx.x, nthreads = blockDim.x;
-    const PairSlab b = pair_slab(p, *c.L, slot);
+    const PairSlab b = pair_slab(p, g.L, slot);
     const Patches nopatch{0, nullptr, nullptr, nullptr, nullptr};
+    PairSlot st{};
     st.inst = inst;
     st.coff = p.col_off[inst];
     st.roff = p.row_off[inst];
@@ -2107,17 +2118,18 @@ __device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairCt
             if (p.out_omega) p.out_omega[inst] = st.omega;
         }
         st.inst = -1;
-        __syncthreads();
+        store_slot(s_st, slot, st);
         return;
     }
     st.eta = sp->eta;
-    st.cur = 0;
-    st.ev = 0;
+    OpsView A, T;
+    pair_views(g, &A, &T);
+    const PairOffsets o = pair_offsets(g.L);
     double v[kRed];
 #pragma unroll
     for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-    kkt_partials_recentred<true, false>(sp, c.A, c.T, c.a_sub, c.t_sub, b.px0, b.py0, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, true, lane_id(),
-                                        v, nopatch);
+    kkt_partials_recentred<true, false>(sp, A, T, o.xbar, o.y, b.px0, b.py0, b.cs, b.ls, b.us, b.bs, b.dcand,
+                                        b.rcand, true, lane_id(), v, nopatch);
     block_reduce(v, s_red, s_tot);
     st.cinf = s_tot[14];
     const Metrics M = evaluate(s_tot, st.omega, p.tol_p, p.tol_d, p.tol_g);
@@ -2125,40 +2137,42 @@ __device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairCt
     if (M.conv) status = p.final_status;
     else if (p.max_iters <= 0) status = M.nan ? kStatusNumerical : kStatusIterationLimit;
     if (status >= 0) {
-        st.it = 0;
-        finish_pair_slot(p, c, st, slot, status, M);
+        finish_pair_slot(p, g, slot, inst, st.coff, st.roff, 0, 0, st.omega, status, M);
+        st.inst = -1;
+        store_slot(s_st, slot, st);
         return;
     }
-    recentre_pair(sp, c.o, slot, b.px0, b.py0, b.dcand, b.rcand, b.ls, b.us);
-    st.k = 0;
-    st.it = 0;
-    st.stall = 0;
-    st.fell_back = false;
+    recentre_pair(sp, o, slot, b.px0, b.py0, b.dcand, b.rcand, b.ls, b.us);
     st.early = p.hint_iters == nullptr || p.hint_iters[inst] < p.check_every;
     st.r_restart = INFINITY;
     st.r_prev = INFINITY;
     st.best_err = INFINITY;
-    __syncthreads();
+    store_slot(s_st, slot, st);
 }
 
 // The convergence test of slot `slot` after a check iteration (its
 // candidate is in the buffer cur ^ 1): termination, stall, hand-off, cold
 // fallback and restart rules of pdhg_recentred.  All threads call it.
-__device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairCtx& c, PairSlot& st, int slot, bool full,
-                                const double* pd, double (*s_red)[kRed], double* s_tot) {
-    const DevSpecies* sp = c.sp;
+__device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairStage& g, PairSlot* s_st, int slot,
+                                             bool full, double pdx2, double pdxa2, double pdy2, double pdya2,
+                                             double (*s_red)[kRed], double* s_tot) {
+    const DevSpecies* sp = g.sp;
     const int n = sp->n, m = sp->m, tid = threadIdx.x, nthreads = blockDim.x;
-    const PairSlab b = pair_slab(p, *c.L, slot);
+    const PairSlab b = pair_slab(p, g.L, slot);
     const Patches nopatch{0, nullptr, nullptr, nullptr, nullptr};
+    PairSlot st = s_st[slot];
+    OpsView A, T;
+    pair_views(g, &A, &T);
+    const PairOffsets o = pair_offsets(g.L);
     double v[kRed];
 #pragma unroll
     for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-    v[5] = pd[0];
-    v[6] = pd[2];
-    v[7] = pd[1];
-    v[8] = pd[3];
-    kkt_partials_recentred<true, false>(sp, c.A, c.T, c.a_sub, c.t_sub, b.X(st.cur ^ 1), b.Y(st.cur ^ 1), b.cs, b.ls, b.us, b.bs, b.dcand,
-                                        b.rcand, false, lane_id(), v, nopatch);
+    v[5] = pdx2;
+    v[6] = pdy2;
+    v[7] = pdxa2;
+    v[8] = pdya2;
+    kkt_partials_recentred<true, false>(sp, A, T, o.xbar, o.y, b.X(st.cur ^ 1), b.Y(st.cur ^ 1), b.cs, b.ls, b.us,
+                                        b.bs, b.dcand, b.rcand, false, lane_id(), v, nopatch);
     block_reduce(v, s_red, s_tot);
     if (tid == 0) s_tot[14] = st.cinf;
     __syncthreads();
@@ -2185,12 +2199,10 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairCt
             status = kStatusHandoff;
     }
     if (status >= 0) {
-        finish_pair_slot(p, c, st, slot, status, M);
-        return;
-    }
-    if (!full) return;
-    if (p.fallback_iters > 0 && !st.fell_back && st.it >= p.fallback_iters &&
-        (p.warm_x != nullptr || p.warm_y != nullptr)) {
+        finish_pair_slot(p, g, slot, st.inst, st.coff, st.roff, st.ev, st.it, st.omega, status, M);
+        st.inst = -1;
+    } else if (full && p.fallback_iters > 0 && !st.fell_back && st.it >= p.fallback_iters &&
+               (p.warm_x != nullptr || p.warm_y != nullptr)) {
         // cold fallback: evaluate the cold point in the candidate buffer
         // and re-centre there
         st.fell_back = true;
@@ -2203,33 +2215,31 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairCt
         double vv[kRed];
 #pragma unroll
         for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-        kkt_partials_recentred<true, false>(sp, c.A, c.T, c.a_sub, c.t_sub, cx, cyv, b.cs, b.ls, b.us, b.bs, b.dcand, b.rcand, false,
-                                            lane_id(), vv, nopatch);
+        kkt_partials_recentred<true, false>(sp, A, T, o.xbar, o.y, cx, cyv, b.cs, b.ls, b.us, b.bs, b.dcand,
+                                            b.rcand, false, lane_id(), vv, nopatch);
         block_reduce(vv, s_red, s_tot);
         st.cur ^= 1;
         st.ev = st.cur;
-        recentre_pair(sp, c.o, slot, b.X(st.cur), b.Y(st.cur), b.dcand, b.rcand, b.ls, b.us);
+        recentre_pair(sp, o, slot, b.X(st.cur), b.Y(st.cur), b.dcand, b.rcand, b.ls, b.us);
         st.k = 0;
         st.r_restart = INFINITY;
         st.r_prev = INFINITY;
         st.best_err = INFINITY;
         st.stall = 0;
-        __syncthreads();
-        return;
-    }
-    if (p.restarts && (M.r <= kBetaSufficient * st.r_restart ||
-                       (M.r <= kBetaNecessary * st.r_restart && M.r > st.r_prev) || st.k >= kBetaArtificial * st.it)) {
+    } else if (full && p.restarts &&
+               (M.r <= kBetaSufficient * st.r_restart || (M.r <= kBetaNecessary * st.r_restart && M.r > st.r_prev) ||
+                st.k >= kBetaArtificial * st.it)) {
         if (nx > 1e-10 && ny > 1e-10)
             st.omega = exp(kOmegaSmoothing * log(ny / nx) + (1.0 - kOmegaSmoothing) * log(st.omega));
         st.cur ^= 1;  // the candidate becomes the base
-        recentre_pair(sp, c.o, slot, b.X(st.cur), b.Y(st.cur), b.dcand, b.rcand, b.ls, b.us);
+        recentre_pair(sp, o, slot, b.X(st.cur), b.Y(st.cur), b.dcand, b.rcand, b.ls, b.us);
         st.k = 0;
         st.r_restart = M.r;
         st.r_prev = INFINITY;
-        __syncthreads();
-    } else {
+    } else if (full) {
         st.r_prev = M.r;
     }
+    store_slot(s_st, slot, st);
 }
 
 template <int MAXT>
@@ -2238,21 +2248,21 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
     __shared__ double s_red[MAXT / 32][kRed];
     __shared__ double s_tot[kRed];
     __shared__ int s_q;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    __shared__ PairSlot s_st[2];
+    __shared__ PairStage s_g;
+    const int tid = threadIdx.x;
     const int warps = blockDim.x >> 5;
     const int count = p.count_dev ? *p.count_dev : p.count;
-    PairSlot st[2];
-    st[0].inst = -1;
-    st[1].inst = -1;
+    if (tid < 2) s_st[tid].inst = -1;
+    __syncthreads();
     int staged = -1, pending = -1;
     bool drained = false;
-    PairCtx c{};
 
     for (;;) {
         // ---- fill the free slots from the work queue ----
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
-            while (st[s].inst < 0 && !drained) {
+            while (s_st[s].inst < 0 && !drained) {
                 int q = pending;
                 if (q < 0) {
                     if (tid == 0) s_q = atomicAdd(p.queue, 1);
@@ -2267,26 +2277,26 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
                 const int inst = p.order[q];
                 const int species = p.inst_species[inst];
                 if (species != staged) {
-                    if (st[s ^ 1].inst >= 0) {  // the other slot still runs the staged species
+                    if (s_st[s ^ 1].inst >= 0) {  // the other slot still runs the staged species
                         pending = q;
                         break;
                     }
-                    const Layout& L = p.layouts[species];
-                    stage_species_pair(p.species + species, L, dyn_smem, warps);
+                    // the species' layout record and context into shared memory
+                    constexpr int words = static_cast<int>(sizeof(Layout) / sizeof(int64_t));
+                    if (tid < words)
+                        reinterpret_cast<int64_t*>(&s_g.L)[tid] =
+                            reinterpret_cast<const int64_t*>(p.layouts + species)[tid];
+                    if (tid == 0) s_g.sp = p.species + species;
+                    __syncthreads();
+                    stage_species_pair(p.species + species, s_g.L, dyn_smem, warps);
                     __syncthreads();
                     staged = species;
-                    c.sp = p.species + species;
-                    c.L = &p.layouts[species];
-                    c.o = pair_offsets(L);
-                    ops_views(L, dyn_smem, warp, &c.A, &c.T);
-                    c.a_sub = c.o.xbar;
-                    c.t_sub = c.o.y;
                 }
                 pending = -1;
-                start_pair_slot(p, c, st[s], s, inst, s_red, s_tot);
+                start_pair_slot(p, s_g, s_st, s, inst, s_red, s_tot);
             }
         }
-        const bool a0 = st[0].inst >= 0, a1 = st[1].inst >= 0;
+        const bool a0 = s_st[0].inst >= 0, a1 = s_st[1].inst >= 0;
         if (!a0 && !a1) {
             if (pending >= 0) continue;
             break;
@@ -2294,48 +2304,66 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
 
         // ---- one iteration of every busy slot ----
         bool chk[2], full[2];
+        int it[2], k[2], cur[2];
         float tau[2], sig[2], w[2], wp[2];
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
-            PairSlot& t = st[s];
-            if (t.inst >= 0) {
-                ++t.it;
-                full[s] = (t.it % p.check_every == 0) || (t.it >= p.max_iters);
-                chk[s] = full[s] || (t.early && t.it >= 8 && t.it < p.check_every && (t.it & (t.it - 1)) == 0);
-                tau[s] = static_cast<float>(t.eta / t.omega);
-                sig[s] = static_cast<float>(t.eta * t.omega);
-                w[s] = static_cast<float>((t.k + 1.0) / (t.k + 2.0));
-                wp[s] = static_cast<float>(t.k / (t.k + 1.0));
+            const bool busy = s ? a1 : a0;
+            if (busy) {
+                it[s] = s_st[s].it + 1;
+                k[s] = s_st[s].k;
+                cur[s] = s_st[s].cur;
+                const double eta = s_st[s].eta, omega = s_st[s].omega;
+                full[s] = (it[s] % p.check_every == 0) || (it[s] >= p.max_iters);
+                chk[s] = full[s] || (s_st[s].early && it[s] >= 8 && it[s] < p.check_every && (it[s] & (it[s] - 1)) == 0);
+                tau[s] = static_cast<float>(eta / omega);
+                sig[s] = static_cast<float>(eta * omega);
+                w[s] = static_cast<float>((k[s] + 1.0) / (k[s] + 2.0));
+                wp[s] = static_cast<float>(k[s] / (k[s] + 1.0));
             } else {
+                it[s] = k[s] = cur[s] = 0;
                 full[s] = chk[s] = false;
                 tau[s] = sig[s] = w[s] = wp[s] = 0.0f;
             }
         }
         const float2 tau2 = make_float2(tau[0], tau[1]), sig2 = make_float2(sig[0], sig[1]);
         const float2 w2 = make_float2(w[0], w[1]), wp2 = make_float2(wp[0], wp[1]);
-        const int n = c.sp->n, m = c.sp->m, neq = c.sp->neq;
+        const DevSpecies* sp = s_g.sp;
+        const int n = sp->n, m = sp->m, neq = sp->neq;
+        const PairOffsets o = pair_offsets(s_g.L);
+        OpsView A, T;
+        pair_views(s_g, &A, &T);
         double pd[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) pd[q] = 0.0;
         if (chk[0] || chk[1]) {
-            const PairSlab b0 = pair_slab(p, *c.L, 0), b1 = pair_slab(p, *c.L, 1);
-            primal_pass_pair<true>(c.o, c.T, n, tau2, wp2, chk[0], chk[1], b0.X(st[0].cur), b0.X(st[0].cur ^ 1),
-                                   b1.X(st[1].cur), b1.X(st[1].cur ^ 1), pd);
+            const PairSlab b0 = pair_slab(p, s_g.L, 0), b1 = pair_slab(p, s_g.L, 1);
+            primal_pass_pair<true>(o, T, n, tau2, wp2, chk[0], chk[1], b0.X(cur[0]), b0.X(cur[0] ^ 1), b1.X(cur[1]),
+                                   b1.X(cur[1] ^ 1), pd);
             __syncthreads();
-            dual_pass_pair<true>(c.o, c.A, m, neq, sig2, w2, chk[0], chk[1], b0.Y(st[0].cur), b0.Y(st[0].cur ^ 1),
-                                 b1.Y(st[1].cur), b1.Y(st[1].cur ^ 1), pd);
+            dual_pass_pair<true>(o, A, m, neq, sig2, w2, chk[0], chk[1], b0.Y(cur[0]), b0.Y(cur[0] ^ 1),
+                                 b1.Y(cur[1]), b1.Y(cur[1] ^ 1), pd);
         } else {
-            primal_pass_pair<false>(c.o, c.T, n, tau2, wp2, false, false, nullptr, nullptr, nullptr, nullptr, pd);
+            primal_pass_pair<false>(o, T, n, tau2, wp2, false, false, nullptr, nullptr, nullptr, nullptr, nullptr);
             __syncthreads();
-            dual_pass_pair<false>(c.o, c.A, m, neq, sig2, w2, false, false, nullptr, nullptr, nullptr, nullptr, pd);
+            dual_pass_pair<false>(o, A, m, neq, sig2, w2, false, false, nullptr, nullptr, nullptr, nullptr, nullptr);
+        }
+        // every thread read this iteration's state before the barrier above
+        if (tid == 0) {
+            if (a0) {
+                s_st[0].it = it[0];
+                s_st[0].k = k[0] + 1;
+            }
+            if (a1) {
+                s_st[1].it = it[1];
+                s_st[1].k = k[1] + 1;
+            }
         }
         __syncthreads();
 #pragma unroll
         for (int s = 0; s < 2; ++s)
-            if (st[s].inst >= 0) ++st[s].k;
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-            if (chk[s]) check_pair_slot(p, c, st[s], s, full[s], pd + 4 * s, s_red, s_tot);
+            if (chk[s]) check_pair_slot(p, s_g, s_st, s, full[s], pd[4 * s], pd[4 * s + 1], pd[4 * s + 2], pd[4 * s + 3],
+                                        s_red, s_tot);
     }
 }
 
