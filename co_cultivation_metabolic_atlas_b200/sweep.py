@@ -7,9 +7,12 @@ columns), uneven batches of 1k / 4k / 16k / 64k instances in one launch.
 
 For every batch size: a cold solve of the whole batch, then a warm-started
 re-solve after a perturbation of every free exchange bound (the previous
-solutions as seeds, as in a dFBA step).  Prints one JSON line per batch:
-certified LPs/s, iteration distribution, streaming-model GB/s of the
-re-centred phase and the launch configuration (autotuned per batch with
+solutions as seeds, as in a dFBA step), and with ``--learned`` the same
+cold batch seeded by the learned warm start (one request network per
+species -- ``warmstart.RequestWarmStart``'s members -- trained on cold
+solves of training batches drawn with other seeds).  Prints one JSON line
+per batch: certified LPs/s, iteration distribution, streaming-model GB/s of
+the re-centred phase and the launch configuration (autotuned per batch with
 ``--autotune``).
 """
 
@@ -78,7 +81,65 @@ def streaming_bytes(models, sid, iters):
     return inst + mat
 
 
-def run(batch, models, args, device):
+def train_members(models, args, device, count=2048, seeds=(101, 102), epochs=20):
+    """One request network per species, trained on cold solves of
+    ``count``-instance training batches (seeds disjoint from the
+    evaluation batches')."""
+    from .warmstart import fit_request_member
+    mats = [(m.S, m.S.shape[0]) for m in models]
+    rows = [dict(lower=[], x=[], y=[], omega=[]) for _ in models]
+    for sd in seeds:
+        sid, lo, up, cost, _ = device_batch(models, count, args.mix, sd, device)
+        eng = LPEngine(mats, device=device)
+        eng.set_instances(sid, lo, up, cost)
+        res = eng.solve(config=SolveConfig())
+        co, ro, _, _ = eng.layout(sid)
+        ok = (res.status == 0).cpu().numpy()
+        lo_h, x_h, y_h, om = lo.cpu().numpy(), res.x.cpu().numpy(), res.y.cpu().numpy(), res.omega.cpu().numpy()
+        for i in np.flatnonzero(ok):
+            s, (m, n) = int(sid[i]), models[int(sid[i])].S.shape
+            rows[s]["lower"].append(lo_h[co[i]:co[i] + n])
+            rows[s]["x"].append(x_h[co[i]:co[i] + n])
+            rows[s]["y"].append(y_h[ro[i]:ro[i] + m])
+            rows[s]["omega"].append(om[i])
+        eng.close()
+    members = []
+    for s, mdl in enumerate(models):
+        d = {k: np.asarray(v) for k, v in rows[s].items()}
+        k = d["lower"].shape[0]
+        n, m = mdl.S.shape[1], mdl.S.shape[0]
+        member, _ = fit_request_member(d["lower"], np.broadcast_to(mdl.upper, (k, n)),
+                                       np.broadcast_to(mdl.cost, (k, n)), np.zeros((k, m)), d["x"], d["y"],
+                                       d["omega"], epochs=epochs, device=device)
+        members.append(member)
+    return members
+
+
+def learned_seed(models, members, sid, lower, eng, device):
+    """Flat (x, y, omega) warm start of a batch from the species' networks."""
+    co, ro, tc, tr = eng.layout(sid)
+    wx = torch.zeros(tc, dtype=torch.float64, device=device)
+    wy = torch.zeros(max(1, tr), dtype=torch.float64, device=device)
+    wo = torch.ones(len(sid), dtype=torch.float64, device=device)
+    lo_h = lower.cpu().numpy()
+    for s, (mdl, mem) in enumerate(zip(models, members)):
+        idx = np.flatnonzero(sid == s)
+        if idx.size == 0:
+            continue
+        m, n = mdl.S.shape
+        lo = np.stack([lo_h[co[i]:co[i] + n] for i in idx])
+        k = len(idx)
+        pred = mem.predict(mem.features(lo, np.broadcast_to(mdl.upper, (k, n)), np.broadcast_to(mdl.cost, (k, n)),
+                                        np.zeros((k, m))))
+        cols = torch.as_tensor(np.concatenate([co[i] + np.arange(n) for i in idx]), device=device)
+        rows = torch.as_tensor(np.concatenate([ro[i] + np.arange(m) for i in idx]), device=device)
+        wx[cols] = pred[:, :n].reshape(-1)
+        wy[rows] = pred[:, n:].reshape(-1)
+        wo[torch.as_tensor(idx, device=device)] = mem.omega
+    return wx, wy[:tr], wo
+
+
+def run(batch, models, args, device, members=None):
     sid, lo, up, cost, free_idx = device_batch(models, batch, args.mix, args.seed, device)
     mats = [(m.S, m.S.shape[0]) for m in models]
     opt, cfg, tuning = EngineOptions(), SolveConfig(), None
@@ -95,8 +156,12 @@ def run(batch, models, args, device):
     out = {"batch": batch, "mix": list(args.mix), "warps_per_block": opt.warps_per_block,
            "check_every": cfg.check_every}
     results = {}
-    for phase in ("cold", "warm"):
+    phases = ("cold", "learned", "warm") if members is not None else ("cold", "warm")
+    for phase in phases:
         kw = {}
+        if phase == "learned":
+            wx, wy, wo = learned_seed(models, members, sid, lo, eng, device)
+            kw = dict(warm_x=wx, warm_y=wy, warm_omega=wo)
         if phase == "warm":
             prev = results["cold_res"]
             lo2 = perturb(models, lo, free_idx, args.seed + 1, device)
@@ -137,14 +202,21 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--cache", default=None)
+    ap.add_argument("--learned", action="store_true",
+                    help="also solve each cold batch from the learned warm start (networks trained first)")
     args = ap.parse_args()
     device = torch.device("cuda", 0)
     t0 = time.perf_counter()
     models = syn.community_models(syn.LARGE_SIZES, fixed_fraction=0.2, duplicate_fraction=0.05)
     print(json.dumps({"workload": "scale sweep: species " + ", ".join(f"{m.S.shape[0]}x{m.S.shape[1]}" for m in models),
                       "generator_seconds": time.perf_counter() - t0}), flush=True)
+    members = None
+    if args.learned:
+        t1 = time.perf_counter()
+        members = train_members(models, args, device)
+        print(json.dumps({"learned_training_seconds": time.perf_counter() - t1}), flush=True)
     for b in args.batches:
-        print(json.dumps(run(b, models, args, device)), flush=True)
+        print(json.dumps(run(b, models, args, device, members)), flush=True)
 
 
 if __name__ == "__main__":
