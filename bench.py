@@ -77,7 +77,7 @@ def parse():
     ap.add_argument("--coop-sample", type=int, default=6, help="environments in the cooperative CPU sample")
     ap.add_argument("--profile", default=None, choices=("fba", "cooperative", "mlp"),
                     help="run a short profiling driver of one workload instead of the benchmark")
-    ap.add_argument("--warps", type=int, default=16, help="--profile fba: warps per CTA")
+    ap.add_argument("--warps", type=int, default=16, help="warps per CTA of the PDHG kernels")
     ap.add_argument("--coop-growth-cap", type=float, default=0.005,
                     help="coexistence growth upper bound (the reference simulator's 0.005 /h; <= 0: the solver "
                          "default 10)")
@@ -89,7 +89,7 @@ def workload_config(args, lps):
     return {"workload": f"community dFBA step: {args.envs} envs x 3 species "
                         f"({', '.join(f'{m}x{n}' for m, n in syn.COMMUNITY_SIZES)}), {lps} LPs/step, dt=0.05 h",
             "envs_per_gpu": args.envs, "lps_per_step": lps, "seed": args.seed,
-            "precision": args.precision,
+            "precision": args.precision, "warps_per_cta": args.warps,
             "l2": "inputs larger than L2 (bounds+objective of one step > 600 MB), no flush"}
 
 
@@ -392,8 +392,12 @@ def run_product(args):
                         "training": f"data-parallel over {world} rank(s)"}
         del data
 
+    from co_cultivation_metabolic_atlas_b200.engine import EngineOptions
+    options = EngineOptions(warps_per_block=args.warps)
+
     def trajectory(warm, learned=None):
-        com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, learned=learned, device=dev)
+        com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=warm, learned=learned, device=dev,
+                              options=options)
         first = None
         if args.warmup:
             # the first (history-free) step: the network's seed or a cold start
@@ -562,7 +566,9 @@ def run_e2e(args, models, medium, biomass, cfg, dev, barrier, max_over_ranks, su
     import torch
 
     from co_cultivation_metabolic_atlas_b200.dfba import DeviceCommunity
-    com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=args.warm, device=dev)
+    from co_cultivation_metabolic_atlas_b200.engine import EngineOptions
+    com = DeviceCommunity(models, medium, biomass, config=cfg, warm_start=args.warm, device=dev,
+                          options=EngineOptions(warps_per_block=args.warps))
     K = args.e2e_steps if args.e2e_steps > 0 else args.steps
     host_lower, host_state = [], []
     for _ in range(args.warmup + K):

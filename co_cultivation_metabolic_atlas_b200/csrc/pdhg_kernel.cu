@@ -979,14 +979,22 @@ struct Patches {
 // is staged, the packed words in shared memory (indices pre-offset to the
 // gather target); otherwise the words are streamed from global memory.
 struct OpsView {
-    const int4* list;
-    int t0, t1;               // this warp's slices
-    const int4* llist;
-    int l0, l1;               // this warp's long lines
-    const uint32_t* lmask;    // per slice id
-    const uint32_t* words;    // staged slice words (or null)
-    const uint32_t* lwords;   // staged long-line words (or null)
+    uint32_t list, llist, lmask;  // byte offsets into dynamic shared memory
+    uint32_t words, lwords;       // staged slice / long-line words (unused when streamed)
+    int t0, t1;                   // this warp's slices
+    int l0, l1;                   // this warp's long lines
 };
+
+// Shared-memory pointers from byte offsets (the extern array keeps the
+// accesses in the shared window).
+__device__ __forceinline__ const int4* sm_int4(uint32_t off) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    return reinterpret_cast<const int4*>(dyn_smem + off);
+}
+__device__ __forceinline__ const uint32_t* sm_u32(uint32_t off) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    return reinterpret_cast<const uint32_t*>(dyn_smem + off);
+}
 
 // The calling warp's views of A (the dual pass) and A^T (the primal pass)
 // from a re-centred layout staged in shared memory.
@@ -995,12 +1003,12 @@ __device__ __forceinline__ void ops_views(const Layout& L, const unsigned char* 
     const int32_t* sot = reinterpret_cast<const int32_t*>(sm + L.sched_at_off);
     const int32_t* loa = reinterpret_cast<const int32_t*>(sm + L.lsched_a_off);
     const int32_t* lot = reinterpret_cast<const int32_t*>(sm + L.lsched_at_off);
-    A->list = reinterpret_cast<const int4*>(sm + L.list_a);
-    T->list = reinterpret_cast<const int4*>(sm + L.list_at);
-    A->llist = reinterpret_cast<const int4*>(sm + L.llist_a);
-    T->llist = reinterpret_cast<const int4*>(sm + L.llist_at);
-    A->lmask = reinterpret_cast<const uint32_t*>(sm + L.lmask_a);
-    T->lmask = reinterpret_cast<const uint32_t*>(sm + L.lmask_at);
+    A->list = static_cast<uint32_t>(L.list_a);
+    T->list = static_cast<uint32_t>(L.list_at);
+    A->llist = static_cast<uint32_t>(L.llist_a);
+    T->llist = static_cast<uint32_t>(L.llist_at);
+    A->lmask = static_cast<uint32_t>(L.lmask_a);
+    T->lmask = static_cast<uint32_t>(L.lmask_at);
     A->t0 = soa[warp];
     A->t1 = soa[warp + 1];
     T->t0 = sot[warp];
@@ -1009,10 +1017,10 @@ __device__ __forceinline__ void ops_views(const Layout& L, const unsigned char* 
     A->l1 = loa[warp + 1];
     T->l0 = lot[warp];
     T->l1 = lot[warp + 1];
-    A->words = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_a_idx) : nullptr;
-    T->words = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_at_idx) : nullptr;
-    A->lwords = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_a_long) : nullptr;
-    T->lwords = L.mat_smem ? reinterpret_cast<const uint32_t*>(sm + L.mat_at_long) : nullptr;
+    A->words = static_cast<uint32_t>(L.mat_a_idx);
+    T->words = static_cast<uint32_t>(L.mat_at_idx);
+    A->lwords = static_cast<uint32_t>(L.mat_a_long);
+    T->lwords = static_cast<uint32_t>(L.mat_at_long);
 }
 
 __device__ __forceinline__ float warp_sum_f(float v) {
@@ -1104,14 +1112,14 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
     for (int t = T.t0; t < T.t1; ++t) {
-        const int4 sl = T.list[t];
+        const int4 sl = sm_int4(T.list)[t];
         const int j = (sl.x << 5) + lane;
-        const bool own = j < n && !((T.lmask[sl.x] >> lane) & 1u);
+        const bool own = j < n && !((sm_u32(T.lmask)[sl.x] >> lane) & 1u);
         const int jj = j < n ? j : 0;
         // the column's operands first: their latency overlaps the product
         const float xo = S[o.x + jj], dj = S[o.c + jj], lj = S[o.l + jj], uj = S[o.u + jj];
         float g = STAGED
-            ? slice_dot_pk(T.words + sl.y + lane, S, sl.z)
+            ? slice_dot_pk(sm_u32(T.words) + sl.y + lane, S, sl.z)
             : slice_dot_pk_global(sp->rat.pk + sl.y + lane, S + o.y, sl.z);
         if (PATCHED && sl.w && pt.n)  // a slice holding a patched column
             for (int q = 0; q < pt.n; ++q)
@@ -1119,9 +1127,9 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
         if (own) primal_update(o, j, xo, dj, lj, uj, g, tau, w, rho, check, bx, cx, pdx2, pdxa2);
     }
     for (int t = T.l0; t < T.l1; ++t) {  // long columns: the warp together, lane 0 updates
-        const int4 ll = T.llist[t];
+        const int4 ll = sm_int4(T.llist)[t];
         const int j = ll.x;
-        float g = STAGED ? long_dot_pk<false>(T.lwords + ll.y, S, ll.z, lane)
+        float g = STAGED ? long_dot_pk<false>(sm_u32(T.lwords) + ll.y, S, ll.z, lane)
                          : long_dot_pk<true>(sp->rat.long_pk + ll.y, S + o.y, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
@@ -1140,13 +1148,13 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     float* const S = reinterpret_cast<float*>(dyn_smem);
     for (int t = A.t0; t < A.t1; ++t) {
-        const int4 sl = A.list[t];
+        const int4 sl = sm_int4(A.list)[t];
         const int i = (sl.x << 5) + lane;
-        const bool own = i < m && !((A.lmask[sl.x] >> lane) & 1u);
+        const bool own = i < m && !((sm_u32(A.lmask)[sl.x] >> lane) & 1u);
         const int ii = i < m ? i : 0;
         const float yo = S[o.y + ii], ri = S[o.b + ii], yl = S[o.ya + ii];
         float h = STAGED
-            ? slice_dot_pk(A.words + sl.y + lane, S, sl.z)
+            ? slice_dot_pk(sm_u32(A.words) + sl.y + lane, S, sl.z)
             : slice_dot_pk_global(sp->ra.pk + sl.y + lane, S + o.xbar, sl.z);
         if (PATCHED && sl.w && pt.n)  // a slice holding a patched row
             for (int q = 0; q < pt.n; ++q)
@@ -1154,9 +1162,9 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
         if (own) dual_update(o, i, neq, yo, ri, yl, h, sigma, w, rho, check, by, cy, pdy2, pdya2);
     }
     for (int t = A.l0; t < A.l1; ++t) {  // long rows
-        const int4 ll = A.llist[t];
+        const int4 ll = sm_int4(A.llist)[t];
         const int i = ll.x;
-        float h = STAGED ? long_dot_pk<false>(A.lwords + ll.y, S, ll.z, lane)
+        float h = STAGED ? long_dot_pk<false>(sm_u32(A.lwords) + ll.y, S, ll.z, lane)
                          : long_dot_pk<true>(sp->ra.long_pk + ll.y, S + o.xbar, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
@@ -1287,20 +1295,20 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
                                                     const Patches& pt) {
     const int n = sp->n, m = sp->m;
     for (int t = T.t0; t < T.t1; ++t) {
-        const int4 sl = T.list[t];
+        const int4 sl = sm_int4(T.list)[t];
         const int j = (sl.x << 5) + lane;
         double g = STAGED
-            ? slice_dot64_staged(T.words + sl.y + lane, t_sub, sp->rat.v64 + sl.y + lane, yc, sl.z)
+            ? slice_dot64_staged(sm_u32(T.words) + sl.y + lane, t_sub, sp->rat.v64 + sl.y + lane, yc, sl.z)
             : slice_dot64_global2(sp->rat.idx + sl.y + lane, sp->rat.v64 + sl.y + lane, yc, sl.z);
         if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fma(pt.v64[q], yc[pt.row[q]], g);
-        if (j < n && !((T.lmask[sl.x] >> lane) & 1u)) kkt_column(sp, j, g, xc, cs, ls, us, dcand, cinf, v);
+        if (j < n && !((sm_u32(T.lmask)[sl.x] >> lane) & 1u)) kkt_column(sp, j, g, xc, cs, ls, us, dcand, cinf, v);
     }
     for (int t = T.l0; t < T.l1; ++t) {
-        const int4 ll = T.llist[t];
+        const int4 ll = sm_int4(T.llist)[t];
         const int j = ll.x;
-        double g = long_dot64<STAGED>(STAGED ? T.lwords + ll.y : nullptr, t_sub, sp->rat.long_idx + ll.y,
+        double g = long_dot64<STAGED>(STAGED ? sm_u32(T.lwords) + ll.y : nullptr, t_sub, sp->rat.long_idx + ll.y,
                                       sp->rat.long_v64 + ll.y, yc, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
@@ -1309,20 +1317,20 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
     }
     __syncthreads();  // the projected xc is the gather target below
     for (int t = A.t0; t < A.t1; ++t) {
-        const int4 sl = A.list[t];
+        const int4 sl = sm_int4(A.list)[t];
         const int i = (sl.x << 5) + lane;
         double h = STAGED
-            ? slice_dot64_staged(A.words + sl.y + lane, a_sub, sp->ra.v64 + sl.y + lane, xc, sl.z)
+            ? slice_dot64_staged(sm_u32(A.words) + sl.y + lane, a_sub, sp->ra.v64 + sl.y + lane, xc, sl.z)
             : slice_dot64_global2(sp->ra.idx + sl.y + lane, sp->ra.v64 + sl.y + lane, xc, sl.z);
         if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fma(pt.v64[q], xc[pt.col[q]], h);
-        if (i < m && !((A.lmask[sl.x] >> lane) & 1u)) kkt_row(sp, i, h, yc, bs, rcand, v);
+        if (i < m && !((sm_u32(A.lmask)[sl.x] >> lane) & 1u)) kkt_row(sp, i, h, yc, bs, rcand, v);
     }
     for (int t = A.l0; t < A.l1; ++t) {
-        const int4 ll = A.llist[t];
+        const int4 ll = sm_int4(A.llist)[t];
         const int i = ll.x;
-        double h = long_dot64<STAGED>(STAGED ? A.lwords + ll.y : nullptr, a_sub, sp->ra.long_idx + ll.y,
+        double h = long_dot64<STAGED>(STAGED ? sm_u32(A.lwords) + ll.y : nullptr, a_sub, sp->ra.long_idx + ll.y,
                                       sp->ra.long_v64 + ll.y, xc, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
@@ -1936,18 +1944,18 @@ __device__ __forceinline__ void primal_pass_pair(const PairOffsets& o, const Ops
     float2* const S2 = reinterpret_cast<float2*>(dyn_smem);
     const int lane = threadIdx.x & 31;
     for (int t = T.t0; t < T.t1; ++t) {
-        const int4 sl = T.list[t];
+        const int4 sl = sm_int4(T.list)[t];
         const int j = (sl.x << 5) + lane;
-        const bool own = j < n && !((T.lmask[sl.x] >> lane) & 1u);
+        const bool own = j < n && !((sm_u32(T.lmask)[sl.x] >> lane) & 1u);
         const int jj = j < n ? j : 0;
         const float2 xbo = S2[o.xbar + jj], dj = S2[o.c + jj], lj = S2[o.l + jj], uj = S2[o.u + jj];
-        const float2 g = slice_dot_pk2(T.words + sl.y + lane, S2, sl.z);
+        const float2 g = slice_dot_pk2(sm_u32(T.words) + sl.y + lane, S2, sl.z);
         if (own) primal_update_pair<CHECK>(o, j, xbo, dj, lj, uj, g, tau, wp, c0, c1, bx0, cx0, bx1, cx1, pd);
     }
     for (int t = T.l0; t < T.l1; ++t) {
-        const int4 ll = T.llist[t];
+        const int4 ll = sm_int4(T.llist)[t];
         const int j = ll.x;
-        const float2 g = long_dot_pk2(T.lwords + ll.y, S2, ll.z, lane);
+        const float2 g = long_dot_pk2(sm_u32(T.lwords) + ll.y, S2, ll.z, lane);
         if (lane == 0)
             primal_update_pair<CHECK>(o, j, S2[o.xbar + j], S2[o.c + j], S2[o.l + j], S2[o.u + j], g, tau, wp, c0, c1,
                                       bx0, cx0, bx1, cx1, pd);
@@ -1964,19 +1972,19 @@ __device__ __forceinline__ void dual_pass_pair(const PairOffsets& o, const OpsVi
     const int lane = threadIdx.x & 31;
     const float2 z = make_float2(0.0f, 0.0f);
     for (int t = A.t0; t < A.t1; ++t) {
-        const int4 sl = A.list[t];
+        const int4 sl = sm_int4(A.list)[t];
         const int i = (sl.x << 5) + lane;
-        const bool own = i < m && !((A.lmask[sl.x] >> lane) & 1u);
+        const bool own = i < m && !((sm_u32(A.lmask)[sl.x] >> lane) & 1u);
         const int ii = i < m ? i : 0;
         const float2 yo = S2[o.y + ii], ri = S2[o.b + ii];
         const float2 yl = (i < m && i >= neq) ? S2[o.ya + (i - neq)] : z;
-        const float2 h = slice_dot_pk2(A.words + sl.y + lane, S2, sl.z);
+        const float2 h = slice_dot_pk2(sm_u32(A.words) + sl.y + lane, S2, sl.z);
         if (own) dual_update_pair<CHECK>(o, i, neq, yo, ri, yl, h, sigma, w, c0, c1, by0, cy0, by1, cy1, pd);
     }
     for (int t = A.l0; t < A.l1; ++t) {
-        const int4 ll = A.llist[t];
+        const int4 ll = sm_int4(A.llist)[t];
         const int i = ll.x;
-        const float2 h = long_dot_pk2(A.lwords + ll.y, S2, ll.z, lane);
+        const float2 h = long_dot_pk2(sm_u32(A.lwords) + ll.y, S2, ll.z, lane);
         if (lane == 0)
             dual_update_pair<CHECK>(o, i, neq, S2[o.y + i], S2[o.b + i], i >= neq ? S2[o.ya + (i - neq)] : z, h,
                                     sigma, w, c0, c1, by0, cy0, by1, cy1, pd);
@@ -2351,12 +2359,12 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
         // every thread read this iteration's state before the barrier above
         if (tid == 0) {
             if (a0) {
-                s_st[0].it = it[0];
-                s_st[0].k = k[0] + 1;
+                s_st[0].it += 1;
+                s_st[0].k += 1;
             }
             if (a1) {
-                s_st[1].it = it[1];
-                s_st[1].k = k[1] + 1;
+                s_st[1].it += 1;
+                s_st[1].k += 1;
             }
         }
         __syncthreads();
@@ -2386,6 +2394,7 @@ template __global__ void pdhg_recentred<768, false, false>(KernelParams);
 template __global__ void pdhg_recentred<768, true, true>(KernelParams);
 template __global__ void pdhg_recentred<768, false, true>(KernelParams);
 template __global__ void pdhg_recentred_pair<512>(KernelParams);
+template __global__ void pdhg_recentred_pair<768>(KernelParams);
 template __global__ void pdhg_recentred_pair<1024>(KernelParams);
 #undef FBALP_INSTANTIATE
 
@@ -2463,12 +2472,14 @@ cudaError_t launch_recentred(bool staged, bool patched, int grid, int threads, s
 }
 
 const void* pair_symbol(int threads) {
-    return threads <= 512 ? reinterpret_cast<const void*>(&pdhg_recentred_pair<512>)
-                          : reinterpret_cast<const void*>(&pdhg_recentred_pair<1024>);
+    if (threads <= 512) return reinterpret_cast<const void*>(&pdhg_recentred_pair<512>);
+    if (threads <= 768) return reinterpret_cast<const void*>(&pdhg_recentred_pair<768>);
+    return reinterpret_cast<const void*>(&pdhg_recentred_pair<1024>);
 }
 
 cudaError_t launch_pair(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p) {
     if (threads <= 512) pdhg_recentred_pair<512><<<grid, threads, smem, stream>>>(p);
+    else if (threads <= 768) pdhg_recentred_pair<768><<<grid, threads, smem, stream>>>(p);
     else pdhg_recentred_pair<1024><<<grid, threads, smem, stream>>>(p);
     return cudaGetLastError();
 }
