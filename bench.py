@@ -156,15 +156,20 @@ def hbm_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per instance-iteration of the re-centred phase from the
-    committed ncu summary of a smaller case of the same step
-    (profiles/pdhg_recentred_community_small.txt), if present."""
-    p = ROOT / "profiles" / "pdhg_recentred_community_small.txt"
-    if not p.exists():
+PROFILE_FOR_KERNEL = {"pdhg_recentred_pair": "pdhg_recentred_pair_community_small.txt",
+                      "pdhg_recentred<staged>": "pdhg_recentred_community_small.txt"}
+
+
+def profiled_figure(kernel, key):
+    """A per-instance-iteration figure (``key: value ...`` line) from the
+    committed ncu summary of a smaller case of the same step for ``kernel``
+    (profiles/), or None."""
+    name = PROFILE_FOR_KERNEL.get(kernel)
+    p = ROOT / "profiles" / name if name else None
+    if p is None or not p.exists():
         return None
     for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_instance_iteration:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -297,21 +302,6 @@ def streaming_bytes(models, species_id, it, w=4):
     return total
 
 
-def profiled_onchip():
-    """Shared-memory wavefronts per instance-iteration of the re-centred
-    phase from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "pdhg_recentred_community_small.txt"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        if line.startswith("shared_wavefronts_per_instance_iteration:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
-
-
 def certificate_summary(res, lps):
     """Distribution of the kernel's FP64 certificate fields over every LP of
     a step (primal residual, dual violation, relative KKT gap)."""
@@ -427,16 +417,16 @@ def run_product(args):
     kernel_total_ms = float(sum(kernel_ms))
     achieved = sum(step_bytes) / (kernel_total_ms / 1e3) / 1e9
     inst_its = int(it.sum())
-    tpi = profiled_traffic()
-    traffic = None if tpi is None else tpi * inst_its / it.shape[0]
     first_kernel, fp64_kernel = com.engine.phase_kernels()
+    tpi = profiled_figure(first_kernel, "dram_bytes_per_instance_iteration")
+    traffic = None if tpi is None else tpi * inst_its / it.shape[0]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{peak_kind} copy bandwidth",
                 "kernel": first_kernel, "fp64_phase_kernel": fp64_kernel, "algorithmic_bytes": sum(step_bytes) / len(step_bytes),
                 "kernel_ms": kernel_total_ms / len(kernel_ms), "kernel_share_of_step": kernel_total_ms / ms,
                 "instance_iterations_per_launch": inst_its / it.shape[0],
                 "measured_on": f"the {args.steps} timed steps (CUDA events around each step's PDHG launches)"}
-    wf = profiled_onchip()
+    wf = profiled_figure(first_kernel, "shared_wavefronts_per_instance_iteration")
     sm_mhz = clock_summary.get("sm_mhz") or 1965.0
     if wf is not None:
         sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
