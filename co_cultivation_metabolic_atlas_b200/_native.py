@@ -59,11 +59,13 @@ class SolveParams(ctypes.Structure):
                 ("reflection", ctypes.c_double), ("restarts", ctypes.c_int32),
                 ("fp32_stall_checks", ctypes.c_int32), ("fp64_stall_checks", ctypes.c_int32),
                 ("floor_tol", ctypes.c_double), ("fp32_passthrough_tol", ctypes.c_double),
-                ("fallback_iterations", ctypes.c_int32), ("fp32_recentre", ctypes.c_int32)]
+                ("fallback_iterations", ctypes.c_int32), ("fp32_recentre", ctypes.c_int32),
+                ("fp32_values_phase", ctypes.c_int32)]
 
 
 KERNEL_NAMES = {-1: None, 0: "pdhg_persistent<float>", 1: "pdhg_persistent<double>", 2: "pdhg_recentred<staged>",
-                3: "pdhg_recentred<streamed>", 4: "pdhg_recentred_pair"}
+                3: "pdhg_recentred<streamed>", 4: "pdhg_recentred_pair", 5: "pdhg_recentred<staged, fp32 values>",
+                6: "pdhg_recentred<streamed, fp32 values>"}
 
 
 class NativeError(RuntimeError):

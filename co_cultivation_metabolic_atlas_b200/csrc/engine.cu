@@ -99,8 +99,10 @@ fbalp::DevLines upload_lines(const fbalp::Sell& S, const std::vector<int32_t>& s
     }
     d.idx = dev_upload(S.idx, owned);
     d.v64 = dev_upload(S.val, owned);
+    d.v32 = dev_upload(v32, owned);
     d.long_idx = dev_upload(S.long_idx, owned);
     d.long_v64 = dev_upload(S.long_val, owned);
+    d.long_v32 = dev_upload(l32, owned);
     return d;
 }
 
@@ -141,6 +143,7 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->fp32_passthrough_tol = 1e-3;
     p->fallback_iterations = 4096;
     p->fp32_recentre = 1;
+    p->fp32_values_phase = 1;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -569,10 +572,44 @@ bool pair_mode(fbalp_engine* e, double reflection, bool patched) {
     return true;
 }
 
+// The FP32-valued re-centred phase that continues the instances the BF16
+// re-centred phase hands off: mode 4 when every species of the batch fits
+// it with the matrix (16-bit indices and FP32 values) in shared memory, 5
+// when only the vectors fit (matrix streamed), 0 when neither.
+int f32_mode(fbalp_engine* e) {
+    const int threads = e->opt.warps_per_block * 32;
+    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
+                      ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
+    if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
+    std::vector<char> used(e->species.size(), 0);
+    for (int32_t s : e->h_species) used[s] = 1;
+    bool staged = e->opt.stage_matrix != 0, streamed = true;
+    for (size_t s = 0; s < e->species.size(); ++s) {
+        if (!used[s]) continue;
+        const SpeciesHost& sh = e->species[s];
+        for (int st = 0; st < 2; ++st) {
+            bool& ok = st ? staged : streamed;
+            if (ok && !fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.shape_a(), sh.shape_at(),
+                                                    cap, st != 0, true)
+                           .layout.recentred)
+                ok = false;
+        }
+    }
+    return staged ? 4 : (streamed ? 5 : 0);
+}
+
 // Launch one precision phase over the bound batch (`recentred`: the
-// re-centred FP32 kernel in mode 1 (staged matrix), 2 (streamed) or 3
-// (staged, two instances per CTA)).
-void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred = 0) {
+// re-centred FP32 kernel in mode 1 (staged matrix), 2 (streamed), 3
+// (staged, two instances per CTA), 4 / 5 (FP32 matrix values, staged /
+// streamed)).  `book` is the phase's slot in the engine's per-phase records
+// (0 first phase, 1 FP64 phase, 2 FP32-valued middle phase); the middle and
+// FP64 phases share the second timing pair (`rec_start` / `rec_stop` say
+// which ends of it this launch records).
+void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred = 0, int book = -1,
+               bool rec_start = true, bool rec_stop = true) {
+    if (book < 0) book = fp64 ? 1 : 0;
+    const bool f32v = recentred >= 4;
     const int esz = fp64 ? static_cast<int>(sizeof(double)) : static_cast<int>(sizeof(float));
     const int threads = e->opt.warps_per_block * 32;
     const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
@@ -604,7 +641,7 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
             ? fbalp::plan_layout_pair(sh.n, sh.m, sh.neq, e->opt.warps_per_block, sh.shape_a(), sh.shape_at(), cap)
             : recentred
             ? fbalp::plan_layout_recentred(sh.n, sh.m, e->opt.warps_per_block, sh.shape_a(), sh.shape_at(), cap,
-                                           recentred == 1)
+                                           recentred == 1 || recentred == 4, f32v)
             : unscaled
             ? fbalp::plan_layout_unscaled(sh.n, sh.m, e->opt.warps_per_block, sh.A.nslices, sh.AT.nslices,
                                           sh.A.off.back(), sh.AT.off.back(), cap)
@@ -635,8 +672,9 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     }
     const bool patched = recentred && p.patch_values != nullptr;
     const bool pair = recentred == 3;
+    const bool staged = recentred == 1 || recentred == 4;
     const void* k = pair ? fbalp::pair_symbol(threads)
-                         : recentred ? fbalp::recentred_symbol(threads, recentred == 1, patched)
+                         : recentred ? fbalp::recentred_symbol(threads, staged, patched, f32v)
                                      : fbalp::kernel_symbol(fp64, threads, all_fast);
     // the dynamic shared-memory limit is a property of the kernel in this
     // process (shared by every engine): raise it when this launch needs
@@ -670,33 +708,33 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
         p.spill = nullptr;
         p.spill_stride = 0;
     }
-    p.queue = static_cast<int32_t*>(e->queue.ptr) + (fp64 ? 1 : 0);
+    p.queue = static_cast<int32_t*>(e->queue.ptr) + book;
     check(cudaMemsetAsync(p.queue, 0, sizeof(int32_t), e->stream), "memset queue");
-    const int ph = fp64 ? 1 : 0;
+    const int ph = (fp64 || f32v) ? 1 : 0;
     // phase timing events only outside a capture (a graph replay has no
     // per-phase timing)
-    if (!capturing) check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
+    if (!capturing && rec_start) check(cudaEventRecord(e->ev[2 * ph], e->stream), "cudaEventRecord");
     // a selected timing slot records around the launch in either case (an
     // external event node under capture)
     cudaEvent_t* sev = e->slot >= 0 ? &e->slot_ev[4 * static_cast<size_t>(e->slot)] : nullptr;
     const unsigned rec_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
-    if (sev) check(cudaEventRecordWithFlags(sev[2 * ph], e->stream, rec_flags), "timing slot record");
+    if (sev && rec_start) check(cudaEventRecordWithFlags(sev[2 * ph], e->stream, rec_flags), "timing slot record");
     if (pair)
         check(fbalp::launch_pair(grid, threads, dyn, e->stream, p), "paired re-centred pdhg kernel launch");
     else if (recentred)
-        check(fbalp::launch_recentred(recentred == 1, patched, grid, threads, dyn, e->stream, p),
+        check(fbalp::launch_recentred(staged, patched, grid, threads, dyn, e->stream, p, f32v),
               "re-centred pdhg kernel launch");
     else
         check(fbalp::launch_pdhg(fp64, all_fast, grid, threads, dyn, e->stream, p), "pdhg kernel launch");
-    if (sev) {
+    if (sev && rec_stop) {
         check(cudaEventRecordWithFlags(sev[2 * ph + 1], e->stream, rec_flags), "timing slot record");
         e->slot_ran[2 * static_cast<size_t>(e->slot) + ph] = 1;
     }
-    if (!capturing) check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
-    e->ran[ph] = !capturing;
-    e->last_grid[fp64 ? 1 : 0] = grid;
-    e->last_kind[fp64 ? 1 : 0] = kind;
-    e->last_smem[fp64 ? 1 : 0] = dyn;
+    if (!capturing && rec_stop) check(cudaEventRecord(e->ev[2 * ph + 1], e->stream), "cudaEventRecord");
+    if (rec_stop) e->ran[ph] = !capturing;
+    e->last_grid[book] = grid;
+    e->last_kind[book] = kind;
+    e->last_smem[book] = dyn;
 }
 
 
@@ -718,7 +756,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
     if (!valid_params(q, &err)) return fail(FBALP_ERR_INVALID, err);
     try {
         e->ran[0] = e->ran[1] = false;
-        e->last_kind[0] = e->last_kind[1] = -1;
+        e->last_kind[0] = e->last_kind[1] = e->last_kind[2] = -1;
         fbalp::KernelParams p{};
         p.species = e->dev_species;
         p.count = static_cast<int32_t>(e->count);
@@ -807,13 +845,56 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             if (patched) pr.handoff_on_stall = 0;  // the FP64 phase has no patched entries
             const int mode = recentred_mode(e);
             run_phase(e, false, pr, mode == 1 && pair_mode(e, q.reflection, patched) ? 3 : mode);
+            // instances the BF16-matrix phase hands off (a stall: on badly
+            // scaled models the BF16-rounded matrix limits the correction
+            // LPs) continue from their own point with FP32 matrix values;
+            // what that phase hands off in turn finishes in FP64
+            const int fmode = (q.fp32_values_phase && !patched) ? f32_mode(e) : 0;
+            const int32_t* c_list = static_cast<const int32_t*>(e->hand_list.ptr);
+            const int32_t* c_count = static_cast<const int32_t*>(e->hand_count.ptr);
+            const double* c_x = static_cast<const double*>(e->mid_x.ptr);
+            const double* c_y = static_cast<const double*>(e->mid_y.ptr);
+            const double* c_omega = static_cast<const double*>(e->mid_omega.ptr);
+            const int32_t* c_iters = static_cast<const int32_t*>(e->mid_iters.ptr);
+            if (fmode) {
+                e->mid2_x.ensure(e->total_cols * sizeof(double));
+                e->mid2_y.ensure(std::max<int64_t>(1, e->total_rows) * sizeof(double));
+                e->mid2_omega.ensure(e->count * sizeof(double));
+                e->mid2_iters.ensure(e->count * sizeof(int32_t));
+                e->hand2_list.ensure(e->count * sizeof(int32_t));
+                e->hand2_count.ensure(sizeof(int32_t));
+                check(cudaMemsetAsync(e->hand2_count.ptr, 0, sizeof(int32_t), e->stream), "memset handoff count");
+                fbalp::KernelParams pb = pr;
+                pb.order = c_list;
+                pb.count_dev = c_count;
+                pb.warm_x = c_x;
+                pb.warm_y = c_y;
+                pb.warm_omega = c_omega;
+                pb.prior_iters = c_iters;
+                pb.fallback_iters = 0;  // a stalled point restarting cold would lose its progress
+                pb.hint_iters = nullptr;
+                pb.patch_values = nullptr;
+                pb.handoff_list = static_cast<int32_t*>(e->hand2_list.ptr);
+                pb.handoff_count = static_cast<int32_t*>(e->hand2_count.ptr);
+                pb.hand_x = static_cast<double*>(e->mid2_x.ptr);
+                pb.hand_y = static_cast<double*>(e->mid2_y.ptr);
+                pb.hand_omega = static_cast<double*>(e->mid2_omega.ptr);
+                pb.hand_iters = static_cast<int32_t*>(e->mid2_iters.ptr);
+                run_phase(e, false, pb, fmode, 2, true, false);
+                c_list = static_cast<const int32_t*>(e->hand2_list.ptr);
+                c_count = static_cast<const int32_t*>(e->hand2_count.ptr);
+                c_x = static_cast<const double*>(e->mid2_x.ptr);
+                c_y = static_cast<const double*>(e->mid2_y.ptr);
+                c_omega = static_cast<const double*>(e->mid2_omega.ptr);
+                c_iters = static_cast<const int32_t*>(e->mid2_iters.ptr);
+            }
             fbalp::KernelParams p64 = p;
-            p64.order = static_cast<const int32_t*>(e->hand_list.ptr);
-            p64.count_dev = static_cast<const int32_t*>(e->hand_count.ptr);
-            p64.warm_x = static_cast<const double*>(e->mid_x.ptr);
-            p64.warm_y = static_cast<const double*>(e->mid_y.ptr);
-            p64.warm_omega = static_cast<const double*>(e->mid_omega.ptr);
-            p64.prior_iters = static_cast<const int32_t*>(e->mid_iters.ptr);
+            p64.order = c_list;
+            p64.count_dev = c_count;
+            p64.warm_x = c_x;
+            p64.warm_y = c_y;
+            p64.warm_omega = c_omega;
+            p64.prior_iters = c_iters;
             p64.out_x = out_x;
             p64.out_y = out_y;
             p64.out_obj = out_objective;
@@ -831,7 +912,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p64.floor_tol = q.floor_tol;
             p64.passthrough_tol = 0.0;
             p64.fallback_iters = q.fallback_iterations;
-            run_phase(e, true, p64);
+            run_phase(e, true, p64, 0, 1, !fmode, true);
         } else {
             e->mid_x.ensure(e->total_cols * sizeof(double));
             e->mid_y.ensure(std::max<int64_t>(1, e->total_rows) * sizeof(double));

@@ -101,6 +101,7 @@ inline bool valid_params(const fbalp_solve_params& q, std::string* err) {
     if (q.fp32_recentre != 0 && q.fp32_recentre != 1) return *err = "fp32_recentre must be 0 or 1", false;
     if (!(q.fp32_passthrough_tol >= 0.0) || !std::isfinite(q.fp32_passthrough_tol))
         return *err = "fp32_passthrough_tol must be finite and non-negative", false;
+    if (q.fp32_values_phase != 0 && q.fp32_values_phase != 1) return *err = "fp32_values_phase must be 0 or 1", false;
     return true;
 }
 
@@ -130,19 +131,22 @@ struct fbalp_engine {
     bool bound = false;
     // workspace
     Buffer queue, mid_x, mid_y, mid_omega, mid_iters, mid_status, mid_obj, mid_metrics, spill;
-    Buffer hand_list, hand_count;  // re-centred phase -> FP64 phase work list
+    Buffer hand_list, hand_count;  // re-centred phase -> next phase work list
+    // FP32-valued re-centred phase -> FP64 phase: work list and hand-off point
+    Buffer hand2_list, hand2_count, mid2_x, mid2_y, mid2_omega, mid2_iters;
     Buffer layout32_buf, layout64_buf;
     // device copies of the launch layouts, one per kernel kind (plain FP32,
     // FP64, re-centred staged, re-centred streamed, paired re-centred),
     // uploaded only when their
     // content changes: a solve that reuses them issues no host-to-device
     // copy, so it can be captured in a CUDA graph
-    Buffer layout_dev[5];
-    std::vector<fbalp::Layout> layout_host[5];
+    Buffer layout_dev[7];
+    std::vector<fbalp::Layout> layout_host[7];
     std::vector<fbalp::Layout> layouts32, layouts64;
-    int last_grid[2] = {0, 0};
-    int last_kind[2] = {-1, -1};  // kernel kind of the last solve's phases (the layout_dev index)
-    int64_t last_smem[2] = {0, 0};
+    // per phase of the last solve (first, FP64, FP32-valued middle phase)
+    int last_grid[3] = {0, 0, 0};
+    int last_kind[3] = {-1, -1, -1};  // kernel kind (the layout_dev index)
+    int64_t last_smem[3] = {0, 0, 0};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase start/stop: fp32, fp64
     bool ran[2] = {false, false};
     // timing slots: per slot the same four events, recorded around the
@@ -161,7 +165,8 @@ struct fbalp_engine {
         for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
                           &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill, &layout32_buf,
                           &layout64_buf, &hand_list, &hand_count, &layout_dev[0], &layout_dev[1],
-                          &layout_dev[2], &layout_dev[3], &layout_dev[4]})
+                          &layout_dev[2], &layout_dev[3], &layout_dev[4], &layout_dev[5], &layout_dev[6],
+                          &hand2_list, &hand2_count, &mid2_x, &mid2_y, &mid2_omega, &mid2_iters})
             b->release();
     }
 };

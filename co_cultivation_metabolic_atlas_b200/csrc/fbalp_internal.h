@@ -210,7 +210,7 @@ inline int64_t place_recentred_lists(Layout& L, int warps, const LinesShape& a, 
 // matrix is not staged (it is streamed from L2 every iteration) and only the
 // lists and vectors need to fit.
 inline LayoutPlan plan_layout_recentred(int n, int m, int warps, const LinesShape& sa, const LinesShape& sat,
-                                        int64_t smem_cap, bool stage = true) {
+                                        int64_t smem_cap, bool stage = true, bool f32_values = false) {
     LayoutPlan P{};
     Layout& L = P.layout;
     int64_t off = place_recentred_lists(L, warps, sa, sat);
@@ -224,7 +224,7 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, const LinesShap
     };
     put(kXbar);
     put(kY);
-    if (stage) {  // packed 32-bit words (16-bit index | BF16 value)
+    if (stage && !f32_values) {  // packed 32-bit words (16-bit index | BF16 value)
         L.mat_a_idx = off;
         off += align_up(4 * sa.elems, 16);
         L.mat_at_idx = off;
@@ -235,7 +235,21 @@ inline LayoutPlan plan_layout_recentred(int n, int m, int warps, const LinesShap
         off += align_up(4 * sat.long_elems, 16);
         L.mat_a_val = L.mat_a_idx;
         L.mat_at_val = L.mat_at_idx;
+    } else if (stage) {  // 16-bit indices and FP32 values in separate arrays
+        for (auto* pr : {&L.mat_a_idx, &L.mat_at_idx, &L.mat_a_long, &L.mat_at_long}) {
+            const int64_t cnt = pr == &L.mat_a_idx ? sa.elems : pr == &L.mat_at_idx ? sat.elems
+                                : pr == &L.mat_a_long ? sa.long_elems : sat.long_elems;
+            *pr = off;
+            off += align_up(2 * cnt, 16);
+        }
+        for (auto* pr : {&L.mat_a_val, &L.mat_at_val, &L.mat_a_lval, &L.mat_at_lval}) {
+            const int64_t cnt = pr == &L.mat_a_val ? sa.elems : pr == &L.mat_at_val ? sat.elems
+                                : pr == &L.mat_a_lval ? sa.long_elems : sat.long_elems;
+            *pr = off;
+            off += align_up(4 * cnt, 16);
+        }
     }
+    L.f32_values = f32_values ? 1 : 0;
     for (int a : {kX, kC, kL, kU, kB, kYa}) put(a);
     if (off > smem_cap) return P;
     // every staged 16-bit index is an element offset from the start of
@@ -337,7 +351,7 @@ inline LayoutPlan plan_layout_pair(int n, int m, int neq, int warps, const Lines
 // Every region must start on a 16-byte boundary (int4 lists, FP64 arrays).
 inline bool layout_aligned(const Layout& L) {
     const int64_t offs[] = {L.list_a, L.list_at, L.mat_a_idx, L.mat_at_idx, L.mat_a_val, L.mat_at_val,
-                            L.llist_a, L.llist_at, L.mat_a_long, L.mat_at_long};
+                            L.llist_a, L.llist_at, L.mat_a_long, L.mat_at_long, L.mat_a_lval, L.mat_at_lval};
     for (int64_t o : offs)
         if (o % 16 != 0) return false;
     for (int a = 0; a < kArrayCount; ++a)
@@ -348,9 +362,9 @@ inline bool layout_aligned(const Layout& L) {
 }
 
 const void* kernel_symbol(bool fp64, int threads, bool fast);
-const void* recentred_symbol(int threads, bool staged, bool patched);
+const void* recentred_symbol(int threads, bool staged, bool patched, bool f32_values = false);
 cudaError_t launch_recentred(bool staged, bool patched, int grid, int threads, size_t smem, cudaStream_t stream,
-                             const KernelParams& p);
+                             const KernelParams& p, bool f32_values = false);
 const void* pair_symbol(int threads);
 cudaError_t launch_pair(int grid, int threads, size_t smem, cudaStream_t stream, const KernelParams& p);
 cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem, cudaStream_t stream,

@@ -250,6 +250,22 @@ __device__ void stage_recentred_ops(const DevSpecies* sp, const Layout& L, unsig
     for (int q = tid; q < t.nlong; q += nt) llt[q] = t.long_list[q];
     if (!L.mat_smem) return;
     const uint32_t a_add = static_cast<uint32_t>(L.arr[kXbar] / unit), t_add = static_cast<uint32_t>(L.arr[kY] / unit);
+    if (L.f32_values) {  // 16-bit indices (pre-offset) and FP32 values
+        auto put16 = [&](int64_t off_idx, int64_t off_val, const int32_t* idx, const float* val, int64_t count,
+                         uint32_t add) {
+            uint16_t* di = reinterpret_cast<uint16_t*>(sm + off_idx);
+            float* dv = reinterpret_cast<float*>(sm + off_val);
+            for (int64_t e = tid; e < count; e += nt) {
+                di[e] = static_cast<uint16_t>(static_cast<uint32_t>(idx[e]) + add);
+                dv[e] = val[e];
+            }
+        };
+        put16(L.mat_a_idx, L.mat_a_val, a.idx, a.v32, a.elems, a_add);
+        put16(L.mat_at_idx, L.mat_at_val, t.idx, t.v32, t.elems, t_add);
+        put16(L.mat_a_long, L.mat_a_lval, a.long_idx, a.long_v32, a.long_elems, a_add);
+        put16(L.mat_at_long, L.mat_at_lval, t.long_idx, t.long_v32, t.long_elems, t_add);
+        return;
+    }
     auto put = [&](uint32_t* dst, const uint32_t* src, int64_t count, uint32_t add) {
         for (int64_t e = tid; e < count; e += nt) {
             const uint32_t w = src[e];
@@ -980,7 +996,8 @@ struct Patches {
 // gather target); otherwise the words are streamed from global memory.
 struct OpsView {
     uint32_t list, llist, lmask;  // byte offsets into dynamic shared memory
-    uint32_t words, lwords;       // staged slice / long-line words (unused when streamed)
+    uint32_t words, lwords;       // staged slice / long-line words, or 16-bit indices with FP32 values
+    uint32_t vals, lvals;         // staged FP32 values (FP32-valued layouts)
     int t0, t1;                   // this warp's slices
     int l0, l1;                   // this warp's long lines
 };
@@ -1021,6 +1038,19 @@ __device__ __forceinline__ void ops_views(const Layout& L, const unsigned char* 
     T->words = static_cast<uint32_t>(L.mat_at_idx);
     A->lwords = static_cast<uint32_t>(L.mat_a_long);
     T->lwords = static_cast<uint32_t>(L.mat_at_long);
+    A->vals = static_cast<uint32_t>(L.mat_a_val);
+    T->vals = static_cast<uint32_t>(L.mat_at_val);
+    A->lvals = static_cast<uint32_t>(L.mat_a_lval);
+    T->lvals = static_cast<uint32_t>(L.mat_at_lval);
+}
+
+__device__ __forceinline__ const uint16_t* sm_u16(uint32_t off) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    return reinterpret_cast<const uint16_t*>(dyn_smem + off);
+}
+__device__ __forceinline__ const float* sm_f32(uint32_t off) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    return reinterpret_cast<const float*>(dyn_smem + off);
 }
 
 __device__ __forceinline__ float warp_sum_f(float v) {
@@ -1049,15 +1079,80 @@ __device__ __forceinline__ float long_dot_pk(const uint32_t* wp, const float* g,
     return warp_sum_f(acc);
 }
 
+// Slice product over separate 16-bit indices (pre-offset to the gather
+// target) and FP32 values in shared memory -- the FP32-valued layout of
+// solves the BF16-rounded matrix stalls -- in the order of slice_dot_pk.
+__device__ __forceinline__ float slice_dot_sv(const uint16_t* ip, const float* vp, const float* g, int len) {
+    float a0 = 0.0f, a1 = 0.0f;
+    int k = 0;
+    for (; k + 4 <= len; k += 4, ip += 128, vp += 128) {
+        const int i0 = ip[0], i1 = ip[32], i2 = ip[64], i3 = ip[96];
+        const float v0 = vp[0], v1 = vp[32], v2 = vp[64], v3 = vp[96];
+        a0 = fmaf(v0, g[i0], a0);
+        a1 = fmaf(v1, g[i1], a1);
+        a0 = fmaf(v2, g[i2], a0);
+        a1 = fmaf(v3, g[i3], a1);
+    }
+    if (k + 2 <= len) {
+        a0 = fmaf(vp[0], g[ip[0]], a0);
+        a1 = fmaf(vp[32], g[ip[32]], a1);
+        k += 2;
+        ip += 64;
+        vp += 64;
+    }
+    if (k < len) a0 = fmaf(vp[0], g[ip[0]], a0);
+    return a0 + a1;
+}
+
+// The same with the raw int32 indices and FP32 values streamed from global
+// memory (indices relative to `g`); identical accumulation order.
+__device__ __forceinline__ float slice_dot_sv_global(const int32_t* __restrict__ ip, const float* __restrict__ vp,
+                                                     const float* g, int len) {
+    constexpr int U = 8;
+    float a0 = 0.0f, a1 = 0.0f;
+    for (int k0 = 0; k0 < len; k0 += U) {
+        int ii[U];
+        float vv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u < len) {
+                ii[u] = __ldg(ip + ((k0 + u) << 5));
+                vv[u] = __ldg(vp + ((k0 + u) << 5));
+            }
+#pragma unroll
+        for (int u = 0; u < U; u += 2) {
+            if (k0 + u < len) a0 = fmaf(vv[u], g[ii[u]], a0);
+            if (k0 + u + 1 < len) a1 = fmaf(vv[u + 1], g[ii[u + 1]], a1);
+        }
+    }
+    return a0 + a1;
+}
+
+// A long line with separate indices and FP32 values (staged 16-bit or
+// streamed int32), the warp together in long_dot_pk's order.
+template <bool GLOBAL>
+__device__ __forceinline__ float long_dot_sv(const uint16_t* ip16, const int32_t* ip32, const float* vp, const float* g,
+                                             int len, int lane) {
+    float acc = 0.0f;
+    for (int k = lane; k < len; k += 32) {
+        const int i = GLOBAL ? __ldg(ip32 + k) : static_cast<int>(ip16[k]);
+        const float v = GLOBAL ? __ldg(vp + k) : vp[k];
+        acc = fmaf(v, g[i], acc);
+    }
+    return warp_sum_f(acc);
+}
+
 // The FP64 product of one long line for the convergence test (the same
 // order): indices from the staged words (minus the gather-target offset
 // `sub`) or from global memory, FP64 values from global memory.
-template <bool STAGED>
-__device__ __forceinline__ double long_dot64(const uint32_t* wp, int sub, const int32_t* __restrict__ ip,
+template <bool STAGED, bool F32V = false>
+__device__ __forceinline__ double long_dot64(const void* wp, int sub, const int32_t* __restrict__ ip,
                                              const double* __restrict__ vp, const double* g, int len, int lane) {
     double acc = 0.0;
     for (int k = lane; k < len; k += 32) {
-        const int i = STAGED ? static_cast<int>(wp[k] & 0xffffu) - sub : __ldg(ip + k);
+        const int i = !STAGED ? __ldg(ip + k)
+                              : (F32V ? static_cast<int>(static_cast<const uint16_t*>(wp)[k])
+                                      : static_cast<int>(static_cast<const uint32_t*>(wp)[k] & 0xffffu)) - sub;
         acc = fma(__ldg(vp + k), g[i], acc);
     }
     return warp_sum_d(acc);
@@ -1104,7 +1199,7 @@ __device__ __forceinline__ void dual_update(const FastOffsets& o, int i, int neq
 
 // STAGED: the species' packed matrix words are in shared memory (indices
 // pre-offset to the gather target); otherwise they are streamed from L2.
-template <bool STAGED, bool PATCHED>
+template <bool STAGED, bool PATCHED, bool F32V>
 __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const OpsView& T,
                                                       int n, int lane, float tau, float w, float rho, bool check,
                                                       const double* bx, double* cx, double& pdx2, double& pdxa2,
@@ -1118,9 +1213,13 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
         const int jj = j < n ? j : 0;
         // the column's operands first: their latency overlaps the product
         const float xo = S[o.x + jj], dj = S[o.c + jj], lj = S[o.l + jj], uj = S[o.u + jj];
-        float g = STAGED
-            ? slice_dot_pk(sm_u32(T.words) + sl.y + lane, S, sl.z)
-            : slice_dot_pk_global(sp->rat.pk + sl.y + lane, S + o.y, sl.z);
+        float g;
+        if (F32V)
+            g = STAGED ? slice_dot_sv(sm_u16(T.words) + sl.y + lane, sm_f32(T.vals) + sl.y + lane, S, sl.z)
+                       : slice_dot_sv_global(sp->rat.idx + sl.y + lane, sp->rat.v32 + sl.y + lane, S + o.y, sl.z);
+        else
+            g = STAGED ? slice_dot_pk(sm_u32(T.words) + sl.y + lane, S, sl.z)
+                       : slice_dot_pk_global(sp->rat.pk + sl.y + lane, S + o.y, sl.z);
         if (PATCHED && sl.w && pt.n)  // a slice holding a patched column
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fmaf(pt.v32[q], S[o.y + pt.row[q]], g);
@@ -1129,8 +1228,14 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
     for (int t = T.l0; t < T.l1; ++t) {  // long columns: the warp together, lane 0 updates
         const int4 ll = sm_int4(T.llist)[t];
         const int j = ll.x;
-        float g = STAGED ? long_dot_pk<false>(sm_u32(T.lwords) + ll.y, S, ll.z, lane)
-                         : long_dot_pk<true>(sp->rat.long_pk + ll.y, S + o.y, ll.z, lane);
+        float g;
+        if (F32V)
+            g = STAGED ? long_dot_sv<false>(sm_u16(T.lwords) + ll.y, nullptr, sm_f32(T.lvals) + ll.y, S, ll.z, lane)
+                       : long_dot_sv<true>(nullptr, sp->rat.long_idx + ll.y, sp->rat.long_v32 + ll.y, S + o.y, ll.z,
+                                           lane);
+        else
+            g = STAGED ? long_dot_pk<false>(sm_u32(T.lwords) + ll.y, S, ll.z, lane)
+                       : long_dot_pk<true>(sp->rat.long_pk + ll.y, S + o.y, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fmaf(pt.v32[q], S[o.y + pt.row[q]], g);
@@ -1140,7 +1245,7 @@ __device__ __forceinline__ void primal_pass_recentred(const DevSpecies* sp, cons
     }
 }
 
-template <bool STAGED, bool PATCHED>
+template <bool STAGED, bool PATCHED, bool F32V>
 __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const FastOffsets& o, const OpsView& A,
                                                     int m, int neq, int lane, float sigma, float w, float rho,
                                                     bool check, const double* by, double* cy, double& pdy2,
@@ -1153,9 +1258,13 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
         const bool own = i < m && !((sm_u32(A.lmask)[sl.x] >> lane) & 1u);
         const int ii = i < m ? i : 0;
         const float yo = S[o.y + ii], ri = S[o.b + ii], yl = S[o.ya + ii];
-        float h = STAGED
-            ? slice_dot_pk(sm_u32(A.words) + sl.y + lane, S, sl.z)
-            : slice_dot_pk_global(sp->ra.pk + sl.y + lane, S + o.xbar, sl.z);
+        float h;
+        if (F32V)
+            h = STAGED ? slice_dot_sv(sm_u16(A.words) + sl.y + lane, sm_f32(A.vals) + sl.y + lane, S, sl.z)
+                       : slice_dot_sv_global(sp->ra.idx + sl.y + lane, sp->ra.v32 + sl.y + lane, S + o.xbar, sl.z);
+        else
+            h = STAGED ? slice_dot_pk(sm_u32(A.words) + sl.y + lane, S, sl.z)
+                       : slice_dot_pk_global(sp->ra.pk + sl.y + lane, S + o.xbar, sl.z);
         if (PATCHED && sl.w && pt.n)  // a slice holding a patched row
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fmaf(pt.v32[q], S[o.xbar + pt.col[q]], h);
@@ -1164,8 +1273,14 @@ __device__ __forceinline__ void dual_pass_recentred(const DevSpecies* sp, const 
     for (int t = A.l0; t < A.l1; ++t) {  // long rows
         const int4 ll = sm_int4(A.llist)[t];
         const int i = ll.x;
-        float h = STAGED ? long_dot_pk<false>(sm_u32(A.lwords) + ll.y, S, ll.z, lane)
-                         : long_dot_pk<true>(sp->ra.long_pk + ll.y, S + o.xbar, ll.z, lane);
+        float h;
+        if (F32V)
+            h = STAGED ? long_dot_sv<false>(sm_u16(A.lwords) + ll.y, nullptr, sm_f32(A.lvals) + ll.y, S, ll.z, lane)
+                       : long_dot_sv<true>(nullptr, sp->ra.long_idx + ll.y, sp->ra.long_v32 + ll.y, S + o.xbar, ll.z,
+                                           lane);
+        else
+            h = STAGED ? long_dot_pk<false>(sm_u32(A.lwords) + ll.y, S, ll.z, lane)
+                       : long_dot_pk<true>(sp->ra.long_pk + ll.y, S + o.xbar, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fmaf(pt.v32[q], S[o.xbar + pt.col[q]], h);
@@ -1191,6 +1306,32 @@ __device__ __forceinline__ double slice_dot64_staged(const uint32_t* wp, int sub
             if (k < len) {
                 vv[u] = __ldg(vp + (k << 5));
                 gg[u] = g[static_cast<int>(wp[k << 5] & 0xffffu) - sub];
+            } else {
+                vv[u] = 0.0;
+                gg[u] = 0.0;
+            }
+        }
+        acc0 = fma(vv[0], gg[0], acc0);
+        acc1 = fma(vv[1], gg[1], acc1);
+        acc0 = fma(vv[2], gg[2], acc0);
+        acc1 = fma(vv[3], gg[3], acc1);
+    }
+    return acc0 + acc1;
+}
+
+// slice_dot64_staged over staged 16-bit indices (the FP32-valued layout).
+__device__ __forceinline__ double slice_dot64_staged16(const uint16_t* ip, int sub, const double* __restrict__ vp,
+                                                       const double* g, int len) {
+    constexpr int U = 4;
+    double acc0 = 0.0, acc1 = 0.0;
+    for (int k0 = 0; k0 < len; k0 += U) {
+        double vv[U], gg[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int k = k0 + u;
+            if (k < len) {
+                vv[u] = __ldg(vp + (k << 5));
+                gg[u] = g[static_cast<int>(ip[k << 5]) - sub];
             } else {
                 vv[u] = 0.0;
                 gg[u] = 0.0;
@@ -1287,7 +1428,7 @@ __device__ __forceinline__ void kkt_row(const DevSpecies* sp, int i, double h, c
 // |c|_inf (v[14]) is accumulated only when `cinf` is set.  Long lines are
 // walked by the whole warp and counted by its lane 0.  All threads call it
 // (it synchronises between the column and the row loops).
-template <bool STAGED, bool PATCHED>
+template <bool STAGED, bool PATCHED, bool F32V>
 __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const OpsView& A, const OpsView& T, int a_sub,
                                                     int t_sub, double* xc, const double* yc, const double* cs,
                                                     const double* ls, const double* us, const double* bs,
@@ -1297,9 +1438,11 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
     for (int t = T.t0; t < T.t1; ++t) {
         const int4 sl = sm_int4(T.list)[t];
         const int j = (sl.x << 5) + lane;
-        double g = STAGED
-            ? slice_dot64_staged(sm_u32(T.words) + sl.y + lane, t_sub, sp->rat.v64 + sl.y + lane, yc, sl.z)
-            : slice_dot64_global2(sp->rat.idx + sl.y + lane, sp->rat.v64 + sl.y + lane, yc, sl.z);
+        double g = !STAGED ? slice_dot64_global2(sp->rat.idx + sl.y + lane, sp->rat.v64 + sl.y + lane, yc, sl.z)
+                   : F32V  ? slice_dot64_staged16(sm_u16(T.words) + sl.y + lane, t_sub, sp->rat.v64 + sl.y + lane,
+                                                  yc, sl.z)
+                           : slice_dot64_staged(sm_u32(T.words) + sl.y + lane, t_sub, sp->rat.v64 + sl.y + lane, yc,
+                                                sl.z);
         if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fma(pt.v64[q], yc[pt.row[q]], g);
@@ -1308,8 +1451,10 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
     for (int t = T.l0; t < T.l1; ++t) {
         const int4 ll = sm_int4(T.llist)[t];
         const int j = ll.x;
-        double g = long_dot64<STAGED>(STAGED ? sm_u32(T.lwords) + ll.y : nullptr, t_sub, sp->rat.long_idx + ll.y,
-                                      sp->rat.long_v64 + ll.y, yc, ll.z, lane);
+        const void* lw = F32V ? static_cast<const void*>(sm_u16(T.lwords) + ll.y)
+                              : static_cast<const void*>(sm_u32(T.lwords) + ll.y);
+        double g = long_dot64<STAGED, F32V>(STAGED ? lw : nullptr, t_sub, sp->rat.long_idx + ll.y,
+                                            sp->rat.long_v64 + ll.y, yc, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.col[q] == j) g = fma(pt.v64[q], yc[pt.row[q]], g);
@@ -1319,9 +1464,11 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
     for (int t = A.t0; t < A.t1; ++t) {
         const int4 sl = sm_int4(A.list)[t];
         const int i = (sl.x << 5) + lane;
-        double h = STAGED
-            ? slice_dot64_staged(sm_u32(A.words) + sl.y + lane, a_sub, sp->ra.v64 + sl.y + lane, xc, sl.z)
-            : slice_dot64_global2(sp->ra.idx + sl.y + lane, sp->ra.v64 + sl.y + lane, xc, sl.z);
+        double h = !STAGED ? slice_dot64_global2(sp->ra.idx + sl.y + lane, sp->ra.v64 + sl.y + lane, xc, sl.z)
+                   : F32V  ? slice_dot64_staged16(sm_u16(A.words) + sl.y + lane, a_sub, sp->ra.v64 + sl.y + lane,
+                                                  xc, sl.z)
+                           : slice_dot64_staged(sm_u32(A.words) + sl.y + lane, a_sub, sp->ra.v64 + sl.y + lane, xc,
+                                                sl.z);
         if (PATCHED && sl.w && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fma(pt.v64[q], xc[pt.col[q]], h);
@@ -1330,8 +1477,10 @@ __device__ __noinline__ void kkt_partials_recentred(const DevSpecies* sp, const 
     for (int t = A.l0; t < A.l1; ++t) {
         const int4 ll = sm_int4(A.llist)[t];
         const int i = ll.x;
-        double h = long_dot64<STAGED>(STAGED ? sm_u32(A.lwords) + ll.y : nullptr, a_sub, sp->ra.long_idx + ll.y,
-                                      sp->ra.long_v64 + ll.y, xc, ll.z, lane);
+        const void* lw = F32V ? static_cast<const void*>(sm_u16(A.lwords) + ll.y)
+                              : static_cast<const void*>(sm_u32(A.lwords) + ll.y);
+        double h = long_dot64<STAGED, F32V>(STAGED ? lw : nullptr, a_sub, sp->ra.long_idx + ll.y,
+                                            sp->ra.long_v64 + ll.y, xc, ll.z, lane);
         if (PATCHED && pt.n)
             for (int q = 0; q < pt.n; ++q)
                 if (pt.row[q] == i) h = fma(pt.v64[q], xc[pt.col[q]], h);
@@ -1362,7 +1511,7 @@ __device__ __forceinline__ void recentre(const DevSpecies* sp, const FastOffsets
     }
 }
 
-template <int MAXT, bool STAGED, bool PATCHED>
+template <int MAXT, bool STAGED, bool PATCHED, bool F32V>
 __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ double s_red[MAXT / 32][kRed];
@@ -1479,7 +1628,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             for (int i = tid; i < m; i += nthreads) p.out_y[roff + sp->row_perm[i]] = NAN;
             if (tid == 0) {
                 p.out_status[inst] = kStatusInvalid;
-                p.out_iters[inst] = 0;
+                p.out_iters[inst] = p.prior_iters ? p.prior_iters[inst] : 0;
                 if (p.hand_iters) p.hand_iters[inst] = 0;
                 p.out_obj[inst] = NAN;
                 for (int k = 0; k < kMetrics; ++k) p.out_metrics[static_cast<int64_t>(inst) * kMetrics + k] = NAN;
@@ -1511,7 +1660,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             double v[kRed];
 #pragma unroll
             for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-            kkt_partials_recentred<STAGED, PATCHED>(sp, OA, OT, a_sub, t_sub, PX(0), PY(0), cs, ls,
+            kkt_partials_recentred<STAGED, PATCHED, F32V>(sp, OA, OT, a_sub, t_sub, PX(0), PY(0), cs, ls,
                                    us, bs, dcand, rcand, true, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             cinf = s_tot[14];
@@ -1536,10 +1685,10 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             const float tau = static_cast<float>(eta / omega), sigma = static_cast<float>(eta * omega);
             const float w = static_cast<float>((k + 1.0) / (k + 2.0));
             double pdx2 = 0.0, pdy2 = 0.0, pdxa2 = 0.0, pdya2 = 0.0;
-            primal_pass_recentred<STAGED, PATCHED>(sp, o, OT, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
+            primal_pass_recentred<STAGED, PATCHED, F32V>(sp, o, OT, n, lane, tau, w, rho, check, PX(cur), PX(cur ^ 1),
                                           pdx2, pdxa2, pt);
             __syncthreads();
-            dual_pass_recentred<STAGED, PATCHED>(sp, o, OA, m, neq, lane, sigma, w, rho, check, PY(cur),
+            dual_pass_recentred<STAGED, PATCHED, F32V>(sp, o, OA, m, neq, lane, sigma, w, rho, check, PY(cur),
                                         PY(cur ^ 1), pdy2, pdya2, pt);
             __syncthreads();
             ++k;
@@ -1552,7 +1701,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
             v[6] = pdy2;
             v[7] = pdxa2;
             v[8] = pdya2;
-            kkt_partials_recentred<STAGED, PATCHED>(sp, OA, OT, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
+            kkt_partials_recentred<STAGED, PATCHED, F32V>(sp, OA, OT, a_sub, t_sub, PX(cur ^ 1), PY(cur ^ 1),
                                    cs, ls, us, bs, dcand, rcand, false, lane, v, pt);
             block_reduce(v, s_red, s_tot);
             if (threadIdx.x == 0) s_tot[14] = cinf;
@@ -1607,7 +1756,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 double vv[kRed];
 #pragma unroll
                 for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-                kkt_partials_recentred<STAGED, PATCHED>(sp, OA, OT, a_sub, t_sub, cx, cyv, cs, ls, us,
+                kkt_partials_recentred<STAGED, PATCHED, F32V>(sp, OA, OT, a_sub, t_sub, cx, cyv, cs, ls, us,
                                        bs, dcand, rcand, false, lane, vv, pt);
                 block_reduce(vv, s_red, s_tot);
                 cur ^= 1;
@@ -1655,7 +1804,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
         }
         for (int i = tid; i < m; i += nthreads) oy[roff + sp->row_perm[i]] = fy[i] * sp->dr[i];
         if (tid == 0) {
-            if (p.hand_iters) p.hand_iters[inst] = it;
+            if (p.hand_iters) p.hand_iters[inst] = (p.prior_iters ? p.prior_iters[inst] : 0) + it;
             if (hand) {
                 p.hand_omega[inst] = omega;
                 p.handoff_list[atomicAdd(p.handoff_count, 1)] = inst;
@@ -1671,7 +1820,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 mo[7] = omega;
                 p.out_obj[inst] = M.pobj;
                 p.out_status[inst] = status;
-                p.out_iters[inst] = it;
+                p.out_iters[inst] = (p.prior_iters ? p.prior_iters[inst] : 0) + it;
                 if (p.out_omega) p.out_omega[inst] = omega;
             }
         }
@@ -2136,7 +2285,7 @@ __device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairSt
     double v[kRed];
 #pragma unroll
     for (int qq = 0; qq < kRed; ++qq) v[qq] = 0.0;
-    kkt_partials_recentred<true, false>(sp, A, T, o.xbar, o.y, b.px0, b.py0, b.cs, b.ls, b.us, b.bs, b.dcand,
+    kkt_partials_recentred<true, false, false>(sp, A, T, o.xbar, o.y, b.px0, b.py0, b.cs, b.ls, b.us, b.bs, b.dcand,
                                         b.rcand, true, lane_id(), v, nopatch);
     block_reduce(v, s_red, s_tot);
     st.cinf = s_tot[14];
@@ -2179,7 +2328,7 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairSt
     v[6] = pdy2;
     v[7] = pdxa2;
     v[8] = pdya2;
-    kkt_partials_recentred<true, false>(sp, A, T, o.xbar, o.y, b.X(st.cur ^ 1), b.Y(st.cur ^ 1), b.cs, b.ls, b.us,
+    kkt_partials_recentred<true, false, false>(sp, A, T, o.xbar, o.y, b.X(st.cur ^ 1), b.Y(st.cur ^ 1), b.cs, b.ls, b.us,
                                         b.bs, b.dcand, b.rcand, false, lane_id(), v, nopatch);
     block_reduce(v, s_red, s_tot);
     if (tid == 0) s_tot[14] = st.cinf;
@@ -2223,7 +2372,7 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairSt
         double vv[kRed];
 #pragma unroll
         for (int qq = 0; qq < kRed; ++qq) vv[qq] = 0.0;
-        kkt_partials_recentred<true, false>(sp, A, T, o.xbar, o.y, cx, cyv, b.cs, b.ls, b.us, b.bs, b.dcand,
+        kkt_partials_recentred<true, false, false>(sp, A, T, o.xbar, o.y, cx, cyv, b.cs, b.ls, b.us, b.bs, b.dcand,
                                             b.rcand, false, lane_id(), vv, nopatch);
         block_reduce(vv, s_red, s_tot);
         st.cur ^= 1;
@@ -2375,28 +2524,30 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
     }
 }
 
+#define FBALP_INSTANTIATE_RECENTRED(MAXT)                                            \
+    template __global__ void pdhg_recentred<MAXT, true, false, false>(KernelParams);  \
+    template __global__ void pdhg_recentred<MAXT, false, false, false>(KernelParams); \
+    template __global__ void pdhg_recentred<MAXT, true, true, false>(KernelParams);   \
+    template __global__ void pdhg_recentred<MAXT, false, true, false>(KernelParams);  \
+    template __global__ void pdhg_recentred<MAXT, true, false, true>(KernelParams);   \
+    template __global__ void pdhg_recentred<MAXT, false, false, true>(KernelParams);
 #define FBALP_INSTANTIATE(MAXT)                                               \
     template __global__ void pdhg_persistent<float, MAXT, 0>(KernelParams);   \
     template __global__ void pdhg_persistent<float, MAXT, 1>(KernelParams);   \
     template __global__ void pdhg_persistent<double, MAXT, 0>(KernelParams);  \
     template __global__ void pdhg_persistent<double, MAXT, 1>(KernelParams);  \
     template __global__ void pdhg_persistent<double, MAXT, 2>(KernelParams);  \
-    template __global__ void pdhg_recentred<MAXT, true, false>(KernelParams); \
-    template __global__ void pdhg_recentred<MAXT, false, false>(KernelParams); \
-    template __global__ void pdhg_recentred<MAXT, true, true>(KernelParams);  \
-    template __global__ void pdhg_recentred<MAXT, false, true>(KernelParams);
+    FBALP_INSTANTIATE_RECENTRED(MAXT)
 FBALP_INSTANTIATE(512)
 FBALP_INSTANTIATE(1024)
 // the re-centred kernel also at 768 threads (an 85-register budget: more
 // warps per scheduler to hide shared-memory latency)
-template __global__ void pdhg_recentred<768, true, false>(KernelParams);
-template __global__ void pdhg_recentred<768, false, false>(KernelParams);
-template __global__ void pdhg_recentred<768, true, true>(KernelParams);
-template __global__ void pdhg_recentred<768, false, true>(KernelParams);
+FBALP_INSTANTIATE_RECENTRED(768)
 template __global__ void pdhg_recentred_pair<512>(KernelParams);
 template __global__ void pdhg_recentred_pair<768>(KernelParams);
 template __global__ void pdhg_recentred_pair<1024>(KernelParams);
 #undef FBALP_INSTANTIATE
+#undef FBALP_INSTANTIATE_RECENTRED
 
 // Blocks of up to 512 threads use the variant with a 128-register budget,
 // larger blocks the 64-register one.  `fast`: FP32 launches take the
@@ -2435,39 +2586,45 @@ cudaError_t launch_pdhg(bool fp64, bool fast, int grid, int threads, size_t smem
 
 // `patched`: the variant that applies per-instance patched entries (launched
 // only for batches that bind patch values; the other variant has none of
-// that code).
+// that code); `f32`: FP32 matrix values (unpatched batches only).
 template <int MAXT>
-static const void* recentred_for(bool staged, bool patched) {
+static const void* recentred_for(bool staged, bool patched, bool f32) {
+    if (f32)
+        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<MAXT, true, false, true>)
+                      : reinterpret_cast<const void*>(&pdhg_recentred<MAXT, false, false, true>);
     if (patched)
-        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<MAXT, true, true>)
-                      : reinterpret_cast<const void*>(&pdhg_recentred<MAXT, false, true>);
-    return staged ? reinterpret_cast<const void*>(&pdhg_recentred<MAXT, true, false>)
-                  : reinterpret_cast<const void*>(&pdhg_recentred<MAXT, false, false>);
+        return staged ? reinterpret_cast<const void*>(&pdhg_recentred<MAXT, true, true, false>)
+                      : reinterpret_cast<const void*>(&pdhg_recentred<MAXT, false, true, false>);
+    return staged ? reinterpret_cast<const void*>(&pdhg_recentred<MAXT, true, false, false>)
+                  : reinterpret_cast<const void*>(&pdhg_recentred<MAXT, false, false, false>);
 }
 
-const void* recentred_symbol(int threads, bool staged, bool patched) {
-    if (threads <= 512) return recentred_for<512>(staged, patched);
-    if (threads <= 768) return recentred_for<768>(staged, patched);
-    return recentred_for<1024>(staged, patched);
+const void* recentred_symbol(int threads, bool staged, bool patched, bool f32) {
+    if (threads <= 512) return recentred_for<512>(staged, patched, f32);
+    if (threads <= 768) return recentred_for<768>(staged, patched, f32);
+    return recentred_for<1024>(staged, patched, f32);
 }
 
 template <int MAXT>
-static void launch_recentred_for(bool staged, bool patched, int grid, int threads, size_t smem,
+static void launch_recentred_for(bool staged, bool patched, bool f32, int grid, int threads, size_t smem,
                                  cudaStream_t stream, const KernelParams& p) {
-    if (patched) {
-        if (staged) pdhg_recentred<MAXT, true, true><<<grid, threads, smem, stream>>>(p);
-        else pdhg_recentred<MAXT, false, true><<<grid, threads, smem, stream>>>(p);
+    if (f32) {
+        if (staged) pdhg_recentred<MAXT, true, false, true><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<MAXT, false, false, true><<<grid, threads, smem, stream>>>(p);
+    } else if (patched) {
+        if (staged) pdhg_recentred<MAXT, true, true, false><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<MAXT, false, true, false><<<grid, threads, smem, stream>>>(p);
     } else {
-        if (staged) pdhg_recentred<MAXT, true, false><<<grid, threads, smem, stream>>>(p);
-        else pdhg_recentred<MAXT, false, false><<<grid, threads, smem, stream>>>(p);
+        if (staged) pdhg_recentred<MAXT, true, false, false><<<grid, threads, smem, stream>>>(p);
+        else pdhg_recentred<MAXT, false, false, false><<<grid, threads, smem, stream>>>(p);
     }
 }
 
 cudaError_t launch_recentred(bool staged, bool patched, int grid, int threads, size_t smem, cudaStream_t stream,
-                             const KernelParams& p) {
-    if (threads <= 512) launch_recentred_for<512>(staged, patched, grid, threads, smem, stream, p);
-    else if (threads <= 768) launch_recentred_for<768>(staged, patched, grid, threads, smem, stream, p);
-    else launch_recentred_for<1024>(staged, patched, grid, threads, smem, stream, p);
+                             const KernelParams& p, bool f32) {
+    if (threads <= 512) launch_recentred_for<512>(staged, patched, f32, grid, threads, smem, stream, p);
+    else if (threads <= 768) launch_recentred_for<768>(staged, patched, f32, grid, threads, smem, stream, p);
+    else launch_recentred_for<1024>(staged, patched, f32, grid, threads, smem, stream, p);
     return cudaGetLastError();
 }
 

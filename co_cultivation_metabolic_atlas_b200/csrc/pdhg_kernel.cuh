@@ -52,9 +52,11 @@ struct DevLines {
     const uint32_t* pk;           // packed slice words (16-bit index | BF16 value)
     const int32_t* idx;           // slice indices (pad -> n or m)
     const double* v64;            // slice FP64 scaled values
+    const float* v32;             // slice FP32 scaled values
     const uint32_t* long_pk;      // long-line words
     const int32_t* long_idx;
     const double* long_v64;
+    const float* long_v32;
 };
 
 struct DevSpecies {
@@ -118,6 +120,11 @@ struct Layout {
     // re-centred layouts only: the long lines' schedule offsets [warps + 1],
     // lists (int4), per-slice lane masks (uint32) and packed words
     int64_t lsched_a_off, lsched_at_off, llist_a, llist_at, lmask_a, lmask_at, mat_a_long, mat_at_long;
+    // re-centred layouts with FP32 matrix values (f32_values = 1): the
+    // staged 16-bit indices sit at mat_*_idx (slices) and mat_*_long (long
+    // lines), the FP32 values at mat_*_val and mat_*_lval
+    int64_t mat_a_lval, mat_at_lval;
+    int32_t f32_values, pad4_;
     // re-centred FP32 layout only (slab offsets): the two FP64 point buffers
     // of x (n+1) and y (m+1) -- base and candidate, roles swapped at every
     // re-centring -- and the FP32 reduced cost / primal residual of the last

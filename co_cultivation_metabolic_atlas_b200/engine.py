@@ -56,6 +56,7 @@ class SolveConfig:
     fp32_passthrough_tol: float = 1e-3
     fallback_iterations: int = 4096
     recentre: bool = True              # MIXED: re-centred FP32 phase (FP64 tolerances)
+    fp32_values_phase: bool = True     # MIXED re-centred: hand-offs continue with FP32 matrix values first
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -74,6 +75,7 @@ class SolveConfig:
             setattr(p, name, float(getattr(self, name)))
         p.restarts = 1 if self.restarts else 0
         p.fp32_recentre = 1 if self.recentre else 0
+        p.fp32_values_phase = 1 if self.fp32_values_phase else 0
         return p
 
 

@@ -145,6 +145,13 @@ typedef struct fbalp_solve_params {
                                     layout, else the plain schedule below.
                                     0: plain schedule -- FP32 iterates to the
                                     fp32_* tolerances, then FP64 iterates    */
+    int32_t fp32_values_phase;   /* MIXED re-centred schedule: 1 (default) --
+                                    instances the re-centred phase hands off
+                                    (its matrix words hold BF16 values) first
+                                    continue in a re-centred phase with FP32
+                                    matrix values, and only what that phase
+                                    hands off goes to the FP64 phase; 0: the
+                                    hand-offs go to the FP64 phase directly  */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);
@@ -305,12 +312,15 @@ int fbalp_engine_phase_times(fbalp_engine* engine, float* ms_fp32, float* ms_fp6
 
 /* Kernel kinds the last fbalp_engine_solve launched for its first (FP32 /
  * re-centred) and FP64 phases: FBALP_KERNEL_* or -1 for a phase that did not
- * run.  Instrumentation for tests and benchmarks. */
+ * run (the FP32-valued middle phase of the mixed schedule is not reported).
+ * Instrumentation for tests and benchmarks. */
 #define FBALP_KERNEL_FP32 0
 #define FBALP_KERNEL_FP64 1
 #define FBALP_KERNEL_RECENTRED_STAGED 2
 #define FBALP_KERNEL_RECENTRED_STREAMED 3
 #define FBALP_KERNEL_RECENTRED_PAIRED 4
+#define FBALP_KERNEL_RECENTRED_F32_STAGED 5
+#define FBALP_KERNEL_RECENTRED_F32_STREAMED 6
 int fbalp_engine_phase_kernels(fbalp_engine* engine, int32_t* fp32_kind, int32_t* fp64_kind);
 
 /* Timing slots (benchmark instrumentation): create `slots` (0..64) pairs of

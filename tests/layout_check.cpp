@@ -40,7 +40,7 @@ int main() {
         for (int neqf : {0, 1, 2})
           for (int nl : {0, 1, 12})
             for (long cap : {8192L, 100000L, 225000L})
-              for (int kind : {0, 1, 2}) {  // 0 staged, 1 streamed, 2 paired
+              for (int kind : {0, 1, 2, 3}) {  // 0 staged, 1 streamed, 2 paired, 3 staged with FP32 values
                 const int neq = neqf == 0 ? m : (neqf == 1 ? m / 2 : 0);
                 fbalp::LinesShape sa, sat;
                 sa.nslices = (m+31)/32; sat.nslices = (n+31)/32;
@@ -48,7 +48,7 @@ int main() {
                 sa.nlong = std::min(nl, m); sat.nlong = std::min(nl, n);
                 sa.long_elems = 70L*sa.nlong; sat.long_elems = 45L*sat.nlong;
                 auto P = kind == 2 ? fbalp::plan_layout_pair(n, m, neq, w, sa, sat, cap)
-                                   : fbalp::plan_layout_recentred(n, m, w, sa, sat, cap, kind == 0);
+                                   : fbalp::plan_layout_recentred(n, m, w, sa, sat, cap, kind != 1, kind == 3);
                 auto& L = P.layout; total++;
                 if (!L.recentred) continue;
                 const long u = kind == 2 ? 8 : 4;  // vector element bytes
@@ -63,11 +63,18 @@ int main() {
                                      {L.arr[fbalp::kU], L.arr[fbalp::kU] + u*n}, {L.arr[fbalp::kB], L.arr[fbalp::kB] + u*m},
                                      {L.arr[fbalp::kYa], L.arr[fbalp::kYa] + (kind == 2 ? u*(m-neq) : u*m)}};
                 if (kind != 2) rs.push_back({L.arr[fbalp::kX], L.arr[fbalp::kX] + u*n});
-                if (L.mat_smem) {
+                if (L.mat_smem && kind != 3) {
                   rs.push_back({L.mat_a_idx, L.mat_a_idx + 4*sa.elems}); rs.push_back({L.mat_at_idx, L.mat_at_idx + 4*sat.elems});
                   rs.push_back({L.mat_a_long, L.mat_a_long + 4*sa.long_elems}); rs.push_back({L.mat_at_long, L.mat_at_long + 4*sat.long_elems});
                 }
-                bool ok = fbalp::layout_aligned(L) && P.smem_bytes <= cap && L.recentred == (kind == 2 ? 2 : 1);
+                if (L.mat_smem && kind == 3) {
+                  rs.push_back({L.mat_a_idx, L.mat_a_idx + 2*sa.elems}); rs.push_back({L.mat_at_idx, L.mat_at_idx + 2*sat.elems});
+                  rs.push_back({L.mat_a_long, L.mat_a_long + 2*sa.long_elems}); rs.push_back({L.mat_at_long, L.mat_at_long + 2*sat.long_elems});
+                  rs.push_back({L.mat_a_val, L.mat_a_val + 4*sa.elems}); rs.push_back({L.mat_at_val, L.mat_at_val + 4*sat.elems});
+                  rs.push_back({L.mat_a_lval, L.mat_a_lval + 4*sa.long_elems}); rs.push_back({L.mat_at_lval, L.mat_at_lval + 4*sat.long_elems});
+                }
+                bool ok = fbalp::layout_aligned(L) && P.smem_bytes <= cap && L.recentred == (kind == 2 ? 2 : 1) &&
+                          L.f32_values == (kind == 3 ? 1 : 0);
                 for (auto& r : rs) if (r.e > P.smem_bytes) ok = false;
                 for (size_t i = 0; i < rs.size(); ++i) for (size_t j = i+1; j < rs.size(); ++j)
                   if (rs[i].b < rs[j].e && rs[j].b < rs[i].e && rs[i].e > rs[i].b && rs[j].e > rs[j].b) ok = false;
