@@ -872,6 +872,11 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
                 pb.warm_omega = c_omega;
                 pb.prior_iters = c_iters;
                 pb.fallback_iters = 0;  // a stalled point restarting cold would lose its progress
+                // no stall rule (on real models slow phases outlast any window:
+                // measured plateaus beyond 512 tests); the phase's own budget
+                // ends it, and what it leaves goes to the FP64 phase
+                pb.handoff_on_stall = 0;
+                pb.limit_handoff = 1;
                 pb.hint_iters = nullptr;
                 pb.patch_values = nullptr;
                 pb.handoff_list = static_cast<int32_t*>(e->hand2_list.ptr);
