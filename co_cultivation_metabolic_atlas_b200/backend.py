@@ -31,9 +31,9 @@ expanded and the duals lifted back; the row is accepted only when the
 original-LP certificate passes on the lifted pair.
 
 Requests stopped by the iteration cap get one more GPU pass, alone, from
-their own iterates, of up to ``retry_iterations`` (default 400,000; 0
-disables) iterations; cold genome-scale LPs need 10^5 iterations, far above
-the first pass's budget.  A row is still accepted only on its certificate.
+their own iterates, of up to ``retry_iterations`` (default 1,000,000; 0
+disables) iterations; cold genome-scale LPs need 10^5 to 7 x 10^5
+iterations, far above the first pass's budget.  A row is still accepted only on its certificate.
 
 With ``split_rows=L`` (off by default) rows longer than ``L`` (the hub
 metabolites of genome-scale models hold up to ~1,200 reactions) are split
@@ -73,7 +73,7 @@ class B200LPBackend:
     def __init__(self, *, mode='previous', precision='mixed', iterations=20000,
                  fp32_iterations=20000, check_interval=64, stage=None,
                  options: EngineOptions | None = None, warm_start_model=None, device=None,
-                 equality_reduction=False, split_rows=None, retry_iterations=400_000):
+                 equality_reduction=False, split_rows=None, retry_iterations=1_000_000):
         if mode not in ('cold', 'previous', 'mlp'):
             raise ValueError('Unknown warm-start mode')
         if mode == 'mlp' and warm_start_model is None:

@@ -850,74 +850,48 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             // LPs) continue from their own point with FP32 matrix values;
             // what that phase hands off in turn finishes in FP64
             const int fmode = (q.fp32_values_phase && !patched) ? f32_mode(e) : 0;
-            const int32_t* c_list = static_cast<const int32_t*>(e->hand_list.ptr);
-            const int32_t* c_count = static_cast<const int32_t*>(e->hand_count.ptr);
-            const double* c_x = static_cast<const double*>(e->mid_x.ptr);
-            const double* c_y = static_cast<const double*>(e->mid_y.ptr);
-            const double* c_omega = static_cast<const double*>(e->mid_omega.ptr);
-            const int32_t* c_iters = static_cast<const int32_t*>(e->mid_iters.ptr);
+            // the handed-off instances continue from their own point
+            fbalp::KernelParams pn = p;
+            pn.order = static_cast<const int32_t*>(e->hand_list.ptr);
+            pn.count_dev = static_cast<const int32_t*>(e->hand_count.ptr);
+            pn.warm_x = static_cast<const double*>(e->mid_x.ptr);
+            pn.warm_y = static_cast<const double*>(e->mid_y.ptr);
+            pn.warm_omega = static_cast<const double*>(e->mid_omega.ptr);
+            pn.prior_iters = static_cast<const int32_t*>(e->mid_iters.ptr);
+            pn.out_x = out_x;
+            pn.out_y = out_y;
+            pn.out_obj = out_objective;
+            pn.out_metrics = out_metrics;
+            pn.out_omega = out_omega;
+            pn.out_status = out_status;
+            pn.out_iters = out_iterations;
+            pn.max_iters = q.max_iterations;
+            pn.tol_p = q.tol_primal;
+            pn.tol_d = q.tol_dual;
+            pn.tol_g = q.tol_gap;
+            pn.final_status = fbalp::kStatusOptimal;
+            pn.clip_output = 1;
+            pn.floor_tol = q.floor_tol;
+            pn.passthrough_tol = 0.0;
             if (fmode) {
-                e->mid2_x.ensure(e->total_cols * sizeof(double));
-                e->mid2_y.ensure(std::max<int64_t>(1, e->total_rows) * sizeof(double));
-                e->mid2_omega.ensure(e->count * sizeof(double));
-                e->mid2_iters.ensure(e->count * sizeof(int32_t));
-                e->hand2_list.ensure(e->count * sizeof(int32_t));
-                e->hand2_count.ensure(sizeof(int32_t));
-                check(cudaMemsetAsync(e->hand2_count.ptr, 0, sizeof(int32_t), e->stream), "memset handoff count");
-                fbalp::KernelParams pb = pr;
-                pb.order = c_list;
-                pb.count_dev = c_count;
-                pb.warm_x = c_x;
-                pb.warm_y = c_y;
-                pb.warm_omega = c_omega;
-                pb.prior_iters = c_iters;
-                pb.fallback_iters = 0;  // a stalled point restarting cold would lose its progress
-                // no stall rule (on real models slow phases outlast any window:
-                // measured plateaus beyond 512 tests); the phase's own budget
-                // ends it, and what it leaves goes to the FP64 phase
-                pb.handoff_on_stall = 0;
-                pb.limit_handoff = 1;
-                pb.hint_iters = nullptr;
-                pb.patch_values = nullptr;
-                pb.handoff_list = static_cast<int32_t*>(e->hand2_list.ptr);
-                pb.handoff_count = static_cast<int32_t*>(e->hand2_count.ptr);
-                pb.hand_x = static_cast<double*>(e->mid2_x.ptr);
-                pb.hand_y = static_cast<double*>(e->mid2_y.ptr);
-                pb.hand_omega = static_cast<double*>(e->mid2_omega.ptr);
-                pb.hand_iters = static_cast<int32_t*>(e->mid2_iters.ptr);
-                run_phase(e, false, pb, fmode, 2, true, false);
-                c_list = static_cast<const int32_t*>(e->hand2_list.ptr);
-                c_count = static_cast<const int32_t*>(e->hand2_count.ptr);
-                c_x = static_cast<const double*>(e->mid2_x.ptr);
-                c_y = static_cast<const double*>(e->mid2_y.ptr);
-                c_omega = static_cast<const double*>(e->mid2_omega.ptr);
-                c_iters = static_cast<const int32_t*>(e->mid2_iters.ptr);
+                // with FP32 matrix values (the BF16-rounded matrix of the
+                // first phase is what stalls on badly scaled models); no
+                // stall rule and no further hand-off: on real models slow
+                // phases outlast any stall window (measured plateaus beyond
+                // 512 tests) and converge at this phase's rate, which the
+                // FP64 phase would only repeat at ~20x the cost per
+                // iteration; an instance that exhausts the budget reports
+                // the iteration limit with its iterate (a caller's next pass
+                // continues from it)
+                pn.stall_checks = q.fp64_stall_checks;
+                pn.fallback_iters = 0;  // a stalled point restarting cold would lose its progress
+                pn.handoff_on_stall = 0;
+                run_phase(e, false, pn, fmode, 2, true, true);
+            } else {
+                pn.stall_checks = q.fp64_stall_checks;
+                pn.fallback_iters = q.fallback_iterations;
+                run_phase(e, true, pn, 0, 1, true, true);
             }
-            fbalp::KernelParams p64 = p;
-            p64.order = c_list;
-            p64.count_dev = c_count;
-            p64.warm_x = c_x;
-            p64.warm_y = c_y;
-            p64.warm_omega = c_omega;
-            p64.prior_iters = c_iters;
-            p64.out_x = out_x;
-            p64.out_y = out_y;
-            p64.out_obj = out_objective;
-            p64.out_metrics = out_metrics;
-            p64.out_omega = out_omega;
-            p64.out_status = out_status;
-            p64.out_iters = out_iterations;
-            p64.max_iters = q.max_iterations;
-            p64.tol_p = q.tol_primal;
-            p64.tol_d = q.tol_dual;
-            p64.tol_g = q.tol_gap;
-            p64.final_status = fbalp::kStatusOptimal;
-            p64.clip_output = 1;
-            p64.stall_checks = q.fp64_stall_checks;
-            p64.floor_tol = q.floor_tol;
-            p64.passthrough_tol = 0.0;
-            p64.fallback_iters = q.fallback_iterations;
-            run_phase(e, true, p64, 0, 1, !fmode, true);
         } else {
             e->mid_x.ensure(e->total_cols * sizeof(double));
             e->mid_y.ensure(std::max<int64_t>(1, e->total_rows) * sizeof(double));
@@ -998,7 +972,7 @@ extern "C" int fbalp_engine_phase_times(fbalp_engine* e, float* ms_fp32, float* 
 extern "C" int fbalp_engine_phase_kernels(fbalp_engine* e, int32_t* fp32_kind, int32_t* fp64_kind) {
     if (!e) return fail(FBALP_ERR_INVALID, "engine is NULL");
     if (fp32_kind) *fp32_kind = e->last_kind[0];
-    if (fp64_kind) *fp64_kind = e->last_kind[1];
+    if (fp64_kind) *fp64_kind = e->last_kind[2] >= 0 ? e->last_kind[2] : e->last_kind[1];
     return FBALP_OK;
 }
 

@@ -132,8 +132,6 @@ struct fbalp_engine {
     // workspace
     Buffer queue, mid_x, mid_y, mid_omega, mid_iters, mid_status, mid_obj, mid_metrics, spill;
     Buffer hand_list, hand_count;  // re-centred phase -> next phase work list
-    // FP32-valued re-centred phase -> FP64 phase: work list and hand-off point
-    Buffer hand2_list, hand2_count, mid2_x, mid2_y, mid2_omega, mid2_iters;
     Buffer layout32_buf, layout64_buf;
     // device copies of the launch layouts, one per kernel kind (plain FP32,
     // FP64, re-centred staged, re-centred streamed, paired re-centred),
@@ -165,8 +163,7 @@ struct fbalp_engine {
         for (Buffer* b : {&inst_species, &col_off, &row_off, &order, &queue, &mid_x, &mid_y, &mid_omega,
                           &mid_iters, &mid_status, &mid_obj, &mid_metrics, &spill, &layout32_buf,
                           &layout64_buf, &hand_list, &hand_count, &layout_dev[0], &layout_dev[1],
-                          &layout_dev[2], &layout_dev[3], &layout_dev[4], &layout_dev[5], &layout_dev[6],
-                          &hand2_list, &hand2_count, &mid2_x, &mid2_y, &mid2_omega, &mid2_iters})
+                          &layout_dev[2], &layout_dev[3], &layout_dev[4], &layout_dev[5], &layout_dev[6]})
             b->release();
     }
 };

@@ -1717,7 +1717,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 break;
             }
             if (it >= p.max_iters) {
-                status = (p.limit_handoff && p.handoff_list) ? kStatusHandoff : kStatusIterationLimit;
+                status = kStatusIterationLimit;
                 break;
             }
             if (!full) continue;

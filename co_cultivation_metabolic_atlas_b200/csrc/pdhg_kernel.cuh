@@ -192,10 +192,7 @@ struct KernelParams {
                                   // off to the FP64 phase (0 = never)
     const double* patch_values;   // may be null: per instance, npatch deltas
                                   // (original units) at patch_stride apart
-    int32_t patch_stride;
-    int32_t limit_handoff;        // >0 (with handoff_list): an instance that
-                                  // reaches max_iters is handed off instead
-                                  // of reporting the iteration limit
+    int32_t patch_stride, pad3_;
     const int32_t* hint_iters;    // may be null: per instance, the iteration
                                   // count of its previous solve; an instance
                                   // whose hint is >= check_every skips the

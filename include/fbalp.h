@@ -147,11 +147,11 @@ typedef struct fbalp_solve_params {
                                     fp32_* tolerances, then FP64 iterates    */
     int32_t fp32_values_phase;   /* MIXED re-centred schedule: 1 (default) --
                                     instances the re-centred phase hands off
-                                    (its matrix words hold BF16 values) first
+                                    (its matrix words hold BF16 values)
                                     continue in a re-centred phase with FP32
-                                    matrix values, and only what that phase
-                                    hands off goes to the FP64 phase; 0: the
-                                    hand-offs go to the FP64 phase directly  */
+                                    matrix values (same budget, no stall rule)
+                                    where the species fit it; 0: the
+                                    hand-offs continue in the FP64 phase     */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);
@@ -312,7 +312,8 @@ int fbalp_engine_phase_times(fbalp_engine* engine, float* ms_fp32, float* ms_fp6
 
 /* Kernel kinds the last fbalp_engine_solve launched for its first (FP32 /
  * re-centred) and FP64 phases: FBALP_KERNEL_* or -1 for a phase that did not
- * run (the FP32-valued middle phase of the mixed schedule is not reported).
+ * run; the second phase of the mixed re-centred schedule is the FP32-valued
+ * re-centred kernel (FBALP_KERNEL_RECENTRED_F32_*) or the FP64 kernel.
  * Instrumentation for tests and benchmarks. */
 #define FBALP_KERNEL_FP32 0
 #define FBALP_KERNEL_FP64 1

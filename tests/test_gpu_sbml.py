@@ -16,7 +16,7 @@ pytestmark = pytest.mark.gpu
 
 SBML_DIR = Path(__file__).resolve().parent / "golden" / "sbml"
 OBJ_TOL = 1e-6
-COLD_CAP = 400_000
+COLD_CAP = 1_000_000
 
 
 def test_real_model_traces_replay_through_the_backend(tmp_path, forbid_cpu_optimizers):
@@ -24,7 +24,7 @@ def test_real_model_traces_replay_through_the_backend(tmp_path, forbid_cpu_optim
     d = tmp_path / "sbml"
     shutil.copytree(SBML_DIR, d)
     # default drop-in settings: the first pass's 20 k cap stops every one of
-    # these LPs, the second GPU pass (retry_iterations, 4e5) finishes them
+    # these LPs, the second GPU pass (retry_iterations, 1e6) finishes them
     be = B200LPBackend(mode="cold")
     assert be.split_rows is None and be.retry_iterations == COLD_CAP
     rows, ref = lp_trace.replay(d, be)
