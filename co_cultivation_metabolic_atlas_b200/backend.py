@@ -285,8 +285,11 @@ class B200LPBackend:
         rows = [np.arange(ro[i], ro[i] + eng.shapes[species[i]][0]) for i in lag]
         ci, ri = np.concatenate(cols), np.concatenate(rows) if tr else np.empty(0, np.int64)
         eng.set_instances(species[lag], t(lower[ci]), t(upper[ci]), t(cost[ci]), t(rhs[ri]) if tr else None)
+        # a continuation: the FP32-valued re-centred phase from the first
+        # pass's iterates (no BF16 phase, no cold fallback)
         cfg = SolveConfig(**{**self.config.__dict__, 'max_iterations': self.retry_iterations,
-                             'fp32_max_iterations': self.retry_iterations})
+                             'fp32_max_iterations': self.retry_iterations, 'fp32_values_phase': 2,
+                             'fallback_iterations': 0})
         r2 = eng.solve(warm_x=res.x[torch.as_tensor(ci, device=res.x.device)],
                        warm_y=res.y[torch.as_tensor(ri, device=res.y.device)] if tr else None,
                        warm_omega=res.omega[torch.as_tensor(lag, device=res.omega.device)], config=cfg)

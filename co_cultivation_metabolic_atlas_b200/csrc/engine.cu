@@ -144,6 +144,9 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->fallback_iterations = 4096;
     p->fp32_recentre = 1;
     p->fp32_values_phase = 1;
+    p->gate_primal = 1e-5;
+    p->gate_dual = 1e-7;
+    p->gate_gap = 1e-7;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -771,6 +774,9 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
         p.check_every = q.check_every;
         p.rho = q.reflection;
         p.restarts = q.restarts;
+        p.gate_p = q.gate_primal;
+        p.gate_d = q.gate_dual;
+        p.gate_g = q.gate_gap;
         bool patched = false;
         if (e->patch_values)
             for (int32_t sp_id : e->h_species) patched = patched || e->dev_species_host[sp_id].npatch > 0;
@@ -800,6 +806,36 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
             p.passthrough_tol = 0.0;
             p.fallback_iters = q.fallback_iterations;
             run_phase(e, fp64, p);
+        } else if (q.fp32_recentre && q.fp32_values_phase == 2 && !patched && recentred_mode(e) != 0 &&
+                   f32_mode(e) != 0) {
+            // continuation: every instance runs in the FP32-valued re-centred
+            // phase directly, from the caller's point (iterates that an
+            // earlier call left in that phase would only be set back by the
+            // BF16-matrix phase and its cold fallback)
+            fbalp::KernelParams pn = p;
+            pn.warm_x = warm_x;
+            pn.warm_y = warm_y;
+            pn.warm_omega = warm_omega;
+            pn.prior_iters = nullptr;
+            pn.out_x = out_x;
+            pn.out_y = out_y;
+            pn.out_obj = out_objective;
+            pn.out_metrics = out_metrics;
+            pn.out_omega = out_omega;
+            pn.out_status = out_status;
+            pn.out_iters = out_iterations;
+            pn.max_iters = q.max_iterations;
+            pn.tol_p = q.tol_primal;
+            pn.tol_d = q.tol_dual;
+            pn.tol_g = q.tol_gap;
+            pn.final_status = fbalp::kStatusOptimal;
+            pn.clip_output = 1;
+            pn.stall_checks = q.fp64_stall_checks;
+            pn.floor_tol = q.floor_tol;
+            pn.passthrough_tol = 0.0;
+            pn.fallback_iters = 0;
+            pn.handoff_on_stall = 0;
+            run_phase(e, false, pn, f32_mode(e), 2, true, true);
         } else if (q.fp32_recentre && recentred_mode(e) != 0) {
             // re-centred FP32 phase to the FP64 tolerances; what it does not
             // certify (stalled instances) continues in the FP64 phase

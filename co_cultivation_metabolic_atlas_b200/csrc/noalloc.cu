@@ -198,6 +198,9 @@ extern "C" int fbalp_engine_solve_noalloc(fbalp_engine* e, int64_t count, const 
         p.clip_output = 1;
         p.stall_checks = q.fp64_stall_checks;
         p.floor_tol = q.floor_tol;
+        p.gate_p = q.gate_primal;
+        p.gate_d = q.gate_dual;
+        p.gate_g = q.gate_gap;
         p.passthrough_tol = 0.0;
         p.fallback_iters = q.fallback_iterations;
 

@@ -202,6 +202,15 @@ __device__ Metrics evaluate(const double* s_tot, double omega, double tol_p, dou
     return M;
 }
 
+// The stall-floor rule accepts a point that meets floor_tol relative to the
+// iterate's and the cost's magnitudes AND the original-LP certificate gate
+// in absolute terms (with open 1000 bounds the relative test alone admits
+// primal residuals of 1e-4).
+__device__ __forceinline__ bool floor_accepts(const Metrics& M, const KernelParams& p) {
+    return M.primal <= p.floor_tol * (1.0 + M.xinf) && M.dual <= p.floor_tol * (1.0 + M.cinf) &&
+           M.primal <= p.gate_p && M.dual <= p.gate_d && M.kgap <= p.gate_g;
+}
+
 // Stage one species' warp schedule (and, when the layout says so, its matrix
 // slices with 16-bit indices) into shared memory.
 template <typename T>
@@ -817,8 +826,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
                         status = p.final_status;
                         break;
                     }
-                    if (p.final_status == kStatusOptimal && e <= p.floor_tol &&
-                        M.primal <= p.floor_tol * (1.0 + M.xinf) && M.dual <= p.floor_tol * (1.0 + M.cinf)) {
+                    if (p.final_status == kStatusOptimal && e <= p.floor_tol && floor_accepts(M, p)) {
                         status = p.final_status;
                         break;
                     }
@@ -1730,8 +1738,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
                 } else {
                     ++stall;
                 }
-                if (p.stall_checks > 0 && stall >= p.stall_checks && e <= p.floor_tol &&
-                    M.primal <= p.floor_tol * (1.0 + M.xinf) && M.dual <= p.floor_tol * (1.0 + M.cinf)) {
+                if (p.stall_checks > 0 && stall >= p.stall_checks && e <= p.floor_tol && floor_accepts(M, p)) {
                     status = p.final_status;
                     break;
                 }
@@ -2349,8 +2356,7 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairSt
         } else {
             ++st.stall;
         }
-        if (p.stall_checks > 0 && st.stall >= p.stall_checks && e <= p.floor_tol &&
-            M.primal <= p.floor_tol * (1.0 + M.xinf) && M.dual <= p.floor_tol * (1.0 + M.cinf))
+        if (p.stall_checks > 0 && st.stall >= p.stall_checks && e <= p.floor_tol && floor_accepts(M, p))
             status = p.final_status;
         else if (p.handoff_on_stall > 0 && st.stall >= p.handoff_on_stall)
             status = kStatusHandoff;

@@ -171,6 +171,8 @@ struct KernelParams {
     int32_t stall_checks;         // >0: stall rule after this many
                                   // non-improving convergence tests
     double floor_tol;             // FP64 phase: tolerance accepted after a stall
+    double gate_p, gate_d, gate_g;  // ... where the point also passes the
+                                    // original-LP certificate gate
     double passthrough_tol;       // FP32 phase: warm starts with error <= this
                                   // skip the phase unchanged (0 = never)
     int32_t fallback_iters;       // warm starts not converged after this many

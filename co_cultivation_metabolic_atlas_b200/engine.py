@@ -56,7 +56,16 @@ class SolveConfig:
     fp32_passthrough_tol: float = 1e-3
     fallback_iterations: int = 4096
     recentre: bool = True              # MIXED: re-centred FP32 phase (FP64 tolerances)
-    fp32_values_phase: bool = True     # MIXED re-centred: hand-offs continue with FP32 matrix values first
+    # MIXED re-centred: True / 1 -- hand-offs continue with FP32 matrix
+    # values; False / 0 -- in FP64; 2 -- continuation: every instance runs
+    # with FP32 matrix values from the warm point (no BF16 phase, no cold
+    # fallback), for iterates an earlier call stopped at its cap
+    fp32_values_phase: int = 1
+    # the certificate gate a stall-floor acceptance must also pass
+    # (src/gpu_block_lp.py:84)
+    gate_primal: float = 1e-5
+    gate_dual: float = 1e-7
+    gate_gap: float = 1e-7
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -71,11 +80,17 @@ class SolveConfig:
                 raise ValueError(f"{name} must be an integer")
             setattr(p, name, int(value))
         for name in ("tol_primal", "tol_dual", "tol_gap", "fp32_tol_primal", "fp32_tol_dual",
-                     "fp32_tol_gap", "reflection", "floor_tol", "fp32_passthrough_tol"):
+                     "fp32_tol_gap", "reflection", "floor_tol", "fp32_passthrough_tol", "gate_primal",
+                     "gate_dual", "gate_gap"):
             setattr(p, name, float(getattr(self, name)))
         p.restarts = 1 if self.restarts else 0
         p.fp32_recentre = 1 if self.recentre else 0
-        p.fp32_values_phase = 1 if self.fp32_values_phase else 0
+        fv = self.fp32_values_phase
+        if isinstance(fv, (bool, np.bool_)):
+            fv = int(fv)
+        if not isinstance(fv, (int, np.integer)) or fv not in (0, 1, 2):
+            raise ValueError("fp32_values_phase must be a bool or 0, 1 or 2")
+        p.fp32_values_phase = int(fv)
         return p
 
 

@@ -151,7 +151,20 @@ typedef struct fbalp_solve_params {
                                     continue in a re-centred phase with FP32
                                     matrix values (same budget, no stall rule)
                                     where the species fit it; 0: the
-                                    hand-offs continue in the FP64 phase     */
+                                    hand-offs continue in the FP64 phase;
+                                    2: continuation -- every instance runs in
+                                    the FP32-valued phase from the warm point
+                                    (no BF16 phase, no cold fallback); for
+                                    iterates an earlier call stopped at its
+                                    cap; as 1 where the species do not fit  */
+    /* the original-LP certificate gate a point accepted by the stall-floor
+       rule must also pass: absolute primal residual, absolute dual
+       violation, relative KKT gap (default 1e-5 / 1e-7 / 1e-7, the
+       reference's gate); floor_tol is relative to |x|_inf, which open 1000
+       bounds make large                                                    */
+    double gate_primal;
+    double gate_dual;
+    double gate_gap;
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);
