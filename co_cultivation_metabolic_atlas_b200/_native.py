@@ -47,7 +47,7 @@ class Options(ctypes.Structure):
                 ("step_safety", ctypes.c_double), ("warps_per_block", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("max_dynamic_smem", ctypes.c_int32),
                 ("stage_matrix", ctypes.c_int32), ("fp64_max_dynamic_smem", ctypes.c_int32),
-                ("pair_instances", ctypes.c_int32)]
+                ("pair_instances", ctypes.c_int32), ("spread_banks", ctypes.c_int32)]
 
 
 class SolveParams(ctypes.Structure):

@@ -121,6 +121,7 @@ void fbalp_default_options(fbalp_options* o) {
     o->stage_matrix = 1;
     o->fp64_max_dynamic_smem = 0;
     o->pair_instances = 1;
+    o->spread_banks = 1;
 }
 
 void fbalp_default_solve_params(fbalp_solve_params* p) {
@@ -162,6 +163,7 @@ static bool valid_options(const fbalp_options& o, std::string* err) {
     if (o.stage_matrix != 0 && o.stage_matrix != 1) return *err = "stage_matrix must be 0 or 1", false;
     if (o.fp64_max_dynamic_smem < 0) return *err = "fp64_max_dynamic_smem must be non-negative", false;
     if (o.pair_instances != 0 && o.pair_instances != 1) return *err = "pair_instances must be 0 or 1", false;
+    if (o.spread_banks != 0 && o.spread_banks != 1) return *err = "spread_banks must be 0 or 1", false;
     return true;
 }
 
@@ -243,6 +245,10 @@ int fbalp_engine_create(int32_t num_species, const int32_t* rows, const int32_t*
             fbalp::warp_schedule(sh.AT, o.warps_per_block, &sh.at_sched_off, &sh.at_sched);
             sh.Ar = fbalp::build_sell(a, sh.row_perm, col_new, sh.scaling.dr, sh.scaling.dc, sh.n, fbalp::kLongCut);
             sh.ATr = fbalp::build_sell(at, sh.col_perm, row_new, sh.scaling.dc, sh.scaling.dr, sh.m, fbalp::kLongCut);
+            if (o.spread_banks) {
+                fbalp::spread_banks(&sh.Ar, sh.n);
+                fbalp::spread_banks(&sh.ATr, sh.m);
+            }
             fbalp::warp_schedule_split(sh.Ar, o.warps_per_block, &sh.ra_sched_off, &sh.ra_sched, &sh.ra_lsched_off,
                                        &sh.ra_lsched);
             fbalp::warp_schedule_split(sh.ATr, o.warps_per_block, &sh.rat_sched_off, &sh.rat_sched,

@@ -566,7 +566,7 @@ __device__ __forceinline__ void dual_pass_unscaled(const DevSpecies* sp, const L
 // memory, scaled values; 2 (UNSCALED, FP64 only): unscaled FP32 matrix with
 // FP64 remainders staged, FP64 gather targets in shared memory.
 template <typename T, int MAXT, int MODE>
-__global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(KernelParams p) {
+__global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(const __grid_constant__ KernelParams p) {
     constexpr bool FAST = MODE == 1;
     constexpr bool UNS = MODE == 2;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -1520,7 +1520,7 @@ __device__ __forceinline__ void recentre(const DevSpecies* sp, const FastOffsets
 }
 
 template <int MAXT, bool STAGED, bool PATCHED, bool F32V>
-__global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(KernelParams p) {
+__global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(const __grid_constant__ KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ double s_red[MAXT / 32][kRed];
     __shared__ double s_tot[kRed];
@@ -1981,9 +1981,25 @@ struct PairSlot {
     int inst;  // -1: free
     int cur, ev, k, it, stall;
     bool fell_back, early;
+    bool full, chk;           // the next iteration's tests (slot_next)
+    float tau, sig, w, wp;    // the next iteration's steps and weights
     int64_t coff, roff;
     double omega, eta, cinf, r_restart, r_prev, best_err;
 };
+
+// The next iteration's tests and FP32 steps of a slot (the formulas of
+// pdhg_recentred: steps eta / omega and eta omega, Halpern weights
+// (k + 1) / (k + 2) and k / (k + 1) in FP64, rounded once), computed once
+// where the slot's state changes instead of by every thread every iteration.
+__device__ __forceinline__ void slot_next(PairSlot& st, const KernelParams& p) {
+    const int it = st.it + 1;
+    st.full = (it % p.check_every == 0) || (it >= p.max_iters);
+    st.chk = st.full || (st.early && it >= 8 && it < p.check_every && (it & (it - 1)) == 0);
+    st.tau = static_cast<float>(st.eta / st.omega);
+    st.sig = static_cast<float>(st.eta * st.omega);
+    st.w = static_cast<float>((st.k + 1.0) / (st.k + 2.0));
+    st.wp = static_cast<float>(st.k / (st.k + 1.0));
+}
 
 __device__ __forceinline__ float& comp(float2* a, int slot) { return reinterpret_cast<float*>(a)[slot]; }
 
@@ -2151,6 +2167,7 @@ __device__ __forceinline__ void dual_pass_pair(const PairOffsets& o, const OpsVi
 struct PairStage {
     Layout L;                 // the species' layout record
     const DevSpecies* sp;
+    int n, m, neq;            // its dimensions
 };
 
 // This warp's views of the staged operands, and the gather-target offsets of
@@ -2311,6 +2328,7 @@ __device__ __noinline__ void start_pair_slot(const KernelParams& p, const PairSt
     st.r_restart = INFINITY;
     st.r_prev = INFINITY;
     st.best_err = INFINITY;
+    slot_next(st, p);
     store_slot(s_st, slot, st);
 }
 
@@ -2402,11 +2420,12 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairSt
     } else if (full) {
         st.r_prev = M.r;
     }
+    if (st.inst >= 0) slot_next(st, p);
     store_slot(s_st, slot, st);
 }
 
 template <int MAXT>
-__global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
+__global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(const __grid_constant__ KernelParams p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ double s_red[MAXT / 32][kRed];
     __shared__ double s_tot[kRed];
@@ -2449,7 +2468,13 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
                     if (tid < words)
                         reinterpret_cast<int64_t*>(&s_g.L)[tid] =
                             reinterpret_cast<const int64_t*>(p.layouts + species)[tid];
-                    if (tid == 0) s_g.sp = p.species + species;
+                    if (tid == 0) {
+                        const DevSpecies* sp = p.species + species;
+                        s_g.sp = sp;
+                        s_g.n = sp->n;
+                        s_g.m = sp->m;
+                        s_g.neq = sp->neq;
+                    }
                     __syncthreads();
                     stage_species_pair(p.species + species, s_g.L, dyn_smem, warps);
                     __syncthreads();
@@ -2467,32 +2492,28 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
 
         // ---- one iteration of every busy slot ----
         bool chk[2], full[2];
-        int it[2], k[2], cur[2];
+        int cur[2];
         float tau[2], sig[2], w[2], wp[2];
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
             const bool busy = s ? a1 : a0;
             if (busy) {
-                it[s] = s_st[s].it + 1;
-                k[s] = s_st[s].k;
                 cur[s] = s_st[s].cur;
-                const double eta = s_st[s].eta, omega = s_st[s].omega;
-                full[s] = (it[s] % p.check_every == 0) || (it[s] >= p.max_iters);
-                chk[s] = full[s] || (s_st[s].early && it[s] >= 8 && it[s] < p.check_every && (it[s] & (it[s] - 1)) == 0);
-                tau[s] = static_cast<float>(eta / omega);
-                sig[s] = static_cast<float>(eta * omega);
-                w[s] = static_cast<float>((k[s] + 1.0) / (k[s] + 2.0));
-                wp[s] = static_cast<float>(k[s] / (k[s] + 1.0));
+                full[s] = s_st[s].full;
+                chk[s] = s_st[s].chk;
+                tau[s] = s_st[s].tau;
+                sig[s] = s_st[s].sig;
+                w[s] = s_st[s].w;
+                wp[s] = s_st[s].wp;
             } else {
-                it[s] = k[s] = cur[s] = 0;
+                cur[s] = 0;
                 full[s] = chk[s] = false;
                 tau[s] = sig[s] = w[s] = wp[s] = 0.0f;
             }
         }
         const float2 tau2 = make_float2(tau[0], tau[1]), sig2 = make_float2(sig[0], sig[1]);
         const float2 w2 = make_float2(w[0], w[1]), wp2 = make_float2(wp[0], wp[1]);
-        const DevSpecies* sp = s_g.sp;
-        const int n = sp->n, m = sp->m, neq = sp->neq;
+        const int n = s_g.n, m = s_g.m, neq = s_g.neq;
         const PairOffsets o = pair_offsets(s_g.L);
         OpsView A, T;
         pair_views(s_g, &A, &T);
@@ -2516,10 +2537,12 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
             if (a0) {
                 s_st[0].it += 1;
                 s_st[0].k += 1;
+                slot_next(s_st[0], p);
             }
             if (a1) {
                 s_st[1].it += 1;
                 s_st[1].k += 1;
+                slot_next(s_st[1], p);
             }
         }
         __syncthreads();
@@ -2531,27 +2554,27 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred_pair(KernelParams p) {
 }
 
 #define FBALP_INSTANTIATE_RECENTRED(MAXT)                                            \
-    template __global__ void pdhg_recentred<MAXT, true, false, false>(KernelParams);  \
-    template __global__ void pdhg_recentred<MAXT, false, false, false>(KernelParams); \
-    template __global__ void pdhg_recentred<MAXT, true, true, false>(KernelParams);   \
-    template __global__ void pdhg_recentred<MAXT, false, true, false>(KernelParams);  \
-    template __global__ void pdhg_recentred<MAXT, true, false, true>(KernelParams);   \
-    template __global__ void pdhg_recentred<MAXT, false, false, true>(KernelParams);
+    template __global__ void pdhg_recentred<MAXT, true, false, false>(const __grid_constant__ KernelParams);  \
+    template __global__ void pdhg_recentred<MAXT, false, false, false>(const __grid_constant__ KernelParams); \
+    template __global__ void pdhg_recentred<MAXT, true, true, false>(const __grid_constant__ KernelParams);   \
+    template __global__ void pdhg_recentred<MAXT, false, true, false>(const __grid_constant__ KernelParams);  \
+    template __global__ void pdhg_recentred<MAXT, true, false, true>(const __grid_constant__ KernelParams);   \
+    template __global__ void pdhg_recentred<MAXT, false, false, true>(const __grid_constant__ KernelParams);
 #define FBALP_INSTANTIATE(MAXT)                                               \
-    template __global__ void pdhg_persistent<float, MAXT, 0>(KernelParams);   \
-    template __global__ void pdhg_persistent<float, MAXT, 1>(KernelParams);   \
-    template __global__ void pdhg_persistent<double, MAXT, 0>(KernelParams);  \
-    template __global__ void pdhg_persistent<double, MAXT, 1>(KernelParams);  \
-    template __global__ void pdhg_persistent<double, MAXT, 2>(KernelParams);  \
+    template __global__ void pdhg_persistent<float, MAXT, 0>(const __grid_constant__ KernelParams);   \
+    template __global__ void pdhg_persistent<float, MAXT, 1>(const __grid_constant__ KernelParams);   \
+    template __global__ void pdhg_persistent<double, MAXT, 0>(const __grid_constant__ KernelParams);  \
+    template __global__ void pdhg_persistent<double, MAXT, 1>(const __grid_constant__ KernelParams);  \
+    template __global__ void pdhg_persistent<double, MAXT, 2>(const __grid_constant__ KernelParams);  \
     FBALP_INSTANTIATE_RECENTRED(MAXT)
 FBALP_INSTANTIATE(512)
 FBALP_INSTANTIATE(1024)
 // the re-centred kernel also at 768 threads (an 85-register budget: more
 // warps per scheduler to hide shared-memory latency)
 FBALP_INSTANTIATE_RECENTRED(768)
-template __global__ void pdhg_recentred_pair<512>(KernelParams);
-template __global__ void pdhg_recentred_pair<768>(KernelParams);
-template __global__ void pdhg_recentred_pair<1024>(KernelParams);
+template __global__ void pdhg_recentred_pair<512>(const __grid_constant__ KernelParams);
+template __global__ void pdhg_recentred_pair<768>(const __grid_constant__ KernelParams);
+template __global__ void pdhg_recentred_pair<1024>(const __grid_constant__ KernelParams);
 #undef FBALP_INSTANTIATE
 #undef FBALP_INSTANTIATE_RECENTRED
 

@@ -214,6 +214,139 @@ Sell build_sell(const Csr& a, const std::vector<int32_t>& row_order,
     return s;
 }
 
+namespace {
+
+// Shared-memory wavefronts of one step k of a slice: the lanes gather
+// target[lane] (an element index).  Paired kernel: float2 targets, 16
+// lanes (half a warp) per 128-byte wavefront, 16 bank pairs; single
+// kernel: float targets, 32 lanes, 32 banks.  Per group the count is the
+// largest number of DISTINCT targets sharing a bank (equal targets are one
+// broadcast).
+int step_wavefronts(const int32_t* t) {
+    // per bank, the distinct targets seen so far (a target is compared only
+    // with the targets of its own bank)
+    int total = 0;
+    int32_t seen[32][32];
+    int cnt[32];
+    for (int g = 0; g < 32; g += 16) {  // float2: two half-warps, 16 bank pairs
+        int worst = 0;
+        for (int c = 0; c < 16; ++c) cnt[c] = 0;
+        for (int q = g; q < g + 16; ++q) {
+            const int c = t[q] & 15;
+            bool dup = false;
+            for (int r = 0; r < cnt[c] && !dup; ++r) dup = seen[c][r] == t[q];
+            if (!dup) {
+                seen[c][cnt[c]++] = t[q];
+                worst = std::max(worst, cnt[c]);
+            }
+        }
+        total += worst;
+    }
+    int worst = 0;
+    for (int c = 0; c < 32; ++c) cnt[c] = 0;
+    for (int q = 0; q < 32; ++q) {  // float: one warp, 32 banks
+        const int c = t[q] & 31;
+        bool dup = false;
+        for (int r = 0; r < cnt[c] && !dup; ++r) dup = seen[c][r] == t[q];
+        if (!dup) {
+            seen[c][cnt[c]++] = t[q];
+            worst = std::max(worst, cnt[c]);
+        }
+    }
+    return total + worst;
+}
+
+}  // namespace
+
+void spread_banks(Sell* s, int32_t pad_index, int rounds) {
+    std::vector<int32_t> grid;   // [k][lane] targets of one slice
+    std::vector<double> gval;
+    std::vector<int> cost;
+    for (int32_t sl = 0; sl < s->nslices; ++sl) {
+        const int32_t L = s->length[sl];
+        if (L < 2) continue;
+        const int32_t base = s->off[sl];
+        // greedy: step by step, each lane with entries left places the one
+        // whose bank is least used by the distinct targets placed so far
+        std::vector<std::vector<std::pair<int32_t, double>>> left(32);
+        for (int lane = 0; lane < 32; ++lane)
+            for (int32_t k = 0; k < L; ++k) {
+                const int32_t e = base + k * 32 + lane;
+                if (s->idx[e] != pad_index) left[lane].emplace_back(s->idx[e], s->val[e]);
+            }
+        grid.assign(static_cast<size_t>(L) * 32, pad_index);
+        gval.assign(static_cast<size_t>(L) * 32, 0.0);
+        for (int32_t k = 0; k < L; ++k) {
+            int32_t* t = &grid[static_cast<size_t>(k) * 32];
+            for (int g = 0; g < 32; g += 16) {
+                int cnt[16] = {0};
+                for (int lane = g; lane < g + 16; ++lane) {
+                    auto& cand = left[lane];
+                    if (cand.empty()) continue;
+                    size_t best = 0;
+                    int best_cost = 1 << 30;
+                    for (size_t c = 0; c < cand.size(); ++c) {
+                        bool dup = false;
+                        for (int r = g; r < lane && !dup; ++r) dup = t[r] == cand[c].first;
+                        const int cc = dup ? 0 : cnt[cand[c].first & 15] + 1;
+                        if (cc < best_cost) {
+                            best_cost = cc;
+                            best = c;
+                        }
+                    }
+                    bool dup = false;
+                    for (int r = g; r < lane && !dup; ++r) dup = t[r] == cand[best].first;
+                    if (!dup) ++cnt[cand[best].first & 15];
+                    t[lane] = cand[best].first;
+                    gval[static_cast<size_t>(k) * 32 + lane] = cand[best].second;
+                    cand.erase(cand.begin() + static_cast<std::ptrdiff_t>(best));
+                }
+            }
+        }
+        // local search: swap two positions of one lane (an entry with a
+        // hole included) while that lowers the two steps' wavefronts
+        cost.assign(L, 0);
+        for (int32_t k = 0; k < L; ++k) cost[k] = step_wavefronts(&grid[static_cast<size_t>(k) * 32]);
+        for (int round = 0; round < rounds; ++round) {
+            bool improved = false;
+            for (int lane = 0; lane < 32; ++lane) {
+                if ((s->lmask[sl] >> lane) & 1u) continue;
+                for (int32_t a = 0; a < L; ++a)
+                    for (int32_t b = a + 1; b < L; ++b) {
+                        int32_t& ta = grid[static_cast<size_t>(a) * 32 + lane];
+                        int32_t& tb = grid[static_cast<size_t>(b) * 32 + lane];
+                        if (ta == tb) continue;
+                        std::swap(ta, tb);
+                        const int ca = step_wavefronts(&grid[static_cast<size_t>(a) * 32]);
+                        const int cb = step_wavefronts(&grid[static_cast<size_t>(b) * 32]);
+                        if (ca + cb < cost[a] + cost[b]) {
+                            cost[a] = ca;
+                            cost[b] = cb;
+                            std::swap(gval[static_cast<size_t>(a) * 32 + lane], gval[static_cast<size_t>(b) * 32 + lane]);
+                            improved = true;
+                        } else {
+                            std::swap(ta, tb);
+                        }
+                    }
+            }
+            if (!improved) break;
+        }
+        for (int32_t k = 0; k < L; ++k)
+            for (int lane = 0; lane < 32; ++lane) {
+                const int32_t e = base + k * 32 + lane;
+                s->idx[e] = grid[static_cast<size_t>(k) * 32 + lane];
+                s->val[e] = gval[static_cast<size_t>(k) * 32 + lane];
+            }
+    }
+}
+
+int64_t gather_wavefronts(const Sell& s) {
+    int64_t total = 0;
+    for (int32_t sl = 0; sl < s.nslices; ++sl)
+        for (int32_t k = 0; k < s.length[sl]; ++k) total += step_wavefronts(&s.idx[s.off[sl] + k * 32]);
+    return total;
+}
+
 void warp_schedule(const Sell& s, int warps, std::vector<int32_t>* sched_off,
                    std::vector<int32_t>* sched) {
     std::vector<int32_t> order(s.nslices);

@@ -54,6 +54,19 @@ Sell build_sell(const Csr& a, const std::vector<int32_t>& row_order,
                 const std::vector<int32_t>& col_rename, const std::vector<double>& row_scale,
                 const std::vector<double>& col_scale, int32_t pad_index, int32_t long_cut = 0);
 
+// Reorder the entries inside each row of a slice (padding slots included:
+// a row's entries may sit at any of the slice's steps) so that the lanes
+// of one step gather from distinct shared-memory banks: a greedy placement
+// step by step, then `rounds` passes of pairwise swaps within a lane.  The
+// cost of a step is its gather wavefronts in the paired kernel (float2
+// targets, per half-warp, 16 bank pairs) plus in the single-instance kernel
+// (float targets, per warp, 32 banks).  Row sums are unchanged; only the
+// FP32 accumulation order moves.
+void spread_banks(Sell* s, int32_t pad_index, int rounds = 3);
+
+// The same cost summed over every step of every slice (both kernels).
+int64_t gather_wavefronts(const Sell& s);
+
 // Rows longer than this many entries are long lines (walked by a whole warp
 // in the re-centred kernels): one warp step covers 32 of their entries.
 constexpr int32_t kLongCut = 32;

@@ -105,6 +105,7 @@ class EngineOptions:
     stage_matrix: bool = True
     fp64_max_dynamic_smem: int = 0
     pair_instances: bool = True        # two instances per CTA in the re-centred phase where possible
+    spread_banks: bool = True          # order row entries for conflict-free shared-memory gathers
 
     def native(self) -> N.Options:
         o = N.default_options()
@@ -117,6 +118,7 @@ class EngineOptions:
         o.stage_matrix = 1 if self.stage_matrix else 0
         o.fp64_max_dynamic_smem = int(self.fp64_max_dynamic_smem)
         o.pair_instances = 1 if self.pair_instances else 0
+        o.spread_banks = 1 if self.spread_banks else 0
         return o
 
 

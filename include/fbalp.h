@@ -101,6 +101,12 @@ typedef struct fbalp_options {
                                   1, no entries are patched and the batch has
                                   at least two instances per CTA; 0: one
                                   instance per CTA.  Same results.          */
+    int32_t spread_banks;      /* 1 (default): the re-centred kernels' matrix
+                                  entries are ordered inside each row so that
+                                  one step's gathers hit distinct shared-memory
+                                  banks (fewer conflicts; only the FP32
+                                  accumulation order changes); 0: column
+                                  order                                     */
 } fbalp_options;
 
 /* Solve parameters.  Replaces `iterations` / `check_interval` of
