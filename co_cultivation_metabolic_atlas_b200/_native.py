@@ -61,7 +61,8 @@ class SolveParams(ctypes.Structure):
                 ("floor_tol", ctypes.c_double), ("fp32_passthrough_tol", ctypes.c_double),
                 ("fallback_iterations", ctypes.c_int32), ("fp32_recentre", ctypes.c_int32),
                 ("fp32_values_phase", ctypes.c_int32), ("gate_primal", ctypes.c_double),
-                ("gate_dual", ctypes.c_double), ("gate_gap", ctypes.c_double)]
+                ("gate_dual", ctypes.c_double), ("gate_gap", ctypes.c_double),
+                ("primal_weight_smoothing", ctypes.c_double)]
 
 
 KERNEL_NAMES = {-1: None, 0: "pdhg_persistent<float>", 1: "pdhg_persistent<double>", 2: "pdhg_recentred<staged>",

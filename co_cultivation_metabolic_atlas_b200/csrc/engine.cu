@@ -148,6 +148,7 @@ void fbalp_default_solve_params(fbalp_solve_params* p) {
     p->gate_primal = 1e-5;
     p->gate_dual = 1e-7;
     p->gate_gap = 1e-7;
+    p->primal_weight_smoothing = 0.5;
 }
 
 const char* fbalp_last_error(void) { return g_last_error.c_str(); }
@@ -783,6 +784,7 @@ extern "C" int fbalp_engine_solve(fbalp_engine* e, const double* warm_x, const d
         p.gate_p = q.gate_primal;
         p.gate_d = q.gate_dual;
         p.gate_g = q.gate_gap;
+        p.omega_smoothing = q.primal_weight_smoothing;
         bool patched = false;
         if (e->patch_values)
             for (int32_t sp_id : e->h_species) patched = patched || e->dev_species_host[sp_id].npatch > 0;

@@ -99,6 +99,8 @@ inline bool valid_params(const fbalp_solve_params& q, std::string* err) {
     if (!(q.floor_tol >= 0.0) || !std::isfinite(q.floor_tol)) return *err = "floor_tol must be finite and non-negative", false;
     for (double t : {q.gate_primal, q.gate_dual, q.gate_gap})
         if (!(t >= 0.0) || !std::isfinite(t)) return *err = "certificate gates must be finite and non-negative", false;
+    if (!(q.primal_weight_smoothing >= 0.0 && q.primal_weight_smoothing <= 1.0))
+        return *err = "primal_weight_smoothing must be in [0, 1]", false;
     if (q.fallback_iterations < 0) return *err = "fallback_iterations must be non-negative", false;
     if (q.fp32_recentre != 0 && q.fp32_recentre != 1) return *err = "fp32_recentre must be 0 or 1", false;
     if (!(q.fp32_passthrough_tol >= 0.0) || !std::isfinite(q.fp32_passthrough_tol))

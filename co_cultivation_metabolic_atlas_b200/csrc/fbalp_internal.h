@@ -20,11 +20,10 @@ constexpr int kStatusNotRun = 4;
 constexpr int kStatusHandoff = 5;
 
 // Restart rule of the Halpern scheme (Lu & Yang; cuPDLPx) and the PDLP
-// primal-weight smoothing.
+// primal-weight smoothing (a solve parameter, primal_weight_smoothing).
 constexpr double kBetaSufficient = 0.2;
 constexpr double kBetaNecessary = 0.8;
 constexpr double kBetaArtificial = 0.36;
-constexpr double kOmegaSmoothing = 0.5;
 // the FP32 phase only hands off on a stall once its error is below this
 constexpr double kStallFloor = 1.0;
 

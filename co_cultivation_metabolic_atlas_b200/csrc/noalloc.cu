@@ -201,6 +201,7 @@ extern "C" int fbalp_engine_solve_noalloc(fbalp_engine* e, int64_t count, const 
         p.gate_p = q.gate_primal;
         p.gate_d = q.gate_dual;
         p.gate_g = q.gate_gap;
+        p.omega_smoothing = q.primal_weight_smoothing;
         p.passthrough_tol = 0.0;
         p.fallback_iters = q.fallback_iterations;
 

@@ -199,7 +199,7 @@ __device__ Metrics evaluate(const double* s_tot, double omega, double tol_p, dou
     M.rgap = fabs(M.pobj - M.dobj) / (1.0 + fabs(M.pobj) + fabs(M.dobj));
     M.xinf = s_tot[13];
     M.cinf = s_tot[14];
-    M.r = sqrt(omega * s_tot[5] + s_tot[6] / omega);
+    M.r = sqrt(__fma_rn(omega, s_tot[5], s_tot[6] / omega));  // explicit: both re-centred kernels round alike
     M.nan = s_tot[15] > 0.0 || !isfinite(M.pobj) || !isfinite(M.dobj) || !isfinite(M.kgap) ||
             !isfinite(M.primal);
     M.conv = !M.nan && M.primal <= tol_p * (1.0 + M.xinf) && M.dual <= tol_d * (1.0 + M.cinf) &&
@@ -867,7 +867,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_persistent(const __grid_constant
                                k >= kBetaArtificial * it)) {
                 const double nx = sqrt(s_tot[7]), ny = sqrt(s_tot[8]);
                 if (nx > 1e-10 && ny > 1e-10)
-                    omega = exp(kOmegaSmoothing * log(ny / nx) + (1.0 - kOmegaSmoothing) * log(omega));
+                    omega = exp(__fma_rn(p.omega_smoothing, log(ny / nx), (1.0 - p.omega_smoothing) * log(omega)));
                 for (int j = tid; j < n; j += nthreads) {
                     const T xv = A.xs[j];
                     A.x[j] = xv;
@@ -1188,8 +1188,8 @@ __device__ __forceinline__ void primal_update(const FastOffsets& o, int j, float
     if (check) {
         cx[j] = bx[j] + static_cast<double>(xn);
         const double d = static_cast<double>(xn) - static_cast<double>(xo);
-        pdx2 += d * d;
-        pdxa2 += static_cast<double>(xn) * static_cast<double>(xn);
+        pdx2 = __fma_rn(d, d, pdx2);
+        pdxa2 = __fma_rn(static_cast<double>(xn), static_cast<double>(xn), pdxa2);
     }
 }
 
@@ -1205,8 +1205,8 @@ __device__ __forceinline__ void dual_update(const FastOffsets& o, int i, int neq
     if (check) {
         cy[i] = by[i] + static_cast<double>(yn);
         const double d = static_cast<double>(yn) - static_cast<double>(yo);
-        pdy2 += d * d;
-        pdya2 += static_cast<double>(yn) * static_cast<double>(yn);
+        pdy2 = __fma_rn(d, d, pdy2);
+        pdya2 = __fma_rn(static_cast<double>(yn), static_cast<double>(yn), pdya2);
     }
 }
 
@@ -1401,12 +1401,12 @@ __device__ __forceinline__ void kkt_column(const DevSpecies* sp, int j, double g
     }
     const double rs = cj - g;
     dcand[j] = static_cast<float>(rs);
-    v[0] += cj * xsc;
+    v[0] = __fma_rn(cj, xsc, v[0]);
     if (rs > 0.0) {
-        if (isfinite(lj)) v[2] += rs * lj;
+        if (isfinite(lj)) v[2] = __fma_rn(rs, lj, v[2]);
         else v[11] = fmax(v[11], rs * __ldg(sp->inv_dc + j));
     } else if (rs < 0.0) {
-        if (isfinite(uj)) v[2] += rs * uj;
+        if (isfinite(uj)) v[2] = __fma_rn(rs, uj, v[2]);
         else v[11] = fmax(v[11], -rs * __ldg(sp->inv_dc + j));
     }
     const double tg = (rs >= 0.0) ? lj : uj;
@@ -1430,7 +1430,7 @@ __device__ __forceinline__ void kkt_row(const DevSpecies* sp, int i, double h, c
         v[4] += fabs(ysc * rr);
         v[11] = fmax(v[11], ysc * __ldg(sp->dr + i));
     }
-    v[1] += bi * ysc;
+    v[1] = __fma_rn(bi, ysc, v[1]);
     if (isnan(h) || isnan(ysc)) v[15] = 1.0;
 }
 
@@ -1805,7 +1805,7 @@ __global__ void __launch_bounds__(MAXT, 1) pdhg_recentred(const __grid_constant_
                                k >= kBetaArtificial * it)) {
                 const double nx = sqrt(s_tot[7]), ny = sqrt(s_tot[8]);
                 if (nx > 1e-10 && ny > 1e-10)
-                    omega = exp(kOmegaSmoothing * log(ny / nx) + (1.0 - kOmegaSmoothing) * log(omega));
+                    omega = exp(__fma_rn(p.omega_smoothing, log(ny / nx), (1.0 - p.omega_smoothing) * log(omega)));
                 cur ^= 1;  // the candidate becomes the base
                 recentre(sp, o, PX(cur), PY(cur), dcand, rcand, ls, us);
                 k = 0;
@@ -2087,14 +2087,14 @@ __device__ __forceinline__ void primal_update_pair(const PairOffsets& o, int j, 
         if (c0) {
             cx0[j] = bx0[j] + static_cast<double>(xn0);
             const double d = static_cast<double>(xn0) - static_cast<double>(xo0);
-            pd[0] += d * d;
-            pd[1] += static_cast<double>(xn0) * static_cast<double>(xn0);
+            pd[0] = __fma_rn(d, d, pd[0]);
+            pd[1] = __fma_rn(static_cast<double>(xn0), static_cast<double>(xn0), pd[1]);
         }
         if (c1) {
             cx1[j] = bx1[j] + static_cast<double>(xn1);
             const double d = static_cast<double>(xn1) - static_cast<double>(xo1);
-            pd[4] += d * d;
-            pd[5] += static_cast<double>(xn1) * static_cast<double>(xn1);
+            pd[4] = __fma_rn(d, d, pd[4]);
+            pd[5] = __fma_rn(static_cast<double>(xn1), static_cast<double>(xn1), pd[5]);
         }
     }
 }
@@ -2118,14 +2118,14 @@ __device__ __forceinline__ void dual_update_pair(const PairOffsets& o, int i, in
         if (c0) {
             cy0[i] = by0[i] + static_cast<double>(yn0);
             const double d = static_cast<double>(yn0) - static_cast<double>(yo.x);
-            pd[2] += d * d;
-            pd[3] += static_cast<double>(yn0) * static_cast<double>(yn0);
+            pd[2] = __fma_rn(d, d, pd[2]);
+            pd[3] = __fma_rn(static_cast<double>(yn0), static_cast<double>(yn0), pd[3]);
         }
         if (c1) {
             cy1[i] = by1[i] + static_cast<double>(yn1);
             const double d = static_cast<double>(yn1) - static_cast<double>(yo.y);
-            pd[6] += d * d;
-            pd[7] += static_cast<double>(yn1) * static_cast<double>(yn1);
+            pd[6] = __fma_rn(d, d, pd[6]);
+            pd[7] = __fma_rn(static_cast<double>(yn1), static_cast<double>(yn1), pd[7]);
         }
     }
 }
@@ -2434,7 +2434,7 @@ __device__ __noinline__ void check_pair_slot(const KernelParams& p, const PairSt
                (M.r <= kBetaSufficient * st.r_restart || (M.r <= kBetaNecessary * st.r_restart && M.r > st.r_prev) ||
                 st.k >= kBetaArtificial * st.it)) {
         if (nx > 1e-10 && ny > 1e-10)
-            st.omega = exp(kOmegaSmoothing * log(ny / nx) + (1.0 - kOmegaSmoothing) * log(st.omega));
+            st.omega = exp(__fma_rn(p.omega_smoothing, log(ny / nx), (1.0 - p.omega_smoothing) * log(st.omega)));
         st.cur ^= 1;  // the candidate becomes the base
         recentre_pair(sp, o, slot, b.X(st.cur), b.Y(st.cur), b.dcand, b.rcand, b.ls, b.us);
         st.k = 0;

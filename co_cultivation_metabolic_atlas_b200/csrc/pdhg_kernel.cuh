@@ -173,6 +173,7 @@ struct KernelParams {
     double floor_tol;             // FP64 phase: tolerance accepted after a stall
     double gate_p, gate_d, gate_g;  // ... where the point also passes the
                                     // original-LP certificate gate
+    double omega_smoothing;       // primal-weight update at a restart
     double passthrough_tol;       // FP32 phase: warm starts with error <= this
                                   // skip the phase unchanged (0 = never)
     int32_t fallback_iters;       // warm starts not converged after this many

@@ -66,6 +66,10 @@ class SolveConfig:
     gate_primal: float = 1e-5
     gate_dual: float = 1e-7
     gate_gap: float = 1e-7
+    # primal-weight update at a restart: log w <- theta log(|dy|/|dx|) +
+    # (1 - theta) log w (0.3 measured: 5 % fewer cold iterations, but 25 %
+    # more on the warm-started community steps on the GPU)
+    primal_weight_smoothing: float = 0.5
 
     def native(self) -> N.SolveParams:
         p = N.default_solve_params()
@@ -81,7 +85,7 @@ class SolveConfig:
             setattr(p, name, int(value))
         for name in ("tol_primal", "tol_dual", "tol_gap", "fp32_tol_primal", "fp32_tol_dual",
                      "fp32_tol_gap", "reflection", "floor_tol", "fp32_passthrough_tol", "gate_primal",
-                     "gate_dual", "gate_gap"):
+                     "gate_dual", "gate_gap", "primal_weight_smoothing"):
             setattr(p, name, float(getattr(self, name)))
         p.restarts = 1 if self.restarts else 0
         p.fp32_recentre = 1 if self.recentre else 0

@@ -171,6 +171,10 @@ typedef struct fbalp_solve_params {
     double gate_primal;
     double gate_dual;
     double gate_gap;
+    double primal_weight_smoothing; /* theta of the primal-weight update at a
+                                    restart, log w <- theta log(|dy| / |dx|)
+                                    + (1 - theta) log w, in [0, 1] (default
+                                    0.5, PDLP's; 0 keeps the weight fixed)   */
 } fbalp_solve_params;
 
 void fbalp_default_options(fbalp_options* options);

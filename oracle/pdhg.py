@@ -35,8 +35,9 @@ the fixed-point residual ``r = sqrt(omega |xn-x|^2 + |yn-y|^2/omega)``::
             or k >= 0.36 * it
 
 On restart the primal weight becomes
-``exp(0.5 log(|yn-ya|/|xn-xa|) + 0.5 log omega)`` (when both distances exceed
-1e-10) and ``x = xa = xn``, ``y = ya = yn``, ``k = 0``.
+``exp(theta log(|yn-ya|/|xn-xa|) + (1 - theta) log omega)`` with ``theta =
+OMEGA_SMOOTHING`` (0.5, the engine's default ``primal_weight_smoothing``;
+when both distances exceed 1e-10) and ``x = xa = xn``, ``y = ya = yn``, ``k = 0``.
 """
 
 from __future__ import annotations

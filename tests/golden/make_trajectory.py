@@ -35,9 +35,25 @@ SEED = 11          # environments (disjoint from the bench and training seeds)
 DT = 0.05
 EVERY = 10
 HIGHS_STEPS = (0, 120, 480, 959)
+# the fixture was generated with the primal-weight smoothing 0.5 (the
+# engine's default); the rollout pins it so that re-running the first steps
+# reproduces the fixture bit for bit whatever the default becomes
+FIXTURE_OMEGA_SMOOTHING = 0.5
 
 
 def rollout(env, envs, steps):
+    """``_rollout`` with the fixture's primal-weight smoothing (restored
+    afterwards)."""
+    from oracle import pdhg
+    old = pdhg.OMEGA_SMOOTHING
+    pdhg.OMEGA_SMOOTHING = FIXTURE_OMEGA_SMOOTHING
+    try:
+        return _rollout(env, envs, steps)
+    finally:
+        pdhg.OMEGA_SMOOTHING = old
+
+
+def _rollout(env, envs, steps):
     from co_cultivation_metabolic_atlas_b200 import synthetic as syn
     from oracle import dfba, pdhg
     models = syn.community_models(seed=0)
