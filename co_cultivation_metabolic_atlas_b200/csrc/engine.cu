@@ -532,12 +532,44 @@ int fbalp_engine_layout(const fbalp_engine* e, int64_t* total_cols, int64_t* tot
 
 namespace {
 
+// Static shared memory the dynamic allocation must leave room for: the
+// largest actual static size (runtime attributes) among the kernels of a
+// family at this engine's block size -- 0 the persistent kernels, 1 the
+// re-centred ones, 2 the paired one -- and never below the reduction
+// buffers' size.
+int64_t static_smem_of(fbalp_engine* e, int family) {
+    if (e->static_smem[family] >= 0) return e->static_smem[family];
+    const int threads = e->opt.warps_per_block * 32;
+    int64_t s = static_cast<int64_t>(sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64);
+    std::vector<const void*> ks;
+    if (family == 0) {
+        for (int f = 0; f < 2; ++f)
+            for (int fast = 0; fast < 2; ++fast) ks.push_back(fbalp::kernel_symbol(f != 0, threads, fast != 0));
+    } else if (family == 1) {
+        for (int st = 0; st < 2; ++st)
+            for (int pa = 0; pa < 2; ++pa)
+                for (int fv = 0; fv < 2; ++fv)
+                    if (!(pa && fv)) ks.push_back(fbalp::recentred_symbol(threads, st != 0, pa != 0, fv != 0));
+    } else {
+        ks.push_back(fbalp::pair_symbol(threads));
+    }
+    for (const void* k : ks) {
+        cudaFuncAttributes fa{};
+        if (k && cudaFuncGetAttributes(&fa, k) == cudaSuccess)
+            s = std::max<int64_t>(s, static_cast<int64_t>(fa.sharedSizeBytes));
+        else
+            cudaGetLastError();
+    }
+    e->static_smem[family] = s;
+    return s;
+}
+
 // Re-centred FP32 layout of the bound batch: 1 when every species fits with
 // its matrix staged in shared memory, 2 when every species' vectors fit
 // with the matrix streamed from L2 (one variant per launch), 0 otherwise.
 int recentred_mode(fbalp_engine* e) {
     const int threads = e->opt.warps_per_block * 32;
-    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    const size_t static_smem = static_cast<size_t>(static_smem_of(e, 1));
     int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
                       ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
     if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
@@ -566,7 +598,7 @@ bool pair_mode(fbalp_engine* e, double reflection, bool patched) {
     if (!e->opt.pair_instances || reflection != 1.0 || patched) return false;
     if (e->count < 2 * static_cast<int64_t>(e->sm_count)) return false;
     const int threads = e->opt.warps_per_block * 32;
-    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    const size_t static_smem = static_cast<size_t>(static_smem_of(e, 2));
     int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
                       ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
     if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
@@ -588,7 +620,7 @@ bool pair_mode(fbalp_engine* e, double reflection, bool patched) {
 // when only the vectors fit (matrix streamed), 0 when neither.
 int f32_mode(fbalp_engine* e) {
     const int threads = e->opt.warps_per_block * 32;
-    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    const size_t static_smem = static_cast<size_t>(static_smem_of(e, 1));
     int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
                       ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
     if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);
@@ -622,7 +654,8 @@ void run_phase(fbalp_engine* e, bool fp64, fbalp::KernelParams p, int recentred 
     const bool f32v = recentred >= 4;
     const int esz = fp64 ? static_cast<int>(sizeof(double)) : static_cast<int>(sizeof(float));
     const int threads = e->opt.warps_per_block * 32;
-    const size_t static_smem = sizeof(double) * (threads / 32 * fbalp::kRed + fbalp::kRed) + 64;
+    const size_t static_smem = static_cast<size_t>(
+        static_smem_of(e, recentred == 3 ? 2 : recentred ? 1 : 0));
     int64_t cap = e->smem_optin > static_cast<int>(static_smem) + 1024
                       ? e->smem_optin - static_cast<int64_t>(static_smem) - 1024 : 0;
     if (e->opt.max_dynamic_smem > 0) cap = std::min<int64_t>(cap, e->opt.max_dynamic_smem);

@@ -148,6 +148,9 @@ struct fbalp_engine {
     std::vector<fbalp::Layout> layouts32, layouts64;
     // per phase of the last solve (first, FP64, FP32-valued middle phase)
     int last_grid[3] = {0, 0, 0};
+    // largest static shared memory of each kernel family at this engine's
+    // block size (persistent, re-centred, paired; -1 until queried)
+    int64_t static_smem[3] = {-1, -1, -1};
     int last_kind[3] = {-1, -1, -1};  // kernel kind (the layout_dev index)
     int64_t last_smem[3] = {0, 0, 0};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // phase start/stop: fp32, fp64
