@@ -49,3 +49,32 @@ def test_package_lp_equals_oracle_restatement_and_is_unique():
     np.testing.assert_allclose(r_ds.x[:k], v[:k], atol=1e-6)
     np.testing.assert_allclose(r_ipm.x[:k], v[:k], atol=1e-6)
     assert v[m.biomass] == np.float64(l2[0, m.biomass]) or abs(v[m.biomass] - l2[0, m.biomass]) <= 1e-7
+
+
+def test_parsimonious_trajectory_fixture_replays_its_first_step(golden_dir):
+    """The committed HiGHS trajectory fixture is what its generator makes:
+    environment 0's first step (stage 1 by HiGHS, the parsimonious stage 2
+    by HiGHS, the oracle's Euler updates) reproduces the fixture's state at
+    step 1 and the stored stage-1 growth.  Environments evolve
+    independently, so one environment suffices."""
+    import importlib.util
+    g = np.load(golden_dir / "trajectory_parsimonious.npz")
+    spec = importlib.util.spec_from_file_location("make_parsimonious_trajectory",
+                                                  golden_dir / "make_parsimonious_trajectory.py")
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    models = mk._models()
+    medium = g["medium"][0][:1].copy()
+    biomass = g["biomass"][0][:1].copy()
+    med0, bio0 = syn.initial_environments(int(g["envs"]), seed=0)
+    np.testing.assert_array_equal(medium, med0[:1])
+    np.testing.assert_array_equal(biomass, bio0[:1])
+    out = [mk._solve((s, dfba.uptake_lower_bounds(m, medium, biomass, mk.DT)[0])) for s, m in enumerate(models)]
+    growth = np.array([o[0] for o in out])
+    fluxes = [o[1][None, :] for o in out]
+    mu = np.stack([f[:, m.biomass] for f, m in zip(fluxes, models)], axis=1)
+    b1 = dfba.update_biomass(biomass, mu, mk.DT)
+    m1 = dfba.update_medium(medium, models, fluxes, biomass, mk.DT)
+    np.testing.assert_allclose(growth, g["growth_stage1"][0][0], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(b1[0], g["biomass"][1][0], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(m1[0], g["medium"][1][0], rtol=1e-7, atol=1e-10)
