@@ -111,8 +111,34 @@ class B200LPBackend:
         self._keys: list[str] = []
         self._matrices = []
         self._engine: LPEngine | None = None
+        self._staging: dict = {}
         self.last_certified: dict = {}
         self.history: list[dict] = []
+
+    def _pinned(self, name, size, dtype):
+        """A pinned host buffer kept across calls (grown when a batch needs
+        more): pinning a fresh copy of every batch array each call costs
+        more than the copy itself."""
+        buf = self._staging.get(name)
+        if buf is None or buf.dtype != dtype or buf.numel() < size:
+            buf = torch.empty(max(1, int(size * 1.25)), dtype=dtype, pin_memory=True)
+            self._staging[name] = buf
+        return buf[:size]
+
+    def _to_device(self, name, a):
+        """Host array -> device through the named pinned staging buffer.  The
+        copy is asynchronous; the buffer is not rewritten before the solve's
+        results are read back (a synchronisation) in the same call."""
+        a = np.asarray(a, dtype=np.float64)
+        buf = self._pinned(name, a.size, torch.float64)
+        buf.numpy()[:] = a.ravel()
+        return buf.to(self.device, non_blocking=True)
+
+    def _to_host(self, name, t):
+        """Device tensor -> NumPy through the named pinned staging buffer."""
+        buf = self._pinned(name, t.numel(), t.dtype)
+        buf.copy_(t.reshape(-1))
+        return buf.numpy().reshape(tuple(t.shape))
 
     # ------------------------------------------------------------------
     def reset(self, environment_ids=None):
@@ -203,17 +229,25 @@ class B200LPBackend:
             warm_x, warm_y, warm_o = wx, wy, wo
         elif self.mode == 'mlp':
             warm_x, warm_y, warm_o = self.model.propose(ids, problems, species, eng, keys=keys)
-        dev = self.device
-        t = lambda a: torch.as_tensor(a, dtype=torch.float64).pin_memory().to(dev, non_blocking=True)
-        eng.set_instances(species, t(lower), t(upper), t(cost), t(rhs) if tr else None)
-        res = eng.solve(warm_x=None if warm_x is None else t(warm_x),
-                        warm_y=None if warm_y is None or not tr else t(warm_y),
-                        warm_omega=None if warm_o is None else t(warm_o), config=self.config)
-        status = res.status.cpu().numpy()
-        iters = res.iterations.cpu().numpy()
-        metrics = res.metrics.cpu().numpy()
-        x = res.x.cpu().numpy()
-        y = res.y.cpu().numpy()
+        d = self._to_device
+        if warm_x is not None and isinstance(warm_x, torch.Tensor):
+            wxd, wyd, wod = warm_x, warm_y, warm_o    # proposed on the device (learned warm start)
+        else:
+            wxd = None if warm_x is None else d('warm_x', warm_x)
+            wyd = None if warm_y is None or not tr else d('warm_y', warm_y)
+            wod = None if warm_o is None else d('warm_omega', warm_o)
+        eng.set_instances(species, d('lower', lower), d('upper', upper), d('cost', cost),
+                          d('rhs', rhs) if tr else None)
+        res = eng.solve(warm_x=wxd, warm_y=wyd if tr else None, warm_omega=wod, config=self.config)
+        status = self._to_host('status', res.status).copy()
+        iters = self._to_host('iterations', res.iterations).copy()
+        metrics = self._to_host('metrics', res.metrics).copy()
+        # x and y stay in the staging buffers: every row copies its slice
+        # before the next call can rewrite them
+        x = self._to_host('x', res.x[:tc])
+        y = self._to_host('y', res.y[:tr]) if tr else np.zeros(0)
+        # (the retry pass is rare: plain transfers)
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64)).to(self.device)  # noqa: E731
         retried = self._retry(eng, res, species, co, ro, lower, upper, cost, rhs, tr, status, iters, metrics, x, y, t)
         solved = time.perf_counter()
         rows = []
