@@ -43,12 +43,21 @@ def normalize(objective, kwargs, _cache=None):
 
     ``_cache`` (a dict owned by one ``normalize_batch`` call) maps the
     identities of the request's ``A_eq`` / ``A_ub`` objects to their
-    canonical stacked matrix, so requests that pass the same matrix objects
-    (every environment of a species in a dFBA rollout) canonicalise it once.
+    canonical stacked matrix, and of its objective object to its validated
+    copy, so requests that pass the same objects (every environment of a
+    species in a dFBA rollout) canonicalise them once.
     """
-    c = np.asarray(objective, dtype=np.float64)
-    if c.ndim != 1 or not len(c) or not np.isfinite(c).all():
-        raise ValueError('A finite one-dimensional objective is required')
+    c_hit = None if _cache is None else _cache.get(('c', id(objective)))
+    if c_hit is not None and c_hit[0] is objective:
+        c = c_hit[1]
+    else:
+        c = np.asarray(objective, dtype=np.float64)
+        if c.ndim != 1 or not len(c) or not np.isfinite(c).all():
+            raise ValueError('A finite one-dimensional objective is required')
+        c = c.copy()
+        if _cache is not None:
+            # the entry keeps the object alive, so its id stays its own
+            _cache[('c', id(objective))] = (objective, c)
     n = len(c)
     integrality = kwargs.get('integrality')
     if integrality is not None and np.any(np.asarray(integrality)):
@@ -92,13 +101,14 @@ def normalize(objective, kwargs, _cache=None):
     lower, upper = split_bounds(kwargs.get('bounds'), n)
     if np.isnan(lower).any() or np.isnan(upper).any() or (lower > upper).any():
         raise ValueError('Invalid variable bounds')
-    return a, np.concatenate(rhs), lower, upper, c.copy(), neq
+    return a, np.concatenate(rhs), lower, upper, c, neq
 
 
 def normalize_batch(requests):
     """``normalize`` of every request of one batch, canonicalising each
-    distinct matrix object once.  The returned problems of requests that
-    share matrix objects share one canonical matrix (treat it as read-only)."""
+    distinct matrix and objective object once.  The returned problems of
+    requests that share those objects share one canonical matrix and one
+    objective copy (treat them as read-only)."""
     cache = {}
     return [normalize(c, kw, cache) for c, kw in requests]
 

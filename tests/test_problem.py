@@ -57,3 +57,21 @@ def test_request_round_trip(golden):
         for u, v in zip(p[1:5], q[1:5]):
             np.testing.assert_array_equal(u, v)
         assert (p[0] != q[0]).nnz == 0 and p[5] == q[5]
+
+
+def test_normalize_batch_shares_one_objective_copy_per_object():
+    """Requests that pass the same objective object share one validated
+    copy; it does not follow later changes to the caller's array, and a
+    non-finite objective is still rejected."""
+    from co_cultivation_metabolic_atlas_b200.problem import normalize_batch
+    c = np.array([1.0, -2.0, 0.5])
+    a = np.array([[1.0, 1.0, 0.0]])
+    kw = dict(A_eq=a, b_eq=np.zeros(1), bounds=[(0, 1)] * 3)
+    out = normalize_batch([(c, kw), (c, dict(kw)), (c.copy(), dict(kw))])
+    assert out[0][4] is out[1][4] and out[2][4] is not out[0][4]
+    c[0] = 7.0
+    np.testing.assert_array_equal(out[0][4], [1.0, -2.0, 0.5])
+    np.testing.assert_array_equal(out[2][4], [1.0, -2.0, 0.5])
+    bad = np.array([1.0, np.inf, 0.0])
+    with pytest.raises(ValueError):
+        normalize_batch([(bad, kw), (bad, dict(kw))])
