@@ -38,6 +38,24 @@ def test_defaults(native_built):
     assert p.precision == N.PRECISION_MIXED and p.check_every == 64
     assert p.tol_gap == pytest.approx(1e-7) and p.fp32_tol_gap == pytest.approx(1e-4)
     assert p.fp64_stall_checks == 8 and p.floor_tol == pytest.approx(1e-7)
+    # the fields after the original ones: read through the ctypes mirror, so
+    # a layout that drifted from the header would read other fields' bytes
+    assert p.fp32_recentre == 1 and p.fp32_values_phase == 1
+    assert (p.gate_primal, p.gate_dual, p.gate_gap) == pytest.approx((1e-5, 1e-7, 1e-7))
+    assert p.primal_weight_smoothing == pytest.approx(0.5)
+    assert o.pair_instances == 1 and o.spread_banks == 1
+
+
+def test_solve_config_converts_and_checks_the_schedule_fields():
+    from co_cultivation_metabolic_atlas_b200.engine import EngineOptions, SolveConfig
+    for value, want in ((True, 1), (False, 0), (0, 0), (1, 1), (2, 2)):
+        assert SolveConfig(fp32_values_phase=value).native().fp32_values_phase == want
+    for bad in (3, -1, 1.5, "2"):
+        with pytest.raises(ValueError):
+            SolveConfig(fp32_values_phase=bad).native()
+    q = SolveConfig(gate_primal=2e-5, primal_weight_smoothing=0.3).native()
+    assert q.gate_primal == pytest.approx(2e-5) and q.primal_weight_smoothing == pytest.approx(0.3)
+    assert EngineOptions(spread_banks=False).native().spread_banks == 0
 
 
 def test_host_preprocessing_matches_oracle(native_built):
