@@ -262,16 +262,21 @@ def test_recentred_reaches_fp64_tolerances_in_fp32(golden_dir):
         assert np.all(np.abs(obj - fun) <= OBJ_TOL * np.maximum(1.0, np.abs(fun)))
 
 
-def test_recentred_handoff_continues_in_fp64(golden_dir):
+@pytest.mark.parametrize("values_phase, second", [(1, "fp32 values"), (0, "pdhg_persistent<double>")])
+def test_recentred_handoff_continues_in_the_second_phase(golden_dir, values_phase, second):
     """Instances the re-centred phase hands off (forced by a one-test stall
-    rule and short test period) finish in the FP64 phase from the compacted
-    work list; every objective still matches HiGHS."""
+    rule and short test period) finish in the second phase from the
+    compacted work list -- the re-centred kernel with FP32 matrix values by
+    default, the FP64 kernel with fp32_values_phase=0; every objective still
+    matches HiGHS."""
     import torch
     g = np.load(golden_dir / "highs_single.npz")
     model, lower, upper = syn.single_species_workload(8)
     eng = engine([(model.S, 1200)])
     eng.set_instances(np.zeros(8, np.int32), flat(lower), flat(upper), flat([model.cost] * 8))
-    res = eng.solve(config=cfg(fp64_stall_checks=1, check_every=16))
+    res = eng.solve(config=cfg(fp64_stall_checks=1, check_every=16, fp32_values_phase=values_phase))
+    kernels = eng.phase_kernels()
+    assert second in (kernels[1] or ""), kernels
     it32 = eng.phase_iterations().cpu().numpy()
     torch.cuda.synchronize()
     st = res.status.cpu().numpy()
@@ -279,7 +284,7 @@ def test_recentred_handoff_continues_in_fp64(golden_dir):
     obj = res.objective.cpu().numpy()
     eng.close()
     assert (st == 0).all(), st
-    assert (it > it32).any(), "no instance reached the FP64 phase"
+    assert (it > it32).any(), "no instance reached the second phase"
     fun = g["fun"]
     assert np.all(np.abs(obj - fun) <= OBJ_TOL * np.maximum(1.0, np.abs(fun)))
 
