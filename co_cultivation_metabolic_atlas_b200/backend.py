@@ -385,3 +385,4 @@ class B200LPBackend:
         if self._engine is not None:
             self._engine.close()
             self._engine = None
+        self._staging.clear()  # the pinned host buffers
